@@ -1,0 +1,120 @@
+/*
+ * tea_b200.h -- additive C-ABI entry points shared by the 2D and 3D libraries
+ * (libtea2d_b200.so, libtea3d_b200.so).  The reference's own ext_* entry points
+ * are declared in tea_ext_2d.h / tea_ext_3d.h; everything here is new and has
+ * no counterpart in tealeaf_2d|3d/ext_core.cpp unless a line says otherwise.
+ *
+ * Conventions follow the reference ABI: Fortran-callable names carry a trailing
+ * underscore, every argument is passed by pointer, chunk ids are 1-based.
+ */
+#ifndef TEA_B200_H
+#define TEA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Field ids.  1..6 are the reference's FIELD_* ids (tealeaf_2d/ext_shared.hpp:19-25,
+ * tealeaf_3d/ext_shared.hpp:21-27); 7..15 name the remaining chunk arrays of
+ * TeaLeafChunk (tealeaf_2d/ext_chunk.hpp:28-53). */
+enum {
+    TEA_FIELD_DENSITY = 1,
+    TEA_FIELD_ENERGY0 = 2,
+    TEA_FIELD_ENERGY1 = 3,
+    TEA_FIELD_U = 4,
+    TEA_FIELD_P = 5,
+    TEA_FIELD_SD = 6,
+    TEA_FIELD_U0 = 7,
+    TEA_FIELD_R = 8,
+    TEA_FIELD_W = 9,
+    TEA_FIELD_Z = 10,
+    TEA_FIELD_MI = 11,
+    TEA_FIELD_KX = 12,
+    TEA_FIELD_KY = 13,
+    TEA_FIELD_KZ = 14, /* 3D only */
+    TEA_FIELD_VOLUME = 15
+};
+
+/* Status codes reported by ext_get_status_.  The reference aborts the process on
+ * misuse (abort(), tealeaf_2d/ext_core.cpp:571-584); this library still aborts on
+ * the same fatal misuse but records device-side and numerical failures here. */
+enum {
+    TEA_OK = 0,
+    TEA_ERR_BAD_CHUNK = 1,      /* chunk id not initialised */
+    TEA_ERR_BAD_ARGUMENT = 2,   /* unknown field/face/solver, sizes out of range */
+    TEA_ERR_CUDA = 3,           /* a CUDA runtime call failed */
+    TEA_ERR_NONFINITE = 4,      /* NaN/Inf reached a reduction (pw, rrn, error) */
+    TEA_ERR_EIGEN = 5,          /* tqli failed or produced a negative eigenvalue */
+    TEA_ERR_NO_DEVICE = 6,      /* no CUDA device visible */
+    TEA_ERR_NOT_CONVERGED = 7   /* informational: max_iters reached */
+};
+
+/* Inspection: copy a whole chunk array between the device and a host buffer laid
+ * out as the reference lays it out (flat, x fastest, HALO_PAD=2 on every side:
+ * dims = {nx+4, ny+4, nz+4 (1 in 2D)}).  Return 0 on success. */
+int tea_chunk_dims_(const int* chunk, int* dims);
+int tea_read_field_(const int* chunk, const int* field, double* out);
+int tea_write_field_(const int* chunk, const int* field, const double* in);
+
+/* Last recorded status (0 = TEA_OK) and clear it. */
+void ext_get_status_(int* status);
+/* Message for the last non-zero status (empty string if none). */
+const char* tea_last_error(void);
+
+/* Solver ids for the whole-solve entry point. */
+enum {
+    TEA_SOLVER_JACOBI = 1,
+    TEA_SOLVER_CG = 2,
+    TEA_SOLVER_CHEBYSHEV = 3,
+    TEA_SOLVER_PPCG = 4
+};
+
+/* Inputs of one implicit solve: the tea.in keywords that tea_leaf() reads
+ * (tealeaf_2d/tea_solve.f90:36-605, defaults at tealeaf_2d/read_input.f90:49-80). */
+typedef struct {
+    int solver;             /* TEA_SOLVER_* */
+    int coefficient;        /* 1 = CONDUCTIVITY (w = rho), 2 = RECIP_CONDUCTIVITY (w = 1/rho) */
+    int preconditioner;     /* tl_preconditioner_on: diagonal (Jacobi) preconditioner */
+    int max_iters;          /* tl_max_iters */
+    int ch_cg_presteps;     /* tl_ch_cg_presteps */
+    int ch_cg_errswitch;    /* tl_ch_cg_errswitch */
+    int ppcg_inner_steps;   /* tl_ppcg_inner_steps */
+    int check_result;       /* tl_check_result */
+    double dt;              /* timestep */
+    double eps;             /* absolute threshold on the solver's error (sum r^2 or sum r.z) */
+    double ch_cg_epslim;    /* tl_ch_cg_epslim */
+    double eps_rel;         /* > 0: replace eps by eps_rel^2 * sum(u0^2) each solve */
+    int reserved[8];        /* must be zero */
+} tea_solve_params;
+
+/* Outputs of one implicit solve. */
+typedef struct {
+    int iterations;         /* the "Iteration count" that tea_leaf() prints (n-1) */
+    int status;             /* TEA_* status of this solve */
+    int cg_steps;           /* CG iterations before a Chebyshev/PPCG switch */
+    int cheby_steps;        /* Chebyshev iterations or PPCG outer iterations after it */
+    int switch_step;        /* n at the switch, 0 if none */
+    int est_itc;            /* Chebyshev iteration estimate, 0 if none */
+    double error;           /* final recursive error */
+    double exact_error;     /* sum (u0 - A u)^2 when check_result is set, else 0 */
+    double eps_used;        /* the absolute threshold that was applied */
+    double eigmin, eigmax;  /* scaled eigenvalue bounds at the switch (0 if none) */
+    double reserved[8];
+} tea_solve_result;
+
+/* Whole implicit solve of one timestep on the device: the control flow of
+ * tea_leaf() (tealeaf_2d/tea_solve.f90:36-605, tealeaf_3d/tea_solve.f90:36-653),
+ * from the depth-2 halo update of energy/density to ext_solver_finalise_ and the
+ * final energy halo update, with the iteration loop captured in CUDA graphs and
+ * the scalar recurrences and convergence test evaluated on the device.  Single
+ * chunk only (every face external).  Replaces the per-iteration sequence of
+ * ext_cg_calc_w_/ext_cg_calc_ur_/ext_cg_calc_p_/... calls that the Fortran driver
+ * makes; produces the same fields and iteration counts. */
+void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* params,
+                         tea_solve_result* result);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TEA_B200_H */

@@ -1,0 +1,165 @@
+// Shared device-side infrastructure of the TeaLeaf B200 library: the field layout in
+// HBM, the tile walk used by the per-call kernels, and the deterministic double-double
+// grid reduction.  Compiled into both libtea2d_b200.so and libtea3d_b200.so
+// (-DTEA_DIM=2 / -DTEA_DIM=3).  Build with -fmad=false: every multiply and add is
+// rounded separately, exactly as the reference's C++ (and the oracle) evaluate them.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#ifndef TEA_DIM
+#error "compile with -DTEA_DIM=2 or -DTEA_DIM=3"
+#endif
+
+namespace tea {
+
+constexpr int DIM = TEA_DIM;
+constexpr int HALO_PAD = 2;
+// Field layout: element (kk, jj, ii) of a padded array (kk in [0, nx+4) etc., the
+// reference's flat index kk + jj*X + ii*X*Y) lives at f[kk + jj*pitch + ii*page] with
+// pitch = roundup(nx+4, 32) doubles and f = allocation + kLeadPad, so the first inner
+// cell of every row (kk = 2) starts on a 256-byte boundary.
+constexpr int kLeadPad = 30;
+constexpr int kPitchAlign = 32;
+
+// Per-call kernels walk the inner domain in 32 x 8 tiles (one z-plane per tile in 3D).
+constexpr int TILE_X = 32;
+constexpr int TILE_Y = 8;
+constexpr int BLOCK = TILE_X * TILE_Y;
+constexpr int MAX_RED = 4;  // values per reduction (field summary needs 4)
+
+struct Geom {
+    int nx, ny, nz;     // inner cells (nz = 1 in 2D)
+    int X, Y, Z;        // padded extents (Z = 1 in 2D)
+    long pitch, page;   // elements
+    int tiles_x, tiles_y;
+    long tiles_inner;   // tiles covering the inner domain
+    int ftiles_x, ftiles_y;
+    long tiles_full;    // tiles covering the whole padded array
+};
+
+__host__ __device__ inline long fidx(const Geom& g, int kk, int jj, int ii)
+{
+    return (long)kk + (long)jj * g.pitch + (long)ii * g.page;
+}
+
+// ------------------------------------------------------------------ double-double sums
+
+struct DD {
+    double hi, lo;
+};
+
+// Knuth's TwoSum accumulation (cascaded summation): hi + lo carries the running sum to
+// about twice the working precision, so the final hi + lo is the correctly rounded sum
+// except within ~n*2^-106 of a rounding boundary, independent of the summation order.
+__device__ __forceinline__ void dd_add(DD& a, double x)
+{
+    const double s = a.hi + x;
+    const double bp = s - a.hi;
+    const double e = (a.hi - (s - bp)) + (x - bp);
+    a.hi = s;
+    a.lo = a.lo + e;
+}
+
+__device__ __forceinline__ DD dd_merge(DD a, DD b)
+{
+    const double s = a.hi + b.hi;
+    const double bp = s - a.hi;
+    const double e = (a.hi - (s - bp)) + (b.hi - bp);
+    DD r;
+    r.hi = s;
+    r.lo = (a.lo + b.lo) + e;
+    return r;
+}
+
+__device__ __forceinline__ double dd_value(DD a) { return a.hi + a.lo; }
+
+template <int NV>
+struct DDVec {
+    DD v[NV];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k].hi = v[k].lo = 0.0;
+    }
+};
+
+// Grid reduction scratch: one DD per value per block, and an arrival counter.
+struct RedScratch {
+    DD* partials;           // [max_blocks * MAX_RED]
+    unsigned int* counter;  // reset to 0 by the last block
+    int max_blocks;
+};
+
+template <int NV>
+__device__ __forceinline__ void warp_merge(DDVec<NV>& a)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            DD b;
+            b.hi = __shfl_xor_sync(0xffffffffu, a.v[k].hi, o);
+            b.lo = __shfl_xor_sync(0xffffffffu, a.v[k].lo, o);
+            a.v[k] = dd_merge(a.v[k], b);
+        }
+    }
+}
+
+// Block-reduce `acc`, then the last block to arrive merges every block's partial in
+// block order and writes the rounded results to out[0..NV).  Deterministic for a given
+// grid size; no block waits on another.  Must be called by every thread of the block.
+template <int NV>
+__device__ void grid_reduce(DDVec<NV> acc, const RedScratch& rs, double* out)
+{
+    __shared__ DD s_warp[BLOCK / 32][NV];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int warp = tid >> 5;
+    const int nwarps = (blockDim.x * blockDim.y) >> 5;
+    warp_merge<NV>(acc);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s_warp[warp][k] = acc.v[k];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        DDVec<NV> b;
+        b.zero();
+        for (int w = 0; w < nwarps; ++w)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) b.v[k] = dd_merge(b.v[k], s_warp[w][k]);
+#pragma unroll
+        for (int k = 0; k < NV; ++k) rs.partials[(long)blockIdx.x * MAX_RED + k] = b.v[k];
+        __threadfence();
+        const unsigned int prev = atomicAdd(rs.counter, 1u);
+        s_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    // Last block: lanes of warp 0 merge strided partials, then a fixed-order warp merge.
+    __threadfence();
+    if (warp == 0) {
+        DDVec<NV> b;
+        b.zero();
+        for (int blk = lane; blk < (int)gridDim.x; blk += 32)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                DD p;
+                p.hi = __ldcg(&rs.partials[(long)blk * MAX_RED + k].hi);
+                p.lo = __ldcg(&rs.partials[(long)blk * MAX_RED + k].lo);
+                b.v[k] = dd_merge(b.v[k], p);
+            }
+        warp_merge<NV>(b);
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) out[k] = dd_value(b.v[k]);
+            *rs.counter = 0u;
+        }
+    }
+}
+
+}  // namespace tea

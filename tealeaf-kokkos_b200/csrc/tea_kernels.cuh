@@ -1,0 +1,572 @@
+// Per-call device kernels behind the reference's ext_* entry points.  Each kernel states
+// the functor(s) it replaces (crtrott/TeaLeaf-Kokkos tealeaf_2d|3d/ext_*.hpp); every
+// expression keeps the reference's evaluation order so that, with -fmad=false, each
+// stored value is bit-identical to the reference's.  Reductions are double-double
+// (tea_common.cuh) and therefore match the oracle's compensated mode bit for bit.
+//
+// Unlike the reference (one thread per padded index, most masked off by a region test),
+// each kernel walks only its region in 32 x 8 tiles with a grid-stride loop sized to the
+// SM count; the halo is read from memory, as the reference reads it, so the per-call
+// path also serves chunks whose halos hold a neighbour's data.
+#pragma once
+
+#include "tea_chunk.cuh"
+
+namespace tea {
+
+// SMVP(a), tealeaf_2d/ext_shared.hpp:37-41 / tealeaf_3d/ext_shared.hpp:39-45, with the
+// reference's dims.x (row length) replaced by the row pitch and dims.x*dims.y by the page.
+__device__ __forceinline__ double smvp(const double* __restrict__ a, const double* __restrict__ kx,
+                                       const double* __restrict__ ky, const double* __restrict__ kz,
+                                       long i, long pitch, long page)
+{
+#if TEA_DIM == 2
+    (void)kz;
+    (void)page;
+    return (1.0 + (kx[i + 1] + kx[i]) + (ky[i + pitch] + ky[i])) * a[i]
+        - (kx[i + 1] * a[i + 1] + kx[i] * a[i - 1])
+        - (ky[i + pitch] * a[i + pitch] + ky[i] * a[i - pitch]);
+#else
+    return (1.0 + (kx[i + 1] + kx[i]) + (ky[i + pitch] + ky[i]) + (kz[i + page] + kz[i])) * a[i]
+        - (kx[i + 1] * a[i + 1] + kx[i] * a[i - 1])
+        - (ky[i + pitch] * a[i + pitch] + ky[i] * a[i - pitch])
+        - (kz[i + page] * a[i + page] + kz[i] * a[i - page]);
+#endif
+}
+
+// Diagonal of the operator (the preconditioner's 1/Mi), tealeaf_2d/ext_cg_kernel.hpp:119-121.
+__device__ __forceinline__ double diag(const double* __restrict__ kx, const double* __restrict__ ky,
+                                       const double* __restrict__ kz, long i, long pitch, long page)
+{
+#if TEA_DIM == 2
+    (void)kz;
+    (void)page;
+    return (1.0 + (kx[i + 1] + kx[i]) + (ky[i + pitch] + ky[i]));
+#else
+    return (1.0 + (kx[i + 1] + kx[i]) + (ky[i + pitch] + ky[i]) + (kz[i + page] + kz[i]));
+#endif
+}
+
+// ---------------------------------------------------------------- set-up
+
+// InitialiseChunkAreas, tealeaf_2d/ext_initialise_chunk.hpp:63-90 (3D :66-99): volume only
+// (the face areas are never read by any kernel).
+__global__ void __launch_bounds__(BLOCK) k_init_volume(Geom g, Box full, double* volume, double v)
+{
+    walk(full, [&](int kk, int jj, int ii) { volume[fidx(g, kk, jj, ii)] = v; });
+}
+
+struct StateTable {
+    int n, rect, circ, point;
+    const double *density, *energy, *xmin, *xmax, *ymin, *ymax, *zmin, *zmax, *radius;
+    const int* geometry;
+};
+
+// GenerateChunk, tealeaf_2d/ext_generate_chunk.hpp:13-101 (3D :13-109).
+__global__ void __launch_bounds__(BLOCK) k_generate(Geom g, Box full, Fields f, StateTable s,
+                                                    const double* __restrict__ vx,
+                                                    const double* __restrict__ vy,
+                                                    const double* __restrict__ vz,
+                                                    const double* __restrict__ cx,
+                                                    const double* __restrict__ cy,
+                                                    const double* __restrict__ cz)
+{
+    walk(full, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        double e0 = s.energy[0], den = s.density[0];
+        for (int ss = 1; ss < s.n; ++ss) {
+            bool apply = false;
+            const int geo = s.geometry[ss];
+            if (geo == s.rect) {
+                apply = vx[kk + 1] >= s.xmin[ss] && vx[kk] < s.xmax[ss] && vy[jj + 1] >= s.ymin[ss]
+                    && vy[jj] < s.ymax[ss];
+#if TEA_DIM == 3
+                apply = apply && vz[ii + 1] >= s.zmin[ss] && vz[ii] < s.zmax[ss];
+#endif
+            } else if (geo == s.circ) {
+#if TEA_DIM == 2
+                const double radius = sqrt((cx[kk] - s.xmin[ss]) * (cx[kk] - s.xmin[ss])
+                                           + (cy[jj] - s.ymin[ss]) * (cy[jj] - s.ymin[ss]));
+#else
+                const double radius = sqrt((cx[kk] - s.xmin[ss]) * (cx[kk] - s.xmin[ss])
+                                           + (cy[jj] - s.ymin[ss]) * (cy[jj] - s.ymin[ss])
+                                           + (cz[ii] - s.zmin[ss]) * (cz[ii] - s.zmin[ss]));
+#endif
+                apply = radius <= s.radius[ss];
+            } else if (geo == s.point) {
+                apply = vx[kk] == s.xmin[ss] && vy[jj] == s.ymin[ss];
+#if TEA_DIM == 3
+                apply = apply && vz[ii] == s.zmin[ss];
+#endif
+            }
+            if (apply) {
+                e0 = s.energy[ss];
+                den = s.density[ss];
+            }
+        }
+        f.energy0[i] = e0;
+        f.density[i] = den;
+        bool one = kk > 0 && kk < g.X - 1 && jj > 0 && jj < g.Y - 1;
+#if TEA_DIM == 3
+        one = one && ii > 0 && ii < g.Z - 1;
+#endif
+        if (one) f.u[i] = e0 * den;
+    });
+    (void)vz;
+    (void)cz;
+}
+
+// FieldSummary, tealeaf_2d/ext_field_summary.hpp:13-67.
+__global__ void __launch_bounds__(BLOCK) k_field_summary(Geom g, Box inner, Fields f, RedScratch rs,
+                                                         double* out)
+{
+    DDVec<4> acc;
+    acc.zero();
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        const double cellVol = f.volume[i];
+        const double cellMass = cellVol * f.density[i];
+        dd_add(acc.v[0], cellVol);
+        dd_add(acc.v[1], cellMass);
+        dd_add(acc.v[2], cellMass * f.energy0[i]);
+        dd_add(acc.v[3], cellMass * f.u[i]);
+    });
+    grid_reduce<4>(acc, rs, out);
+}
+
+// ---------------------------------------------------------------- halo and packing
+
+// One reflective face update: halo[HALO_PAD-1-f] = interior[HALO_PAD+f].
+struct HaloSeg {
+    double* field;
+    int face;   // 1 left, 2 right, 3 bottom, 4 top, 5 back, 6 front
+    long count;
+};
+
+struct HaloJob {
+    HaloSeg seg[36];
+    int nseg;
+    int depth;
+};
+
+// UpdateHalo, tealeaf_2d/ext_update_halo.hpp:12-76 (3D :12-136).  2D faces span the whole
+// padded row/column; 3D faces only their inner part.  Within a face no element is both
+// read and written, so the result does not depend on the thread mapping.
+__global__ void k_update_halo(Geom g, HaloJob job)
+{
+    const HaloSeg sg = job.seg[blockIdx.y];
+    const int depth = job.depth;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < sg.count;
+         idx += (long)gridDim.x * blockDim.x) {
+        long to, from;
+#if TEA_DIM == 2
+        if (sg.face == 1 || sg.face == 2) {
+            const int jj = (int)(idx / depth), fl = (int)(idx % depth);
+            const int kt = sg.face == 1 ? HALO_PAD - 1 - fl : g.X - HALO_PAD + fl;
+            const int kf = sg.face == 1 ? HALO_PAD + fl : g.X - HALO_PAD - 1 - fl;
+            to = fidx(g, kt, jj, 0);
+            from = fidx(g, kf, jj, 0);
+        } else {
+            const int kk = (int)(idx % g.X), fl = (int)(idx / g.X);
+            const int jt = sg.face == 3 ? HALO_PAD - 1 - fl : g.Y - HALO_PAD + fl;
+            const int jf = sg.face == 3 ? HALO_PAD + fl : g.Y - HALO_PAD - 1 - fl;
+            to = fidx(g, kk, jt, 0);
+            from = fidx(g, kk, jf, 0);
+        }
+#else
+        if (sg.face == 1 || sg.face == 2) {
+            const int fl = (int)(idx % depth);
+            const long line = idx / depth;
+            const int jj = HALO_PAD + (int)(line % g.ny), ii = HALO_PAD + (int)(line / g.ny);
+            const int kt = sg.face == 1 ? HALO_PAD - 1 - fl : g.X - HALO_PAD + fl;
+            const int kf = sg.face == 1 ? HALO_PAD + fl : g.X - HALO_PAD - 1 - fl;
+            to = fidx(g, kt, jj, ii);
+            from = fidx(g, kf, jj, ii);
+        } else if (sg.face == 3 || sg.face == 4) {
+            const int kk = HALO_PAD + (int)(idx % g.nx);
+            const long line = idx / g.nx;
+            const int fl = (int)(line % depth), ii = HALO_PAD + (int)(line / depth);
+            const int jt = sg.face == 3 ? HALO_PAD - 1 - fl : g.Y - HALO_PAD + fl;
+            const int jf = sg.face == 3 ? HALO_PAD + fl : g.Y - HALO_PAD - 1 - fl;
+            to = fidx(g, kk, jt, ii);
+            from = fidx(g, kk, jf, ii);
+        } else {
+            const int kk = HALO_PAD + (int)(idx % g.nx);
+            const long line = idx / g.nx;
+            const int jj = HALO_PAD + (int)(line % g.ny), fl = (int)(line / g.ny);
+            const int it = sg.face == 5 ? HALO_PAD - 1 - fl : g.Z - HALO_PAD + fl;
+            const int iF = sg.face == 5 ? HALO_PAD + fl : g.Z - HALO_PAD - 1 - fl;
+            to = fidx(g, kk, jj, it);
+            from = fidx(g, kk, jj, iF);
+        }
+#endif
+        sg.field[to] = sg.field[from];
+    }
+}
+
+// Packers, tealeaf_2d/ext_pack_kernel.hpp:8-97 and tealeaf_3d/ext_pack_kernel.hpp: the
+// padded flat index of buffer element `index`, restated from each packer's offset
+// expression, then mapped to the pitched layout.
+__device__ __forceinline__ long pack_flat_index(const Geom& g, int face, int depth, bool pack, long index)
+{
+    const long X = g.X, Y = g.Y;
+#if TEA_DIM == 2
+    if (face == 1 || face == 2) {
+        const long lines = index / depth;
+        long off;
+        if (face == 1) off = pack ? HALO_PAD + lines * (X - depth) : HALO_PAD - depth + lines * (X - depth);
+        else off = pack ? X - HALO_PAD - depth + lines * (X - depth) : X - HALO_PAD + lines * (X - depth);
+        return off + index;
+    }
+    const long width = X - 2 * HALO_PAD;
+    const long lines = index / width;
+    long off;
+    if (face == 4) off = pack ? X * (Y - HALO_PAD - depth) + lines * 2 * HALO_PAD : X * (Y - HALO_PAD) + lines * 2 * HALO_PAD;
+    else off = pack ? X * HALO_PAD + lines * 2 * HALO_PAD : X * (HALO_PAD - depth) + lines * 2 * HALO_PAD;
+    return off + index;
+#else
+    const long Z = g.Z, HP2 = 2 * HALO_PAD, page = X * Y;
+    if (face == 1 || face == 2) {
+        const long height = Y - HP2;
+        const long lines = index / depth;
+        const long base = page * HALO_PAD + X * HALO_PAD + lines * (X - depth) + (lines / height) * X * HP2;
+        long xoff;
+        if (face == 1) xoff = pack ? HALO_PAD : HALO_PAD - depth;
+        else xoff = pack ? X - HALO_PAD - depth : X - HALO_PAD;
+        return base + xoff + index;
+    }
+    if (face == 3 || face == 4) {
+        const long width = X - HP2;
+        const long lines = index / width;
+        long yoff;
+        if (face == 4) yoff = pack ? X * (Y - HALO_PAD - depth) : X * (Y - HALO_PAD);
+        else yoff = pack ? X * HALO_PAD : X * (HALO_PAD - depth);
+        return page * HALO_PAD + yoff + HALO_PAD + lines * HP2 + X * (Y - depth) * (lines / depth) + index;
+    }
+    const long height = Y - HP2;
+    const long lines = index / (X - HP2);
+    long zoff;
+    if (face == 6) zoff = pack ? page * (Z - HALO_PAD - depth) : page * (Z - HALO_PAD);
+    else zoff = pack ? page * HALO_PAD : page * (HALO_PAD - depth);
+    return zoff + X * HALO_PAD + HALO_PAD + lines * HP2 + (lines / height) * X * HP2 + index;
+#endif
+}
+
+__global__ void k_pack(Geom g, double* field, double* buf, long len, int face, int depth, int pack)
+{
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < len; idx += (long)gridDim.x * blockDim.x) {
+        const long flat = pack_flat_index(g, face, depth, pack != 0, idx);
+        const long kk = flat % g.X;
+        const long rest = flat / g.X;
+        const long jj = rest % g.Y;
+        const long ii = rest / g.Y;
+        const long p = fidx(g, (int)kk, (int)jj, (int)ii);
+        if (pack) buf[idx] = field[p];
+        else field[p] = buf[idx];
+    }
+}
+
+// ---------------------------------------------------------------- shared solver methods
+
+// SetField, tealeaf_2d/ext_set_field.hpp:13-29.
+__global__ void __launch_bounds__(BLOCK) k_set_field(Geom g, Box full, Fields f)
+{
+    walk(full, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.energy[i] = f.energy0[i];
+    });
+}
+
+// CopyU, tealeaf_2d/ext_solver_methods.hpp:12-35.
+__global__ void __launch_bounds__(BLOCK) k_copy_u(Geom g, Box inner, Fields f)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.u0[i] = f.u[i];
+    });
+}
+
+// CalculateResidual, tealeaf_2d/ext_solver_methods.hpp:38-66.
+__global__ void __launch_bounds__(BLOCK) k_residual(Geom g, Box inner, Fields f)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        const double s = smvp(f.u, f.kx, f.ky, f.kz, i, g.pitch, g.page);
+        f.r[i] = f.u0[i] - s;
+    });
+}
+
+// Calculate2Norm, tealeaf_2d/ext_solver_methods.hpp:70-92.
+__global__ void __launch_bounds__(BLOCK) k_2norm(Geom g, Box inner, const double* __restrict__ b,
+                                                 RedScratch rs, double* out)
+{
+    DDVec<1> acc;
+    acc.zero();
+    walk(inner, [&](int kk, int jj, int ii) {
+        const double v = b[fidx(g, kk, jj, ii)];
+        dd_add(acc.v[0], v * v);
+    });
+    grid_reduce<1>(acc, rs, out);
+}
+
+// Finalise, tealeaf_2d/ext_solver_methods.hpp:96-121.
+__global__ void __launch_bounds__(BLOCK) k_finalise(Geom g, Box inner, Fields f)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.energy[i] = f.u[i] / f.density[i];
+    });
+}
+
+// ---------------------------------------------------------------- Jacobi
+
+// JacobiInit, tealeaf_2d/ext_jacobi_kernel.hpp:12-62 (3D :12-66).
+__global__ void __launch_bounds__(BLOCK) k_jacobi_init(Geom g, Box full, Fields f, int cond, double rx,
+                                                       double ry, double rz)
+{
+    walk(full, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        bool one = jj > 0 && jj < g.Y - 1 && kk > 0 && kk < g.X - 1;
+        bool skew = jj >= HALO_PAD && jj < g.Y - 1 && kk >= HALO_PAD && kk < g.X - 1;
+#if TEA_DIM == 3
+        one = one && ii > 0 && ii < g.Z - 1;
+        skew = skew && ii >= HALO_PAD && ii < g.Z - 1;
+#endif
+        if (one) {
+            const double v = f.energy[i] * f.density[i];
+            f.u0[i] = v;
+            f.u[i] = v;
+        }
+        if (skew) {
+            const double centre = cond ? f.density[i] : 1.0 / f.density[i];
+            const double left = cond ? f.density[i - 1] : 1.0 / f.density[i - 1];
+            const double down = cond ? f.density[i - g.pitch] : 1.0 / f.density[i - g.pitch];
+            f.kx[i] = rx * (left + centre) / (2.0 * left * centre);
+            f.ky[i] = ry * (down + centre) / (2.0 * down * centre);
+#if TEA_DIM == 3
+            const double back = cond ? f.density[i - g.page] : 1.0 / f.density[i - g.page];
+            f.kz[i] = rz * (back + centre) / (2.0 * back * centre);
+#endif
+        }
+    });
+    (void)rz;
+}
+
+// JacobiCopyU, tealeaf_2d/ext_jacobi_kernel.hpp:66-82: r = u over the padded array.
+__global__ void __launch_bounds__(BLOCK) k_jacobi_copy(Geom g, Box full, Fields f)
+{
+    walk(full, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.r[i] = f.u[i];
+    });
+}
+
+// JacobiSolve, tealeaf_2d/ext_jacobi_kernel.hpp:86-117 (3D :90-126).
+__global__ void __launch_bounds__(BLOCK) k_jacobi_solve(Geom g, Box inner, Fields f, RedScratch rs,
+                                                        double* out)
+{
+    DDVec<1> acc;
+    acc.zero();
+    const double* __restrict__ kx = f.kx;
+    const double* __restrict__ ky = f.ky;
+    const double* __restrict__ r = f.r;
+    const long px = g.pitch;
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+#if TEA_DIM == 2
+        const double un = (f.u0[i] + (kx[i + 1] * r[i + 1] + kx[i] * r[i - 1])
+                           + (ky[i + px] * r[i + px] + ky[i] * r[i - px]))
+            / (1.0 + (kx[i] + kx[i + 1]) + (ky[i] + ky[i + px]));
+#else
+        const double* __restrict__ kz = f.kz;
+        const long pg = g.page;
+        const double un = (f.u0[i] + (kx[i + 1] * r[i + 1] + kx[i] * r[i - 1])
+                           + (ky[i + px] * r[i + px] + ky[i] * r[i - px])
+                           + (kz[i + pg] * r[i + pg] + kz[i] * r[i - pg]))
+            / (1.0 + (kx[i] + kx[i + 1]) + (ky[i] + ky[i + px]) + (kz[i] + kz[i + pg]));
+#endif
+        f.u[i] = un;
+        dd_add(acc.v[0], fabs(un - r[i]));
+    });
+    grid_reduce<1>(acc, rs, out);
+}
+
+// ---------------------------------------------------------------- CG
+
+// CGInitU (tealeaf_2d/ext_cg_kernel.hpp:12-34) over the padded array, fused with CGInitW
+// (:36-61) on the one-cell halo domain: both are pointwise.
+__global__ void __launch_bounds__(BLOCK) k_cg_init_uw(Geom g, Box full, Fields f, int cond)
+{
+    walk(full, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.p[i] = 0.0;
+        f.r[i] = 0.0;
+        f.u[i] = f.energy[i] * f.density[i];
+        bool one = jj > 0 && jj < g.Y - 1 && kk > 0 && kk < g.X - 1;
+#if TEA_DIM == 3
+        one = one && ii > 0 && ii < g.Z - 1;
+#endif
+        if (one) f.w[i] = cond ? f.density[i] : 1.0 / f.density[i];
+    });
+}
+
+// CGInitK, tealeaf_2d/ext_cg_kernel.hpp:63-91 (3D :59-91), on the skew domain.
+__global__ void __launch_bounds__(BLOCK) k_cg_init_k(Geom g, Box skew, Fields f, double rx, double ry,
+                                                     double rz)
+{
+    walk(skew, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        const double* __restrict__ w = f.w;
+        f.kx[i] = rx * (w[i - 1] + w[i]) / (2.0 * w[i - 1] * w[i]);
+        f.ky[i] = ry * (w[i - g.pitch] + w[i]) / (2.0 * w[i - g.pitch] * w[i]);
+#if TEA_DIM == 3
+        f.kz[i] = rz * (w[i - g.page] + w[i]) / (2.0 * w[i - g.page] * w[i]);
+#endif
+    });
+    (void)rz;
+}
+
+// CGCalcRRO, tealeaf_2d/ext_cg_kernel.hpp:93-145 (3D :93-149).
+__global__ void __launch_bounds__(BLOCK) k_cg_calc_rro(Geom g, Box inner, Fields f, int precond,
+                                                       RedScratch rs, double* out)
+{
+    DDVec<1> acc;
+    acc.zero();
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        const double w = smvp(f.u, f.kx, f.ky, f.kz, i, g.pitch, g.page);
+        f.w[i] = w;
+        const double r = f.u[i] - w;
+        f.r[i] = r;
+        double p;
+        if (precond) {
+            const double mi = 1.0 / diag(f.kx, f.ky, f.kz, i, g.pitch, g.page);
+            f.mi[i] = mi;
+            const double z = mi * r;
+            f.z[i] = z;
+            p = z;
+        } else {
+            p = r;
+        }
+        f.p[i] = p;
+        dd_add(acc.v[0], r * p);
+    });
+    grid_reduce<1>(acc, rs, out);
+}
+
+// CGCalcW, tealeaf_2d/ext_cg_kernel.hpp:148-197 (non-team operator, :177-189).
+__global__ void __launch_bounds__(BLOCK) k_cg_calc_w(Geom g, Box inner, Fields f, RedScratch rs, double* out)
+{
+    DDVec<1> acc;
+    acc.zero();
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        const double w = smvp(f.p, f.kx, f.ky, f.kz, i, g.pitch, g.page);
+        f.w[i] = w;
+        dd_add(acc.v[0], w * f.p[i]);
+    });
+    grid_reduce<1>(acc, rs, out);
+}
+
+// CGCalcUr, tealeaf_2d/ext_cg_kernel.hpp:200-275 (non-team operator, :244-264).
+__global__ void __launch_bounds__(BLOCK) k_cg_calc_ur(Geom g, Box inner, Fields f, double alpha, int precond,
+                                                      RedScratch rs, double* out)
+{
+    DDVec<1> acc;
+    acc.zero();
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.u[i] = f.u[i] + alpha * f.p[i];
+        const double r = f.r[i] - alpha * f.w[i];
+        f.r[i] = r;
+        if (precond) {
+            const double z = f.mi[i] * r;
+            f.z[i] = z;
+            dd_add(acc.v[0], r * z);
+        } else {
+            dd_add(acc.v[0], r * r);
+        }
+    });
+    grid_reduce<1>(acc, rs, out);
+}
+
+// CGCalcP, tealeaf_2d/ext_cg_kernel.hpp:278-319 (non-team operator, :301-310).
+__global__ void __launch_bounds__(BLOCK) k_cg_calc_p(Geom g, Box inner, Fields f, double beta, int precond)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.p[i] = beta * f.p[i] + (precond ? f.z[i] : f.r[i]);
+    });
+}
+
+// ---------------------------------------------------------------- Chebyshev
+
+// ChebyInit, tealeaf_2d/ext_cheby_kernel.hpp:11-47.
+__global__ void __launch_bounds__(BLOCK) k_cheby_init(Geom g, Box inner, Fields f, double theta, int precond)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        const double w = smvp(f.u, f.kx, f.ky, f.kz, i, g.pitch, g.page);
+        f.w[i] = w;
+        const double r = f.u0[i] - w;
+        f.r[i] = r;
+        f.p[i] = (precond ? f.mi[i] * r : r) / theta;
+    });
+}
+
+// ChebyCalcU, tealeaf_2d/ext_cheby_kernel.hpp:50-72.
+__global__ void __launch_bounds__(BLOCK) k_cheby_calc_u(Geom g, Box inner, Fields f)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.u[i] = f.u[i] + f.p[i];
+    });
+}
+
+// ChebyIterate, tealeaf_2d/ext_cheby_kernel.hpp:75-115.
+__global__ void __launch_bounds__(BLOCK) k_cheby_iterate(Geom g, Box inner, Fields f, double alpha,
+                                                         double beta, int precond)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        const double w = smvp(f.u, f.kx, f.ky, f.kz, i, g.pitch, g.page);
+        f.w[i] = w;
+        const double r = f.u0[i] - w;
+        f.r[i] = r;
+        f.p[i] = alpha * f.p[i] + beta * (precond ? f.mi[i] * r : r);
+    });
+}
+
+// ---------------------------------------------------------------- PPCG
+
+// PPCGInitSd, tealeaf_2d/ext_ppcg_kernel.hpp:8-34.
+__global__ void __launch_bounds__(BLOCK) k_ppcg_init_sd(Geom g, Box inner, Fields f, double theta, int precond)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.sd[i] = (precond ? f.mi[i] * f.r[i] : f.r[i]) / theta;
+    });
+}
+
+// PPCGCalcU, tealeaf_2d/ext_ppcg_kernel.hpp:37-65.
+__global__ void __launch_bounds__(BLOCK) k_ppcg_calc_u(Geom g, Box inner, Fields f)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        const double s = smvp(f.sd, f.kx, f.ky, f.kz, i, g.pitch, g.page);
+        f.r[i] = f.r[i] - s;
+        f.u[i] = f.u[i] + f.sd[i];
+    });
+}
+
+// PPCGCalcSd, tealeaf_2d/ext_ppcg_kernel.hpp:68-100.
+__global__ void __launch_bounds__(BLOCK) k_ppcg_calc_sd(Geom g, Box inner, Fields f, double alpha, double beta,
+                                                        int precond)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.sd[i] = alpha * f.sd[i] + beta * (precond ? f.mi[i] * f.r[i] : f.r[i]);
+    });
+}
+
+}  // namespace tea

@@ -1,0 +1,76 @@
+/*
+ * tea_driver.h -- C API of libtea_driver.so, the host-side restatement of the
+ * reference's Fortran driver (tealeaf_2d|3d: tea_leaf.f90, start.f90, diffuse.f90,
+ * timestep.f90, tea_solve.f90, field_summary.f90, read_input.f90, parse.f90).
+ *
+ * The driver runs a tea.in deck against any library that exports the reference's
+ * ext_* C ABI (include/tea_ext_2d.h or tea_ext_3d.h), loaded with dlopen: the CUDA
+ * library libtea{2,3}d_b200.so is the product backend.  No Fortran compiler exists
+ * in this image, so this C++ restatement stands in for the Fortran caller.
+ */
+#ifndef TEA_DRIVER_H
+#define TEA_DRIVER_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int dim;                 /* 2 or 3 */
+    const char* backend;     /* path of the ext_* library */
+    int use_fused_solve;     /* call ext_tea_leaf_solve_ instead of the per-call sequence */
+    int summary_every_step;  /* call ext_field_summary_kernel_ after every step */
+    int end_step_override;   /* > 0: stop after this many steps */
+    int quiet;               /* 1: no tea.out lines on stdout */
+    const char* out_path;    /* write the tea.out log here (NULL: none) */
+    double eps_override;     /* > 0: replace tl_eps */
+    double eps_rel_override; /* > 0: replace tl_eps_rel */
+    int reserved[8];
+} tea_run_options;
+
+typedef struct {
+    int step;
+    int iterations;          /* "Iteration count" printed by tea_leaf (n-1) */
+    int status;
+    int cheby_steps;
+    double time;
+    double dt;
+    double error;
+    double exact_error;
+    double eps_used;
+    double solve_seconds;    /* wall time of tea_leaf() for this step */
+    double vol, mass, ie, temp; /* field summary after the step (0 unless computed) */
+    int has_summary;
+    int switch_step;
+    int est_itc;
+    int pad;
+} tea_step_record;
+
+typedef struct {
+    int steps;
+    int test_problem;
+    int kat_available;
+    int kat_passed;
+    double qa_diff;          /* percent difference to the known answer */
+    double kat_expected;
+    double vol, mass, ie, temp;  /* final field summary */
+    double wall_seconds;     /* whole run (set-up excluded) */
+    double solve_seconds;    /* sum of tea_leaf() wall times */
+    long total_iterations;
+    int x_cells, y_cells, z_cells;
+    int solver;              /* TEA_SOLVER_* */
+} tea_run_summary;
+
+/* Run a deck (the text of a tea.in file).  `steps` may be NULL; at most `max_steps`
+ * records are written.  Returns 0 on success, non-zero on a driver or backend error
+ * (message in tea_driver_last_error()). */
+int tea_run_deck(const char* deck_text, const tea_run_options* options,
+                 tea_run_summary* summary, tea_step_record* steps, int max_steps);
+
+const char* tea_driver_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TEA_DRIVER_H */

@@ -1,0 +1,115 @@
+"""Host logic of the C++ driver: tea.in semantics of the reference's parser and
+read_input, and the switch-time scalar algorithms (eigenvalues, Chebyshev coefficients).
+Runs on the CPU against the oracle backend."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import SUM_SEQUENTIAL, port_lib, tea
+
+BASE = """*tea
+state 1 density=100.0 energy=0.0001
+state 2 density=0.1 energy=25.0 geometry=rectangle xmin=0.0 xmax=1.0 ymin=1.0 ymax=2.0
+x_cells=24
+y_cells=20
+xmin=0.0
+ymin=0.0
+xmax=10.0
+ymax=10.0
+tl_use_cg
+{extra}
+*endtea
+"""
+
+
+def run(extra="", **kw):
+    return tea.run_deck(BASE.format(extra=extra), 2, backend=port_lib(2, SUM_SEQUENTIAL), **kw)
+
+
+def test_defaults_use_single_precision_literals():
+    # read_input.f90:49,51: dtinit=0.1 and eps=1.0e-10 are default-real literals.
+    summary, recs = run("end_step=2")
+    assert recs[0]["dt"] == float(np.float32(0.1))
+    assert recs[0]["eps_used"] == float(np.float32(1.0e-10))
+    assert summary["steps"] == 2
+
+
+def test_end_time_stops_the_run():
+    # diffuse.f90:89: stop when time + g_small > end_time.  g_small (1e-16) is below half
+    # an ulp of 1.0, so time == end_time does not stop the run: 0.25 x 5 steps.
+    summary, recs = run("initial_timestep=0.25\nend_time=1.0")
+    assert summary["steps"] == 5
+    summary, recs = run("initial_timestep=0.3\nend_time=1.0")
+    assert summary["steps"] == 4
+
+
+def test_parser_comments_case_and_separators():
+    a, ra = run("end_step=2\ninitial_timestep=0.004")
+    b, rb = run("END_STEP 2 ! a comment\nInitial_Timestep,0.004 ; another")
+    assert [r["iterations"] for r in ra] == [r["iterations"] for r in rb]
+    assert a["temp"] == b["temp"]
+
+
+def test_value_on_the_next_line_is_read():
+    # parse_getword(.TRUE.) wraps to the next line for a missing value.
+    a, _ = run("end_step\n2\ninitial_timestep=0.004")
+    assert a["steps"] == 2
+
+
+def test_relative_target_sets_eps_from_b():
+    _, recs = run("end_step=1\ninitial_timestep=0.004\ntl_eps_rel=1e-10")
+    assert recs[0]["eps_used"] > 0 and recs[0]["eps_used"] != float(np.float32(1e-10))
+
+
+def test_missing_states_is_an_error():
+    with pytest.raises(RuntimeError, match="No states"):
+        tea.run_deck("*tea\nx_cells=4\n*endtea\n", 2, backend=port_lib(2, SUM_SEQUENTIAL))
+
+
+def _drv():
+    lib = tea.driver()
+    lib.tea_calc_eigenvalues_c.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_double)]
+    lib.tea_calc_ch_coefs_c.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                        ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.c_int]
+    return lib
+
+
+@pytest.mark.parametrize("n,seed", [(5, 0), (20, 1), (30, 2), (64, 3)])
+def test_eigenvalues_match_dense_solver(n, seed):
+    """The Lanczos tridiagonal of tea_leaf_cheby.f90:285-332 solved by the restated tqli
+    agrees with LAPACK on the same matrix."""
+    rng = np.random.default_rng(seed)
+    alphas = rng.uniform(0.2, 2.0, n)
+    betas = rng.uniform(0.01, 0.9, n)
+    lo, hi = ctypes.c_double(), ctypes.c_double()
+    P = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    info = _drv().tea_calc_eigenvalues_c(P(alphas), P(betas), n, ctypes.byref(lo), ctypes.byref(hi))
+    assert info == 0
+    d = np.array([1 / alphas[k] + (betas[k - 1] / alphas[k - 1] if k else 0.0) for k in range(n)])
+    e = np.array([np.sqrt(betas[k]) / alphas[k] for k in range(n - 1)])
+    ev = np.linalg.eigvalsh(np.diag(d) + np.diag(e, 1) + np.diag(e, -1))
+    assert abs(lo.value - ev[0]) <= 1e-12 * abs(ev[-1])
+    assert abs(hi.value - ev[-1]) <= 1e-12 * abs(ev[-1])
+
+
+def test_chebyshev_coefficients_recurrence():
+    n = 40
+    al = np.zeros(n)
+    be = np.zeros(n)
+    th = ctypes.c_double()
+    P = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    _drv().tea_calc_ch_coefs_c(P(al), P(be), 0.05, 3.9, ctypes.byref(th), n)
+    theta = (3.9 + 0.05) / 2
+    delta = (3.9 - 0.05) / 2
+    sigma = theta / delta
+    rho_old = 1.0 / sigma
+    for k in range(n):
+        rho_new = 1.0 / (2.0 * sigma - rho_old)
+        assert al[k] == rho_new * rho_old
+        assert be[k] == 2.0 * rho_new / delta
+        rho_old = rho_new
+    assert th.value == theta
