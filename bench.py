@@ -1,0 +1,505 @@
+#!/usr/bin/env python
+"""Benchmark of the TeaLeaf implicit heat-conduction solve on B200.
+
+Metric (the reference's headline): seconds per timestep of the implicit solve at a
+relative residual of 1e-10 (sum r^2 < 1e-20 sum b^2, b = rho*e), plain FP64; lower is
+better.  Workload (the 2D 4096^2 configuration): 4096 x 4096 cells on a 10 x 10 domain,
+dt = 0.004, the seeded 16-state layout (rectangles/circles, density log-uniform in
+[0.1, 100], energy uniform in [1, 25], conductivity 1/density), Chebyshev with 30 CG
+presteps.  (PPCG, the configuration's other solver, does not reach 1e-10 on this deck in
+FP64: its recursive residual stalls near 2e-9 relative, on the reference's own kernels
+too.)  A step is one timestep: one call of ext_tea_leaf_solve_ (tea_leaf() of the
+reference) on data resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Timing: W untimed timesteps, then K timesteps between CUDA events recorded on the
+library's own stream, barrier + synchronize on both sides, max over ranks.  Every field
+array is 135 MB (> 126 MB of L2), so no L2 flush is needed between steps.  With N > 1
+(torchrun) each rank solves its own replica of the workload (this build does not shard
+the solve) and rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+
+# One GPU per process: restrict visibility before any CUDA initialisation.
+if "LOCAL_RANK" in os.environ and "CUDA_VISIBLE_DEVICES" not in os.environ:
+    os.environ["CUDA_VISIBLE_DEVICES"] = os.environ["LOCAL_RANK"]
+
+sys.path.insert(0, str(ROOT))
+import __graft_entry__  # noqa: E402
+
+tea = __graft_entry__.load_package()
+
+CELLS = 4096
+STATES = 16
+SEED = 4096
+EPS_REL = 1e-10
+SOLVER = "chebyshev"
+METRIC = "s/timestep at rel residual 1e-10 (plain FP64, 2D 4096^2, Chebyshev)"
+WORDS = {  # algorithmic FP64 words per interior cell of one launch
+    "cg_sweep_a": 8,   # read p, r, u, Kx, Ky; write u, p, w
+    "cg_sweep_b": 3,   # read r, w; write r
+    "cheby_iterate": 7,  # read u, u0, p, Kx, Ky; write u', p
+}
+KERNEL_IDS = {"cg_sweep_a": 2, "cheby_iterate": 3}
+PROFILES = ROOT / "profiles"
+# Per-timestep iteration counts of this deck (CG iterations before the Chebyshev switch,
+# Chebyshev iterations after it) for simulation steps 1..20, measured with this build; the
+# reference's counts agree within +-1 (tests/test_gpu_solvers.py).  They scale the
+# reference arm's per-iteration costs to seconds per timestep.
+STEP_COUNTS = {}
+
+
+def workload_spec(steps=1):
+    return tea.DeckSpec(dim=2, cells=CELLS, states=STATES, seed=SEED, solver=SOLVER, end_step=steps, dt=0.004,
+                        eps=1e-15, eps_rel=EPS_REL, max_iters=20000, presteps=30, inner_steps=10,
+                        check_result=False, summary_frequency=0)
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(kernel: str):
+    """dram bytes per launch of `kernel` from the committed ncu summary, or None."""
+    p = PROFILES / f"{kernel}_2d4096.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("dram_bytes_per_launch")
+    return None
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples taken during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        visible = os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or (visible.isdigit() and f[0] != visible):
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ----------------------------------------------------------------------------- distributed
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=900))
+    return rank, world
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def dist_done(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------- GPU arm
+
+def parse_states(deck: str, dx: float, dy: float):
+    """The state tables as read_input builds them (tealeaf_2d/read_input.f90:216-297)."""
+    states = {}
+    for line in deck.splitlines():
+        w = line.replace("=", " ").split()
+        if not w or w[0] != "state":
+            continue
+        sid = int(w[1])
+        st = {"density": 0.0, "energy": 0.0, "xmin": 0.0, "xmax": 0.0, "ymin": 0.0, "ymax": 0.0, "radius": 0.0,
+              "geometry": 0}
+        k = 2
+        while k + 1 < len(w):
+            key, val = w[k], w[k + 1]
+            if key == "geometry":
+                st["geometry"] = {"rectangle": 1, "circle": 2, "point": 3}[val]
+            else:
+                st[key] = float(val)
+            k += 2
+        if sid >= 2:
+            st["xmin"] += dx / 100.0
+            st["ymin"] += dy / 100.0
+            st["xmax"] -= dx / 100.0
+            st["ymax"] -= dy / 100.0
+        states[sid] = st
+    return [states[k] for k in sorted(states)]
+
+
+def setup_chunk(lib, spec):
+    """start() of the reference (tealeaf_2d/start.f90:24-162) through the C ABI."""
+    import numpy as np
+
+    n = spec.cells
+    ch = tea.ExtChunk(lib, 2, n, n)
+    dx = (spec.domain - 0.0) / float(n)
+    ch.initialise(0.0, 0.0, dx, dx)
+    states = parse_states(tea.seeded_deck(spec), dx, dx)
+    arr = {k: np.array([s[k] for s in states], dtype=np.float64) for k in
+           ("density", "energy", "xmin", "xmax", "ymin", "ymax", "radius")}
+    geo = np.array([s["geometry"] for s in states], dtype=np.int32)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    I = lambda v: ctypes.byref(ctypes.c_int(v))
+    ch.call("ext_generate_chunk_", I(len(states)), P(arr["density"]), P(arr["energy"]), P(arr["xmin"]),
+            P(arr["xmax"]), P(arr["ymin"]), P(arr["ymax"]), P(arr["radius"]), P(geo), I(1), I(2), I(3))
+    ch.update_halo({1, 2, 3}, 2)
+    ch.call("ext_set_field_kernel_")
+    return ch
+
+
+def solve_params(spec):
+    p = tea.SolveParams()
+    p.solver = tea.SOLVERS[spec.solver]
+    p.coefficient = 2 if spec.inverse_density else 1
+    p.preconditioner = 1 if spec.preconditioner else 0
+    p.max_iters = spec.max_iters
+    p.ch_cg_presteps = spec.presteps
+    p.ch_cg_errswitch = 0
+    p.ppcg_inner_steps = spec.inner_steps
+    p.check_result = 0
+    p.dt = spec.dt
+    p.eps = spec.eps
+    p.ch_cg_epslim = float(ctypes.c_float(1e-5).value)
+    p.eps_rel = spec.eps_rel
+    return p
+
+
+def gpu_arm(args, world):
+    import torch
+
+    lib = tea.cuda_library(2)
+    spec = workload_spec()
+    ch = setup_chunk(lib, spec)
+    stream_ptr = ctypes.c_void_p()
+    lib.tea_chunk_stream_(ch.cid, ctypes.byref(stream_ptr))
+    stream = torch.cuda.ExternalStream(stream_ptr.value)
+    params = solve_params(spec)
+    results = []
+    for _ in range(args.warmup):
+        results.append(ch.solve(params))
+    warm = list(results)
+    results.clear()
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for _ in range(args.steps):
+        results.append(ch.solve(params))
+    t_end.record(stream)
+    t_end.synchronize()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    dist_barrier(world)
+    ms = t_start.elapsed_time(t_end)
+    ms_max = dist_max(ms, world)
+    sec_per_step = ms_max / 1000.0 / args.steps
+    bad = [r for r in results if r["status"] not in (0, 7)]
+
+    # Kernel-level: the fused kernels of the timestep, launched back to back on the same
+    # stream between CUDA events, on the chunk's live fields (steady-state operands).
+    cells = CELLS * CELLS
+    kernel_ms = {}
+    for name, kid in KERNEL_IDS.items():
+        kms = ctypes.c_double(0.0)
+        lib.tea_kernel_timing_(ch.cid, ctypes.byref(ctypes.c_int(kid)), ctypes.byref(ctypes.c_int(30)),
+                               ctypes.byref(kms))
+        kernel_ms[name] = kms.value
+    lib.ext_finalise_()
+
+    cg = [r["cg_steps"] for r in results]
+    cheby = [r["cheby_steps"] for r in results]
+    iters = [r["iterations"] for r in results]
+    mean_cg = sum(cg) / len(cg)
+    mean_ch = sum(cheby) / len(cheby)
+    share = {"cg_sweep_a": mean_cg * kernel_ms["cg_sweep_a"], "cheby_iterate": mean_ch * kernel_ms["cheby_iterate"]}
+    dominant = max(share, key=share.get)
+    alg_bytes = WORDS[dominant] * 8 * cells
+    step_words = (WORDS["cg_sweep_a"] + WORDS["cg_sweep_b"]) * mean_cg + WORDS["cheby_iterate"] * mean_ch
+    return {
+        "sec_per_step": sec_per_step, "ms_total": ms_max, "clocks": clock_info, "iterations": iters,
+        "cg_steps": cg, "cheby_steps": cheby, "kernel_ms": kernel_ms, "dominant": dominant,
+        "alg_bytes": alg_bytes, "step_alg_gbs": step_words * 8 * cells / sec_per_step / 1e9,
+        "cells_iters_per_s": cells * (sum(iters) / len(iters)) / sec_per_step,
+        "warmup_iterations": [r["iterations"] for r in warm], "bad_status": [r["status"] for r in bad],
+    }
+
+
+def e2e_arm(args):
+    """End to end through the public API: tea_run_deck (the C++ driver) runs the deck
+    through the C ABI -- host state tables in, set-up, timesteps, a field summary read back
+    after every step -- and the wall clock of the K steps after W warm-up steps is taken
+    from the driver's per-step records."""
+    spec = workload_spec(steps=args.warmup + args.steps)
+    deck = tea.seeded_deck(spec)
+    summary, recs = tea.run_deck(deck, 2, fused=True, summary_every_step=True)
+    w, k = args.warmup, args.steps
+    t0 = recs[w - 1]["wall_end"] if w > 0 else 0.0
+    t1 = recs[w + k - 1]["wall_end"]
+    h0 = recs[w - 1]["h2d_bytes"] if w > 0 else 0
+    d0 = recs[w - 1]["d2h_bytes"] if w > 0 else 0
+    return {
+        "value": (t1 - t0) / k,
+        "h2d_bytes_per_step": (recs[w + k - 1]["h2d_bytes"] - h0) / k,
+        "d2h_bytes_per_step": (recs[w + k - 1]["d2h_bytes"] - d0) / k,
+        "iterations": [r["iterations"] for r in recs],
+        "temp": summary["temp"],
+    }
+
+
+# ----------------------------------------------------------------------------- CPU (reference) arm
+
+def reference_costs(threads: int, n_cg=40, n_cheby=40):
+    """Per-iteration costs of the reference's own Kokkos-OpenMP kernels (oracle/_ref,
+    compiled from the reference sources) on this deck, timed by the driver around
+    tea_leaf() on `threads` host cores.  A full 4096^2 timestep takes the CPU minutes, so
+    the sample is bounded: the first timestep cut after n_cg CG iterations (no switch),
+    and again with the Chebyshev switch forced at iteration 20 (tl_ch_cg_errswitch with
+    an unbounded tl_ch_cg_epslim) and cut n_cheby iterations later."""
+    ref = ROOT / "oracle" / "_ref" / "libtea_ref2d.so"
+    if not ref.exists():
+        raise FileNotFoundError(str(ref))
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="true")
+
+    def run(max_iters, force_switch):
+        spec = workload_spec()
+        spec.max_iters = max_iters
+        spec.eps_rel = 0.0
+        spec.eps = 1e-300
+        if not force_switch:
+            spec.presteps = 10 ** 6
+        deck = tea.seeded_deck(spec)
+        if force_switch:
+            deck = deck.replace("*endtea", "tl_ch_cg_errswitch\ntl_ch_cg_epslim=1e300\n*endtea")
+        with tempfile.TemporaryDirectory() as td:
+            (pathlib.Path(td) / "tea.in").write_text(deck)
+            subprocess.run([str(tea.tea_leaf_exe()), "--dim", "2", "--backend", str(ref), "--quiet", "--json",
+                            str(pathlib.Path(td) / "o.json"), str(pathlib.Path(td) / "tea.in")],
+                           check=True, env=env, capture_output=True, timeout=1200)
+            return json.loads((pathlib.Path(td) / "o.json").read_text())["records"][0]
+
+    t0 = time.perf_counter()
+    a = run(n_cg, False)
+    t_cg = a["solve_seconds"] / n_cg
+    b = run(19 + n_cheby, True)
+    # 19 CG iterations, the switch iteration (first Chebyshev step: about two iterations of
+    # work plus two norms) and n_cheby - 1 further Chebyshev iterations.
+    t_cheby = max(b["solve_seconds"] - 19 * t_cg, 0.0) / (n_cheby + 1)
+    return {"t_cg": t_cg, "t_cheby": t_cheby, "wall": time.perf_counter() - t0, "threads": threads,
+            "cg_iters": a["iterations"], "cheby_run_iters": b["iterations"]}
+
+
+def cpu_estimate(costs, mean_cg, mean_cheby):
+    return costs["t_cg"] * mean_cg + costs["t_cheby"] * mean_cheby
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args, rank, world):
+    """--impl reference: the reference's CPU implementation on this box's host cores."""
+    if rank != 0:
+        dist_done(world)
+        return
+    threads = host_threads()
+    steps = list(range(args.warmup + 1, args.warmup + args.steps + 1))
+    counts = [STEP_COUNTS.get(s) for s in steps]
+    line = {"impl": "reference", "metric": METRIC, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False}
+    if not (ROOT / "oracle" / "_ref" / "libtea_ref2d.so").exists() or None in counts:
+        line["unavailable"] = ("oracle/_ref (the reference's Kokkos-OpenMP kernels built from its sources) is not "
+                               "built" if None not in counts else "iteration counts of this deck are not recorded")
+        print(json.dumps(line))
+        dist_done(world)
+        return
+    mean_cg = sum(c[0] for c in counts) / len(counts)
+    mean_ch = sum(c[1] for c in counts) / len(counts)
+    for _ in range(args.warmup):
+        reference_costs(threads, 10, 10)
+    samples = []
+    for _ in range(args.steps):
+        c = reference_costs(threads, 20, 20)
+        samples.append(cpu_estimate(c, mean_cg, mean_ch))
+    value = statistics.mean(samples)
+    line.update({
+        "value": value, "ms_per_step": value * 1000.0, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 16-state layout)",
+        "config": {"workload": "2d_4096x4096_16states_chebyshev_rel1e-10", "cells": CELLS * CELLS,
+                   "solver": SOLVER, "timesteps_timed": steps},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference",
+                         "sample": "per step: the first timestep cut after 20 CG iterations, and with the Chebyshev "
+                                   "switch forced at iteration 20 cut 20 iterations later; per-iteration costs "
+                                   f"scaled by this deck's counts (mean {mean_cg:.0f} CG + {mean_ch:.0f} Chebyshev "
+                                   "iterations per timestep)"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    })
+    print(json.dumps(line))
+    dist_done(world)
+
+
+# ----------------------------------------------------------------------------- main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 1:
+        ap.error("--warmup must be >= 1")
+    rank, world = dist_init()
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+
+    g = gpu_arm(args, world)
+    e2e = None if args.no_e2e else e2e_arm(args)
+    if rank != 0:
+        dist_done(world)
+        return
+    peak, peak_kind = load_peaks()
+    dom = g["dominant"]
+    achieved = g["alg_bytes"] / (g["kernel_ms"][dom] / 1000.0) / 1e9
+    traffic = load_traffic(dom)
+    mean_cg = sum(g["cg_steps"]) / len(g["cg_steps"])
+    mean_ch = sum(g["cheby_steps"]) / len(g["cheby_steps"])
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            threads = host_threads()
+            costs = reference_costs(threads)
+            cpu = {"value": cpu_estimate(costs, mean_cg, mean_ch), "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": (f"the first timestep cut after 40 CG iterations, and with the Chebyshev switch forced "
+                              f"at iteration 20 cut 40 iterations later ({costs['wall']:.1f} s of CPU work); "
+                              f"{costs['t_cg'] * 1e3:.2f} ms per CG and {costs['t_cheby'] * 1e3:.2f} ms per Chebyshev "
+                              f"iteration scaled by the timed steps' mean {mean_cg:.0f} CG + {mean_ch:.0f} Chebyshev "
+                              "iterations")}
+        except Exception as exc:  # noqa: BLE001
+            cpu = {"value": None, "unit": "s", "cores": None, "kind": "reference", "sample": f"unavailable: {exc}"}
+    line = {
+        "metric": METRIC, "value": g["sec_per_step"], "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": g["sec_per_step"] * 1000.0, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 16-state layout)",
+        "config": {"workload": "2d_4096x4096_16states_chebyshev_rel1e-10", "cells": CELLS * CELLS,
+                   "solver": SOLVER, "presteps": 30, "dt": 0.004, "l2": "inputs larger than L2 (135 MB per field)",
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "timesteps_timed": list(range(args.warmup + 1, args.warmup + args.steps + 1)),
+                   "iterations": g["iterations"], "cg_steps": g["cg_steps"], "cheby_steps": g["cheby_steps"]},
+        "cells_iterations_per_s": g["cells_iters_per_s"],
+        "step_algorithmic_gbs": g["step_alg_gbs"],
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic, "alg_bytes_per_launch": g["alg_bytes"],
+                     "launch_ms": g["kernel_ms"][dom], "kernel_ms": g["kernel_ms"]},
+        "clocks": g["clocks"],
+        # 2 fused launches per CG iteration, 1 per Chebyshev iteration, and about 27
+        # per-call launches per timestep (set-up, halo updates, the switch, finalise).
+        "gpu_launches": int(sum(2 * c + h + 27 for c, h in zip(g["cg_steps"], g["cheby_steps"]))),
+        "cpu_baseline": cpu,
+    }
+    if e2e:
+        timed = e2e["iterations"][args.warmup:args.warmup + args.steps]
+        line["config"]["e2e_iterations_match"] = timed == g["iterations"]
+        line["e2e"] = {"value": e2e["value"], "unit": "s", "h2d_bytes_per_step": e2e["h2d_bytes_per_step"],
+                       "d2h_bytes_per_step": e2e["d2h_bytes_per_step"]}
+    if g["bad_status"]:
+        line["status_warnings"] = g["bad_status"]
+    print(json.dumps(line))
+    dist_done(world)
+
+
+if __name__ == "__main__":
+    main()

@@ -61,6 +61,19 @@ void ext_get_status_(int* status);
 /* Message for the last non-zero status (empty string if none). */
 const char* tea_last_error(void);
 
+/* The chunk's CUDA stream (a cudaStream_t); every entry point of the chunk runs on it. */
+int tea_chunk_stream_(const int* chunk, void** stream);
+
+/* Measurement hook: `reps` back-to-back launches of one fused kernel of the whole-solve
+ * path on the chunk's stream, between two CUDA events, on the chunk's current fields
+ * (which it modifies).  kernel: 1 PPCG inner step, 2 CG/PPCG sweep A, 3 Chebyshev
+ * iteration, 4 Jacobi sweep.  Writes the mean milliseconds per launch. */
+void tea_kernel_timing_(const int* chunk, const int* kernel, const int* reps, double* ms_per_launch);
+
+/* Host<->device bytes the library has moved for the chunk so far: state tables,
+ * coefficients, scalars and results (the field arrays never leave the device). */
+int tea_transfer_bytes_(const int* chunk, long long* h2d, long long* d2h);
+
 /* Solver ids for the whole-solve entry point. */
 enum {
     TEA_SOLVER_JACOBI = 1,

@@ -79,7 +79,7 @@ class RunOptions(ctypes.Structure):
         ("dim", ctypes.c_int), ("backend", ctypes.c_char_p), ("use_fused_solve", ctypes.c_int),
         ("summary_every_step", ctypes.c_int), ("end_step_override", ctypes.c_int), ("quiet", ctypes.c_int),
         ("out_path", ctypes.c_char_p), ("eps_override", ctypes.c_double), ("eps_rel_override", ctypes.c_double),
-        ("reserved", ctypes.c_int * 8),
+        ("keep_chunk", ctypes.c_int), ("reserved", ctypes.c_int * 7),
     ]
 
 
@@ -91,6 +91,7 @@ class StepRecord(ctypes.Structure):
         ("solve_seconds", ctypes.c_double), ("vol", ctypes.c_double), ("mass", ctypes.c_double),
         ("ie", ctypes.c_double), ("temp", ctypes.c_double), ("has_summary", ctypes.c_int),
         ("switch_step", ctypes.c_int), ("est_itc", ctypes.c_int), ("pad", ctypes.c_int),
+        ("wall_end", ctypes.c_double), ("h2d_bytes", ctypes.c_longlong), ("d2h_bytes", ctypes.c_longlong),
     ]
 
 
@@ -119,7 +120,7 @@ def driver() -> ctypes.CDLL:
 
 def run_deck(deck_text: str, dim: int, backend=None, *, fused: bool = False, summary_every_step: bool = False,
              end_step: int = 0, quiet: bool = True, out_path=None, eps: float = 0.0, eps_rel: float = 0.0,
-             max_records: int = 100000):
+             keep_chunk: bool = False, max_records: int = 100000):
     """Run a tea.in deck through the C++ driver against ``backend`` (default: the CUDA
     library for ``dim``).  Returns ``(summary, records)`` as dicts."""
     backend = str(backend) if backend is not None else str(lib_path(dim))
@@ -135,6 +136,7 @@ def run_deck(deck_text: str, dim: int, backend=None, *, fused: bool = False, sum
     opt.out_path = str(out_path).encode() if out_path else None
     opt.eps_override = float(eps)
     opt.eps_rel_override = float(eps_rel)
+    opt.keep_chunk = 1 if keep_chunk else 0
     summary = RunSummary()
     records = (StepRecord * max_records)()
     lib = driver()

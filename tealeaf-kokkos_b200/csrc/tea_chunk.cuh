@@ -80,6 +80,8 @@ struct Chunk {
     int grid_blocks = 0;      // blocks for grid-stride per-call kernels
     int device = 0;
     void* fused = nullptr;    // whole-solve state (tea_fused.cuh)
+    long long h2d_bytes = 0;  // host<->device bytes moved for this chunk (inputs, results)
+    long long d2h_bytes = 0;
 };
 
 // ------------------------------------------------------------------ status

@@ -162,4 +162,58 @@ __device__ void grid_reduce(DDVec<NV> acc, const RedScratch& rs, double* out)
     }
 }
 
+// As grid_reduce, but the last block's lane 0 hands the rounded values to `f` (the
+// solver's scalar recurrence and loop control run there, with every other block done).
+template <int NV, class F>
+__device__ void grid_reduce_then(DDVec<NV> acc, const RedScratch& rs, F&& f)
+{
+    __shared__ DD s_warp2[32][NV];
+    __shared__ bool s_last2;
+    const int lane = threadIdx.x & 31;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int warp = tid >> 5;
+    const int nwarps = (blockDim.x * blockDim.y) >> 5;
+    warp_merge<NV>(acc);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s_warp2[warp][k] = acc.v[k];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        DDVec<NV> b;
+        b.zero();
+        for (int w = 0; w < nwarps; ++w)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) b.v[k] = dd_merge(b.v[k], s_warp2[w][k]);
+#pragma unroll
+        for (int k = 0; k < NV; ++k) rs.partials[(long)blockIdx.x * MAX_RED + k] = b.v[k];
+        __threadfence();
+        const unsigned int prev = atomicAdd(rs.counter, 1u);
+        s_last2 = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last2) return;
+    __threadfence();
+    if (warp == 0) {
+        DDVec<NV> b;
+        b.zero();
+        for (int blk = lane; blk < (int)gridDim.x; blk += 32)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                DD p;
+                p.hi = __ldcg(&rs.partials[(long)blk * MAX_RED + k].hi);
+                p.lo = __ldcg(&rs.partials[(long)blk * MAX_RED + k].lo);
+                b.v[k] = dd_merge(b.v[k], p);
+            }
+        warp_merge<NV>(b);
+        if (lane == 0) {
+            double vals[NV];
+#pragma unroll
+            for (int k = 0; k < NV; ++k) vals[k] = dd_value(b.v[k]);
+            *rs.counter = 0u;
+            f(vals);
+        }
+    }
+}
+
 }  // namespace tea

@@ -168,6 +168,7 @@ void destroy_chunk(Chunk* c)
 double result(Chunk* c, int k)
 {
     sync(c);
+    c->d2h_bytes += sizeof(double);
     return ((volatile double*)c->h_out)[k];
 }
 
@@ -183,6 +184,7 @@ void store_coefs(Chunk* c, const double* alphas, const double* betas, int n)
     TEA_CK(cudaMalloc(&c->d_betas, sizeof(double) * n));
     TEA_CK(cudaMemcpy(c->d_alphas, alphas, sizeof(double) * n, cudaMemcpyHostToDevice));
     TEA_CK(cudaMemcpy(c->d_betas, betas, sizeof(double) * n, cudaMemcpyHostToDevice));
+    c->h2d_bytes += 2 * sizeof(double) * (long long)n;
 }
 
 // InitialiseChunkVertices, tealeaf_2d/ext_initialise_chunk.hpp:13-61: computed on the
@@ -255,6 +257,7 @@ void generate_chunk(Chunk* c, int n, const double* den, const double* en, const 
     TEA_CK(cudaMalloc(&dg, sizeof(int) * n));
     TEA_CK(cudaMemcpy(d, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
     TEA_CK(cudaMemcpy(dg, geo, sizeof(int) * n, cudaMemcpyHostToDevice));
+    c->h2d_bytes += (long long)(sizeof(double) * h.size() + sizeof(int) * n);
     StateTable st;
     st.n = n;
     st.rect = rect;
@@ -413,6 +416,7 @@ TEA_EXPORT void ext_field_summary_kernel_(const int* chunk, double* vol, double*
     k_field_summary<<<launch_blocks(c, c->inner.ntiles), dim3(TILE_X, TILE_Y), 0, c->stream>>>(
         c->g, c->inner, c->f, c->red, c->d_out);
     sync(c);
+    c->d2h_bytes += 4 * sizeof(double);
     volatile double* h = c->h_out;
     *vol = h[0];
     *mass = h[1];
@@ -442,12 +446,18 @@ static void pack_message(const int* chunk, const int* fields, const int* offsets
     for (int fid = 1; fid <= 6; ++fid) {
         if (!fields[fid - 1]) continue;
         double* ext = buffer + offsets[fid - 1];
-        if (!do_pack) TEA_CK(cudaMemcpy(dbuf, ext, sizeof(double) * len, cudaMemcpyHostToDevice));
+        if (!do_pack) {
+            TEA_CK(cudaMemcpy(dbuf, ext, sizeof(double) * len, cudaMemcpyHostToDevice));
+            c->h2d_bytes += (long long)sizeof(double) * len;
+        }
         const int blocks = (int)std::min<long>((len + 255) / 256, 4096);
         k_pack<<<std::max(blocks, 1), 256, 0, c->stream>>>(c->g, halo_field(c, fid), dbuf, len, *face, *depth,
                                                            do_pack ? 1 : 0);
         sync(c);
-        if (do_pack) TEA_CK(cudaMemcpy(ext, dbuf, sizeof(double) * len, cudaMemcpyDeviceToHost));
+        if (do_pack) {
+            TEA_CK(cudaMemcpy(ext, dbuf, sizeof(double) * len, cudaMemcpyDeviceToHost));
+            c->d2h_bytes += (long long)sizeof(double) * len;
+        }
     }
     TEA_CK(cudaFree(dbuf));
 }
@@ -710,3 +720,24 @@ TEA_EXPORT void ext_get_status_(int* status)
 }
 
 TEA_EXPORT const char* tea_last_error(void) { return status_store().message.c_str(); }
+
+// The chunk's CUDA stream (cudaStream_t), for callers that order their own work or
+// record events after the library's.
+TEA_EXPORT int tea_chunk_stream_(const int* chunk, void** stream)
+{
+    auto& v = chunks();
+    if (!chunk || *chunk < 1 || (size_t)*chunk > v.size()) return 1;
+    *stream = (void*)v[*chunk - 1]->stream;
+    return 0;
+}
+
+// Host<->device bytes the library has moved for this chunk so far (state tables,
+// coefficients, scalars, results, solve-state records); field arrays stay on the device.
+TEA_EXPORT int tea_transfer_bytes_(const int* chunk, long long* h2d, long long* d2h)
+{
+    auto& v = chunks();
+    if (!chunk || *chunk < 1 || (size_t)*chunk > v.size()) return 1;
+    *h2d = v[*chunk - 1]->h2d_bytes;
+    *d2h = v[*chunk - 1]->d2h_bytes;
+    return 0;
+}

@@ -1,18 +1,608 @@
-// Whole-solve path (ext_tea_leaf_solve_): provisional entry point until the fused
-// kernels land; it records TEA_ERR_BAD_ARGUMENT.
-#include "tea_chunk.cuh"
+// ext_tea_leaf_solve_: the whole implicit solve of one timestep on the device.
+//
+// Follows tea_leaf() (tealeaf_2d/tea_solve.f90:36-605; 3D :36-653) step for step.  The
+// once-per-solve parts -- set-up, the Chebyshev/PPCG switch with its eigenvalue estimate
+// (host FP64, tea_eigen.h), the first Chebyshev step and the first PPCG outer iteration,
+// the exact-residual check and the finalise -- call the same per-call kernels as the ext_*
+// entry points.  The iteration loops run as CUDA graphs whose body is one iteration of
+// fused kernels (tea_fused.cuh) inside a while-node; the scalars and the EXIT test live on
+// the device.  Results (fields, iteration counts, errors) equal the per-call sequence that
+// the driver would make bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
 #include "../../include/tea_b200.h"
+#if TEA_DIM == 2
+#include "../../include/tea_ext_2d.h"
+#else
+#include "../../include/tea_ext_3d.h"
+#endif
+#include "../driver/tea_eigen.h"
+#include "tea_fused.cuh"
+
+#define TEA_EXPORT extern "C" __attribute__((visibility("default")))
 
 namespace tea {
-void destroy_fused(Chunk* c) { (void)c; }
+
+Chunk* get_chunk(const int* chunk);
+void sync(Chunk* c);
+void update_halo(Chunk* c, const int* neighbours, const int* fields, int depth);
+
+namespace {
+
+enum { LOOP_CG = 0, LOOP_CHEBY = 1, LOOP_PPCG = 2, LOOP_JACOBI = 3, LOOP_COUNT = 4 };
+
+struct Loop {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int key = -1;
+};
+
+struct Fused {
+    SolveState* d_st = nullptr;
+    SolveState* h_st = nullptr;  // pinned
+    double* alt[3] = {nullptr, nullptr, nullptr};  // allocations of u, p, sd second buffers
+    double *d_cg_alphas = nullptr, *d_cg_betas = nullptr;
+    double *d_ch_alphas = nullptr, *d_ch_betas = nullptr;
+    int cap = 0;  // entries of the coefficient arrays
+    FusedArgs base{};
+    int stencil_blocks = 0, point_blocks = 0;
+    Loop loops[LOOP_COUNT];
+    bool use_graph = true;
+};
+
+Fused* fused_of(Chunk* c) { return static_cast<Fused*>(c->fused); }
+
+void free_loops(Fused* F)
+{
+    for (Loop& l : F->loops) {
+        if (l.exec) cudaGraphExecDestroy(l.exec);
+        if (l.graph) cudaGraphDestroy(l.graph);
+        l = Loop();
+    }
+}
+
+template <class K>
+int occupancy(K kernel, int threads)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess || n < 1) n = 1;
+    return n;
+}
+
+Fused* ensure_fused(Chunk* c, int max_iters)
+{
+    Fused* F = fused_of(c);
+    if (!F) {
+        F = new Fused();
+        c->fused = F;
+        const char* env = std::getenv("TEA_B200_NO_GRAPH");
+        F->use_graph = !(env && env[0] == '1');
+        TEA_CK(cudaMalloc(&F->d_st, sizeof(SolveState)));
+        TEA_CK(cudaHostAlloc(&F->h_st, sizeof(SolveState), cudaHostAllocDefault));
+        for (int k = 0; k < 3; ++k) {
+            TEA_CK(cudaMalloc(&F->alt[k], c->field_elems * sizeof(double)));
+            if (F->alt[k]) TEA_CK(cudaMemset(F->alt[k], 0, c->field_elems * sizeof(double)));
+        }
+        const Geom& g = c->g;
+        FusedArgs& a = F->base;
+        a.g = g;
+        a.u[0] = c->f.u;
+        a.u[1] = F->alt[0] + kLeadPad;
+        a.p[0] = c->f.p;
+        a.p[1] = F->alt[1] + kLeadPad;
+        a.sd[0] = c->f.sd;
+        a.sd[1] = F->alt[2] + kLeadPad;
+        a.r = c->f.r;
+        a.w = c->f.w;
+        a.z = c->f.z;
+        a.mi = c->f.mi;
+        a.u0 = c->f.u0;
+        a.kx = c->f.kx;
+        a.ky = c->f.ky;
+        a.kz = c->f.kz;
+        a.st = F->d_st;
+        a.red = c->red;
+        a.use_handle = 0;
+        a.step = 0;
+        a.timing = 0;
+        int sms = 148;
+        TEA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        if (DIM == 2) {
+            a.tiles_x = (g.nx + SBLOCK - 1) / SBLOCK;
+            a.tiles_y = (g.ny + SY - 1) / SY;
+            a.zseg = 1;
+            a.ntiles = (long)a.tiles_x * a.tiles_y;
+        } else {
+            a.tiles_x = (g.nx + FT_X - 1) / FT_X;
+            a.tiles_y = (g.ny + FT_Y3 - 1) / FT_Y3;
+            const long txy = (long)a.tiles_x * a.tiles_y;
+            int zseg = g.nz;
+            const long want = 8L * sms * 4;
+            while (zseg > 8 && txy * ((g.nz + zseg - 1) / zseg) < want) zseg = (zseg + 1) / 2;
+            a.zseg = zseg;
+            a.ntiles = txy * ((g.nz + zseg - 1) / zseg);
+        }
+        const int nthr = (int)(TEA_STENCIL_BLOCK.x * TEA_STENCIL_BLOCK.y);
+        int occ = occupancy(TEA_STENCIL<OpSweepA>, nthr);
+        occ = std::min(occ, occupancy(TEA_STENCIL<OpCheby>, nthr));
+        occ = std::min(occ, occupancy(TEA_STENCIL<OpPPCGInner<true>>, nthr));
+        occ = std::min(occ, occupancy(TEA_STENCIL<OpJacobi>, nthr));
+        F->stencil_blocks = (int)std::min<long>(a.ntiles, (long)sms * occ);
+        F->stencil_blocks = std::min(F->stencil_blocks, c->red.max_blocks);
+        F->stencil_blocks = std::max(F->stencil_blocks, 1);
+        F->point_blocks = launch_blocks(c, c->inner.ntiles);
+    }
+    if (F->cap < max_iters + 2) {
+        free_loops(F);  // the graphs hold the old pointers
+        for (double* p : {F->d_cg_alphas, F->d_cg_betas, F->d_ch_alphas, F->d_ch_betas})
+            if (p) TEA_CK(cudaFree(p));
+        F->cap = max_iters + 2;
+        TEA_CK(cudaMalloc(&F->d_cg_alphas, sizeof(double) * F->cap));
+        TEA_CK(cudaMalloc(&F->d_cg_betas, sizeof(double) * F->cap));
+        TEA_CK(cudaMalloc(&F->d_ch_alphas, sizeof(double) * F->cap));
+        TEA_CK(cudaMalloc(&F->d_ch_betas, sizeof(double) * F->cap));
+        TEA_CK(cudaMemset(F->d_ch_alphas, 0, sizeof(double) * F->cap));
+        TEA_CK(cudaMemset(F->d_ch_betas, 0, sizeof(double) * F->cap));
+        F->base.cg_alphas = F->d_cg_alphas;
+        F->base.cg_betas = F->d_cg_betas;
+        F->base.ch_alphas = F->d_ch_alphas;
+        F->base.ch_betas = F->d_ch_betas;
+    }
+    return F;
+}
+
+// Enqueue one iteration of loop `kind` on the chunk's stream.
+void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs& a)
+{
+    const dim3 sb = TEA_STENCIL_BLOCK;
+    const dim3 pb(TILE_X, TILE_Y);
+    cudaStream_t s = c->stream;
+    switch (kind) {
+    case LOOP_CG:
+        TEA_STENCIL<OpSweepA><<<F->stencil_blocks, sb, 0, s>>>(a);
+        k_cg_sweep_b<<<F->point_blocks, pb, 0, s>>>(a, c->inner);
+        break;
+    case LOOP_CHEBY:
+        TEA_STENCIL<OpCheby><<<F->stencil_blocks, sb, 0, s>>>(a);
+        break;
+    case LOOP_PPCG: {
+        TEA_STENCIL<OpSweepA><<<F->stencil_blocks, sb, 0, s>>>(a);
+        k_ppcg_sweep_b<<<F->point_blocks, pb, 0, s>>>(a, c->inner);
+        for (int k = 1; k <= inner_steps; ++k) {
+            FusedArgs ak = a;
+            ak.step = k;
+            if (k < inner_steps) TEA_STENCIL<OpPPCGInner<false>><<<F->stencil_blocks, sb, 0, s>>>(ak);
+            else TEA_STENCIL<OpPPCGInner<true>><<<F->stencil_blocks, sb, 0, s>>>(ak);
+        }
+        break;
+    }
+    case LOOP_JACOBI:
+        TEA_STENCIL<OpJacobi><<<F->stencil_blocks, sb, 0, s>>>(a);
+        TEA_STENCIL<OpJacobiResidual><<<F->stencil_blocks, sb, 0, s>>>(a);
+        break;
+    }
+}
+
+// Build (once per chunk, loop kind and inner-step count) a graph holding a while-node
+// whose body is one iteration.
+bool build_loop(Chunk* c, Fused* F, int kind, int inner_steps)
+{
+    Loop& L = F->loops[kind];
+    const int key = kind == LOOP_PPCG ? inner_steps : 0;
+    if (L.exec && L.key == key) return true;
+    if (L.exec) cudaGraphExecDestroy(L.exec);
+    if (L.graph) cudaGraphDestroy(L.graph);
+    L = Loop();
+    cudaGraph_t graph = nullptr;
+    if (cudaGraphCreate(&graph, 0) != cudaSuccess) return false;
+    cudaGraphConditionalHandle handle;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) {
+        set_status(TEA_ERR_CUDA, "cudaGraphConditionalHandleCreate: %s", cudaGetErrorString(e));
+        cudaGraphDestroy(graph);
+        return false;
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+    if (e != cudaSuccess) {
+        set_status(TEA_ERR_CUDA, "cudaGraphAddNode(while): %s", cudaGetErrorString(e));
+        cudaGraphDestroy(graph);
+        return false;
+    }
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    FusedArgs a = F->base;
+    a.handle = handle;
+    a.use_handle = 1;
+    TEA_CK(cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    enqueue_body(c, F, kind, inner_steps, a);
+    cudaGraph_t captured = nullptr;
+    TEA_CK(cudaStreamEndCapture(c->stream, &captured));
+    e = cudaGraphInstantiate(&L.exec, graph, 0);
+    if (e != cudaSuccess) {
+        set_status(TEA_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+        cudaGraphDestroy(graph);
+        L = Loop();
+        return false;
+    }
+    L.graph = graph;
+    L.key = key;
+    return true;
+}
+
+void push_state(Chunk* c, Fused* F)
+{
+    TEA_CK(cudaMemcpyAsync(F->d_st, F->h_st, sizeof(SolveState), cudaMemcpyHostToDevice, c->stream));
+    c->h2d_bytes += sizeof(SolveState);
+}
+
+void pull_state(Chunk* c, Fused* F)
+{
+    TEA_CK(cudaMemcpyAsync(F->h_st, F->d_st, sizeof(SolveState), cudaMemcpyDeviceToHost, c->stream));
+    c->d2h_bytes += sizeof(SolveState);
+    sync(c);
+}
+
+// Run loop `kind` from the current state until its exit; the host state is refreshed.
+void run_loop(Chunk* c, Fused* F, int kind, int inner_steps)
+{
+    push_state(c, F);
+    if (F->use_graph && build_loop(c, F, kind, inner_steps)) {
+        TEA_CK(cudaGraphLaunch(F->loops[kind].exec, c->stream));
+        pull_state(c, F);
+        return;
+    }
+    // Without graphs: one iteration per launch sequence, the exit flag read back each time.
+    FusedArgs a = F->base;
+    for (;;) {
+        enqueue_body(c, F, kind, inner_steps, a);
+        pull_state(c, F);
+        if (!F->h_st->cont || status_store().status == TEA_ERR_CUDA) break;
+    }
+}
+
+// Host mirror of end_iteration() for the iterations run by per-call kernels.
+void end_iteration_host(SolveState& s, int phase)
+{
+    const int n = s.n;
+    int cont = 1, reason = EXIT_NONE;
+    if (std::fabs(s.error) < s.eps) {
+        cont = 0;
+        reason = EXIT_CONVERGED;
+    } else if (n + 1 > s.max_iters) {
+        cont = 0;
+        reason = EXIT_MAXITER;
+    } else if (s.solver == SOLVER_CHEBY || s.solver == SOLVER_PPCG) {
+        const bool sw = s.errswitch ? (s.cheby_calc_steps > 0) || ((s.error <= s.epslim) && (n + 1 >= 20))
+                                    : (n + 1 >= s.presteps) && (s.error <= 1.0);
+        if ((phase == PHASE_CG) == sw) {
+            cont = 0;
+            reason = EXIT_PHASE;
+        }
+    }
+    if (reason != EXIT_CONVERGED) s.n = n + 1;
+    s.cont = cont;
+    s.exit_reason = reason;
+}
+
+bool switch_check_host(const SolveState& s, int n)
+{
+    if (s.errswitch) return (s.cheby_calc_steps > 0) || ((s.error <= s.epslim) && (n >= 20));
+    return (n >= s.presteps) && (s.error <= 1.0);
+}
+
+const int kAllExternal[6] = {-1, -1, -1, -1, -1, -1};
+
+void halo(Chunk* c, std::initializer_list<int> ids, int depth)
+{
+    int fields[6] = {0, 0, 0, 0, 0, 0};
+    for (int id : ids) fields[id - 1] = 1;
+    update_halo(c, kAllExternal, fields, depth);
+}
+
+// Bring u and p to the state the per-call kernels expect: pending updates applied,
+// current values in the canonical buffers, the depth-1 halo of u reflected and that of
+// p reflected when the reference's halo field list holds p at this point (it does not
+// in Chebyshev mode before a CG iteration has run, tealeaf_2d/tea_solve.f90:203-204).
+void canonicalize(Chunk* c, Fused* F, bool refresh_p = true)
+{
+    SolveState& s = *F->h_st;
+    FusedArgs a = F->base;
+    if (s.pending_p || s.pending_u) {
+        push_state(c, F);
+        k_flush<<<F->point_blocks, dim3(TILE_X, TILE_Y), 0, c->stream>>>(a, c->inner);
+        s.pending_p = 0;
+        s.pending_u = 0;
+    }
+    const size_t bytes = c->field_elems * sizeof(double);
+    if (s.par_p) {
+        TEA_CK(cudaMemcpyAsync(c->alloc[F_P], F->alt[1], bytes, cudaMemcpyDeviceToDevice, c->stream));
+        s.par_p = 0;
+    }
+    if (s.par_u) {
+        TEA_CK(cudaMemcpyAsync(c->alloc[F_U], F->alt[0], bytes, cudaMemcpyDeviceToDevice, c->stream));
+        s.par_u = 0;
+    }
+    push_state(c, F);
+    if (refresh_p) halo(c, {4, 5}, 1);
+    else halo(c, {4}, 1);
+}
+
+}  // namespace
+
+void destroy_fused(Chunk* c)
+{
+    Fused* F = fused_of(c);
+    if (!F) return;
+    free_loops(F);
+    for (double* p : {F->d_cg_alphas, F->d_cg_betas, F->d_ch_alphas, F->d_ch_betas})
+        if (p) cudaFree(p);
+    for (double* p : F->alt)
+        if (p) cudaFree(p);
+    if (F->d_st) cudaFree(F->d_st);
+    if (F->h_st) cudaFreeHost(F->h_st);
+    delete F;
+    c->fused = nullptr;
+}
+
 }  // namespace tea
 
-extern "C" __attribute__((visibility("default"))) void ext_tea_leaf_solve_(const int* chunk,
-                                                                           const tea_solve_params* params,
-                                                                           tea_solve_result* result)
+using namespace tea;
+
+TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P, tea_solve_result* R)
 {
-    (void)chunk;
-    (void)params;
-    if (result) result->status = 2;
-    tea::set_status(2, "ext_tea_leaf_solve_ is not available in this build");
+    if (R) std::memset(R, 0, sizeof(*R));
+    Chunk* c = get_chunk(chunk);
+    if (!c || !P || !R) return;
+    const int solver = P->solver;
+    if (solver < TEA_SOLVER_JACOBI || solver > TEA_SOLVER_PPCG || P->max_iters < 1 ||
+        (solver == TEA_SOLVER_PPCG && P->ppcg_inner_steps < 1)) {
+        set_status(TEA_ERR_BAD_ARGUMENT, "ext_tea_leaf_solve_: invalid parameters");
+        R->status = TEA_ERR_BAD_ARGUMENT;
+        return;
+    }
+    Fused* F = ensure_fused(c, P->max_iters);
+    const bool cg_like = solver != TEA_SOLVER_JACOBI;
+    int coefficient = P->coefficient, precond = P->preconditioner ? 1 : 0;
+    double dt = P->dt;
+
+    // INIT, tealeaf_2d/tea_solve.f90:79-164.
+    halo(c, {3, 1}, 2);
+    double rro = 0.0;
+    if (cg_like) {
+        ext_cg_solver_init_(chunk, &coefficient, &precond, &dt, &rro);
+        halo(c, {4, 5}, 1);
+    } else {
+        ext_jacobi_kernel_init_(chunk, &coefficient, &dt);
+    }
+    ext_solver_copy_u_(chunk);
+    double eps = P->eps;
+    if (P->eps_rel > 0.0) {
+        double bb = 0.0;
+        int zero = 0;
+        ext_calculate_2norm_(chunk, &bb, &zero);
+        eps = P->eps_rel * P->eps_rel * bb;
+    }
+    // The second buffers start as copies, so halos the loops never write match u and p.
+    const size_t bytes = c->field_elems * sizeof(double);
+    TEA_CK(cudaMemcpyAsync(F->alt[0], c->alloc[F_U], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    TEA_CK(cudaMemcpyAsync(F->alt[1], c->alloc[F_P], bytes, cudaMemcpyDeviceToDevice, c->stream));
+
+    SolveState& s = *F->h_st;
+    std::memset(&s, 0, sizeof(s));
+    s.rro = rro;
+    s.error = 1e10;
+    s.eps = eps;
+    s.epslim = P->ch_cg_epslim;
+    s.n = 1;
+    s.cont = 1;
+    s.solver = solver;
+    s.precond = precond;
+    s.max_iters = P->max_iters;
+    s.presteps = P->ch_cg_presteps;
+    s.errswitch = P->ch_cg_errswitch ? 1 : 0;
+    s.inner_steps = P->ppcg_inner_steps;
+    const bool cheby = solver == TEA_SOLVER_CHEBYSHEV, ppcg = solver == TEA_SOLVER_PPCG;
+    int switch_step = 0, cg_steps = 0;
+    double eigmin = 0.0, eigmax = 0.0;
+    // Whether the reference's update_halo field list currently includes p (FIELD_P): true
+    // from the CG set-up, false after the Chebyshev switch until a CG iteration runs.
+    bool p_halo_fresh = true;
+
+    if (!cg_like) {
+        run_loop(c, F, LOOP_JACOBI, 0);
+    } else {
+        std::vector<double> ch_alphas, ch_betas;
+        double theta = 0.0, cn = 0.0;
+        int max_cheby_iters = 0;
+        for (int guard = 0; guard < 4 * P->max_iters + 8; ++guard) {
+            if (status_store().status == TEA_ERR_CUDA) break;
+            const int n = s.n;
+            if ((cheby || ppcg) && switch_check_host(s, n)) {
+                if (s.cheby_calc_steps == 0) {
+                    // The switch, tealeaf_2d/tea_solve.f90:184-223, on the host.
+                    canonicalize(c, F);
+                    cg_steps = n - 1;
+                    std::vector<double> ca(n + 1, 0.0), cb(n + 1, 0.0);
+                    TEA_CK(cudaMemcpyAsync(ca.data(), F->d_cg_alphas, sizeof(double) * (n + 1),
+                                           cudaMemcpyDeviceToHost, c->stream));
+                    TEA_CK(cudaMemcpyAsync(cb.data(), F->d_cg_betas, sizeof(double) * (n + 1),
+                                           cudaMemcpyDeviceToHost, c->stream));
+                    sync(c);
+                    c->d2h_bytes += 2 * sizeof(double) * (long long)(n + 1);
+                    max_cheby_iters = P->max_iters - n + 2;
+                    s.rro = s.error;
+                    int info = tea_calc_eigenvalues(ca.data() + 1, cb.data() + 1, n - 1, &eigmin, &eigmax);
+                    if (info != 0) {
+                        set_status(TEA_ERR_EIGEN, "tea_leaf: Error in calculating eigenvalues");
+                        R->status = TEA_ERR_EIGEN;
+                        return;
+                    }
+                    eigmin = eigmin * kEigMinScale;
+                    eigmax = eigmax * kEigMaxScale;
+                    const int ncoef = std::max(max_cheby_iters, P->ppcg_inner_steps) + 1;
+                    ch_alphas.assign(ncoef, 0.0);
+                    ch_betas.assign(ncoef, 0.0);
+                    tea_calc_ch_coefs(ch_alphas.data(), ch_betas.data(), eigmin, eigmax, &theta,
+                                      cheby ? max_cheby_iters : P->ppcg_inner_steps);
+                    cn = eigmax / eigmin;
+                    const int nup = std::min<int>((int)ch_alphas.size(), F->cap);
+                    TEA_CK(cudaMemcpyAsync(F->d_ch_alphas, ch_alphas.data(), sizeof(double) * nup,
+                                           cudaMemcpyHostToDevice, c->stream));
+                    TEA_CK(cudaMemcpyAsync(F->d_ch_betas, ch_betas.data(), sizeof(double) * nup,
+                                           cudaMemcpyHostToDevice, c->stream));
+                    c->h2d_bytes += 2 * sizeof(double) * (long long)nup;
+                    switch_step = n;
+                    if (cheby) {
+                        // tea_leaf_cheby_first_step, tealeaf_2d/tea_solve.f90:658-750.
+                        double bb = 0.0, err = 0.0;
+                        int zero = 0, one = 1;
+                        ext_calculate_2norm_(chunk, &bb, &zero);
+                        ext_cheby_solver_init_(chunk, ch_alphas.data(), ch_betas.data(), &theta, &precond,
+                                               &max_cheby_iters);
+                        halo(c, {4}, 1);
+                        ext_cheby_solver_iterate_(chunk, &max_cheby_iters);
+                        ext_calculate_2norm_(chunk, &err, &one);
+                        s.error = err;
+                        s.est_itc = tea_cheby_est_itc(bb, err, cn);
+                        s.cheby_calc_steps = 2;
+                        halo(c, {4}, 1);
+                        p_halo_fresh = false;
+                        end_iteration_host(s, PHASE_CHEBY);
+                    } else {
+                        // First PPCG outer iteration, tealeaf_2d/tea_solve.f90:276-375.
+                        s.cheby_calc_steps = 1;
+                        ext_ppcg_init_(chunk, ch_alphas.data(), ch_betas.data(), &theta, &max_cheby_iters);
+                        ext_calculate_residual_(chunk);
+                        halo(c, {4, 5}, 1);
+                        double pw = 0.0, rrn = 0.0;
+                        ext_cg_calc_w_(chunk, &pw);
+                        double alpha = s.rro / pw;
+                        ext_cg_calc_ur_(chunk, &alpha, &rrn);
+                        ext_ppcg_init_sd_(chunk);
+                        for (int k = 1; k <= P->ppcg_inner_steps; ++k) {
+                            halo(c, {6}, 1);
+                            ext_ppcg_inner_(chunk, &k);
+                        }
+                        int one = 1;
+                        ext_calculate_2norm_(chunk, &rrn, &one);
+                        double beta = rrn / s.rro;
+                        ext_cg_calc_p_(chunk, &beta);
+                        s.error = rrn;
+                        s.rro = rrn;
+                        s.theta = theta;
+                        s.cheby_calc_steps = 2;
+                        halo(c, {4, 5}, 1);
+                        end_iteration_host(s, PHASE_PPCG);
+                    }
+                    // Fresh copies for the second buffers (halos as in the canonical ones).
+                    TEA_CK(cudaMemcpyAsync(F->alt[0], c->alloc[F_U], bytes, cudaMemcpyDeviceToDevice, c->stream));
+                    TEA_CK(cudaMemcpyAsync(F->alt[1], c->alloc[F_P], bytes, cudaMemcpyDeviceToDevice, c->stream));
+                    if (s.exit_reason == EXIT_CONVERGED || s.exit_reason == EXIT_MAXITER) break;
+                    continue;
+                }
+                run_loop(c, F, cheby ? LOOP_CHEBY : LOOP_PPCG, P->ppcg_inner_steps);
+            } else if (!p_halo_fresh) {
+                // A CG iteration in Chebyshev mode (the error rose above 1 after the switch):
+                // its ext_cg_calc_w_ reads the halo of p as last refreshed before the switch,
+                // so it runs through the per-call kernels, which read halos from memory.
+                double pw = 0.0, rrn = 0.0;
+                ext_cg_calc_w_(chunk, &pw);
+                s.alpha = s.rro / pw;
+                ext_cg_calc_ur_(chunk, &s.alpha, &rrn);
+                s.beta = rrn / s.rro;
+                ext_cg_calc_p_(chunk, &s.beta);
+                s.error = rrn;
+                s.rro = rrn;
+                p_halo_fresh = true;
+                halo(c, {4, 5}, 1);
+                end_iteration_host(s, PHASE_CG);
+                push_state(c, F);
+                if (s.exit_reason == EXIT_CONVERGED || s.exit_reason == EXIT_MAXITER) break;
+                continue;
+            } else {
+                run_loop(c, F, LOOP_CG, 0);
+            }
+            if (s.exit_reason != EXIT_PHASE) break;
+            canonicalize(c, F, p_halo_fresh);
+        }
+    }
+    canonicalize(c, F);
+    if (s.nonfinite) set_status(TEA_ERR_NONFINITE, "ext_tea_leaf_solve_: non-finite value in a reduction");
+    double exact_error = 0.0;
+    if (P->check_result) {
+        int one = 1;
+        ext_calculate_residual_(chunk);
+        ext_calculate_2norm_(chunk, &exact_error, &one);
+    }
+    ext_solver_finalise_(chunk);
+    halo(c, {3}, 1);
+    sync(c);
+    R->iterations = s.n - 1;
+    R->status = status_store().status;
+    R->cg_steps = switch_step ? cg_steps : s.n - 1;
+    R->cheby_steps = s.cheby_calc_steps > 0 ? s.cheby_calc_steps - 1 : 0;
+    R->switch_step = switch_step;
+    R->est_itc = s.est_itc;
+    R->error = s.error;
+    R->exact_error = exact_error;
+    R->eps_used = eps;
+    R->eigmin = eigmin;
+    R->eigmax = eigmax;
+}
+
+// Measurement hook: `reps` back-to-back launches of one fused kernel on the chunk's
+// stream between two CUDA events, on the chunk's current fields (their values change).
+// kernel: 1 PPCG inner step, 2 CG/PPCG sweep A, 3 Chebyshev iteration, 4 Jacobi sweep.
+TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const int* reps, double* ms_per_launch)
+{
+    *ms_per_launch = 0.0;
+    Chunk* c = get_chunk(chunk);
+    if (!c || *reps < 1) return;
+    Fused* F = ensure_fused(c, 1);
+    FusedArgs a = F->base;
+    a.step = 1;
+    a.timing = 1;
+    // Steady-state operands: sweep A applies a pending p and u update, as it does in every
+    // CG iteration after the first.
+    pull_state(c, F);
+    F->h_st->pending_p = 1;
+    F->h_st->pending_u = 1;
+    push_state(c, F);
+    const dim3 sb = TEA_STENCIL_BLOCK;
+    cudaEvent_t e0, e1;
+    TEA_CK(cudaEventCreate(&e0));
+    TEA_CK(cudaEventCreate(&e1));
+    auto launch = [&]() {
+        switch (*kernel) {
+        case 1: TEA_STENCIL<OpPPCGInner<false>><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
+        case 2: TEA_STENCIL<OpSweepA><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
+        case 3: TEA_STENCIL<OpCheby><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
+        default: TEA_STENCIL<OpJacobi><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
+        }
+    };
+    launch();  // warm-up
+    TEA_CK(cudaEventRecord(e0, c->stream));
+    for (int k = 0; k < *reps; ++k) launch();
+    TEA_CK(cudaEventRecord(e1, c->stream));
+    TEA_CK(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    TEA_CK(cudaEventElapsedTime(&ms, e0, e1));
+    *ms_per_launch = (double)ms / *reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    F->h_st->pending_p = 0;
+    F->h_st->pending_u = 0;
+    push_state(c, F);
+    sync(c);
 }

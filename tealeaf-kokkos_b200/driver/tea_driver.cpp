@@ -301,6 +301,7 @@ struct Backend {
     void (*ppcg_inner)(const int*, int*) = nullptr;
     void (*whole_solve)(const int*, const tea_solve_params*, tea_solve_result*) = nullptr;
     void (*get_status)(int*) = nullptr;
+    int (*transfer_bytes)(const int*, long long*, long long*) = nullptr;
 
     template <class F>
     void bind(F& fp, const char* name, bool required = true)
@@ -340,6 +341,7 @@ struct Backend {
         bind(ppcg_inner, "ext_ppcg_inner_");
         bind(whole_solve, "ext_tea_leaf_solve_", false);
         bind(get_status, "ext_get_status_", false);
+        bind(transfer_bytes, "tea_transfer_bytes_", false);
     }
 
     void close()
@@ -354,7 +356,7 @@ struct Backend {
         if (!get_status) return;
         int st = 0;
         get_status(&st);
-        if (st != TEA_OK && st != TEA_ERR_NOT_CONVERGED) fail("backend status %d after %s", st, where);
+        if (st != TEA_OK && st != TEA_ERR_NOT_CONVERGED && st != TEA_ERR_NONFINITE) fail("backend status %d after %s", st, where);
     }
 };
 
@@ -775,6 +777,8 @@ struct Runner {
                 rec.vol = v[0]; rec.mass = v[1]; rec.ie = v[2]; rec.temp = v[3];
                 rec.has_summary = 1;
             }
+            rec.wall_end = now_seconds() - t0;
+            if (be.transfer_bytes) be.transfer_bytes(&chunk, &rec.h2d_bytes, &rec.d2h_bytes);
             if (steps && step - 1 < max_steps) steps[step - 1] = rec;
             if (last) break;
         }
@@ -789,7 +793,7 @@ struct Runner {
         log.line("");
         log.line(" Calculation complete");
         log.line(" Tea is finishing");
-        be.finalise();
+        if (!opt->keep_chunk) be.finalise();
         return 0;
     }
 };

@@ -25,7 +25,8 @@ typedef struct {
     const char* out_path;    /* write the tea.out log here (NULL: none) */
     double eps_override;     /* > 0: replace tl_eps */
     double eps_rel_override; /* > 0: replace tl_eps_rel */
-    int reserved[8];
+    int keep_chunk;          /* 1: skip ext_finalise_ so the caller can inspect the fields */
+    int reserved[7];
 } tea_run_options;
 
 typedef struct {
@@ -44,6 +45,9 @@ typedef struct {
     int switch_step;
     int est_itc;
     int pad;
+    double wall_end;         /* seconds since the start of the timestep loop, at the step's end */
+    long long h2d_bytes;     /* backend host->device bytes so far (0 if not reported) */
+    long long d2h_bytes;     /* backend device->host bytes so far */
 } tea_step_record;
 
 typedef struct {
