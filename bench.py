@@ -55,7 +55,8 @@ WORDS = {  # algorithmic FP64 words per interior cell of one launch
     "cg_sweep_b": 3,   # read r, w; write r
     "cheby_iterate": 7,  # read u, u0, p, Kx, Ky; write u', p
 }
-KERNEL_IDS = {"cg_sweep_a": 2, "cheby_iterate": 3}
+KERNEL_IDS = {"cg_sweep_a": 2, "cheby_iterate": 3, "cg_sweep_b": 5}
+ALL_KERNEL_IDS = {"ppcg_inner": 1, "cg_sweep_a": 2, "cheby_iterate": 3, "jacobi": 4, "cg_sweep_b": 5}
 PROFILES = ROOT / "profiles"
 # Per-timestep iteration counts of this deck (CG iterations before the Chebyshev switch,
 # Chebyshev iterations after it) for simulation steps 1..20, measured with this build; the
@@ -298,7 +299,8 @@ def gpu_arm(args, world):
     iters = [r["iterations"] for r in results]
     mean_cg = sum(cg) / len(cg)
     mean_ch = sum(cheby) / len(cheby)
-    share = {"cg_sweep_a": mean_cg * kernel_ms["cg_sweep_a"], "cheby_iterate": mean_ch * kernel_ms["cheby_iterate"]}
+    share = {"cg_sweep_a": mean_cg * kernel_ms["cg_sweep_a"], "cg_sweep_b": mean_cg * kernel_ms["cg_sweep_b"],
+             "cheby_iterate": mean_ch * kernel_ms["cheby_iterate"]}
     dominant = max(share, key=share.get)
     alg_bytes = WORDS[dominant] * 8 * cells
     step_words = (WORDS["cg_sweep_a"] + WORDS["cg_sweep_b"]) * mean_cg + WORDS["cheby_iterate"] * mean_ch
@@ -427,6 +429,19 @@ def reference_arm(args, rank, world):
     dist_done(world)
 
 
+def kernel_only(args):
+    """Set up the 4096^2 workload and launch one fused kernel 1 + reps times (no solve)."""
+    lib = tea.cuda_library(2)
+    ch = setup_chunk(lib, workload_spec())
+    ms = ctypes.c_double(0.0)
+    lib.tea_kernel_timing_(ch.cid, ctypes.byref(ctypes.c_int(ALL_KERNEL_IDS[args.kernel])),
+                           ctypes.byref(ctypes.c_int(args.reps)), ctypes.byref(ms))
+    words = {"ppcg_inner": 8, "cg_sweep_a": 8, "cheby_iterate": 7, "jacobi": 5, "cg_sweep_b": 3}[args.kernel]
+    gbs = words * 8 * CELLS * CELLS / (ms.value / 1e3) / 1e9 if ms.value > 0 else None
+    print(json.dumps({"kernel": args.kernel, "ms_per_launch": ms.value, "algorithmic_gbs": gbs}))
+    lib.ext_finalise_()
+
+
 # ----------------------------------------------------------------------------- main
 
 def main():
@@ -437,7 +452,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS),
+                    help="only launch one fused kernel --reps times on the 4096^2 workload (for ncu captures)")
+    ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
+    if args.kernel:
+        kernel_only(args)
+        return
     if args.warmup < 1:
         ap.error("--warmup must be >= 1")
     rank, world = dist_init()

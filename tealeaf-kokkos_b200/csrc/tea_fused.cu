@@ -51,7 +51,7 @@ struct Fused {
     double *d_ch_alphas = nullptr, *d_ch_betas = nullptr;
     int cap = 0;  // entries of the coefficient arrays
     FusedArgs base{};
-    int stencil_blocks = 0, point_blocks = 0;
+    int stencil_blocks = 0, point_blocks = 0, pair_blocks = 0;
     Loop loops[LOOP_COUNT];
     bool use_graph = true;
 };
@@ -84,6 +84,7 @@ Fused* ensure_fused(Chunk* c, int max_iters)
         const char* env = std::getenv("TEA_B200_NO_GRAPH");
         F->use_graph = !(env && env[0] == '1');
         TEA_CK(cudaMalloc(&F->d_st, sizeof(SolveState)));
+        TEA_CK(cudaMemset(F->d_st, 0, sizeof(SolveState)));
         TEA_CK(cudaHostAlloc(&F->h_st, sizeof(SolveState), cudaHostAllocDefault));
         for (int k = 0; k < 3; ++k) {
             TEA_CK(cudaMalloc(&F->alt[k], c->field_elems * sizeof(double)));
@@ -137,6 +138,11 @@ Fused* ensure_fused(Chunk* c, int max_iters)
         F->stencil_blocks = std::min(F->stencil_blocks, c->red.max_blocks);
         F->stencil_blocks = std::max(F->stencil_blocks, 1);
         F->point_blocks = launch_blocks(c, c->inner.ntiles);
+        {
+            const long warps = make_seg(g).nseg;  // one 64-cell segment per warp at most
+            const long blocks = (warps + 7) / 8;
+            F->pair_blocks = (int)std::max<long>(1, std::min<long>(blocks, c->red.max_blocks));
+        }
     }
     if (F->cap < max_iters + 2) {
         free_loops(F);  // the graphs hold the old pointers
@@ -166,7 +172,7 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
     switch (kind) {
     case LOOP_CG:
         TEA_STENCIL<OpSweepA><<<F->stencil_blocks, sb, 0, s>>>(a);
-        k_cg_sweep_b<<<F->point_blocks, pb, 0, s>>>(a, c->inner);
+        k_cg_sweep_b<<<F->pair_blocks, 256, 0, s>>>(a);
         break;
     case LOOP_CHEBY:
         TEA_STENCIL<OpCheby><<<F->stencil_blocks, sb, 0, s>>>(a);
@@ -588,6 +594,7 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
         case 1: TEA_STENCIL<OpPPCGInner<false>><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
         case 2: TEA_STENCIL<OpSweepA><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
         case 3: TEA_STENCIL<OpCheby><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
+        case 5: k_cg_sweep_b<<<F->pair_blocks, 256, 0, c->stream>>>(a); break;
         default: TEA_STENCIL<OpJacobi><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
         }
     };

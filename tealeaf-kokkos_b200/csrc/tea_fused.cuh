@@ -296,8 +296,98 @@ __global__ void __launch_bounds__(SBLOCK) k_stream2d(FusedArgs a)
     if (Op::kReduce) grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.control(a, v[0]); });
 }
 
+// 2D register streaming with one row of software prefetch: the loads of row j+2 are in
+// flight while row j is computed.  Per row each lane carries the raw inputs of the
+// operand (Op::Raw) and the interior inputs (Op::In plus Kx, Ky); Kx of the right face
+// comes from the next lane, Ky of the upper face from the next row's bundle.  Inactive
+// lanes past the last column shadow it for the operand and load the boundary face's Kx,
+// so the last active lane sees the reflection and the stored boundary coefficient.
+template <class Op>
+__global__ void __launch_bounds__(SBLOCK) k_pipe2d(FusedArgs a)
+{
+    using Raw = typename Op::Raw;
+    using In = typename Op::In;
+    struct Bundle {
+        In in;
+        double kx, ky, kxe;
+    };
+    Op op;
+    if (op.skip(a)) return;
+    op.begin(a);
+    const Geom& g = a.g;
+    const double* __restrict__ KX = a.kx;
+    const double* __restrict__ KY = a.ky;
+    DDVec<1> acc;
+    acc.zero();
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int xlast = g.X - HALO_PAD - 1;
+    const int ylast = g.Y - HALO_PAD - 1;
+    for (long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+        const int tx = (int)(t % a.tiles_x), ty = (int)(t / a.tiles_x);
+        const int wx = HALO_PAD + tx * SBLOCK + warp * 32;
+        if (wx > xlast) continue;  // the whole warp is past the last column
+        const int kk = wx + lane;
+        const bool active = kk <= xlast;
+        const int kc = min(kk, xlast);          // operand column (shadows the last one)
+        const int kq = min(kk, xlast + 1);      // coefficient column
+        const bool edge = lane == 0 || lane == 31;
+        const int ke = lane == 0 ? refl(kc - 1, g.X) : refl(min(kc + 1, xlast + 1), g.X);
+        const int j0 = HALO_PAD + ty * SY;
+        const int j1 = min(j0 + SY, ylast + 1);
+        auto bundle = [&](int jj) {
+            Bundle b;
+            const long i = fidx(g, kq, jj, 0);
+            b.in = op.load_in(a, fidx(g, kc, jj, 0));
+            b.kx = KX[i];
+            b.ky = KY[fidx(g, kc, jj, 0)];
+            b.kxe = lane == 31 ? KX[fidx(g, min(kk + 1, xlast + 1), jj, 0)] : 0.0;
+            return b;
+        };
+        Raw rc = op.load_raw(a, fidx(g, kc, j0, 0));
+        Raw rp = op.load_raw(a, fidx(g, kc, refl(j0 + 1, g.Y), 0));
+        double sm = op.stage_raw(op.load_raw(a, fidx(g, kc, refl(j0 - 1, g.Y), 0)));
+        double sc = op.stage_raw(rc);
+        Bundle bc = bundle(j0);
+        Bundle bn = bundle(j0 + 1);
+        Raw rec;
+        if (edge) rec = op.load_raw(a, fidx(g, ke, j0, 0));
+        for (int jj = j0; jj < j1; ++jj) {
+            // Prefetch row jj+2 (operand, interior bundle) and the edge operand of row jj+1.
+            const Raw rpp = op.load_raw(a, fidx(g, kc, refl(min(jj + 2, ylast + 2), g.Y), 0));
+            const Bundle bnn = bundle(min(jj + 2, ylast + 1));
+            Raw ren;
+            if (edge) ren = op.load_raw(a, fidx(g, ke, min(jj + 1, ylast), 0));
+            const double sp = op.stage_raw(rp);
+            const double e = edge ? op.stage_raw(rec) : 0.0;
+            const double up = __shfl_up_sync(0xffffffffu, sc, 1);
+            const double dn = __shfl_down_sync(0xffffffffu, sc, 1);
+            const double kxr = __shfl_down_sync(0xffffffffu, bc.kx, 1);
+            if (active) {
+                Nb nb;
+                nb.c = sc;
+                nb.xm = lane == 0 ? e : up;
+                nb.xp = lane == 31 ? e : dn;
+                nb.ym = sm;
+                nb.yp = sp;
+                nb.zm = nb.zp = 0.0;
+                const double kx1 = lane == 31 ? bc.kxe : kxr;
+                op.interior2(a, fidx(g, kk, jj, 0), nb, rc, bc.in, bc.kx, kx1, bc.ky, bn.ky, acc.v[0]);
+            }
+            sm = sc;
+            sc = sp;
+            rc = rp;
+            rp = rpp;
+            bc = bn;
+            bn = bnn;
+            if (edge) rec = ren;
+        }
+    }
+    if (Op::kReduce) grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.control(a, v[0]); });
+}
+
 #if TEA_DIM == 2
-#define TEA_STENCIL k_stream2d
+#define TEA_STENCIL k_pipe2d
 #define TEA_STENCIL_BLOCK dim3(SBLOCK)
 #else
 #define TEA_STENCIL k_stencil3d
@@ -342,6 +432,37 @@ struct OpSweepA {
         a.w[i] = w;
         dd_add(acc, w * nb.c);
     }
+    // Pipelined 2D interface (k_pipe2d): raw loads, staging, interior from registers.
+    struct Raw {
+        double p, q;
+    };
+    struct In {
+        double u;
+    };
+    __device__ Raw load_raw(const FusedArgs& a, long i) const
+    {
+        Raw r;
+        r.p = pcur[i];
+        r.q = pend_p ? (precond ? a.z[i] : a.r[i]) : 0.0;
+        return r;
+    }
+    __device__ double stage_raw(const Raw& r) const { return pend_p ? beta * r.p + r.q : r.p; }
+    __device__ In load_in(const FusedArgs& a, long i) const
+    {
+        In in;
+        in.u = pend_u ? a.u[0][i] : 0.0;
+        return in;
+    }
+    __device__ void interior2(const FusedArgs& a, long i, const Nb& nb, const Raw& rc, const In& in, double kx0,
+                              double kx1, double ky0, double ky1, DD& acc) const
+    {
+        if (pend_u) a.u[0][i] = in.u + alpha * rc.p;
+        pnew[i] = nb.c;
+        const double w = (1.0 + (kx1 + kx0) + (ky1 + ky0)) * nb.c - (kx1 * nb.xp + kx0 * nb.xm)
+            - (ky1 * nb.yp + ky0 * nb.ym);
+        a.w[i] = w;
+        dd_add(acc, w * nb.c);
+    }
     __device__ void control(const FusedArgs& a, double pw)
     {
         if (a.timing) return;
@@ -358,29 +479,85 @@ struct OpSweepA {
 
 // ------------------------------------------------------------------ CG sweep B
 
+// Pointwise sweeps walk the inner domain in row segments of 64 cells: each warp takes a
+// segment, each lane two adjacent cells with 16-byte loads and stores (the first inner
+// cell of every row is 256-byte aligned, so kk = 2 + 2*lane is 16-byte aligned).
+struct Seg {
+    long nseg;   // segments in the inner domain
+    int per_row;
+};
+
+__host__ __device__ inline Seg make_seg(const Geom& g)
+{
+    Seg s;
+    s.per_row = (g.nx + 63) / 64;
+    s.nseg = (long)s.per_row * g.ny * g.nz;
+    return s;
+}
+
+template <class F>
+__device__ __forceinline__ void walk_pairs(const Geom& g, F&& f)
+{
+    const Seg sg = make_seg(g);
+    const int lane = threadIdx.x & 31;
+    const long warp0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    const int xlast = g.X - HALO_PAD - 1;
+    for (long sgi = warp0; sgi < sg.nseg; sgi += nwarps) {
+        const long row = sgi / sg.per_row;
+        const int xs = (int)(sgi - row * sg.per_row);
+        const int jj = HALO_PAD + (int)(row % g.ny);
+        const int ii = DIM == 3 ? HALO_PAD + (int)(row / g.ny) : 0;
+        const int kk = HALO_PAD + xs * 64 + 2 * lane;
+        if (kk <= xlast) f(fidx(g, kk, jj, ii), kk < xlast);
+    }
+}
+
+__device__ __forceinline__ double2 ld2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ void st2(double* p, double a, double b) { *reinterpret_cast<double2*>(p) = make_double2(a, b); }
+
 // CGCalcUr without the u update (deferred to the next sweep A): r -= alpha w, z = Mi r,
 // rrn = sum r.r or r.z; then beta = rrn/rro and the end-of-iteration test.
-__global__ void __launch_bounds__(BLOCK) k_cg_sweep_b(FusedArgs a, Box inner)
+__global__ void __launch_bounds__(256) k_cg_sweep_b(FusedArgs a)
 {
     const SolveState& s = *a.st;
     const double alpha = s.alpha;
     const int precond = s.precond;
-    const Geom& g = a.g;
+    double* __restrict__ R = a.r;
+    const double* __restrict__ W = a.w;
+    const double* __restrict__ MI = a.mi;
+    double* __restrict__ Z = a.z;
     DDVec<1> acc;
     acc.zero();
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        const double r = a.r[i] - alpha * a.w[i];
-        a.r[i] = r;
-        if (precond) {
-            const double z = a.mi[i] * r;
-            a.z[i] = z;
-            dd_add(acc.v[0], r * z);
+    walk_pairs(a.g, [&](long i, bool two) {
+        if (two) {
+            const double2 r2 = ld2(R + i), w2 = ld2(W + i);
+            const double r0 = r2.x - alpha * w2.x, r1 = r2.y - alpha * w2.y;
+            st2(R + i, r0, r1);
+            if (precond) {
+                const double2 m2 = ld2(MI + i);
+                const double z0 = m2.x * r0, z1 = m2.y * r1;
+                st2(Z + i, z0, z1);
+                dd_add(acc.v[0], r0 * z0);
+                dd_add(acc.v[0], r1 * z1);
+            } else {
+                dd_add(acc.v[0], r0 * r0);
+                dd_add(acc.v[0], r1 * r1);
+            }
         } else {
-            dd_add(acc.v[0], r * r);
+            const double r0 = R[i] - alpha * W[i];
+            R[i] = r0;
+            if (precond) {
+                const double z0 = MI[i] * r0;
+                Z[i] = z0;
+                dd_add(acc.v[0], r0 * z0);
+            } else {
+                dd_add(acc.v[0], r0 * r0);
+            }
         }
     });
     grid_reduce_then<1>(acc, a.red, [&](const double* v) {
+        if (a.timing) return;
         SolveState& st = *a.st;
         st.rrn = v[0];
         st.beta = st.rrn / st.rro;
@@ -455,6 +632,38 @@ struct OpPPCGInner {
         sdn[i] = al * nb.c + be * (precond ? a.mi[i] * r : r);
         if (LAST) dd_add(acc, r * r);
     }
+    struct Raw {
+        double sd;
+    };
+    struct In {
+        double r, u, mi;
+    };
+    __device__ Raw load_raw(const FusedArgs&, long i) const
+    {
+        Raw r;
+        r.sd = sdc[i];
+        return r;
+    }
+    __device__ double stage_raw(const Raw& r) const { return r.sd; }
+    __device__ In load_in(const FusedArgs& a, long i) const
+    {
+        In in;
+        in.r = a.r[i];
+        in.u = a.u[0][i];
+        in.mi = precond ? a.mi[i] : 0.0;
+        return in;
+    }
+    __device__ void interior2(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
+                              double kx1, double ky0, double ky1, DD& acc) const
+    {
+        const double s = (1.0 + (kx1 + kx0) + (ky1 + ky0)) * nb.c - (kx1 * nb.xp + kx0 * nb.xm)
+            - (ky1 * nb.yp + ky0 * nb.ym);
+        const double r = in.r - s;
+        a.r[i] = r;
+        a.u[0][i] = in.u + nb.c;
+        sdn[i] = al * nb.c + be * (precond ? in.mi * r : r);
+        if (LAST) dd_add(acc, r * r);
+    }
     __device__ void control(const FusedArgs& a, double rrn)
     {
         if (a.timing) return;
@@ -506,6 +715,38 @@ struct OpCheby {
         unew[i] = nb.c + p;
         if (check) dd_add(acc, r * r);
     }
+    struct Raw {
+        double u;
+    };
+    struct In {
+        double u0, p, mi;
+    };
+    __device__ Raw load_raw(const FusedArgs&, long i) const
+    {
+        Raw r;
+        r.u = ucur[i];
+        return r;
+    }
+    __device__ double stage_raw(const Raw& r) const { return r.u; }
+    __device__ In load_in(const FusedArgs& a, long i) const
+    {
+        In in;
+        in.u0 = a.u0[i];
+        in.p = a.p[0][i];
+        in.mi = precond ? a.mi[i] : 0.0;
+        return in;
+    }
+    __device__ void interior2(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
+                              double kx1, double ky0, double ky1, DD& acc) const
+    {
+        const double w = (1.0 + (kx1 + kx0) + (ky1 + ky0)) * nb.c - (kx1 * nb.xp + kx0 * nb.xm)
+            - (ky1 * nb.yp + ky0 * nb.ym);
+        const double r = in.u0 - w;
+        const double p = al * in.p + be * (precond ? in.mi * r : r);
+        a.p[0][i] = p;
+        unew[i] = nb.c + p;
+        if (check) dd_add(acc, r * r);
+    }
     __device__ void control(const FusedArgs& a, double rr)
     {
         if (a.timing) return;
@@ -551,6 +792,33 @@ struct OpJacobi {
         unew[i] = un;
         dd_add(acc, fabs(un - nb.c));
     }
+    struct Raw {
+        double u;
+    };
+    struct In {
+        double u0;
+    };
+    __device__ Raw load_raw(const FusedArgs&, long i) const
+    {
+        Raw r;
+        r.u = ucur[i];
+        return r;
+    }
+    __device__ double stage_raw(const Raw& r) const { return r.u; }
+    __device__ In load_in(const FusedArgs& a, long i) const
+    {
+        In in;
+        in.u0 = a.u0[i];
+        return in;
+    }
+    __device__ void interior2(const FusedArgs&, long i, const Nb& nb, const Raw&, const In& in, double kx0,
+                              double kx1, double ky0, double ky1, DD& acc) const
+    {
+        const double un = (in.u0 + (kx1 * nb.xp + kx0 * nb.xm) + (ky1 * nb.yp + ky0 * nb.ym))
+            / (1.0 + (kx0 + kx1) + (ky0 + ky1));
+        unew[i] = un;
+        dd_add(acc, fabs(un - nb.c));
+    }
     __device__ void control(const FusedArgs& a, double err)
     {
         if (a.timing) return;
@@ -580,8 +848,37 @@ struct OpJacobiResidual {
         a.r[i] = r;
         dd_add(acc, r * r);
     }
+    struct Raw {
+        double u;
+    };
+    struct In {
+        double u0;
+    };
+    __device__ Raw load_raw(const FusedArgs&, long i) const
+    {
+        Raw r;
+        r.u = ucur[i];
+        return r;
+    }
+    __device__ double stage_raw(const Raw& r) const { return r.u; }
+    __device__ In load_in(const FusedArgs& a, long i) const
+    {
+        In in;
+        in.u0 = a.u0[i];
+        return in;
+    }
+    __device__ void interior2(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
+                              double kx1, double ky0, double ky1, DD& acc) const
+    {
+        const double s = (1.0 + (kx1 + kx0) + (ky1 + ky0)) * nb.c - (kx1 * nb.xp + kx0 * nb.xm)
+            - (ky1 * nb.yp + ky0 * nb.ym);
+        const double r = in.u0 - s;
+        a.r[i] = r;
+        dd_add(acc, r * r);
+    }
     __device__ void control(const FusedArgs& a, double rr)
     {
+        if (a.timing) return;
         SolveState& s = *a.st;
         s.error = rr;
         s.resid_pending = 0;
