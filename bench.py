@@ -232,7 +232,7 @@ def setup_chunk(lib, spec):
     return ch
 
 
-def solve_params(spec):
+def solve_params(spec, precision=0):
     p = tea.SolveParams()
     p.solver = tea.SOLVERS[spec.solver]
     p.coefficient = 2 if spec.inverse_density else 1
@@ -246,10 +246,11 @@ def solve_params(spec):
     p.eps = spec.eps
     p.ch_cg_epslim = float(ctypes.c_float(1e-5).value)
     p.eps_rel = spec.eps_rel
+    p.precision = precision
     return p
 
 
-def gpu_arm(args, world):
+def gpu_arm(args, world, precision=0, kernels=True):
     import torch
 
     lib = tea.cuda_library(2)
@@ -258,7 +259,7 @@ def gpu_arm(args, world):
     stream_ptr = ctypes.c_void_p()
     lib.tea_chunk_stream_(ch.cid, ctypes.byref(stream_ptr))
     stream = torch.cuda.ExternalStream(stream_ptr.value)
-    params = solve_params(spec)
+    params = solve_params(spec, precision)
     results = []
     for _ in range(args.warmup):
         results.append(ch.solve(params))
@@ -286,8 +287,13 @@ def gpu_arm(args, world):
     # Kernel-level: the fused kernels of the timestep, launched back to back on the same
     # stream between CUDA events, on the chunk's live fields (steady-state operands).
     cells = CELLS * CELLS
+    summaries = []
+    for _ in range(1):
+        v = [ctypes.c_double() for _ in range(4)]
+        lib.ext_field_summary_kernel_(ch.cid, *[ctypes.byref(x) for x in v])
+        summaries = [x.value for x in v]
     kernel_ms = {}
-    for name, kid in KERNEL_IDS.items():
+    for name, kid in (KERNEL_IDS.items() if kernels else ()):
         kms = ctypes.c_double(0.0)
         lib.tea_kernel_timing_(ch.cid, ctypes.byref(ctypes.c_int(kid)), ctypes.byref(ctypes.c_int(30)),
                                ctypes.byref(kms))
@@ -299,10 +305,13 @@ def gpu_arm(args, world):
     iters = [r["iterations"] for r in results]
     mean_cg = sum(cg) / len(cg)
     mean_ch = sum(cheby) / len(cheby)
-    share = {"cg_sweep_a": mean_cg * kernel_ms["cg_sweep_a"], "cg_sweep_b": mean_cg * kernel_ms["cg_sweep_b"],
-             "cheby_iterate": mean_ch * kernel_ms["cheby_iterate"]}
-    dominant = max(share, key=share.get)
-    alg_bytes = WORDS[dominant] * 8 * cells
+    if kernels:
+        share = {"cg_sweep_a": mean_cg * kernel_ms["cg_sweep_a"], "cg_sweep_b": mean_cg * kernel_ms["cg_sweep_b"],
+                 "cheby_iterate": mean_ch * kernel_ms["cheby_iterate"]}
+        dominant = max(share, key=share.get)
+        alg_bytes = WORDS[dominant] * 8 * cells
+    else:
+        dominant, alg_bytes = None, None
     step_words = (WORDS["cg_sweep_a"] + WORDS["cg_sweep_b"]) * mean_cg + WORDS["cheby_iterate"] * mean_ch
     return {
         "sec_per_step": sec_per_step, "ms_total": ms_max, "clocks": clock_info, "iterations": iters,
@@ -310,6 +319,8 @@ def gpu_arm(args, world):
         "alg_bytes": alg_bytes, "step_alg_gbs": step_words * 8 * cells / sec_per_step / 1e9,
         "cells_iters_per_s": cells * (sum(iters) / len(iters)) / sec_per_step,
         "warmup_iterations": [r["iterations"] for r in warm], "bad_status": [r["status"] for r in bad],
+        "corrections": [r["corrections"] for r in results], "summary": summaries,
+        "exact_errors": [r["exact_error"] for r in results],
     }
 
 
@@ -452,6 +463,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-refined", action="store_true")
     ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS),
                     help="only launch one fused kernel --reps times on the 4096^2 workload (for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
@@ -467,6 +479,7 @@ def main():
         return
 
     g = gpu_arm(args, world)
+    refined = None if args.no_refined else gpu_arm(args, world, precision=1, kernels=False)
     e2e = None if args.no_e2e else e2e_arm(args)
     if rank != 0:
         dist_done(world)
@@ -516,6 +529,15 @@ def main():
         line["config"]["e2e_iterations_match"] = timed == g["iterations"]
         line["e2e"] = {"value": e2e["value"], "unit": "s", "h2d_bytes_per_step": e2e["h2d_bytes_per_step"],
                        "d2h_bytes_per_step": e2e["d2h_bytes_per_step"]}
+    if refined:
+        # The precision form on the same workload: FP32 inner CG inside FP64 defect
+        # correction to the same relative residual, and its field-summary difference to
+        # the FP64 solve after the same timesteps.
+        diff = max(tea.rel_diff(a, b) for a, b in zip(refined["summary"], g["summary"]))
+        line["fp32_refined"] = {"value": refined["sec_per_step"], "unit": "s",
+                                "speedup_vs_fp64": g["sec_per_step"] / refined["sec_per_step"],
+                                "inner_iterations": refined["iterations"], "corrections": refined["corrections"],
+                                "field_summary_max_rel_diff_vs_fp64": diff, "clocks": refined["clocks"]}
     if g["bad_status"]:
         line["status_warnings"] = g["bad_status"]
     print(json.dumps(line))

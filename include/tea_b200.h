@@ -83,7 +83,8 @@ enum {
 };
 
 /* Inputs of one implicit solve: the tea.in keywords that tea_leaf() reads
- * (tealeaf_2d/tea_solve.f90:36-605, defaults at tealeaf_2d/read_input.f90:49-80). */
+ * (tealeaf_2d/tea_solve.f90:36-605, defaults at tealeaf_2d/read_input.f90:49-80), plus the
+ * precision form. */
 typedef struct {
     int solver;             /* TEA_SOLVER_* */
     int coefficient;        /* 1 = CONDUCTIVITY (w = rho), 2 = RECIP_CONDUCTIVITY (w = 1/rho) */
@@ -97,22 +98,43 @@ typedef struct {
     double eps;             /* absolute threshold on the solver's error (sum r^2 or sum r.z) */
     double ch_cg_epslim;    /* tl_ch_cg_epslim */
     double eps_rel;         /* > 0: replace eps by eps_rel^2 * sum(u0^2) each solve */
-    int reserved[8];        /* must be zero */
+    int precision;          /* TEA_PRECISION_FP64 (the reference's arithmetic) or
+                               TEA_PRECISION_FP32_REFINED */
+    int inner_max_iters;    /* FP32_REFINED: inner iterations per correction, 0 = no limit */
+    double inner_tol;       /* FP32_REFINED: relative drop of the inner residual per
+                               correction, 0 = 1e-4 */
+    int reserved[4];        /* must be zero */
 } tea_solve_params;
+
+/* Precision forms of ext_tea_leaf_solve_. */
+enum {
+    /* FP64 throughout, bit-identical to the per-call ext_* sequence. */
+    TEA_PRECISION_FP64 = 0,
+    /* Defect correction: the outer residual r = b - A u, the update u += d, the sums
+     * that decide convergence (tested on the true FP64 residual) and everything after
+     * the solve stay FP64; each correction A d = r is solved by CG in FP32 storage and
+     * arithmetic, with its dot products accumulated in double-double.  The solver
+     * setting selects nothing here (the inner solver is CG); max_iters bounds the total
+     * of inner iterations. */
+    TEA_PRECISION_FP32_REFINED = 1
+};
 
 /* Outputs of one implicit solve. */
 typedef struct {
-    int iterations;         /* the "Iteration count" that tea_leaf() prints (n-1) */
+    int iterations;         /* the "Iteration count" that tea_leaf() prints (n-1); for
+                               FP32_REFINED the inner iterations in total */
     int status;             /* TEA_* status of this solve */
     int cg_steps;           /* CG iterations before a Chebyshev/PPCG switch */
     int cheby_steps;        /* Chebyshev iterations or PPCG outer iterations after it */
     int switch_step;        /* n at the switch, 0 if none */
     int est_itc;            /* Chebyshev iteration estimate, 0 if none */
-    double error;           /* final recursive error */
+    double error;           /* final error (FP32_REFINED: true residual sum r^2) */
     double exact_error;     /* sum (u0 - A u)^2 when check_result is set, else 0 */
     double eps_used;        /* the absolute threshold that was applied */
     double eigmin, eigmax;  /* scaled eigenvalue bounds at the switch (0 if none) */
-    double reserved[8];
+    int corrections;        /* FP32_REFINED: outer corrections */
+    int reserved_i;
+    double reserved[7];
 } tea_solve_result;
 
 /* Whole implicit solve of one timestep on the device: the control flow of

@@ -33,6 +33,7 @@ FIELD_IDS = {
     "w": 9, "z": 10, "mi": 11, "kx": 12, "ky": 13, "kz": 14, "volume": 15,
 }
 SOLVERS = {"jacobi": 1, "cg": 2, "chebyshev": 3, "ppcg": 4}
+PRECISION_FP64, PRECISION_FP32_REFINED = 0, 1
 SOLVER_KEYWORDS = {1: "tl_use_jacobi", 2: "tl_use_cg", 3: "tl_use_chebyshev", 4: "tl_use_ppcg"}
 
 
@@ -79,7 +80,7 @@ class RunOptions(ctypes.Structure):
         ("dim", ctypes.c_int), ("backend", ctypes.c_char_p), ("use_fused_solve", ctypes.c_int),
         ("summary_every_step", ctypes.c_int), ("end_step_override", ctypes.c_int), ("quiet", ctypes.c_int),
         ("out_path", ctypes.c_char_p), ("eps_override", ctypes.c_double), ("eps_rel_override", ctypes.c_double),
-        ("keep_chunk", ctypes.c_int), ("reserved", ctypes.c_int * 7),
+        ("keep_chunk", ctypes.c_int), ("precision", ctypes.c_int), ("reserved", ctypes.c_int * 6),
     ]
 
 
@@ -92,6 +93,7 @@ class StepRecord(ctypes.Structure):
         ("ie", ctypes.c_double), ("temp", ctypes.c_double), ("has_summary", ctypes.c_int),
         ("switch_step", ctypes.c_int), ("est_itc", ctypes.c_int), ("pad", ctypes.c_int),
         ("wall_end", ctypes.c_double), ("h2d_bytes", ctypes.c_longlong), ("d2h_bytes", ctypes.c_longlong),
+        ("corrections", ctypes.c_int), ("pad2", ctypes.c_int),
     ]
 
 
@@ -120,7 +122,7 @@ def driver() -> ctypes.CDLL:
 
 def run_deck(deck_text: str, dim: int, backend=None, *, fused: bool = False, summary_every_step: bool = False,
              end_step: int = 0, quiet: bool = True, out_path=None, eps: float = 0.0, eps_rel: float = 0.0,
-             keep_chunk: bool = False, max_records: int = 100000):
+             keep_chunk: bool = False, precision: int = 0, max_records: int = 100000):
     """Run a tea.in deck through the C++ driver against ``backend`` (default: the CUDA
     library for ``dim``).  Returns ``(summary, records)`` as dicts."""
     backend = str(backend) if backend is not None else str(lib_path(dim))
@@ -137,6 +139,7 @@ def run_deck(deck_text: str, dim: int, backend=None, *, fused: bool = False, sum
     opt.eps_override = float(eps)
     opt.eps_rel_override = float(eps_rel)
     opt.keep_chunk = 1 if keep_chunk else 0
+    opt.precision = int(precision)
     summary = RunSummary()
     records = (StepRecord * max_records)()
     lib = driver()
@@ -155,7 +158,8 @@ class SolveParams(ctypes.Structure):
         ("max_iters", ctypes.c_int), ("ch_cg_presteps", ctypes.c_int), ("ch_cg_errswitch", ctypes.c_int),
         ("ppcg_inner_steps", ctypes.c_int), ("check_result", ctypes.c_int), ("dt", ctypes.c_double),
         ("eps", ctypes.c_double), ("ch_cg_epslim", ctypes.c_double), ("eps_rel", ctypes.c_double),
-        ("reserved", ctypes.c_int * 8),
+        ("precision", ctypes.c_int), ("inner_max_iters", ctypes.c_int), ("inner_tol", ctypes.c_double),
+        ("reserved", ctypes.c_int * 4),
     ]
 
 
@@ -164,7 +168,8 @@ class SolveResult(ctypes.Structure):
         ("iterations", ctypes.c_int), ("status", ctypes.c_int), ("cg_steps", ctypes.c_int),
         ("cheby_steps", ctypes.c_int), ("switch_step", ctypes.c_int), ("est_itc", ctypes.c_int),
         ("error", ctypes.c_double), ("exact_error", ctypes.c_double), ("eps_used", ctypes.c_double),
-        ("eigmin", ctypes.c_double), ("eigmax", ctypes.c_double), ("reserved", ctypes.c_double * 8),
+        ("eigmin", ctypes.c_double), ("eigmax", ctypes.c_double), ("corrections", ctypes.c_int),
+        ("reserved_i", ctypes.c_int), ("reserved", ctypes.c_double * 7),
     ]
 
 
@@ -249,6 +254,13 @@ class ExtChunk:
     def reduce(self, name, *args):
         out = ctypes.c_double(0.0)
         getattr(self.lib, name)(self.cid, *args, ctypes.byref(out))
+        self.status()
+        return out.value
+
+    def norm2(self, use_r):
+        """ext_calculate_2norm_: the norm comes back through the second argument, ahead of the flag."""
+        out = ctypes.c_double(0.0)
+        self.lib.ext_calculate_2norm_(self.cid, ctypes.byref(out), ctypes.byref(ctypes.c_int(1 if use_r else 0)))
         self.status()
         return out.value
 
@@ -367,7 +379,7 @@ def build(verbose: bool = False, force: bool = False) -> None:
 
 
 __all__ = [
-    "FIELD_IDS", "SOLVERS", "lib_path", "driver_path", "tea_leaf_exe", "load_library", "cuda_library",
+    "FIELD_IDS", "SOLVERS", "PRECISION_FP64", "PRECISION_FP32_REFINED", "lib_path", "driver_path", "tea_leaf_exe", "load_library", "cuda_library",
     "run_deck", "ExtChunk", "SolveParams", "SolveResult", "DeckSpec", "seeded_deck", "rel_diff", "build",
 ]
 

@@ -35,7 +35,7 @@ void update_halo(Chunk* c, const int* neighbours, const int* fields, int depth);
 
 namespace {
 
-enum { LOOP_CG = 0, LOOP_CHEBY = 1, LOOP_PPCG = 2, LOOP_JACOBI = 3, LOOP_COUNT = 4 };
+enum { LOOP_CG = 0, LOOP_CHEBY = 1, LOOP_PPCG = 2, LOOP_JACOBI = 3, LOOP_CG32 = 4, LOOP_COUNT = 5 };
 
 struct Loop {
     cudaGraph_t graph = nullptr;
@@ -47,11 +47,13 @@ struct Fused {
     SolveState* d_st = nullptr;
     SolveState* h_st = nullptr;  // pinned
     double* alt[3] = {nullptr, nullptr, nullptr};  // allocations of u, p, sd second buffers
+    float* alloc32[8] = {};  // FP32 arrays of the defect-correction form (allocated on first use)
     double *d_cg_alphas = nullptr, *d_cg_betas = nullptr;
     double *d_ch_alphas = nullptr, *d_ch_betas = nullptr;
     int cap = 0;  // entries of the coefficient arrays
     FusedArgs base{};
     int stencil_blocks = 0, point_blocks = 0, pair_blocks = 0;
+    int ring_blocks = 0;  // grid of k_ring2d; 0 selects the register-pipelined kernels
     Loop loops[LOOP_COUNT];
     bool use_graph = true;
 };
@@ -73,6 +75,33 @@ int occupancy(K kernel, int threads)
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess || n < 1) n = 1;
     return n;
+}
+
+#if TEA_DIM == 2
+// Opt the ring kernel of Op into its dynamic shared memory; blocks per SM it then reaches.
+template <class Op>
+int ring_occupancy()
+{
+    const int bytes = (int)ring_smem_bytes<Op>();
+    TEA_CK(cudaFuncSetAttribute(k_ring2d<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ring2d<Op>, RWARPS * 32, bytes) != cudaSuccess || n < 1)
+        n = 1;
+    return n;
+}
+#endif
+
+// Launch the streaming stencil kernel of Op over the inner domain.
+template <class Op>
+void stencil(const Fused* F, const FusedArgs& a, cudaStream_t s)
+{
+#if TEA_DIM == 2
+    if (F->ring_blocks > 0) {
+        k_ring2d<Op><<<F->ring_blocks, RWARPS * 32, ring_smem_bytes<Op>(), s>>>(a);
+        return;
+    }
+#endif
+    TEA_STENCIL<Op><<<F->stencil_blocks, TEA_STENCIL_BLOCK, 0, s>>>(a);
 }
 
 Fused* ensure_fused(Chunk* c, int max_iters)
@@ -120,8 +149,8 @@ Fused* ensure_fused(Chunk* c, int max_iters)
             a.zseg = 1;
             a.ntiles = (long)a.tiles_x * a.tiles_y;
         } else {
-            a.tiles_x = (g.nx + FT_X - 1) / FT_X;
-            a.tiles_y = (g.ny + FT_Y3 - 1) / FT_Y3;
+            a.tiles_x = (g.nx + 31) / 32;
+            a.tiles_y = (g.ny + TY3 - 1) / TY3;
             const long txy = (long)a.tiles_x * a.tiles_y;
             int zseg = g.nz;
             const long want = 8L * sms * 4;
@@ -134,9 +163,30 @@ Fused* ensure_fused(Chunk* c, int max_iters)
         occ = std::min(occ, occupancy(TEA_STENCIL<OpCheby>, nthr));
         occ = std::min(occ, occupancy(TEA_STENCIL<OpPPCGInner<true>>, nthr));
         occ = std::min(occ, occupancy(TEA_STENCIL<OpJacobi>, nthr));
+        occ = std::min(occ, occupancy(TEA_STENCIL<OpSweepA32>, nthr));
+        occ = std::min(occ, occupancy(TEA_STENCIL<OpOuterResid>, nthr));
         F->stencil_blocks = (int)std::min<long>(a.ntiles, (long)sms * occ);
         F->stencil_blocks = std::min(F->stencil_blocks, c->red.max_blocks);
         F->stencil_blocks = std::max(F->stencil_blocks, 1);
+#if TEA_DIM == 2
+        {
+            const char* kind = getenv("TEA_B200_STENCIL");
+            if (kind && strcmp(kind, "ring") == 0) {
+                int rocc = ring_occupancy<OpSweepA>();
+                rocc = std::min(rocc, ring_occupancy<OpCheby>());
+                rocc = std::min(rocc, ring_occupancy<OpPPCGInner<true>>());
+                rocc = std::min(rocc, ring_occupancy<OpPPCGInner<false>>());
+                rocc = std::min(rocc, ring_occupancy<OpJacobi>());
+                rocc = std::min(rocc, ring_occupancy<OpJacobiResidual>());
+                rocc = std::min(rocc, ring_occupancy<OpSweepA32>());
+                rocc = std::min(rocc, ring_occupancy<OpOuterResid>());
+                const long segs = (long)((g.nx + 63) / 64) * ((g.ny + RSY - 1) / RSY);
+                long blocks = std::min<long>((segs + RWARPS - 1) / RWARPS, (long)sms * rocc);
+                blocks = std::min<long>(blocks, c->red.max_blocks);
+                F->ring_blocks = (int)std::max<long>(blocks, 1);
+            }
+        }
+#endif
         F->point_blocks = launch_blocks(c, c->inner.ntiles);
         {
             const long warps = make_seg(g).nseg;  // one 64-cell segment per warp at most
@@ -163,34 +213,62 @@ Fused* ensure_fused(Chunk* c, int max_iters)
     return F;
 }
 
+// The FP32 arrays of the defect-correction form, allocated on first use (same pitched
+// layout as the FP64 fields, float elements).
+bool ensure_fp32(Chunk* c, Fused* F)
+{
+    if (F->alloc32[0]) return true;
+    const size_t bytes = c->field_elems * sizeof(float);
+    for (int k = 0; k < 8; ++k) {
+        if (k == 2 && DIM != 3) continue;
+        TEA_CK(cudaMalloc(&F->alloc32[k], bytes));
+        if (!F->alloc32[k]) return false;
+        TEA_CK(cudaMemset(F->alloc32[k], 0, bytes));
+    }
+    free_loops(F);  // graphs captured before hold null FP32 pointers
+    FusedArgs& a = F->base;
+    a.kx32 = F->alloc32[0] + kLeadPad;
+    a.ky32 = F->alloc32[1] + kLeadPad;
+    a.kz32 = DIM == 3 ? F->alloc32[2] + kLeadPad : nullptr;
+    a.r32 = F->alloc32[3] + kLeadPad;
+    a.w32 = F->alloc32[4] + kLeadPad;
+    a.d32 = F->alloc32[5] + kLeadPad;
+    a.p32[0] = F->alloc32[6] + kLeadPad;
+    a.p32[1] = F->alloc32[7] + kLeadPad;
+    return true;
+}
+
 // Enqueue one iteration of loop `kind` on the chunk's stream.
 void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs& a)
 {
-    const dim3 sb = TEA_STENCIL_BLOCK;
     const dim3 pb(TILE_X, TILE_Y);
     cudaStream_t s = c->stream;
     switch (kind) {
     case LOOP_CG:
-        TEA_STENCIL<OpSweepA><<<F->stencil_blocks, sb, 0, s>>>(a);
+        stencil<OpSweepA>(F, a, s);
         k_cg_sweep_b<<<F->pair_blocks, 256, 0, s>>>(a);
         break;
     case LOOP_CHEBY:
-        TEA_STENCIL<OpCheby><<<F->stencil_blocks, sb, 0, s>>>(a);
+        stencil<OpCheby>(F, a, s);
         break;
     case LOOP_PPCG: {
-        TEA_STENCIL<OpSweepA><<<F->stencil_blocks, sb, 0, s>>>(a);
+        stencil<OpSweepA>(F, a, s);
         k_ppcg_sweep_b<<<F->point_blocks, pb, 0, s>>>(a, c->inner);
         for (int k = 1; k <= inner_steps; ++k) {
             FusedArgs ak = a;
             ak.step = k;
-            if (k < inner_steps) TEA_STENCIL<OpPPCGInner<false>><<<F->stencil_blocks, sb, 0, s>>>(ak);
-            else TEA_STENCIL<OpPPCGInner<true>><<<F->stencil_blocks, sb, 0, s>>>(ak);
+            if (k < inner_steps) stencil<OpPPCGInner<false>>(F, ak, s);
+            else stencil<OpPPCGInner<true>>(F, ak, s);
         }
         break;
     }
     case LOOP_JACOBI:
-        TEA_STENCIL<OpJacobi><<<F->stencil_blocks, sb, 0, s>>>(a);
-        TEA_STENCIL<OpJacobiResidual><<<F->stencil_blocks, sb, 0, s>>>(a);
+        stencil<OpJacobi>(F, a, s);
+        stencil<OpJacobiResidual>(F, a, s);
+        break;
+    case LOOP_CG32:
+        stencil<OpSweepA32>(F, a, s);
+        k_cg32_sweep_b<<<F->pair_blocks, 256, 0, s>>>(a);
         break;
     }
 }
@@ -355,6 +433,8 @@ void destroy_fused(Chunk* c)
         if (p) cudaFree(p);
     for (double* p : F->alt)
         if (p) cudaFree(p);
+    for (float* p : F->alloc32)
+        if (p) cudaFree(p);
     if (F->d_st) cudaFree(F->d_st);
     if (F->h_st) cudaFreeHost(F->h_st);
     delete F;
@@ -372,7 +452,8 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
     if (!c || !P || !R) return;
     const int solver = P->solver;
     if (solver < TEA_SOLVER_JACOBI || solver > TEA_SOLVER_PPCG || P->max_iters < 1 ||
-        (solver == TEA_SOLVER_PPCG && P->ppcg_inner_steps < 1)) {
+        (solver == TEA_SOLVER_PPCG && P->ppcg_inner_steps < 1) ||
+        (P->precision != TEA_PRECISION_FP64 && P->precision != TEA_PRECISION_FP32_REFINED)) {
         set_status(TEA_ERR_BAD_ARGUMENT, "ext_tea_leaf_solve_: invalid parameters");
         R->status = TEA_ERR_BAD_ARGUMENT;
         return;
@@ -425,7 +506,48 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
     // from the CG set-up, false after the Chebyshev switch until a CG iteration runs.
     bool p_halo_fresh = true;
 
-    if (!cg_like) {
+    int corrections = 0;
+    if (P->precision == TEA_PRECISION_FP32_REFINED) {
+        // Defect correction: FP64 outer residual and update, FP32 inner CG.
+        if (!ensure_fp32(c, F)) {
+            R->status = TEA_ERR_CUDA;
+            return;
+        }
+        FusedArgs a = F->base;
+        k_coef_to_fp32<<<c->grid_blocks, 256, 0, c->stream>>>(a);
+        const double tol = P->inner_tol > 0.0 ? P->inner_tol : 1e-4;
+        int total_inner = 0;
+        s.error = 0.0;
+        for (int guard = 0; guard < P->max_iters + 2; ++guard) {
+            if (status_store().status == TEA_ERR_CUDA) break;
+            push_state(c, F);
+            stencil<OpOuterResid>(F, a, c->stream);
+            pull_state(c, F);
+            if (std::fabs(s.error) < eps || s.nonfinite) {
+                s.exit_reason = EXIT_CONVERGED;
+                break;
+            }
+            if (total_inner >= P->max_iters) {
+                s.exit_reason = EXIT_MAXITER;
+                break;
+            }
+            const int remaining = P->max_iters - total_inner;
+            s.inner_max = P->inner_max_iters > 0 ? std::min(P->inner_max_iters, remaining) : remaining;
+            s.tol2 = tol * tol * s.rro;
+            s.n_inner = 0;
+            s.cont = 1;
+            run_loop(c, F, LOOP_CG32, 0);
+            total_inner += s.n_inner;
+            k_dc_update<<<F->pair_blocks, 256, 0, c->stream>>>(a);
+            s.pending_p = 0;
+            s.pending_u = 0;
+            ++corrections;
+        }
+        s.n = total_inner + 1;
+        s.pending_p = s.pending_u = 0;
+        s.par_p = 0;
+        push_state(c, F);
+    } else if (!cg_like) {
         run_loop(c, F, LOOP_JACOBI, 0);
     } else {
         std::vector<double> ch_alphas, ch_betas;
@@ -565,6 +687,7 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
     R->eps_used = eps;
     R->eigmin = eigmin;
     R->eigmax = eigmax;
+    R->corrections = corrections;
 }
 
 // Measurement hook: `reps` back-to-back launches of one fused kernel on the chunk's
@@ -585,17 +708,16 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
     F->h_st->pending_p = 1;
     F->h_st->pending_u = 1;
     push_state(c, F);
-    const dim3 sb = TEA_STENCIL_BLOCK;
     cudaEvent_t e0, e1;
     TEA_CK(cudaEventCreate(&e0));
     TEA_CK(cudaEventCreate(&e1));
     auto launch = [&]() {
         switch (*kernel) {
-        case 1: TEA_STENCIL<OpPPCGInner<false>><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
-        case 2: TEA_STENCIL<OpSweepA><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
-        case 3: TEA_STENCIL<OpCheby><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
+        case 1: stencil<OpPPCGInner<false>>(F, a, c->stream); break;
+        case 2: stencil<OpSweepA>(F, a, c->stream); break;
+        case 3: stencil<OpCheby>(F, a, c->stream); break;
         case 5: k_cg_sweep_b<<<F->pair_blocks, 256, 0, c->stream>>>(a); break;
-        default: TEA_STENCIL<OpJacobi><<<F->stencil_blocks, sb, 0, c->stream>>>(a); break;
+        default: stencil<OpJacobi>(F, a, c->stream); break;
         }
     };
     launch();  // warm-up

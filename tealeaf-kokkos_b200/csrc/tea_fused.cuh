@@ -6,11 +6,10 @@
 // neighbour outside the inner domain from its reflected interior cell instead of
 // from the halo: same value, same arithmetic, no halo maintenance inside the loop.
 //
-// Stencil kernels stage the stencil operand for a tile plus a one-cell ring in shared
-// memory (computing it on the way in where it is itself an update, e.g. CG's
-// p = beta p + r), then apply the operator from shared memory.  2D tiles are 32 x 32
-// cells for 256 threads; 3D tiles are 32 x 8 cells marching through a z segment with
-// four rotating planes.  Buffers that a sweep both reads at neighbours and rewrites
+// Stencil kernels stream: lanes own columns and march down rows (2D) or planes (3D),
+// keeping the stencil operand of three rows/planes in registers and the loads of the next
+// ones in flight; where the operand is itself an update (CG's p = beta p + r) it is
+// computed as it is loaded.  Buffers that a sweep both reads at neighbours and rewrites
 // (p, u, sd) are double-buffered.
 //
 // Scalar recurrences (alpha = rro/pw, beta = rrn/rro, ...) and the loop test of
@@ -43,6 +42,9 @@ struct SolveState {
     int resid_pending;    // Jacobi: residual check due this iteration
     int solver, precond, max_iters, presteps, errswitch, inner_steps;
     int nonfinite;
+    // FP32 inner solve of the defect-correction form.
+    int n_inner, inner_max;
+    double tol2;
 };
 
 struct FusedArgs {
@@ -61,12 +63,11 @@ struct FusedArgs {
     long ntiles;
     int step;    // PPCG inner step (1-based) of this launch
     int timing;  // measurement launches: the last block leaves the solve state untouched
+    // FP32 arrays of the defect-correction form (same pitched layout, float elements).
+    float *kx32, *ky32, *kz32, *r32, *w32, *d32;
+    float* p32[2];
 };
 
-constexpr int FT_X = 32;
-constexpr int FT_Y2 = 32;   // 2D tile height
-constexpr int FT_Y3 = 8;    // 3D tile height
-constexpr int FBLOCK = 256;
 
 // Reflection of a padded index into the inner domain (depth 1 and 2): HALO_PAD-1-f
 // maps to HALO_PAD+f and N-HALO_PAD+f to N-HALO_PAD-1-f, as UpdateHalo copies them.
@@ -75,9 +76,11 @@ __device__ __forceinline__ int refl(int k, int n)
     return k < HALO_PAD ? 2 * HALO_PAD - 1 - k : (k >= n - HALO_PAD ? 2 * (n - HALO_PAD) - 1 - k : k);
 }
 
-struct Nb {
-    double c, xm, xp, ym, yp, zm, zp;
+template <class T>
+struct NbT {
+    T c, xm, xp, ym, yp, zm, zp;
 };
+using Nb = NbT<double>;
 
 // SMVP with the operand taken from staged neighbours (same expression as smvp()).
 __device__ __forceinline__ double smvp_nb(const Nb& a, const double* __restrict__ kx,
@@ -93,6 +96,36 @@ __device__ __forceinline__ double smvp_nb(const Nb& a, const double* __restrict_
     const double kz0 = kz[i], kz1 = kz[i + page];
     return (1.0 + (kx1 + kx0) + (ky1 + ky0) + (kz1 + kz0)) * a.c - (kx1 * a.xp + kx0 * a.xm)
         - (ky1 * a.yp + ky0 * a.ym) - (kz1 * a.zp + kz0 * a.zm);
+#endif
+}
+
+// The operator and the Jacobi update from staged neighbours and register-held
+// coefficients (kx0 = Kx[i], kx1 = Kx[i+1], ky1 = Ky[i+pitch], kz1 = Kz[i+page]); the
+// same expressions, in the same order, as smvp() and JacobiSolve.
+template <class T>
+__device__ __forceinline__ T smvp_k(const NbT<T>& a, T kx0, T kx1, T ky0, T ky1, T kz0, T kz1)
+{
+    const T one = (T)1;
+#if TEA_DIM == 2
+    (void)kz0;
+    (void)kz1;
+    return (one + (kx1 + kx0) + (ky1 + ky0)) * a.c - (kx1 * a.xp + kx0 * a.xm) - (ky1 * a.yp + ky0 * a.ym);
+#else
+    return (one + (kx1 + kx0) + (ky1 + ky0) + (kz1 + kz0)) * a.c - (kx1 * a.xp + kx0 * a.xm)
+        - (ky1 * a.yp + ky0 * a.ym) - (kz1 * a.zp + kz0 * a.zm);
+#endif
+}
+
+__device__ __forceinline__ double jacobi_k(double u0, const Nb& a, double kx0, double kx1, double ky0, double ky1,
+                                           double kz0, double kz1)
+{
+#if TEA_DIM == 2
+    (void)kz0;
+    (void)kz1;
+    return (u0 + (kx1 * a.xp + kx0 * a.xm) + (ky1 * a.yp + ky0 * a.ym)) / (1.0 + (kx0 + kx1) + (ky0 + ky1));
+#else
+    return (u0 + (kx1 * a.xp + kx0 * a.xm) + (ky1 * a.yp + ky0 * a.ym) + (kz1 * a.zp + kz0 * a.zm))
+        / (1.0 + (kx0 + kx1) + (ky0 + ky1) + (kz0 + kz1));
 #endif
 }
 
@@ -133,168 +166,21 @@ __device__ void end_iteration(const FusedArgs& a, SolveState& s, int phase)
 
 // ------------------------------------------------------------------ generic stencil drivers
 
-// Op interface:
+// Op interface (one Op per fused stencil sweep):
+//   using T (operand and coefficient type); static constexpr int NV (reduced values);
 //   static constexpr bool kReduce;
-//   __device__ void begin(const FusedArgs&)                      -- read scalars
-//   __device__ double stage(const FusedArgs&, long i)             -- operand at a (reflected) cell
-//   __device__ void interior(const FusedArgs&, long i, const Nb&, DD& acc)
-//   __device__ void control(const FusedArgs&, double v)           -- last block, lane 0
-//   __device__ bool skip(const FusedArgs&)                        -- whole launch is a no-op
+//   skip(a)            -- the whole launch is a no-op (uniform)
+//   begin(a)           -- read the solve state into registers
+//   coef_x/y/z(a)      -- coefficient arrays
+//   Raw load_raw(a, i) / T stage_raw(Raw)  -- loads behind the stencil operand at cell i,
+//                                           and the operand computed from them
+//   In load_in(a, i)   -- the other per-cell inputs of the interior update
+//   interior_k(a, i, nb, raw_c, in, kx0, kx1, ky0, ky1, kz0, kz1, acc)
+//   control(a, v)      -- last block, lane 0, with the rounded sums v[0..NV)
 
-template <class Op>
-__global__ void __launch_bounds__(FBLOCK) k_stencil2d(FusedArgs a)
-{
-    constexpr int SX = FT_X + 2, SY = FT_Y2 + 2;
-    __shared__ double s_op[SY][SX];
-    Op op;
-    if (op.skip(a)) return;
-    op.begin(a);
-    const Geom& g = a.g;
-    DDVec<1> acc;
-    acc.zero();
-    const int tid = threadIdx.x + threadIdx.y * FT_X;
-    for (long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const int tx = (int)(t % a.tiles_x), ty = (int)(t / a.tiles_x);
-        const int x0 = HALO_PAD + tx * FT_X, y0 = HALO_PAD + ty * FT_Y2;
-        for (int s = tid; s < SX * SY; s += FBLOCK) {
-            const int lx = s % SX, ly = s / SX;
-            const int kk = x0 - 1 + lx, jj = y0 - 1 + ly;
-            if (kk <= g.X - 2 && jj <= g.Y - 2) s_op[ly][lx] = op.stage(a, fidx(g, refl(kk, g.X), refl(jj, g.Y), 0));
-        }
-        __syncthreads();
-#pragma unroll
-        for (int c = 0; c < FT_Y2 / 8; ++c) {
-            const int lx = (int)threadIdx.x + 1, ly = (int)threadIdx.y + 8 * c + 1;
-            const int kk = x0 + (int)threadIdx.x, jj = y0 + (int)threadIdx.y + 8 * c;
-            if (kk < g.X - HALO_PAD && jj < g.Y - HALO_PAD) {
-                Nb nb;
-                nb.c = s_op[ly][lx];
-                nb.xm = s_op[ly][lx - 1];
-                nb.xp = s_op[ly][lx + 1];
-                nb.ym = s_op[ly - 1][lx];
-                nb.yp = s_op[ly + 1][lx];
-                nb.zm = nb.zp = 0.0;
-                op.interior(a, fidx(g, kk, jj, 0), nb, acc.v[0]);
-            }
-        }
-        __syncthreads();
-    }
-    if (Op::kReduce) grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.control(a, v[0]); });
-}
-
-template <class Op>
-__global__ void __launch_bounds__(FBLOCK) k_stencil3d(FusedArgs a)
-{
-    constexpr int SX = FT_X + 2, SY = FT_Y3 + 2;
-    __shared__ double s_op[4][SY][SX];
-    Op op;
-    if (op.skip(a)) return;
-    op.begin(a);
-    const Geom& g = a.g;
-    DDVec<1> acc;
-    acc.zero();
-    const int tid = threadIdx.x + threadIdx.y * FT_X;
-    const long txy = (long)a.tiles_x * a.tiles_y;
-    for (long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const int zs = (int)(t / txy);
-        const long rxy = t % txy;
-        const int tx = (int)(rxy % a.tiles_x), ty = (int)(rxy / a.tiles_x);
-        const int x0 = HALO_PAD + tx * FT_X, y0 = HALO_PAD + ty * FT_Y3;
-        const int z0 = HALO_PAD + zs * a.zseg;
-        const int z1 = min(z0 + a.zseg, g.Z - HALO_PAD);
-        auto stage_plane = [&](int ii) {
-            double(*pl)[SX] = s_op[ii & 3];
-            const int ri = refl(ii, g.Z);
-            for (int s = tid; s < SX * SY; s += FBLOCK) {
-                const int lx = s % SX, ly = s / SX;
-                const int kk = x0 - 1 + lx, jj = y0 - 1 + ly;
-                if (kk <= g.X - 2 && jj <= g.Y - 2) pl[ly][lx] = op.stage(a, fidx(g, refl(kk, g.X), refl(jj, g.Y), ri));
-            }
-        };
-        stage_plane(z0 - 1);
-        stage_plane(z0);
-        for (int ii = z0; ii < z1; ++ii) {
-            stage_plane(ii + 1);
-            __syncthreads();
-            const int lx = (int)threadIdx.x + 1, ly = (int)threadIdx.y + 1;
-            const int kk = x0 + (int)threadIdx.x, jj = y0 + (int)threadIdx.y;
-            if (kk < g.X - HALO_PAD && jj < g.Y - HALO_PAD) {
-                const double(*pm)[SX] = s_op[(ii - 1) & 3];
-                const double(*pc)[SX] = s_op[ii & 3];
-                const double(*pp)[SX] = s_op[(ii + 1) & 3];
-                Nb nb;
-                nb.c = pc[ly][lx];
-                nb.xm = pc[ly][lx - 1];
-                nb.xp = pc[ly][lx + 1];
-                nb.ym = pc[ly - 1][lx];
-                nb.yp = pc[ly + 1][lx];
-                nb.zm = pm[ly][lx];
-                nb.zp = pp[ly][lx];
-                op.interior(a, fidx(g, kk, jj, ii), nb, acc.v[0]);
-            }
-        }
-        __syncthreads();
-    }
-    if (Op::kReduce) grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.control(a, v[0]); });
-}
-
-// 2D register streaming: a block of SW warps covers 32*SW adjacent columns and marches
-// down SY rows; each lane owns one column and keeps the staged operand of rows j-1, j,
-// j+1 in registers.  x-neighbours come from the adjacent lanes by shuffle; the two lanes
-// at the warp's edges stage their outside neighbour themselves.  No shared memory and no
-// block barrier: every array is read once per cell (plus the edge columns and one row
-// above and below each column segment, which hit L2).
-constexpr int SW = 4;      // warps per block
-constexpr int SY = 32;     // rows per column segment
+constexpr int SW = 4;      // warps per block (2D)
+constexpr int SY = 32;     // rows per column segment (2D)
 constexpr int SBLOCK = 32 * SW;
-
-template <class Op>
-__global__ void __launch_bounds__(SBLOCK) k_stream2d(FusedArgs a)
-{
-    Op op;
-    if (op.skip(a)) return;
-    op.begin(a);
-    const Geom& g = a.g;
-    DDVec<1> acc;
-    acc.zero();
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int xlast = g.X - HALO_PAD - 1;  // last inner column
-    const int ylast = g.Y - HALO_PAD - 1;
-    for (long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const int tx = (int)(t % a.tiles_x), ty = (int)(t / a.tiles_x);
-        const int kk = HALO_PAD + tx * SBLOCK + warp * 32 + lane;
-        if (HALO_PAD + tx * SBLOCK + warp * 32 > xlast) continue;  // whole warp outside: uniform
-        const bool active = kk <= xlast;
-        const int kc = min(kk, xlast);                 // inactive lanes shadow the last column
-        const bool edge = lane == 0 || lane == 31;
-        const int ke = lane == 0 ? refl(kc - 1, g.X) : refl(min(kc + 1, xlast + 1), g.X);
-        const int j0 = HALO_PAD + ty * SY;
-        const int j1 = min(j0 + SY, ylast + 1);
-        double cm = op.stage(a, fidx(g, kc, refl(j0 - 1, g.Y), 0));
-        double cc = op.stage(a, fidx(g, kc, j0, 0));
-        for (int jj = j0; jj < j1; ++jj) {
-            const double cp = op.stage(a, fidx(g, kc, refl(jj + 1, g.Y), 0));
-            double e = 0.0;
-            if (edge) e = op.stage(a, fidx(g, ke, jj, 0));
-            const double up = __shfl_up_sync(0xffffffffu, cc, 1);
-            const double dn = __shfl_down_sync(0xffffffffu, cc, 1);
-            if (active) {
-                Nb nb;
-                nb.c = cc;
-                nb.xm = lane == 0 ? e : up;
-                nb.xp = lane == 31 ? e : dn;
-                nb.ym = cm;
-                nb.yp = cp;
-                nb.zm = nb.zp = 0.0;
-                op.interior(a, fidx(g, kk, jj, 0), nb, acc.v[0]);
-            }
-            cm = cc;
-            cc = cp;
-        }
-    }
-    if (Op::kReduce) grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.control(a, v[0]); });
-}
 
 // 2D register streaming with one row of software prefetch: the loads of row j+2 are in
 // flight while row j is computed.  Per row each lane carries the raw inputs of the
@@ -307,17 +193,19 @@ __global__ void __launch_bounds__(SBLOCK) k_pipe2d(FusedArgs a)
 {
     using Raw = typename Op::Raw;
     using In = typename Op::In;
+    using T = typename Op::T;
+    constexpr int NV = Op::NV;
     struct Bundle {
         In in;
-        double kx, ky, kxe;
+        T kx, kxe;
     };
     Op op;
     if (op.skip(a)) return;
     op.begin(a);
     const Geom& g = a.g;
-    const double* __restrict__ KX = a.kx;
-    const double* __restrict__ KY = a.ky;
-    DDVec<1> acc;
+    const T* __restrict__ KX = op.coef_x(a);
+    const T* __restrict__ KY = op.coef_y(a);
+    DDVec<NV> acc;
     acc.zero();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -337,61 +225,393 @@ __global__ void __launch_bounds__(SBLOCK) k_pipe2d(FusedArgs a)
         const int j1 = min(j0 + SY, ylast + 1);
         auto bundle = [&](int jj) {
             Bundle b;
-            const long i = fidx(g, kq, jj, 0);
             b.in = op.load_in(a, fidx(g, kc, jj, 0));
-            b.kx = KX[i];
-            b.ky = KY[fidx(g, kc, jj, 0)];
-            b.kxe = lane == 31 ? KX[fidx(g, min(kk + 1, xlast + 1), jj, 0)] : 0.0;
+            b.kx = KX[fidx(g, kq, jj, 0)];
+            b.kxe = lane == 31 ? KX[fidx(g, min(kk + 1, xlast + 1), jj, 0)] : (T)0;
             return b;
         };
+        // Pipelines: operand raw inputs two rows ahead, interior bundle one row ahead,
+        // Ky two rows ahead (row j+1's Ky is row j's upper-face coefficient).
         Raw rc = op.load_raw(a, fidx(g, kc, j0, 0));
         Raw rp = op.load_raw(a, fidx(g, kc, refl(j0 + 1, g.Y), 0));
-        double sm = op.stage_raw(op.load_raw(a, fidx(g, kc, refl(j0 - 1, g.Y), 0)));
-        double sc = op.stage_raw(rc);
+        T sm = op.stage_raw(op.load_raw(a, fidx(g, kc, refl(j0 - 1, g.Y), 0)));
+        T sc = op.stage_raw(rc);
         Bundle bc = bundle(j0);
-        Bundle bn = bundle(j0 + 1);
+        T ky0 = KY[fidx(g, kc, j0, 0)];
+        T ky1 = KY[fidx(g, kc, j0 + 1, 0)];
         Raw rec;
         if (edge) rec = op.load_raw(a, fidx(g, ke, j0, 0));
         for (int jj = j0; jj < j1; ++jj) {
-            // Prefetch row jj+2 (operand, interior bundle) and the edge operand of row jj+1.
+            const int jn = min(jj + 1, ylast);
             const Raw rpp = op.load_raw(a, fidx(g, kc, refl(min(jj + 2, ylast + 2), g.Y), 0));
-            const Bundle bnn = bundle(min(jj + 2, ylast + 1));
+            const Bundle bn = bundle(jn);
+            const T ky2 = KY[fidx(g, kc, min(jj + 2, ylast + 1), 0)];
             Raw ren;
-            if (edge) ren = op.load_raw(a, fidx(g, ke, min(jj + 1, ylast), 0));
-            const double sp = op.stage_raw(rp);
-            const double e = edge ? op.stage_raw(rec) : 0.0;
-            const double up = __shfl_up_sync(0xffffffffu, sc, 1);
-            const double dn = __shfl_down_sync(0xffffffffu, sc, 1);
-            const double kxr = __shfl_down_sync(0xffffffffu, bc.kx, 1);
+            if (edge) ren = op.load_raw(a, fidx(g, ke, jn, 0));
+            const T sp = op.stage_raw(rp);
+            const T e = edge ? op.stage_raw(rec) : (T)0;
+            const T up = __shfl_up_sync(0xffffffffu, sc, 1);
+            const T dn = __shfl_down_sync(0xffffffffu, sc, 1);
+            const T kxr = __shfl_down_sync(0xffffffffu, bc.kx, 1);
             if (active) {
-                Nb nb;
+                NbT<T> nb;
                 nb.c = sc;
                 nb.xm = lane == 0 ? e : up;
                 nb.xp = lane == 31 ? e : dn;
                 nb.ym = sm;
                 nb.yp = sp;
-                nb.zm = nb.zp = 0.0;
-                const double kx1 = lane == 31 ? bc.kxe : kxr;
-                op.interior2(a, fidx(g, kk, jj, 0), nb, rc, bc.in, bc.kx, kx1, bc.ky, bn.ky, acc.v[0]);
+                nb.zm = nb.zp = (T)0;
+                const T kx1 = lane == 31 ? bc.kxe : kxr;
+                op.interior_k(a, fidx(g, kk, jj, 0), nb, rc, bc.in, bc.kx, kx1, ky0, ky1, (T)0, (T)0, acc);
             }
             sm = sc;
             sc = sp;
             rc = rp;
             rp = rpp;
             bc = bn;
-            bn = bnn;
+            ky0 = ky1;
+            ky1 = ky2;
             if (edge) rec = ren;
         }
     }
-    if (Op::kReduce) grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.control(a, v[0]); });
+    if (Op::kReduce) grid_reduce_then<NV>(acc, a.red, [&](const double* v) { op.control(a, v); });
+}
+
+// 3D register streaming: a block of TY3 + 2 warps covers 32 columns x TY3 rows of one
+// x-y tile and marches through a z segment.  Warp w (1..TY3) owns row y0 + w - 1; warps 0
+// and TY3 + 1 only stage the operand of the rows just outside the tile.  Each lane keeps
+// the operand of planes ii-1, ii, ii+1 of its column in registers (z-neighbours) and the
+// raw inputs and interior bundle of the next planes in flight; x-neighbours come by
+// shuffle (edge lanes stage their outside neighbour), y-neighbours through a shared plane
+// that is double-buffered, so one barrier per plane suffices.
+constexpr int TY3 = 8;
+constexpr int P3BLOCK = 32 * (TY3 + 2);
+
+template <class Op>
+__global__ void __launch_bounds__(P3BLOCK, 2) k_pipe3d(FusedArgs a)
+{
+    using Raw = typename Op::Raw;
+    using In = typename Op::In;
+    using T = typename Op::T;
+    constexpr int NV = Op::NV;
+    struct Bundle {
+        In in;
+        T kx, ky, ky1, kxe;
+    };
+    __shared__ T s_pl[2][TY3 + 2][32];
+    Op op;
+    if (op.skip(a)) return;
+    op.begin(a);
+    const Geom& g = a.g;
+    const T* __restrict__ KX = op.coef_x(a);
+    const T* __restrict__ KY = op.coef_y(a);
+    const T* __restrict__ KZ = op.coef_z(a);
+    DDVec<NV> acc;
+    acc.zero();
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const bool owner = warp >= 1 && warp <= TY3;
+    const int xlast = g.X - HALO_PAD - 1;
+    const int ylast = g.Y - HALO_PAD - 1;
+    const int zlast = g.Z - HALO_PAD - 1;
+    const long txy = (long)a.tiles_x * a.tiles_y;
+    for (long t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+        const int zs = (int)(t / txy);
+        const long rxy = t % txy;
+        const int tx = (int)(rxy % a.tiles_x), ty = (int)(rxy / a.tiles_x);
+        const int kk = HALO_PAD + tx * 32 + lane;
+        const bool colok = kk <= xlast;
+        const int kc = min(kk, xlast);
+        const int kq = min(kk, xlast + 1);
+        const bool edge = lane == 0 || lane == 31;
+        const int ke = lane == 0 ? refl(kc - 1, g.X) : refl(min(kc + 1, xlast + 1), g.X);
+        const int y0 = HALO_PAD + ty * TY3;
+        const int jraw = y0 + warp - 1;                      // row of this warp (halo warps outside)
+        const bool rowok = owner && jraw <= ylast;
+        const int jc = refl(min(jraw, ylast + 1), g.Y);      // operand row (reflected, clamped)
+        const int jq = min(max(jraw, HALO_PAD), ylast);      // interior row for loads (valid)
+        const bool active = colok && rowok;
+        const int z0 = HALO_PAD + zs * a.zseg;
+        const int z1 = min(z0 + a.zseg, zlast + 1);
+        auto raw_at = [&](int col, int plane) { return op.load_raw(a, fidx(g, col, jc, refl(plane, g.Z))); };
+        auto bundle = [&](int plane) {
+            Bundle b;
+            b.in = op.load_in(a, fidx(g, kc, jq, plane));
+            b.kx = KX[fidx(g, kq, jq, plane)];
+            b.ky = KY[fidx(g, kc, jq, plane)];
+            b.ky1 = KY[fidx(g, kc, jq + 1, plane)];
+            b.kxe = lane == 31 ? KX[fidx(g, min(kk + 1, xlast + 1), jq, plane)] : (T)0;
+            return b;
+        };
+        // Pipelines: operand raw inputs two planes ahead, interior bundle one plane ahead,
+        // Kz two planes ahead (plane ii+1's Kz is plane ii's upper-face coefficient).
+        Raw rc = raw_at(kc, z0);
+        Raw rp = raw_at(kc, z0 + 1);
+        T sm = op.stage_raw(raw_at(kc, z0 - 1));
+        T sc = op.stage_raw(rc);
+        Bundle bc;
+        T kz0 = 0, kz1 = 0;
+        if (owner) {
+            bc = bundle(z0);
+            kz0 = KZ[fidx(g, kc, jq, z0)];
+            kz1 = KZ[fidx(g, kc, jq, z0 + 1)];
+        }
+        Raw rec;
+        if (edge && owner) rec = raw_at(ke, z0);
+        int buf = 0;
+        for (int ii = z0; ii < z1; ++ii) {
+            const int zn = min(ii + 1, zlast);
+            const Raw rpp = raw_at(kc, min(ii + 2, zlast + 2));
+            Bundle bn;
+            T kz2 = 0;
+            Raw ren;
+            if (owner) {
+                bn = bundle(zn);
+                kz2 = KZ[fidx(g, kc, jq, min(ii + 2, zlast + 1))];
+                if (edge) ren = raw_at(ke, zn);
+            }
+            const T sp = op.stage_raw(rp);
+            s_pl[buf][warp][lane] = sc;
+            __syncthreads();
+            if (owner) {
+                const T e = edge ? op.stage_raw(rec) : (T)0;
+                const T up = __shfl_up_sync(0xffffffffu, sc, 1);
+                const T dn = __shfl_down_sync(0xffffffffu, sc, 1);
+                const T kxr = __shfl_down_sync(0xffffffffu, bc.kx, 1);
+                if (active) {
+                    NbT<T> nb;
+                    nb.c = sc;
+                    nb.xm = lane == 0 ? e : up;
+                    nb.xp = lane == 31 ? e : dn;
+                    nb.ym = s_pl[buf][warp - 1][lane];
+                    nb.yp = s_pl[buf][warp + 1][lane];
+                    nb.zm = sm;
+                    nb.zp = sp;
+                    const T kx1 = lane == 31 ? bc.kxe : kxr;
+                    op.interior_k(a, fidx(g, kk, jraw, ii), nb, rc, bc.in, bc.kx, kx1, bc.ky, bc.ky1, kz0, kz1,
+                                  acc);
+                }
+                bc = bn;
+                kz0 = kz1;
+                kz1 = kz2;
+                if (edge) rec = ren;
+            }
+            sm = sc;
+            sc = sp;
+            rc = rp;
+            rp = rpp;
+            buf ^= 1;
+        }
+        __syncthreads();
+    }
+    if (Op::kReduce) grid_reduce_then<NV>(acc, a.red, [&](const double* v) { op.control(a, v); });
+}
+
+// 2D streaming through a per-warp shared-memory ring filled by cp.async.  Each warp owns a
+// strip of 64 columns (two adjacent cells per lane, 16-byte copies for FP64) and marches
+// down a segment of RSY rows; the rows of every input array are copied asynchronously
+// RP rows ahead of the row being computed, so the data in flight lives in shared memory,
+// not in registers.  A ring row holds columns c0-1 .. c0+64 (the outer two for the
+// x-neighbours of the strip's edge cells).  Rows and columns outside the inner domain are
+// copied from their reflected interior cell; within the strip the right-hand boundary is
+// reflected when the operand is read.  No block barrier: warps are independent.
+constexpr int RP = 3;          // rows in flight beyond row j+1
+constexpr int RQ = RP + 2;     // ring rows per warp
+constexpr int RW = 68;         // elements per ring row: pad, c0-1, c0..c0+63, c0+64, pad
+constexpr int RWARPS = 4;      // warps per block
+constexpr int RSY = 64;        // rows per segment
+
+__device__ __forceinline__ void cp_async_16(void* dst, const void* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_8(void* dst, const void* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_4(void* dst, const void* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <class T>
+__device__ __forceinline__ void ring_copy_pair(T* dst, const T* src)
+{
+    if (sizeof(T) == 8) cp_async_16(dst, src);
+    else cp_async_8(dst, src);
+}
+template <class T>
+__device__ __forceinline__ void ring_copy_one(T* dst, const T* src)
+{
+    if (sizeof(T) == 8) cp_async_8(dst, src);
+    else cp_async_4(dst, src);
+}
+
+template <class Op>
+constexpr size_t ring_smem_bytes()
+{
+    return (size_t)RWARPS * RQ * (Op::NR + Op::NI + 2) * RW * sizeof(typename Op::T);
+}
+
+template <class Op>
+__global__ void __launch_bounds__(RWARPS * 32) k_ring2d(FusedArgs a)
+{
+    using T = typename Op::T;
+    using Raw = typename Op::Raw;
+    using In = typename Op::In;
+    constexpr int NV = Op::NV;
+    constexpr int NR = Op::NR, NI = Op::NI;
+    constexpr int NA = NR + NI + 2;  // + Kx, Ky
+    constexpr int AKX = NR + NI, AKY = NR + NI + 1;
+    extern __shared__ __align__(16) unsigned char s_ring_raw[];
+    Op op;
+    if (op.skip(a)) return;
+    op.begin(a);
+    const Geom& g = a.g;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * RQ * NA * RW;
+    const T* src[NA];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) src[k] = op.raw_ptr(a, k);
+#pragma unroll
+    for (int k = 0; k < NI; ++k) src[NR + k] = op.in_ptr(a, k);
+    src[AKX] = op.coef_x(a);
+    src[AKY] = op.coef_y(a);
+    DDVec<NV> acc;
+    acc.zero();
+    const int xlast = g.X - HALO_PAD - 1;
+    const int ylast = g.Y - HALO_PAD - 1;
+    const int per_x = (g.nx + 63) / 64;
+    const int per_y = (g.ny + RSY - 1) / RSY;
+    const long nseg = (long)per_x * per_y;
+    const long gw = (long)blockIdx.x * RWARPS + warp, nw = (long)gridDim.x * RWARPS;
+    const int cmax = (int)g.pitch - 2;  // last even column whose pair stays inside the row
+    for (long sgi = gw; sgi < nseg; sgi += nw) {
+        const int xs = (int)(sgi % per_x), ys = (int)(sgi / per_x);
+        const int c0 = HALO_PAD + 64 * xs;
+        const int c = c0 + 2 * lane;
+        const int cc = min(c, cmax);
+        const int j0 = HALO_PAD + RSY * ys;
+        const int j1 = min(j0 + RSY, ylast + 1);
+        const int left = refl(c0 - 1, g.X);
+        const int right_op = refl(min(c0 + 64, xlast + 1), g.X);
+        const int right_k = min(c0 + 64, xlast + 1);
+        // Copy ring row for grid row r (relative row rr = r - j0 + 1 selects the slot).
+        auto issue = [&](int r) {
+            if (r <= j1) {
+                T* base = ring + (size_t)((r - j0 + 1) % RQ) * NA * RW;
+                const int srow = refl(min(max(r, 1), ylast + 1), g.Y);
+                const int irow = min(max(r, HALO_PAD), ylast + 1);
+#pragma unroll
+                for (int k = 0; k < NA; ++k) {
+                    const T* sp = src[k];
+                    if (!sp) continue;
+                    const int row = k < NR ? srow : irow;
+                    T* d = base + k * RW;
+                    ring_copy_pair(d + 2 + 2 * lane, sp + fidx(g, cc, row, 0));
+                    if (lane == 0 && k < NR) ring_copy_one(d + 1, sp + fidx(g, left, row, 0));
+                    if (lane == 31 && (k < NR || k == AKX))
+                        ring_copy_one(d + 66, sp + fidx(g, k < NR ? right_op : right_k, row, 0));
+                }
+            }
+            cp_async_commit();
+        };
+        // The operand of ring row `r` at the lane's two cells and at the strip's edge.
+        auto stage_row = [&](int r, T& v0, T& v1, T& ve) {
+            const T* base = ring + (size_t)((r - j0 + 1) % RQ) * NA * RW;
+            T x0[NR], x1[NR], xe[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) {
+                x0[k] = base[k * RW + 2 + 2 * lane];
+                x1[k] = base[k * RW + 3 + 2 * lane];
+                xe[k] = base[k * RW + (lane == 0 ? 1 : 66)];
+            }
+            v0 = op.stage_raw(op.raw_from(x0));
+            v1 = op.stage_raw(op.raw_from(x1));
+            ve = op.stage_raw(op.raw_from(xe));
+        };
+        for (int r = j0 - 1; r <= j0 + RP; ++r) issue(r);
+        cp_async_wait<RP>();
+        __syncwarp();
+        T m0, m1, me, c0v, c1v, ce;
+        stage_row(j0 - 1, m0, m1, me);
+        stage_row(j0, c0v, c1v, ce);
+        for (int jj = j0; jj < j1; ++jj) {
+            cp_async_wait<RP - 1>();
+            __syncwarp();
+            T p0, p1, pe;
+            stage_row(jj + 1, p0, p1, pe);
+            const T* cur = ring + (size_t)((jj - j0 + 1) % RQ) * NA * RW;
+            const T* nxt = ring + (size_t)((jj - j0 + 2) % RQ) * NA * RW;
+            // x-neighbours of the pair (reflection at the last inner column).
+            const T up = __shfl_up_sync(0xffffffffu, c1v, 1);
+            const T dn = __shfl_down_sync(0xffffffffu, c0v, 1);
+            const T kxa = cur[AKX * RW + 2 + 2 * lane], kxb = cur[AKX * RW + 3 + 2 * lane];
+            const T kxn = __shfl_down_sync(0xffffffffu, kxa, 1);
+            const T kxc = lane == 31 ? cur[AKX * RW + 66] : kxn;
+            const T kya = cur[AKY * RW + 2 + 2 * lane], kyb = cur[AKY * RW + 3 + 2 * lane];
+            const T kya1 = nxt[AKY * RW + 2 + 2 * lane], kyb1 = nxt[AKY * RW + 3 + 2 * lane];
+            T r0[NR > 0 ? NR : 1], r1[NR > 0 ? NR : 1], i0[NI], i1[NI];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) {
+                r0[k] = cur[k * RW + 2 + 2 * lane];
+                r1[k] = cur[k * RW + 3 + 2 * lane];
+            }
+#pragma unroll
+            for (int k = 0; k < NI; ++k) {
+                i0[k] = cur[(NR + k) * RW + 2 + 2 * lane];
+                i1[k] = cur[(NR + k) * RW + 3 + 2 * lane];
+            }
+            if (c <= xlast) {
+                NbT<T> nb;
+                nb.c = c0v;
+                nb.xm = lane == 0 ? ce : up;
+                nb.xp = c == xlast ? c0v : c1v;
+                nb.ym = m0;
+                nb.yp = p0;
+                nb.zm = nb.zp = (T)0;
+                op.interior_k(a, fidx(g, c, jj, 0), nb, op.raw_from(r0), op.in_from(i0), kxa, kxb, kya, kya1, (T)0,
+                              (T)0, acc);
+            }
+            if (c + 1 <= xlast) {
+                NbT<T> nb;
+                nb.c = c1v;
+                nb.xm = c0v;
+                nb.xp = c + 1 == xlast ? c1v : (lane == 31 ? ce : dn);
+                nb.ym = m1;
+                nb.yp = p1;
+                nb.zm = nb.zp = (T)0;
+                op.interior_k(a, fidx(g, c + 1, jj, 0), nb, op.raw_from(r1), op.in_from(i1), kxb, kxc, kyb, kyb1,
+                              (T)0, (T)0, acc);
+            }
+            m0 = c0v;
+            m1 = c1v;
+            me = ce;
+            c0v = p0;
+            c1v = p1;
+            ce = pe;
+            __syncwarp();
+            issue(jj + RP + 1);  // into the slot of row jj - 1, which no lane reads any more
+        }
+        cp_async_wait<0>();
+        __syncwarp();
+    }
+    if (Op::kReduce) grid_reduce_then<NV>(acc, a.red, [&](const double* v) { op.control(a, v); });
 }
 
 #if TEA_DIM == 2
 #define TEA_STENCIL k_pipe2d
 #define TEA_STENCIL_BLOCK dim3(SBLOCK)
 #else
-#define TEA_STENCIL k_stencil3d
-#define TEA_STENCIL_BLOCK dim3(FT_X, FBLOCK / FT_X)
+#define TEA_STENCIL k_pipe3d
+#define TEA_STENCIL_BLOCK dim3(P3BLOCK)
 #endif
 
 // ------------------------------------------------------------------ CG / PPCG sweep A
@@ -402,6 +622,11 @@ __global__ void __launch_bounds__(SBLOCK) k_pipe2d(FusedArgs a)
 // p buffer.
 struct OpSweepA {
     static constexpr bool kReduce = true;
+    using T = double;
+    static constexpr int NV = 1;
+    __device__ const double* coef_x(const FusedArgs& a) const { return a.kx; }
+    __device__ const double* coef_y(const FusedArgs& a) const { return a.ky; }
+    __device__ const double* coef_z(const FusedArgs& a) const { return a.kz; }
     const double* pcur;
     double* pnew;
     double beta, alpha;
@@ -417,20 +642,6 @@ struct OpSweepA {
         pend_p = s.pending_p;
         pend_u = s.pending_u;
         precond = s.precond;
-    }
-    __device__ double stage(const FusedArgs& a, long i)
-    {
-        const double p = pcur[i];
-        if (!pend_p) return p;
-        return beta * p + (precond ? a.z[i] : a.r[i]);
-    }
-    __device__ void interior(const FusedArgs& a, long i, const Nb& nb, DD& acc)
-    {
-        if (pend_u) a.u[0][i] = a.u[0][i] + alpha * pcur[i];
-        pnew[i] = nb.c;
-        const double w = smvp_nb(nb, a.kx, a.ky, a.kz, i, a.g.pitch, a.g.page);
-        a.w[i] = w;
-        dd_add(acc, w * nb.c);
     }
     // Pipelined 2D interface (k_pipe2d): raw loads, staging, interior from registers.
     struct Raw {
@@ -453,18 +664,38 @@ struct OpSweepA {
         in.u = pend_u ? a.u[0][i] : 0.0;
         return in;
     }
-    __device__ void interior2(const FusedArgs& a, long i, const Nb& nb, const Raw& rc, const In& in, double kx0,
-                              double kx1, double ky0, double ky1, DD& acc) const
+    // Ring interface (k_ring2d): the arrays behind Raw and In, and Raw/In from their values.
+    static constexpr int NR = 2, NI = 1;
+    __device__ const double* raw_ptr(const FusedArgs& a, int k) const
+    {
+        return k == 0 ? pcur : (pend_p ? (precond ? a.z : a.r) : nullptr);
+    }
+    __device__ const double* in_ptr(const FusedArgs& a, int) const { return pend_u ? a.u[0] : nullptr; }
+    __device__ Raw raw_from(const double* v) const
+    {
+        Raw r;
+        r.p = v[0];
+        r.q = pend_p ? v[1] : 0.0;
+        return r;
+    }
+    __device__ In in_from(const double* v) const
+    {
+        In in;
+        in.u = pend_u ? v[0] : 0.0;
+        return in;
+    }
+    __device__ void interior_k(const FusedArgs& a, long i, const Nb& nb, const Raw& rc, const In& in, double kx0,
+                               double kx1, double ky0, double ky1, double kz0, double kz1, DDVec<1>& acc) const
     {
         if (pend_u) a.u[0][i] = in.u + alpha * rc.p;
         pnew[i] = nb.c;
-        const double w = (1.0 + (kx1 + kx0) + (ky1 + ky0)) * nb.c - (kx1 * nb.xp + kx0 * nb.xm)
-            - (ky1 * nb.yp + ky0 * nb.ym);
+        const double w = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
         a.w[i] = w;
-        dd_add(acc, w * nb.c);
+        dd_add(acc.v[0], w * nb.c);
     }
-    __device__ void control(const FusedArgs& a, double pw)
+    __device__ void control(const FusedArgs& a, const double* v)
     {
+        const double pw = v[0];
         if (a.timing) return;
         SolveState& s = *a.st;
         s.pw = pw;
@@ -606,6 +837,11 @@ __global__ void __launch_bounds__(BLOCK) k_ppcg_sweep_b(FusedArgs a, Box inner)
 template <bool LAST>
 struct OpPPCGInner {
     static constexpr bool kReduce = LAST;
+    using T = double;
+    static constexpr int NV = 1;
+    __device__ const double* coef_x(const FusedArgs& a) const { return a.kx; }
+    __device__ const double* coef_y(const FusedArgs& a) const { return a.ky; }
+    __device__ const double* coef_z(const FusedArgs& a) const { return a.kz; }
     const double* sdc;
     double* sdn;
     double al, be;
@@ -621,16 +857,6 @@ struct OpPPCGInner {
         al = a.ch_alphas[k - 1];
         be = a.ch_betas[k - 1];
         precond = s.precond;
-    }
-    __device__ double stage(const FusedArgs&, long i) { return sdc[i]; }
-    __device__ void interior(const FusedArgs& a, long i, const Nb& nb, DD& acc)
-    {
-        const double s = smvp_nb(nb, a.kx, a.ky, a.kz, i, a.g.pitch, a.g.page);
-        const double r = a.r[i] - s;
-        a.r[i] = r;
-        a.u[0][i] = a.u[0][i] + nb.c;
-        sdn[i] = al * nb.c + be * (precond ? a.mi[i] * r : r);
-        if (LAST) dd_add(acc, r * r);
     }
     struct Raw {
         double sd;
@@ -653,19 +879,39 @@ struct OpPPCGInner {
         in.mi = precond ? a.mi[i] : 0.0;
         return in;
     }
-    __device__ void interior2(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
-                              double kx1, double ky0, double ky1, DD& acc) const
+    static constexpr int NR = 1, NI = 3;
+    __device__ const double* raw_ptr(const FusedArgs&, int) const { return sdc; }
+    __device__ const double* in_ptr(const FusedArgs& a, int k) const
     {
-        const double s = (1.0 + (kx1 + kx0) + (ky1 + ky0)) * nb.c - (kx1 * nb.xp + kx0 * nb.xm)
-            - (ky1 * nb.yp + ky0 * nb.ym);
+        return k == 0 ? a.r : (k == 1 ? a.u[0] : (precond ? a.mi : nullptr));
+    }
+    __device__ Raw raw_from(const double* v) const
+    {
+        Raw r;
+        r.sd = v[0];
+        return r;
+    }
+    __device__ In in_from(const double* v) const
+    {
+        In in;
+        in.r = v[0];
+        in.u = v[1];
+        in.mi = precond ? v[2] : 0.0;
+        return in;
+    }
+    __device__ void interior_k(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
+                               double kx1, double ky0, double ky1, double kz0, double kz1, DDVec<1>& acc) const
+    {
+        const double s = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
         const double r = in.r - s;
         a.r[i] = r;
         a.u[0][i] = in.u + nb.c;
         sdn[i] = al * nb.c + be * (precond ? in.mi * r : r);
-        if (LAST) dd_add(acc, r * r);
+        if (LAST) dd_add(acc.v[0], r * r);
     }
-    __device__ void control(const FusedArgs& a, double rrn)
+    __device__ void control(const FusedArgs& a, const double* v)
     {
+        const double rrn = v[0];
         if (a.timing) return;
         SolveState& s = *a.st;
         s.rrn = rrn;
@@ -689,6 +935,11 @@ struct OpPPCGInner {
 // tealeaf_2d/tea_solve.f90:260).
 struct OpCheby {
     static constexpr bool kReduce = true;
+    using T = double;
+    static constexpr int NV = 1;
+    __device__ const double* coef_x(const FusedArgs& a) const { return a.kx; }
+    __device__ const double* coef_y(const FusedArgs& a) const { return a.ky; }
+    __device__ const double* coef_z(const FusedArgs& a) const { return a.kz; }
     const double* ucur;
     double* unew;
     double al, be;
@@ -704,16 +955,6 @@ struct OpCheby {
         be = a.ch_betas[step];
         precond = s.precond;
         check = (s.n >= s.est_itc) && (s.n % 10 == 0);
-    }
-    __device__ double stage(const FusedArgs&, long i) { return ucur[i]; }
-    __device__ void interior(const FusedArgs& a, long i, const Nb& nb, DD& acc)
-    {
-        const double w = smvp_nb(nb, a.kx, a.ky, a.kz, i, a.g.pitch, a.g.page);
-        const double r = a.u0[i] - w;
-        const double p = al * a.p[0][i] + be * (precond ? a.mi[i] * r : r);
-        a.p[0][i] = p;
-        unew[i] = nb.c + p;
-        if (check) dd_add(acc, r * r);
     }
     struct Raw {
         double u;
@@ -736,19 +977,39 @@ struct OpCheby {
         in.mi = precond ? a.mi[i] : 0.0;
         return in;
     }
-    __device__ void interior2(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
-                              double kx1, double ky0, double ky1, DD& acc) const
+    static constexpr int NR = 1, NI = 3;
+    __device__ const double* raw_ptr(const FusedArgs&, int) const { return ucur; }
+    __device__ const double* in_ptr(const FusedArgs& a, int k) const
     {
-        const double w = (1.0 + (kx1 + kx0) + (ky1 + ky0)) * nb.c - (kx1 * nb.xp + kx0 * nb.xm)
-            - (ky1 * nb.yp + ky0 * nb.ym);
+        return k == 0 ? a.u0 : (k == 1 ? a.p[0] : (precond ? a.mi : nullptr));
+    }
+    __device__ Raw raw_from(const double* v) const
+    {
+        Raw r;
+        r.u = v[0];
+        return r;
+    }
+    __device__ In in_from(const double* v) const
+    {
+        In in;
+        in.u0 = v[0];
+        in.p = v[1];
+        in.mi = precond ? v[2] : 0.0;
+        return in;
+    }
+    __device__ void interior_k(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
+                               double kx1, double ky0, double ky1, double kz0, double kz1, DDVec<1>& acc) const
+    {
+        const double w = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
         const double r = in.u0 - w;
         const double p = al * in.p + be * (precond ? in.mi * r : r);
         a.p[0][i] = p;
         unew[i] = nb.c + p;
-        if (check) dd_add(acc, r * r);
+        if (check) dd_add(acc.v[0], r * r);
     }
-    __device__ void control(const FusedArgs& a, double rr)
+    __device__ void control(const FusedArgs& a, const double* v)
     {
+        const double rr = v[0];
         if (a.timing) return;
         SolveState& s = *a.st;
         s.par_u ^= 1;
@@ -764,6 +1025,11 @@ struct OpCheby {
 // double-buffered instead of copied: u_new from the staged u_old, error = sum|u_new-u_old|.
 struct OpJacobi {
     static constexpr bool kReduce = true;
+    using T = double;
+    static constexpr int NV = 1;
+    __device__ const double* coef_x(const FusedArgs& a) const { return a.kx; }
+    __device__ const double* coef_y(const FusedArgs& a) const { return a.ky; }
+    __device__ const double* coef_z(const FusedArgs& a) const { return a.kz; }
     const double* ucur;
     double* unew;
     __device__ bool skip(const FusedArgs&) { return false; }
@@ -772,25 +1038,6 @@ struct OpJacobi {
         const SolveState& s = *a.st;
         ucur = a.u[s.par_u];
         unew = a.u[s.par_u ^ 1];
-    }
-    __device__ double stage(const FusedArgs&, long i) { return ucur[i]; }
-    __device__ void interior(const FusedArgs& a, long i, const Nb& nb, DD& acc)
-    {
-        const double* __restrict__ kx = a.kx;
-        const double* __restrict__ ky = a.ky;
-        const long px = a.g.pitch;
-#if TEA_DIM == 2
-        const double un = (a.u0[i] + (kx[i + 1] * nb.xp + kx[i] * nb.xm) + (ky[i + px] * nb.yp + ky[i] * nb.ym))
-            / (1.0 + (kx[i] + kx[i + 1]) + (ky[i] + ky[i + px]));
-#else
-        const double* __restrict__ kz = a.kz;
-        const long pg = a.g.page;
-        const double un = (a.u0[i] + (kx[i + 1] * nb.xp + kx[i] * nb.xm) + (ky[i + px] * nb.yp + ky[i] * nb.ym)
-                           + (kz[i + pg] * nb.zp + kz[i] * nb.zm))
-            / (1.0 + (kx[i] + kx[i + 1]) + (ky[i] + ky[i + px]) + (kz[i] + kz[i + pg]));
-#endif
-        unew[i] = un;
-        dd_add(acc, fabs(un - nb.c));
     }
     struct Raw {
         double u;
@@ -811,16 +1058,31 @@ struct OpJacobi {
         in.u0 = a.u0[i];
         return in;
     }
-    __device__ void interior2(const FusedArgs&, long i, const Nb& nb, const Raw&, const In& in, double kx0,
-                              double kx1, double ky0, double ky1, DD& acc) const
+    static constexpr int NR = 1, NI = 1;
+    __device__ const double* raw_ptr(const FusedArgs& a, int) const { (void)a; return ucur; }
+    __device__ const double* in_ptr(const FusedArgs& a, int) const { return a.u0; }
+    __device__ Raw raw_from(const double* v) const
     {
-        const double un = (in.u0 + (kx1 * nb.xp + kx0 * nb.xm) + (ky1 * nb.yp + ky0 * nb.ym))
-            / (1.0 + (kx0 + kx1) + (ky0 + ky1));
-        unew[i] = un;
-        dd_add(acc, fabs(un - nb.c));
+        Raw r;
+        r.u = v[0];
+        return r;
     }
-    __device__ void control(const FusedArgs& a, double err)
+    __device__ In in_from(const double* v) const
     {
+        In in;
+        in.u0 = v[0];
+        return in;
+    }
+    __device__ void interior_k(const FusedArgs&, long i, const Nb& nb, const Raw&, const In& in, double kx0,
+                               double kx1, double ky0, double ky1, double kz0, double kz1, DDVec<1>& acc) const
+    {
+        const double un = jacobi_k(in.u0, nb, kx0, kx1, ky0, ky1, kz0, kz1);
+        unew[i] = un;
+        dd_add(acc.v[0], fabs(un - nb.c));
+    }
+    __device__ void control(const FusedArgs& a, const double* v)
+    {
+        const double err = v[0];
         if (a.timing) return;
         SolveState& s = *a.st;
         s.par_u ^= 1;
@@ -837,17 +1099,14 @@ struct OpJacobi {
 // Jacobi iterations that check the true residual; a no-op launch otherwise.
 struct OpJacobiResidual {
     static constexpr bool kReduce = true;
+    using T = double;
+    static constexpr int NV = 1;
+    __device__ const double* coef_x(const FusedArgs& a) const { return a.kx; }
+    __device__ const double* coef_y(const FusedArgs& a) const { return a.ky; }
+    __device__ const double* coef_z(const FusedArgs& a) const { return a.kz; }
     const double* ucur;
     __device__ bool skip(const FusedArgs& a) { return a.st->resid_pending == 0; }
     __device__ void begin(const FusedArgs& a) { ucur = a.u[a.st->par_u]; }
-    __device__ double stage(const FusedArgs&, long i) { return ucur[i]; }
-    __device__ void interior(const FusedArgs& a, long i, const Nb& nb, DD& acc)
-    {
-        const double s = smvp_nb(nb, a.kx, a.ky, a.kz, i, a.g.pitch, a.g.page);
-        const double r = a.u0[i] - s;
-        a.r[i] = r;
-        dd_add(acc, r * r);
-    }
     struct Raw {
         double u;
     };
@@ -867,17 +1126,32 @@ struct OpJacobiResidual {
         in.u0 = a.u0[i];
         return in;
     }
-    __device__ void interior2(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
-                              double kx1, double ky0, double ky1, DD& acc) const
+    static constexpr int NR = 1, NI = 1;
+    __device__ const double* raw_ptr(const FusedArgs& a, int) const { (void)a; return ucur; }
+    __device__ const double* in_ptr(const FusedArgs& a, int) const { return a.u0; }
+    __device__ Raw raw_from(const double* v) const
     {
-        const double s = (1.0 + (kx1 + kx0) + (ky1 + ky0)) * nb.c - (kx1 * nb.xp + kx0 * nb.xm)
-            - (ky1 * nb.yp + ky0 * nb.ym);
+        Raw r;
+        r.u = v[0];
+        return r;
+    }
+    __device__ In in_from(const double* v) const
+    {
+        In in;
+        in.u0 = v[0];
+        return in;
+    }
+    __device__ void interior_k(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
+                               double kx1, double ky0, double ky1, double kz0, double kz1, DDVec<1>& acc) const
+    {
+        const double s = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
         const double r = in.u0 - s;
         a.r[i] = r;
-        dd_add(acc, r * r);
+        dd_add(acc.v[0], r * r);
     }
-    __device__ void control(const FusedArgs& a, double rr)
+    __device__ void control(const FusedArgs& a, const double* v)
     {
+        const double rr = v[0];
         if (a.timing) return;
         SolveState& s = *a.st;
         s.error = rr;
@@ -885,6 +1159,244 @@ struct OpJacobiResidual {
         end_iteration(a, s, PHASE_JACOBI);
     }
 };
+
+// ------------------------------------------------------------------ FP32 defect correction
+//
+// The precision form: FP64 keeps the outer residual r = b - A u, the update of u, the sums
+// that decide convergence and the field summary; the inner correction solve A d = r runs
+// CG with FP32 storage and arithmetic (its dot products accumulate the FP32 products in
+// double-double), halving the bytes of every inner iteration.
+
+// Kx/Ky/Kz rounded to FP32 once per solve (padded arrays, pointwise).
+__global__ void __launch_bounds__(256) k_coef_to_fp32(FusedArgs a)
+{
+    const Geom& g = a.g;
+    const long n = (long)g.page * g.Z;
+    const long base = -(long)kLeadPad;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n + kLeadPad; t += (long)gridDim.x * blockDim.x) {
+        const long i = base + t;
+        a.kx32[i] = (float)a.kx[i];
+        a.ky32[i] = (float)a.ky[i];
+        if (DIM == 3) a.kz32[i] = (float)a.kz[i];
+    }
+}
+
+// Outer residual in FP64 (CalculateResidual + Calculate2Norm), seeding the FP32 inner CG:
+// r32 = fl32(r), p32 = r32, d32 = 0; sums: r.r (FP64, decides outer convergence) and
+// r32.r32 (the inner rro).
+struct OpOuterResid {
+    static constexpr bool kReduce = true;
+    using T = double;
+    static constexpr int NV = 2;
+    __device__ const double* coef_x(const FusedArgs& a) const { return a.kx; }
+    __device__ const double* coef_y(const FusedArgs& a) const { return a.ky; }
+    __device__ const double* coef_z(const FusedArgs& a) const { return a.kz; }
+    struct Raw {
+        double u;
+    };
+    struct In {
+        double u0;
+    };
+    __device__ bool skip(const FusedArgs&) { return false; }
+    __device__ void begin(const FusedArgs&) {}
+    __device__ Raw load_raw(const FusedArgs& a, long i) const
+    {
+        Raw r;
+        r.u = a.u[0][i];
+        return r;
+    }
+    __device__ double stage_raw(const Raw& r) const { return r.u; }
+    __device__ In load_in(const FusedArgs& a, long i) const
+    {
+        In in;
+        in.u0 = a.u0[i];
+        return in;
+    }
+    static constexpr int NR = 1, NI = 1;
+    __device__ const double* raw_ptr(const FusedArgs& a, int) const { (void)a; return a.u[0]; }
+    __device__ const double* in_ptr(const FusedArgs& a, int) const { return a.u0; }
+    __device__ Raw raw_from(const double* v) const
+    {
+        Raw r;
+        r.u = v[0];
+        return r;
+    }
+    __device__ In in_from(const double* v) const
+    {
+        In in;
+        in.u0 = v[0];
+        return in;
+    }
+    __device__ void interior_k(const FusedArgs& a, long i, const Nb& nb, const Raw&, const In& in, double kx0,
+                               double kx1, double ky0, double ky1, double kz0, double kz1, DDVec<2>& acc) const
+    {
+        const double s = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
+        const double r = in.u0 - s;
+        const float r32 = (float)r;
+        a.r32[i] = r32;
+        a.p32[0][i] = r32;
+        a.d32[i] = 0.0f;
+        dd_add(acc.v[0], r * r);
+        dd_add(acc.v[1], (double)r32 * (double)r32);
+    }
+    __device__ void control(const FusedArgs& a, const double* v)
+    {
+        if (a.timing) return;
+        SolveState& s = *a.st;
+        s.error = v[0];
+        s.rro = v[1];
+        s.pending_p = 0;
+        s.pending_u = 0;
+        s.par_p = 0;
+        s.n_inner = 0;
+        if (!isfinite(v[0])) s.nonfinite = 1;
+    }
+};
+
+// FP32 CG sweep A: pending p = beta p + r and d += alpha p of the previous inner
+// iteration, then w = A p and pw.
+struct OpSweepA32 {
+    static constexpr bool kReduce = true;
+    using T = float;
+    static constexpr int NV = 1;
+    __device__ const float* coef_x(const FusedArgs& a) const { return a.kx32; }
+    __device__ const float* coef_y(const FusedArgs& a) const { return a.ky32; }
+    __device__ const float* coef_z(const FusedArgs& a) const { return a.kz32; }
+    const float* pcur;
+    float* pnew;
+    float beta, alpha;
+    int pend_p, pend_u;
+    struct Raw {
+        float p, r;
+    };
+    struct In {
+        float d;
+    };
+    __device__ bool skip(const FusedArgs&) { return false; }
+    __device__ void begin(const FusedArgs& a)
+    {
+        const SolveState& s = *a.st;
+        pcur = a.p32[s.par_p];
+        pnew = a.p32[s.par_p ^ 1];
+        beta = (float)s.last_beta;
+        alpha = (float)s.last_alpha;
+        pend_p = s.pending_p;
+        pend_u = s.pending_u;
+    }
+    __device__ Raw load_raw(const FusedArgs& a, long i) const
+    {
+        Raw r;
+        r.p = pcur[i];
+        r.r = pend_p ? a.r32[i] : 0.0f;
+        return r;
+    }
+    __device__ float stage_raw(const Raw& r) const { return pend_p ? beta * r.p + r.r : r.p; }
+    __device__ In load_in(const FusedArgs& a, long i) const
+    {
+        In in;
+        in.d = pend_u ? a.d32[i] : 0.0f;
+        return in;
+    }
+    static constexpr int NR = 2, NI = 1;
+    __device__ const float* raw_ptr(const FusedArgs& a, int k) const
+    {
+        return k == 0 ? pcur : (pend_p ? a.r32 : nullptr);
+    }
+    __device__ const float* in_ptr(const FusedArgs& a, int) const { return pend_u ? a.d32 : nullptr; }
+    __device__ Raw raw_from(const float* v) const
+    {
+        Raw r;
+        r.p = v[0];
+        r.r = pend_p ? v[1] : 0.0f;
+        return r;
+    }
+    __device__ In in_from(const float* v) const
+    {
+        In in;
+        in.d = pend_u ? v[0] : 0.0f;
+        return in;
+    }
+    __device__ void interior_k(const FusedArgs& a, long i, const NbT<float>& nb, const Raw& rc, const In& in,
+                               float kx0, float kx1, float ky0, float ky1, float kz0, float kz1,
+                               DDVec<1>& acc) const
+    {
+        if (pend_u) a.d32[i] = in.d + alpha * rc.p;
+        pnew[i] = nb.c;
+        const float w = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
+        a.w32[i] = w;
+        dd_add(acc.v[0], (double)w * (double)nb.c);
+    }
+    __device__ void control(const FusedArgs& a, const double* v)
+    {
+        if (a.timing) return;
+        SolveState& s = *a.st;
+        s.pw = v[0];
+        s.alpha = s.rro / v[0];
+        s.par_p ^= 1;
+        s.pending_p = 0;
+        s.pending_u = 0;
+        if (!isfinite(v[0])) s.nonfinite = 1;
+    }
+};
+
+// FP32 CG sweep B: r -= alpha w, rr; beta, and the inner loop test: stop when the inner
+// residual has dropped below tol2 (inner_tol^2 times its start) or after inner_max.
+__global__ void __launch_bounds__(256) k_cg32_sweep_b(FusedArgs a)
+{
+    const SolveState& s = *a.st;
+    const float alpha = (float)s.alpha;
+    float* __restrict__ R = a.r32;
+    const float* __restrict__ W = a.w32;
+    DDVec<1> acc;
+    acc.zero();
+    walk_pairs(a.g, [&](long i, bool two) {
+        if (two) {
+            const float2 r2 = *reinterpret_cast<const float2*>(R + i);
+            const float2 w2 = *reinterpret_cast<const float2*>(W + i);
+            const float r0 = r2.x - alpha * w2.x, r1 = r2.y - alpha * w2.y;
+            *reinterpret_cast<float2*>(R + i) = make_float2(r0, r1);
+            dd_add(acc.v[0], (double)r0 * (double)r0);
+            dd_add(acc.v[0], (double)r1 * (double)r1);
+        } else {
+            const float r0 = R[i] - alpha * W[i];
+            R[i] = r0;
+            dd_add(acc.v[0], (double)r0 * (double)r0);
+        }
+    });
+    grid_reduce_then<1>(acc, a.red, [&](const double* v) {
+        if (a.timing) return;
+        SolveState& st = *a.st;
+        st.rrn = v[0];
+        st.beta = st.rrn / st.rro;
+        st.rro = st.rrn;
+        st.last_alpha = st.alpha;
+        st.last_beta = st.beta;
+        st.pending_p = 1;
+        st.pending_u = 1;
+        st.n_inner = st.n_inner + 1;
+        if (!isfinite(v[0])) st.nonfinite = 1;
+        const int cont = isfinite(v[0]) && v[0] >= st.tol2 && st.n_inner < st.inner_max;
+        st.cont = cont;
+        if (a.use_handle) cudaGraphSetConditional(a.handle, cont ? 1u : 0u);
+    });
+}
+
+// u += d in FP64, after the pending d += alpha p of the last inner iteration.
+__global__ void __launch_bounds__(256) k_dc_update(FusedArgs a)
+{
+    const SolveState& s = *a.st;
+    const float alpha = (float)s.last_alpha;
+    const int pend = s.pending_u;
+    const float* __restrict__ P = a.p32[s.par_p];
+    walk_pairs(a.g, [&](long i, bool two) {
+        const int n = two ? 2 : 1;
+        for (int k = 0; k < n; ++k) {
+            float d = a.d32[i + k];
+            if (pend) d = d + alpha * P[i + k];
+            a.u[0][i + k] = a.u[0][i + k] + (double)d;
+        }
+    });
+}
 
 // ------------------------------------------------------------------ flush
 

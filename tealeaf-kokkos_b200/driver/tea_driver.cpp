@@ -87,6 +87,9 @@ struct Config {
     // Additive keywords (not in the reference).
     double tl_eps_rel = 0.0;  // relative target: eps = tl_eps_rel^2 * sum(u0^2) per solve
     bool use_fused_solve = false;
+    int precision = 0;          // tl_precision fp64 | fp32 (whole-solve path only)
+    int inner_max_iters = 0;    // tl_inner_max_iters
+    double inner_tol = 0.0;     // tl_inner_tol
     std::vector<State> states;  // states[0] is state 1
 };
 
@@ -224,6 +227,13 @@ Config parse_deck(const std::string& text, int dim)
             else if (word == "test_problem") cfg.test_problem = getival(next_word(true));
             else if (word == "tl_eps_rel") cfg.tl_eps_rel = getrval(next_word(true));
             else if (word == "use_fused_solve") cfg.use_fused_solve = true;
+            else if (word == "tl_precision") {
+                std::string v = next_word(true);
+                if (v == "fp64") cfg.precision = TEA_PRECISION_FP64;
+                else if (v == "fp32") cfg.precision = TEA_PRECISION_FP32_REFINED;
+                else fail("read_input: tl_precision must be fp64 or fp32, not %s", v.c_str());
+            } else if (word == "tl_inner_tol") cfg.inner_tol = getrval(next_word(true));
+            else if (word == "tl_inner_max_iters") cfg.inner_max_iters = getival(next_word(true));
             else if (word == "state") {
                 int s = getival(next_word(true));
                 if (s < 1 || s > state_max) fail("read_input: bad state %d", s);
@@ -541,6 +551,9 @@ struct Runner {
             p.eps = eps;
             p.ch_cg_epslim = cfg.tl_ch_cg_epslim;
             p.eps_rel = cfg.tl_eps_rel;
+            p.precision = cfg.precision;
+            p.inner_max_iters = cfg.inner_max_iters;
+            p.inner_tol = cfg.inner_tol;
             tea_solve_result r;
             std::memset(&r, 0, sizeof(r));
             be.whole_solve(&chunk, &p, &r);
@@ -561,6 +574,7 @@ struct Runner {
             rec->cheby_steps = r.cheby_steps;
             rec->switch_step = r.switch_step;
             rec->est_itc = r.est_itc;
+            rec->corrections = r.corrections;
             return;
         }
 
@@ -814,6 +828,9 @@ extern "C" int tea_run_deck(const char* deck_text, const tea_run_options* option
         r.opt = options;
         r.cfg = parse_deck(deck_text ? deck_text : "", options->dim);
         if (options->use_fused_solve) r.cfg.use_fused_solve = true;
+        if (options->precision > 0) r.cfg.precision = options->precision;
+        if (r.cfg.precision != TEA_PRECISION_FP64 && !r.cfg.use_fused_solve)
+            fail("tl_precision fp32 needs the whole-solve path (use_fused_solve)");
         if (options->eps_override > 0.0) r.cfg.eps = options->eps_override;
         if (options->eps_rel_override > 0.0) r.cfg.tl_eps_rel = options->eps_rel_override;
         r.log.echo = !options->quiet;

@@ -26,7 +26,8 @@ typedef struct {
     double eps_override;     /* > 0: replace tl_eps */
     double eps_rel_override; /* > 0: replace tl_eps_rel */
     int keep_chunk;          /* 1: skip ext_finalise_ so the caller can inspect the fields */
-    int reserved[7];
+    int precision;           /* > 0: TEA_PRECISION_* for the whole-solve path (deck: tl_precision) */
+    int reserved[6];
 } tea_run_options;
 
 typedef struct {
@@ -48,6 +49,8 @@ typedef struct {
     double wall_end;         /* seconds since the start of the timestep loop, at the step's end */
     long long h2d_bytes;     /* backend host->device bytes so far (0 if not reported) */
     long long d2h_bytes;     /* backend device->host bytes so far */
+    int corrections;         /* FP32-refined solves: outer corrections */
+    int pad2;
 } tea_step_record;
 
 typedef struct {

@@ -163,7 +163,7 @@ def test_chebyshev_and_ppcg(pair, precond):
         pair.both(lambda ch: ch.call("ext_ppcg_inner_", I(k)))
         pair.check(f"ext_ppcg_inner_ {k}")
     for flag in (1, 0):
-        g, c = pair.both(lambda ch: ch.reduce("ext_calculate_2norm_", I(flag)))
+        g, c = pair.both(lambda ch: ch.norm2(flag))
         assert g == c
 
 
