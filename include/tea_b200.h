@@ -74,6 +74,23 @@ void tea_kernel_timing_(const int* chunk, const int* kernel, const int* reps, do
  * coefficients, scalars and results (the field arrays never leave the device). */
 int tea_transfer_bytes_(const int* chunk, long long* h2d, long long* d2h);
 
+/* Allocation-free 2-norm, for callers whose device memory belongs to their own pool
+ * allocator and who therefore cannot let a library call cudaMalloc (and who hold their
+ * fields in their own buffers, not in a chunk of this library).  No counterpart in the
+ * reference: it computes what ext_calculate_2norm_ computes (sum of v^2 over the inner
+ * domain, Calculate2Norm of tealeaf_2d/ext_solver_methods.hpp) on the caller's device
+ * array `field`, laid out as the reference lays out a chunk array (flat, x fastest,
+ * HALO_PAD = 2 on every side: (nx+4) x (ny+4) [x (nz+4)]; nz is ignored in 2D), and
+ * writes the result to the caller's device double `norm`, on `stream` (NULL: the legacy
+ * default stream); the call returns without waiting.  It allocates nothing: its
+ * reduction scratch is a static device array of 128 KB per GPU, held until the process
+ * exits, which limits one call to at most 16,777,216 inner cells (larger sizes return
+ * TEA_ERR_BAD_ARGUMENT with a message).  The first call on each device looks the array up
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race.  Returns a TEA_* status. */
+int tea_2norm_noalloc_(const double* field, const int* nx, const int* ny, const int* nz, double* norm,
+                       void* stream);
+
 /* Solver ids for the whole-solve entry point. */
 enum {
     TEA_SOLVER_JACOBI = 1,
