@@ -67,7 +67,8 @@ int tea_chunk_stream_(const int* chunk, void** stream);
 /* Measurement hook: `reps` back-to-back launches of one fused kernel of the whole-solve
  * path on the chunk's stream, between two CUDA events, on the chunk's current fields
  * (which it modifies).  kernel: 1 PPCG inner step, 2 CG/PPCG sweep A, 3 Chebyshev
- * iteration, 4 Jacobi sweep, 5 CG sweep B.  Writes the mean milliseconds per launch. */
+ * iteration, 4 Jacobi sweep, 5 CG sweep B, 6 two Chebyshev iterations in one pass (2D;
+ * in 3D the single iteration).  Writes the mean milliseconds per launch. */
 void tea_kernel_timing_(const int* chunk, const int* kernel, const int* reps, double* ms_per_launch);
 
 /* Host<->device bytes the library has moved for the chunk so far: state tables,

@@ -53,7 +53,9 @@ struct Fused {
     int cap = 0;  // entries of the coefficient arrays
     FusedArgs base{};
     int stencil_blocks = 0, point_blocks = 0, pair_blocks = 0;
-    int ring_blocks = 0;  // grid of k_ring2d; 0 selects the register-pipelined kernels
+    int ring_blocks = 0;  // grid of k_ring2d (2D)
+    int cheby2_blocks = 0;  // grid of k_cheby2_ring2d (2D); 0: one Chebyshev iteration per launch
+    int stencil_mode = 0;  // 0: the faster kernel per sweep, 1: register pipeline only, 2: ring only
     Loop loops[LOOP_COUNT];
     bool use_graph = true;
 };
@@ -91,12 +93,38 @@ int ring_occupancy()
 }
 #endif
 
+#if TEA_DIM == 2
+// Which 2D sweeps run the shared-memory ring by default (measured on B200 at 4096^2: the
+// ring is faster for CG sweep A and the Chebyshev iteration, the register pipeline for the
+// PPCG inner step and Jacobi).
+template <class Op>
+struct RingPreferred {
+    static constexpr bool value = false;
+};
+template <>
+struct RingPreferred<OpSweepA> {
+    static constexpr bool value = true;
+};
+template <>
+struct RingPreferred<OpCheby> {
+    static constexpr bool value = true;
+};
+template <>
+struct RingPreferred<OpSweepA32> {
+    static constexpr bool value = true;
+};
+template <>
+struct RingPreferred<OpOuterResid> {
+    static constexpr bool value = true;
+};
+#endif
+
 // Launch the streaming stencil kernel of Op over the inner domain.
 template <class Op>
 void stencil(const Fused* F, const FusedArgs& a, cudaStream_t s)
 {
 #if TEA_DIM == 2
-    if (F->ring_blocks > 0) {
+    if (F->stencil_mode == 2 || (F->stencil_mode == 0 && RingPreferred<Op>::value)) {
         k_ring2d<Op><<<F->ring_blocks, RWARPS * 32, ring_smem_bytes<Op>(), s>>>(a);
         return;
     }
@@ -170,8 +198,10 @@ Fused* ensure_fused(Chunk* c, int max_iters)
         F->stencil_blocks = std::max(F->stencil_blocks, 1);
 #if TEA_DIM == 2
         {
+            // TEA_B200_STENCIL=pipe|ring forces one kernel family for every sweep (A/B timing).
             const char* kind = getenv("TEA_B200_STENCIL");
-            if (kind && strcmp(kind, "ring") == 0) {
+            F->stencil_mode = !kind ? 0 : (strcmp(kind, "pipe") == 0 ? 1 : (strcmp(kind, "ring") == 0 ? 2 : 0));
+            if (F->stencil_mode != 1) {
                 int rocc = ring_occupancy<OpSweepA>();
                 rocc = std::min(rocc, ring_occupancy<OpCheby>());
                 rocc = std::min(rocc, ring_occupancy<OpPPCGInner<true>>());
@@ -184,6 +214,18 @@ Fused* ensure_fused(Chunk* c, int max_iters)
                 long blocks = std::min<long>((segs + RWARPS - 1) / RWARPS, (long)sms * rocc);
                 blocks = std::min<long>(blocks, c->red.max_blocks);
                 F->ring_blocks = (int)std::max<long>(blocks, 1);
+                const int c2_bytes = (int)cheby2_smem_bytes();
+                TEA_CK(cudaFuncSetAttribute(k_cheby2_ring2d, cudaFuncAttributeMaxDynamicSharedMemorySize, c2_bytes));
+                int c2occ = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c2occ, k_cheby2_ring2d, RWARPS * 32, c2_bytes) !=
+                        cudaSuccess ||
+                    c2occ < 1)
+                    c2occ = 1;
+                const long segs2 = (long)((g.nx + C2_OUT - 1) / C2_OUT) * ((g.ny + RSY - 1) / RSY);
+                long blocks2 = std::min<long>((segs2 + RWARPS - 1) / RWARPS, (long)sms * c2occ);
+                blocks2 = std::max<long>(blocks2, (long)F->ring_blocks);  // also runs single iterations
+                blocks2 = std::min<long>(blocks2, c->red.max_blocks);
+                F->cheby2_blocks = (int)std::max<long>(blocks2, 1);
             }
         }
 #endif
@@ -249,6 +291,12 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         k_cg_sweep_b<<<F->pair_blocks, 256, 0, s>>>(a);
         break;
     case LOOP_CHEBY:
+#if TEA_DIM == 2
+        if (F->cheby2_blocks > 0) {
+            k_cheby2_ring2d<<<F->cheby2_blocks, RWARPS * 32, cheby2_smem_bytes(), s>>>(a);
+            break;
+        }
+#endif
         stencil<OpCheby>(F, a, s);
         break;
     case LOOP_PPCG: {
@@ -639,6 +687,11 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
                     if (s.exit_reason == EXIT_CONVERGED || s.exit_reason == EXIT_MAXITER) break;
                     continue;
                 }
+                if (cheby) {
+                    // The Chebyshev loop may leave p in the second buffer; both start with the
+                    // same contents, so the halo (never written in this phase) agrees.
+                    TEA_CK(cudaMemcpyAsync(F->alt[1], c->alloc[F_P], bytes, cudaMemcpyDeviceToDevice, c->stream));
+                }
                 run_loop(c, F, cheby ? LOOP_CHEBY : LOOP_PPCG, P->ppcg_inner_steps);
             } else if (!p_halo_fresh) {
                 // A CG iteration in Chebyshev mode (the error rose above 1 after the switch):
@@ -703,10 +756,16 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
     a.step = 1;
     a.timing = 1;
     // Steady-state operands: sweep A applies a pending p and u update, as it does in every
-    // CG iteration after the first.
+    // CG iteration after the first; the Chebyshev kernels see an iteration that is neither
+    // a convergence check nor the last one.
     pull_state(c, F);
+    const SolveState saved = *F->h_st;
     F->h_st->pending_p = 1;
     F->h_st->pending_u = 1;
+    F->h_st->n = 1;
+    F->h_st->est_itc = 1 << 30;
+    F->h_st->max_iters = std::max(F->h_st->max_iters, 2);
+    F->h_st->cheby_calc_steps = 1;
     push_state(c, F);
     cudaEvent_t e0, e1;
     TEA_CK(cudaEventCreate(&e0));
@@ -717,6 +776,14 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
         case 2: stencil<OpSweepA>(F, a, c->stream); break;
         case 3: stencil<OpCheby>(F, a, c->stream); break;
         case 5: k_cg_sweep_b<<<F->pair_blocks, 256, 0, c->stream>>>(a); break;
+#if TEA_DIM == 2
+        case 6:
+            if (F->cheby2_blocks > 0)
+                k_cheby2_ring2d<<<F->cheby2_blocks, RWARPS * 32, cheby2_smem_bytes(), c->stream>>>(a);
+            else
+                stencil<OpCheby>(F, a, c->stream);
+            break;
+#endif
         default: stencil<OpJacobi>(F, a, c->stream); break;
         }
     };
@@ -730,8 +797,7 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
     *ms_per_launch = (double)ms / *reps;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    F->h_st->pending_p = 0;
-    F->h_st->pending_u = 0;
+    *F->h_st = saved;
     push_state(c, F);
     sync(c);
 }
