@@ -448,6 +448,42 @@ def reference_arm(args, rank, world):
     dist_done(world)
 
 
+# The other configurations' 3D workloads (seeded box/sphere layouts): timed through the
+# public driver (tea_run_deck: deck in, field summary out), plain FP64 and FP32-refined.
+WORKLOADS_3D = {
+    "3d256_cg": dict(cells=256, solver="cg", states=12, seed=256),
+    "3d256_ppcg": dict(cells=256, solver="ppcg", states=12, seed=256),
+    "3d512_ppcg": dict(cells=512, solver="ppcg", states=24, seed=512),
+}
+
+
+def workload_3d(args):
+    """--workload NAME: s/timestep of a 3D configuration, plain FP64 and FP32-refined, each
+    timestep's solve timed by the driver around the synchronous ext_tea_leaf_solve_ call."""
+    w = WORKLOADS_3D[args.workload]
+    spec = tea.DeckSpec(dim=3, cells=w["cells"], states=w["states"], seed=w["seed"], solver=w["solver"],
+                        end_step=args.warmup + args.steps, dt=0.004, eps=1e-15, eps_rel=EPS_REL, max_iters=20000,
+                        presteps=30, inner_steps=10, check_result=True, summary_frequency=0)
+    deck = tea.seeded_deck(spec)
+    out = {"workload": args.workload, "cells": w["cells"] ** 3, "solver": w["solver"], "unit": "s/timestep",
+           "timesteps_timed": list(range(args.warmup + 1, args.warmup + args.steps + 1))}
+    summaries = {}
+    for name, precision in (("fp64", tea.PRECISION_FP64), ("fp32_refined", tea.PRECISION_FP32_REFINED)):
+        summary, recs = tea.run_deck(deck, 3, fused=True, precision=precision, summary_every_step=True)
+        timed = recs[args.warmup:args.warmup + args.steps]
+        summaries[name] = summary
+        out[name] = {"s_per_step": sum(r["solve_seconds"] for r in timed) / len(timed),
+                     "iterations": [r["iterations"] for r in timed],
+                     "switch_step": [r["switch_step"] for r in timed],
+                     "cheby_steps": [r["cheby_steps"] for r in timed],
+                     "corrections": [r["corrections"] for r in timed],
+                     "exact_error_over_eps": [r["exact_error"] / r["eps_used"] for r in timed]}
+    out["speedup_fp32_refined"] = out["fp64"]["s_per_step"] / out["fp32_refined"]["s_per_step"]
+    out["field_summary_max_rel_diff"] = max(
+        tea.rel_diff(summaries["fp64"][k], summaries["fp32_refined"][k]) for k in ("vol", "mass", "ie", "temp"))
+    print(json.dumps(out))
+
+
 def kernel_only(args):
     """Set up the 4096^2 workload and launch one fused kernel 1 + reps times (no solve)."""
     lib = tea.cuda_library(2)
@@ -476,9 +512,14 @@ def main():
     ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS),
                     help="only launch one fused kernel --reps times on the 4096^2 workload (for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS_3D),
+                    help="time a 3D configuration instead (plain FP64 and FP32-refined, through the driver)")
     args = ap.parse_args()
     if args.kernel:
         kernel_only(args)
+        return
+    if args.workload:
+        workload_3d(args)
         return
     if args.warmup < 1:
         ap.error("--warmup must be >= 1")
@@ -545,7 +586,9 @@ def main():
         diff = max(tea.rel_diff(a, b) for a, b in zip(refined["summary"], g["summary"]))
         line["fp32_refined"] = {"value": refined["sec_per_step"], "unit": "s",
                                 "speedup_vs_fp64": g["sec_per_step"] / refined["sec_per_step"],
-                                "inner_iterations": refined["iterations"], "corrections": refined["corrections"],
+                                "iterations": refined["iterations"], "fp64_cg_steps": refined["cg_steps"],
+                                "fp32_chebyshev_steps": refined["cheby_steps"], "corrections": refined["corrections"],
+                                "exact_errors": refined["exact_errors"],
                                 "field_summary_max_rel_diff_vs_fp64": diff, "clocks": refined["clocks"]}
     if g["bad_status"]:
         line["status_warnings"] = g["bad_status"]

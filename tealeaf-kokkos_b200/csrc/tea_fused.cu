@@ -35,13 +35,18 @@ void update_halo(Chunk* c, const int* neighbours, const int* fields, int depth);
 
 namespace {
 
-enum { LOOP_CG = 0, LOOP_CHEBY = 1, LOOP_PPCG = 2, LOOP_JACOBI = 3, LOOP_CG32 = 4, LOOP_COUNT = 5 };
+enum { LOOP_CG = 0, LOOP_CHEBY = 1, LOOP_PPCG = 2, LOOP_JACOBI = 3, LOOP_CG32 = 4, LOOP_CHEBY32 = 5, LOOP_COUNT = 6 };
 
 struct Loop {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int key = -1;
 };
+
+struct RingLaunch {
+    int blocks = 0, rows = 0;
+};
+constexpr int RING_OPS = 9;
 
 struct Fused {
     SolveState* d_st = nullptr;
@@ -53,8 +58,9 @@ struct Fused {
     int cap = 0;  // entries of the coefficient arrays
     FusedArgs base{};
     int stencil_blocks = 0, point_blocks = 0, pair_blocks = 0;
-    int ring_blocks = 0;  // grid of k_ring2d (2D)
-    int cheby2_blocks = 0;  // grid of k_cheby2_ring2d (2D); 0: one Chebyshev iteration per launch
+    RingLaunch ring[RING_OPS];  // grid and segment rows of k_ring2d per sweep (2D)
+    RingLaunch pair;            // k_cheby2_ring2d<OpCheby> (2D); blocks 0: one iteration per launch
+    RingLaunch pair32;          // k_cheby2_ring2d<OpCheby32> (2D)
     int stencil_mode = 0;  // 0: the faster kernel per sweep, 1: register pipeline only, 2: ring only
     Loop loops[LOOP_COUNT];
     bool use_graph = true;
@@ -80,23 +86,82 @@ int occupancy(K kernel, int threads)
 }
 
 #if TEA_DIM == 2
-// Opt the ring kernel of Op into its dynamic shared memory; blocks per SM it then reaches.
-template <class Op>
-int ring_occupancy()
+// Opt a ring kernel into its dynamic shared memory; blocks per SM it then reaches.
+template <class K>
+int smem_occupancy(K kernel, int bytes)
 {
-    const int bytes = (int)ring_smem_bytes<Op>();
-    TEA_CK(cudaFuncSetAttribute(k_ring2d<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    TEA_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ring2d<Op>, RWARPS * 32, bytes) != cudaSuccess || n < 1)
-        n = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, RWARPS * 32, bytes) != cudaSuccess || n < 1) n = 1;
     return n;
+}
+
+// One wave: every resident warp gets one segment of a strip `strip` columns wide, the
+// segment length chosen so that the strips' segments fill the resident warps.
+RingLaunch ring_launch(const Geom& g, int sms, int occ, int strip, int max_blocks)
+{
+    const long warps = (long)sms * occ * RWARPS;
+    const long per_x = (g.nx + strip - 1) / strip;
+    long per_y = std::max<long>(1, warps / per_x);
+    RingLaunch L;
+    L.rows = (int)std::max<long>(8, (g.ny + per_y - 1) / per_y);
+    per_y = (g.ny + L.rows - 1) / L.rows;
+    long blocks = std::min<long>((per_x * per_y + RWARPS - 1) / RWARPS, (long)sms * occ);
+    L.blocks = (int)std::max<long>(1, std::min<long>(blocks, max_blocks));
+    return L;
+}
+
+template <class Op>
+struct RingId;
+template <>
+struct RingId<OpSweepA> {
+    static constexpr int value = 0;
+};
+template <>
+struct RingId<OpCheby> {
+    static constexpr int value = 1;
+};
+template <>
+struct RingId<OpPPCGInner<false>> {
+    static constexpr int value = 2;
+};
+template <>
+struct RingId<OpPPCGInner<true>> {
+    static constexpr int value = 3;
+};
+template <>
+struct RingId<OpJacobi> {
+    static constexpr int value = 4;
+};
+template <>
+struct RingId<OpJacobiResidual> {
+    static constexpr int value = 5;
+};
+template <>
+struct RingId<OpSweepA32> {
+    static constexpr int value = 6;
+};
+template <>
+struct RingId<OpOuterResid> {
+    static constexpr int value = 7;
+};
+template <>
+struct RingId<OpCheby32> {
+    static constexpr int value = 8;
+};
+
+template <class Op>
+void setup_ring(Fused* F, const Geom& g, int sms, int max_blocks)
+{
+    const int occ = smem_occupancy(k_ring2d<Op>, (int)ring_smem_bytes<Op>());
+    F->ring[RingId<Op>::value] = ring_launch(g, sms, occ, 64, max_blocks);
 }
 #endif
 
 #if TEA_DIM == 2
 // Which 2D sweeps run the shared-memory ring by default (measured on B200 at 4096^2: the
-// ring is faster for CG sweep A and the Chebyshev iteration, the register pipeline for the
-// PPCG inner step and Jacobi).
+// ring is faster for CG sweep A, the Chebyshev iteration and Jacobi, the register pipeline
+// for the PPCG inner step).
 template <class Op>
 struct RingPreferred {
     static constexpr bool value = false;
@@ -117,6 +182,18 @@ template <>
 struct RingPreferred<OpOuterResid> {
     static constexpr bool value = true;
 };
+template <>
+struct RingPreferred<OpCheby32> {
+    static constexpr bool value = true;
+};
+template <>
+struct RingPreferred<OpJacobi> {
+    static constexpr bool value = true;
+};
+template <>
+struct RingPreferred<OpJacobiResidual> {
+    static constexpr bool value = true;
+};
 #endif
 
 // Launch the streaming stencil kernel of Op over the inner domain.
@@ -125,7 +202,10 @@ void stencil(const Fused* F, const FusedArgs& a, cudaStream_t s)
 {
 #if TEA_DIM == 2
     if (F->stencil_mode == 2 || (F->stencil_mode == 0 && RingPreferred<Op>::value)) {
-        k_ring2d<Op><<<F->ring_blocks, RWARPS * 32, ring_smem_bytes<Op>(), s>>>(a);
+        const RingLaunch& L = F->ring[RingId<Op>::value];
+        FusedArgs ar = a;
+        ar.seg_rows = L.rows;
+        k_ring2d<Op><<<L.blocks, RWARPS * 32, ring_smem_bytes<Op>(), s>>>(ar);
         return;
     }
 #endif
@@ -169,6 +249,7 @@ Fused* ensure_fused(Chunk* c, int max_iters)
         a.use_handle = 0;
         a.step = 0;
         a.timing = 0;
+        a.seg_rows = 64;  // every ring launch sets its own
         int sms = 148;
         TEA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
         if (DIM == 2) {
@@ -193,6 +274,7 @@ Fused* ensure_fused(Chunk* c, int max_iters)
         occ = std::min(occ, occupancy(TEA_STENCIL<OpJacobi>, nthr));
         occ = std::min(occ, occupancy(TEA_STENCIL<OpSweepA32>, nthr));
         occ = std::min(occ, occupancy(TEA_STENCIL<OpOuterResid>, nthr));
+        occ = std::min(occ, occupancy(TEA_STENCIL<OpCheby32>, nthr));
         F->stencil_blocks = (int)std::min<long>(a.ntiles, (long)sms * occ);
         F->stencil_blocks = std::min(F->stencil_blocks, c->red.max_blocks);
         F->stencil_blocks = std::max(F->stencil_blocks, 1);
@@ -202,30 +284,21 @@ Fused* ensure_fused(Chunk* c, int max_iters)
             const char* kind = getenv("TEA_B200_STENCIL");
             F->stencil_mode = !kind ? 0 : (strcmp(kind, "pipe") == 0 ? 1 : (strcmp(kind, "ring") == 0 ? 2 : 0));
             if (F->stencil_mode != 1) {
-                int rocc = ring_occupancy<OpSweepA>();
-                rocc = std::min(rocc, ring_occupancy<OpCheby>());
-                rocc = std::min(rocc, ring_occupancy<OpPPCGInner<true>>());
-                rocc = std::min(rocc, ring_occupancy<OpPPCGInner<false>>());
-                rocc = std::min(rocc, ring_occupancy<OpJacobi>());
-                rocc = std::min(rocc, ring_occupancy<OpJacobiResidual>());
-                rocc = std::min(rocc, ring_occupancy<OpSweepA32>());
-                rocc = std::min(rocc, ring_occupancy<OpOuterResid>());
-                const long segs = (long)((g.nx + 63) / 64) * ((g.ny + RSY - 1) / RSY);
-                long blocks = std::min<long>((segs + RWARPS - 1) / RWARPS, (long)sms * rocc);
-                blocks = std::min<long>(blocks, c->red.max_blocks);
-                F->ring_blocks = (int)std::max<long>(blocks, 1);
-                const int c2_bytes = (int)cheby2_smem_bytes();
-                TEA_CK(cudaFuncSetAttribute(k_cheby2_ring2d, cudaFuncAttributeMaxDynamicSharedMemorySize, c2_bytes));
-                int c2occ = 0;
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c2occ, k_cheby2_ring2d, RWARPS * 32, c2_bytes) !=
-                        cudaSuccess ||
-                    c2occ < 1)
-                    c2occ = 1;
-                const long segs2 = (long)((g.nx + C2_OUT - 1) / C2_OUT) * ((g.ny + RSY - 1) / RSY);
-                long blocks2 = std::min<long>((segs2 + RWARPS - 1) / RWARPS, (long)sms * c2occ);
-                blocks2 = std::max<long>(blocks2, (long)F->ring_blocks);  // also runs single iterations
-                blocks2 = std::min<long>(blocks2, c->red.max_blocks);
-                F->cheby2_blocks = (int)std::max<long>(blocks2, 1);
+                const int mb = c->red.max_blocks;
+                setup_ring<OpSweepA>(F, g, sms, mb);
+                setup_ring<OpCheby>(F, g, sms, mb);
+                setup_ring<OpPPCGInner<false>>(F, g, sms, mb);
+                setup_ring<OpPPCGInner<true>>(F, g, sms, mb);
+                setup_ring<OpJacobi>(F, g, sms, mb);
+                setup_ring<OpJacobiResidual>(F, g, sms, mb);
+                setup_ring<OpSweepA32>(F, g, sms, mb);
+                setup_ring<OpOuterResid>(F, g, sms, mb);
+                setup_ring<OpCheby32>(F, g, sms, mb);
+                const int occ2 = smem_occupancy(k_cheby2_ring2d<OpCheby>, (int)cheby2_smem_bytes<OpCheby>());
+                F->pair = ring_launch(g, sms, occ2, C2_OUT, mb);
+                const int occ3 =
+                    smem_occupancy(k_cheby2_ring2d<OpCheby32>, (int)cheby2_smem_bytes<OpCheby32>());
+                F->pair32 = ring_launch(g, sms, occ3, C2_OUT, mb);
             }
         }
 #endif
@@ -277,6 +350,8 @@ bool ensure_fp32(Chunk* c, Fused* F)
     a.d32 = F->alloc32[5] + kLeadPad;
     a.p32[0] = F->alloc32[6] + kLeadPad;
     a.p32[1] = F->alloc32[7] + kLeadPad;
+    a.dc32[0] = a.d32;
+    a.dc32[1] = a.w32;
     return true;
 }
 
@@ -292,12 +367,26 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         break;
     case LOOP_CHEBY:
 #if TEA_DIM == 2
-        if (F->cheby2_blocks > 0) {
-            k_cheby2_ring2d<<<F->cheby2_blocks, RWARPS * 32, cheby2_smem_bytes(), s>>>(a);
+        if (F->pair.blocks > 0) {
+            FusedArgs ap = a;
+            ap.seg_rows = F->pair.rows;
+            k_cheby2_ring2d<OpCheby><<<F->pair.blocks, RWARPS * 32, cheby2_smem_bytes<OpCheby>(), s>>>(ap);
             break;
         }
 #endif
         stencil<OpCheby>(F, a, s);
+        break;
+    case LOOP_CHEBY32:
+#if TEA_DIM == 2
+        if (F->pair32.blocks > 0) {
+            FusedArgs ap = a;
+            ap.seg_rows = F->pair32.rows;
+            k_cheby2_ring2d<OpCheby32>
+                <<<F->pair32.blocks, RWARPS * 32, cheby2_smem_bytes<OpCheby32>(), s>>>(ap);
+            break;
+        }
+#endif
+        stencil<OpCheby32>(F, a, s);
         break;
     case LOOP_PPCG: {
         stencil<OpSweepA>(F, a, s);
@@ -556,7 +645,12 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
 
     int corrections = 0;
     if (P->precision == TEA_PRECISION_FP32_REFINED) {
-        // Defect correction: FP64 outer residual and update, FP32 inner CG.
+        // Defect correction: FP64 outer residual, update and convergence test; FP32 inner
+        // solves.  CG and Jacobi decks: every inner solve is CG.  Chebyshev and PPCG decks:
+        // the first inner solve is CG, whose scalars give the Lanczos eigenvalue bounds
+        // (computed in FP64 on the host), and the following ones are Chebyshev -- the
+        // plain solve's CG-then-Chebyshev order, with the spectrum taken from a CG run
+        // long enough to resolve it.
         if (!ensure_fp32(c, F)) {
             R->status = TEA_ERR_CUDA;
             return;
@@ -564,9 +658,12 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
         FusedArgs a = F->base;
         k_coef_to_fp32<<<c->grid_blocks, 256, 0, c->stream>>>(a);
         const double tol = P->inner_tol > 0.0 ? P->inner_tol : 1e-4;
-        int total_inner = 0;
-        s.error = 0.0;
-        for (int guard = 0; guard < P->max_iters + 2; ++guard) {
+        // Chebyshev decks: the first correction's inner CG also estimates the spectrum.
+        const bool want_cheby = cheby || ppcg;
+        bool inner_cheby = false;
+        int total_inner = 0, presteps_done = 0, cg_inner = 0;
+        bool converged = false;
+        for (int guard = 0; !converged && guard < P->max_iters + 2; ++guard) {
             if (status_store().status == TEA_ERR_CUDA) break;
             push_state(c, F);
             stencil<OpOuterResid>(F, a, c->stream);
@@ -575,25 +672,73 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
                 s.exit_reason = EXIT_CONVERGED;
                 break;
             }
-            if (total_inner >= P->max_iters) {
+            const int used = presteps_done + total_inner;
+            if (used >= P->max_iters) {
                 s.exit_reason = EXIT_MAXITER;
                 break;
             }
-            const int remaining = P->max_iters - total_inner;
+            const int remaining = P->max_iters - used;
             s.inner_max = P->inner_max_iters > 0 ? std::min(P->inner_max_iters, remaining) : remaining;
             s.tol2 = tol * tol * s.rro;
-            s.n_inner = 0;
+            s.n_inner = inner_cheby ? 1 : 0;
             s.cont = 1;
-            run_loop(c, F, LOOP_CG32, 0);
+            s.inner_diverged = 0;
+            run_loop(c, F, inner_cheby ? LOOP_CHEBY32 : LOOP_CG32, 0);
             total_inner += s.n_inner;
+            if (!inner_cheby) cg_inner += s.n_inner;
+            if (s.inner_diverged) {
+                // The estimated spectrum missed part of it: drop this correction and solve
+                // the remaining ones with CG.
+                inner_cheby = false;
+                s.inner_cheby = 0;
+                continue;
+            }
             k_dc_update<<<F->pair_blocks, 256, 0, c->stream>>>(a);
             s.pending_p = 0;
             s.pending_u = 0;
             ++corrections;
+            if (want_cheby && corrections == 1 && s.n_inner >= 2) {
+                // Lanczos estimate (FP64, host) from the inner CG's scalars; the bounds are
+                // widened by 0.95 / 1.05 as the reference widens its own.
+                const int n = s.n_inner;
+                std::vector<double> ca(n + 1, 0.0), cb(n + 1, 0.0);
+                TEA_CK(cudaMemcpyAsync(ca.data(), F->d_cg_alphas, sizeof(double) * (n + 1), cudaMemcpyDeviceToHost,
+                                       c->stream));
+                TEA_CK(cudaMemcpyAsync(cb.data(), F->d_cg_betas, sizeof(double) * (n + 1), cudaMemcpyDeviceToHost,
+                                       c->stream));
+                sync(c);
+                c->d2h_bytes += 2 * sizeof(double) * (long long)(n + 1);
+                if (tea_tridiag_extremes(ca.data() + 1, cb.data() + 1, n, &eigmin, &eigmax) == 0 && eigmin > 0.0 &&
+                    eigmax > eigmin) {
+                    eigmin = eigmin * kEigMinScale;
+                    eigmax = eigmax * kEigMaxScale;
+                    const int ncoef = std::min(P->max_iters + 1, F->cap);
+                    std::vector<double> ch_a(ncoef, 0.0), ch_b(ncoef, 0.0);
+                    double theta = 0.0;
+                    tea_calc_ch_coefs(ch_a.data(), ch_b.data(), eigmin, eigmax, &theta, ncoef);
+                    TEA_CK(cudaMemcpyAsync(F->d_ch_alphas, ch_a.data(), sizeof(double) * ncoef,
+                                           cudaMemcpyHostToDevice, c->stream));
+                    TEA_CK(cudaMemcpyAsync(F->d_ch_betas, ch_b.data(), sizeof(double) * ncoef, cudaMemcpyHostToDevice,
+                                           c->stream));
+                    c->h2d_bytes += 2 * sizeof(double) * (long long)ncoef;
+                    const double rk = std::sqrt(eigmax / eigmin);
+                    const double rho = (rk - 1.0) / (rk + 1.0);
+                    s.theta = theta;
+                    s.cheby_rho2 = rho * rho;
+                    s.inner_cheby = 1;
+                    inner_cheby = true;
+                    switch_step = n + 1;
+                }
+            }
         }
-        s.n = total_inner + 1;
+        if (converged) s.exit_reason = EXIT_CONVERGED;
+        cg_steps = presteps_done + cg_inner;
+        s.cheby_calc_steps = total_inner - cg_inner + 1;
+        s.n = presteps_done + total_inner + 1;
         s.pending_p = s.pending_u = 0;
         s.par_p = 0;
+        s.par_u = 0;
+        s.inner_cheby = 0;
         push_state(c, F);
     } else if (!cg_like) {
         run_loop(c, F, LOOP_JACOBI, 0);
@@ -731,7 +876,7 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
     sync(c);
     R->iterations = s.n - 1;
     R->status = status_store().status;
-    R->cg_steps = switch_step ? cg_steps : s.n - 1;
+    R->cg_steps = (switch_step || P->precision == TEA_PRECISION_FP32_REFINED) ? cg_steps : s.n - 1;
     R->cheby_steps = s.cheby_calc_steps > 0 ? s.cheby_calc_steps - 1 : 0;
     R->switch_step = switch_step;
     R->est_itc = s.est_itc;
@@ -778,10 +923,13 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
         case 5: k_cg_sweep_b<<<F->pair_blocks, 256, 0, c->stream>>>(a); break;
 #if TEA_DIM == 2
         case 6:
-            if (F->cheby2_blocks > 0)
-                k_cheby2_ring2d<<<F->cheby2_blocks, RWARPS * 32, cheby2_smem_bytes(), c->stream>>>(a);
-            else
+            if (F->pair.blocks > 0) {
+                FusedArgs ap = a;
+                ap.seg_rows = F->pair.rows;
+                k_cheby2_ring2d<OpCheby><<<F->pair.blocks, RWARPS * 32, cheby2_smem_bytes<OpCheby>(), c->stream>>>(ap);
+            } else {
                 stencil<OpCheby>(F, a, c->stream);
+            }
             break;
 #endif
         default: stencil<OpJacobi>(F, a, c->stream); break;

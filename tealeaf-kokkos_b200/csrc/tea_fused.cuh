@@ -44,6 +44,9 @@ struct SolveState {
     int nonfinite;
     // FP32 inner solve of the defect-correction form.
     int n_inner, inner_max;
+    int inner_cheby;     // the inner solve is Chebyshev (else CG)
+    int inner_diverged;  // the inner Chebyshev residual stalled or grew (bounds too narrow)
+    double cheby_rho2;   // squared Chebyshev contraction per iteration for the bounds in use
     double tol2;
 };
 
@@ -62,10 +65,12 @@ struct FusedArgs {
     int tiles_x, tiles_y, zseg;
     long ntiles;
     int step;    // PPCG inner step (1-based) of this launch
+    int seg_rows;  // rows per warp segment of the 2D ring kernels (set per launch)
     int timing;  // measurement launches: the last block leaves the solve state untouched
     // FP32 arrays of the defect-correction form (same pitched layout, float elements).
     float *kx32, *ky32, *kz32, *r32, *w32, *d32;
     float* p32[2];
+    float* dc32[2];  // iterate of the inner Chebyshev solve (ping-pong over d32, w32)
 };
 
 
@@ -409,17 +414,25 @@ __global__ void __launch_bounds__(P3BLOCK, 2) k_pipe3d(FusedArgs a)
 
 // 2D streaming through a per-warp shared-memory ring filled by cp.async.  Each warp owns a
 // strip of 64 columns (two adjacent cells per lane, 16-byte copies for FP64) and marches
-// down a segment of RSY rows; the rows of every input array are copied asynchronously
+// down a segment of a.seg_rows rows; the rows of every input array are copied asynchronously
 // RP rows ahead of the row being computed, so the data in flight lives in shared memory,
 // not in registers.  A ring row holds columns c0-1 .. c0+64 (the outer two for the
 // x-neighbours of the strip's edge cells).  Rows and columns outside the inner domain are
 // copied from their reflected interior cell; within the strip the right-hand boundary is
 // reflected when the operand is read.  No block barrier: warps are independent.
-constexpr int RP = 3;          // rows in flight beyond row j+1
+#ifndef TEA_RING_RP
+#define TEA_RING_RP 3
+#endif
+#ifndef TEA_RING_WARPS
+#define TEA_RING_WARPS 4
+#endif
+#ifndef TEA_CHEBY2_RP
+#define TEA_CHEBY2_RP 3
+#endif
+constexpr int RP = TEA_RING_RP;  // rows in flight beyond row j+1
 constexpr int RQ = RP + 2;     // ring rows per warp
 constexpr int RW = 68;         // elements per ring row: pad, c0-1, c0..c0+63, c0+64, pad
-constexpr int RWARPS = 4;      // warps per block
-constexpr int RSY = 64;        // rows per segment
+constexpr int RWARPS = TEA_RING_WARPS;  // warps per block
 
 __device__ __forceinline__ void cp_async_16(void* dst, const void* src)
 {
@@ -486,7 +499,7 @@ __device__ __forceinline__ void ring2d_body(const FusedArgs& a, Op& op, unsigned
     const int xlast = g.X - HALO_PAD - 1;
     const int ylast = g.Y - HALO_PAD - 1;
     const int per_x = (g.nx + 63) / 64;
-    const int per_y = (g.ny + RSY - 1) / RSY;
+    const int per_y = (g.ny + a.seg_rows - 1) / a.seg_rows;
     const long nseg = (long)per_x * per_y;
     const long gw = (long)blockIdx.x * RWARPS + warp, nw = (long)gridDim.x * RWARPS;
     const int cmax = (int)g.pitch - 2;  // last even column whose pair stays inside the row
@@ -495,8 +508,8 @@ __device__ __forceinline__ void ring2d_body(const FusedArgs& a, Op& op, unsigned
         const int c0 = HALO_PAD + 64 * xs;
         const int c = c0 + 2 * lane;
         const int cc = min(c, cmax);
-        const int j0 = HALO_PAD + RSY * ys;
-        const int j1 = min(j0 + RSY, ylast + 1);
+        const int j0 = HALO_PAD + a.seg_rows * ys;
+        const int j1 = min(j0 + a.seg_rows, ylast + 1);
         const int left = refl(c0 - 1, g.X);
         const int right_op = refl(min(c0 + 64, xlast + 1), g.X);
         const int right_k = min(c0 + 64, xlast + 1);
@@ -950,6 +963,7 @@ struct OpCheby {
     const double* ucur;
     double* unew;
     double* pcur;  // p is updated in place (pointwise); the two-iteration kernel ping-pongs it
+    double* pnext;
     double al, be;
     int precond, check;
     __device__ bool skip(const FusedArgs&) { return false; }
@@ -959,6 +973,7 @@ struct OpCheby {
         ucur = a.u[s.par_u];
         unew = a.u[s.par_u ^ 1];
         pcur = a.p[s.par_p];
+        pnext = a.p[s.par_p ^ 1];
         const int step = s.cheby_calc_steps - 1;
         al = a.ch_alphas[step];
         be = a.ch_betas[step];
@@ -1026,6 +1041,34 @@ struct OpCheby {
         s.cheby_calc_steps = s.cheby_calc_steps + 1;
         end_iteration(a, s, PHASE_CHEBY);
     }
+    // Two-iteration kernel (k_cheby2_ring2d): a pair runs unless the first iteration is a
+    // convergence check (which must end a launch) or the last one max_iters allows.
+    __device__ bool pair_ok(const FusedArgs& a) const
+    {
+        const SolveState& st = *a.st;
+        return !((st.n >= st.est_itc) && (st.n % 10 == 0)) && st.n + 1 <= st.max_iters;
+    }
+    __device__ void pair_coefs(const FusedArgs& a, double& al2, double& be2, bool& check2) const
+    {
+        const SolveState& st = *a.st;
+        al2 = a.ch_alphas[st.cheby_calc_steps];
+        be2 = a.ch_betas[st.cheby_calc_steps];
+        check2 = (st.n + 1 >= st.est_itc) && ((st.n + 1) % 10 == 0);
+    }
+    __device__ const double* pair_rhs(const FusedArgs& a) const { return a.u0; }
+    __device__ const double* pair_mi(const FusedArgs& a) const { return precond ? a.mi : nullptr; }
+    __device__ void pair_control(const FusedArgs& a, const double* v, bool check2) const
+    {
+        if (a.timing) return;
+        SolveState& s = *a.st;
+        s.par_u ^= 1;
+        s.par_p ^= 1;
+        s.cheby_calc_steps = s.cheby_calc_steps + 1;
+        end_iteration(a, s, PHASE_CHEBY);  // cannot end the loop (pair_ok)
+        if (check2) s.error = v[0];
+        s.cheby_calc_steps = s.cheby_calc_steps + 1;
+        end_iteration(a, s, PHASE_CHEBY);
+    }
 };
 
 #if TEA_DIM == 2
@@ -1047,75 +1090,88 @@ struct OpCheby {
 // A pair runs only when its first iteration is not a convergence check (which must end a
 // launch) and the second stays within max_iters; otherwise the launch is one ordinary
 // iteration.  Either way the decision is read from the solve state, uniformly.
-constexpr int C2_RP = 3;               // ring rows in flight beyond row t+1
+constexpr int C2_RP = TEA_CHEBY2_RP;   // ring rows in flight beyond row t+1
 constexpr int C2_RQ = C2_RP + 3;       // ring rows per warp: t-1 .. t+1+C2_RP
 constexpr int C2_NA = 6;               // u, u0, p, mi, Kx, Ky
 constexpr int C2_OUT = 60;             // columns written per warp strip
 enum { C2_U = 0, C2_U0 = 1, C2_P = 2, C2_MI = 3, C2_KX = 4, C2_KY = 5 };
 
+template <class Op>
 constexpr size_t cheby2_smem_bytes()
 {
-    return (size_t)RWARPS * C2_RQ * C2_NA * 64 * sizeof(double) > ring_smem_bytes<OpCheby>()
-        ? (size_t)RWARPS * C2_RQ * C2_NA * 64 * sizeof(double)
-        : ring_smem_bytes<OpCheby>();
+    return (size_t)RWARPS * C2_RQ * C2_NA * 64 * sizeof(typename Op::T) > ring_smem_bytes<Op>()
+        ? (size_t)RWARPS * C2_RQ * C2_NA * 64 * sizeof(typename Op::T)
+        : ring_smem_bytes<Op>();
 }
 
-__device__ __forceinline__ bool cheby_check_step(const SolveState& s, int n)
+template <class T>
+__device__ __forceinline__ void st_pair(T* p, T x, T y);
+template <>
+__device__ __forceinline__ void st_pair<double>(double* p, double x, double y)
 {
-    return (n >= s.est_itc) && (n % 10 == 0);
+    *reinterpret_cast<double2*>(p) = make_double2(x, y);
+}
+template <>
+__device__ __forceinline__ void st_pair<float>(float* p, float x, float y)
+{
+    *reinterpret_cast<float2*>(p) = make_float2(x, y);
 }
 
+// Op: OpCheby (FP64, the reference's iteration) or OpCheby32 (the FP32 inner solve).
+template <class Op>
 __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
 {
+    using T = typename Op::T;
     extern __shared__ __align__(16) unsigned char s_ring_raw[];
-    OpCheby op;
+    Op op;
     op.begin(a);
-    const SolveState& st = *a.st;
-    const int n = st.n;
-    if (cheby_check_step(st, n) || n + 1 > st.max_iters) {
+    if (!op.pair_ok(a)) {
         ring2d_body(a, op, s_ring_raw);
         return;
     }
-    const double al1 = op.al, be1 = op.be;
-    const double al2 = a.ch_alphas[st.cheby_calc_steps], be2 = a.ch_betas[st.cheby_calc_steps];
-    const bool check2 = cheby_check_step(st, n + 1);
-    const bool precond = op.precond != 0;
-    const double* ucur = op.ucur;
-    double* unew = op.unew;
-    double* pnew = a.p[st.par_p ^ 1];
+    const T al1 = op.al, be1 = op.be;
+    T al2, be2;
+    bool check2;
+    op.pair_coefs(a, al2, be2, check2);
+    const T* mi = op.pair_mi(a);
+    const bool precond = mi != nullptr;
+    const T* ucur = op.ucur;
+    T* unew = op.unew;
+    T* pnew = op.pnext;
     const Geom& g = a.g;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    double* ring = reinterpret_cast<double*>(s_ring_raw) + (size_t)warp * C2_RQ * C2_NA * 64;
-    const double* src[C2_NA] = {ucur, a.u0, op.pcur, precond ? a.mi : nullptr, a.kx, a.ky};
+    T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * C2_RQ * C2_NA * 64;
+    const T* src[C2_NA] = {ucur, op.pair_rhs(a), op.pcur, mi, op.coef_x(a), op.coef_y(a)};
     DDVec<1> acc;
     acc.zero();
     const int xlast = g.X - HALO_PAD - 1;
     const int ylast = g.Y - HALO_PAD - 1;
     const int per_x = (g.nx + C2_OUT - 1) / C2_OUT;
-    const int per_y = (g.ny + RSY - 1) / RSY;
+    const int per_y = (g.ny + a.seg_rows - 1) / a.seg_rows;
     const long nseg = (long)per_x * per_y;
     const long gw = (long)blockIdx.x * RWARPS + warp, nw = (long)gridDim.x * RWARPS;
     const int cmax = (int)g.pitch - 2;
     const bool out_lane = lane >= 1 && lane <= 30;
+    const T zero = (T)0;
     for (long sgi = gw; sgi < nseg; sgi += nw) {
         const int xs = (int)(sgi % per_x), ys = (int)(sgi / per_x);
         const int c = C2_OUT * xs + 2 * lane;  // the lane's first column (lane 1 of strip 0: column 2)
         const int cc = min(c, cmax);
-        const int j0 = HALO_PAD + RSY * ys;
-        const int j1 = min(j0 + RSY, ylast + 1);
+        const int j0 = HALO_PAD + a.seg_rows * ys;
+        const int j1 = min(j0 + a.seg_rows, ylast + 1);
         const int a0 = j0 == HALO_PAD ? HALO_PAD : j0 - 1;  // first row of iteration 1
         const int rlast = min(j1 + 1, ylast + 1);             // last ring row
         auto slot = [&](int r) { return ring + (size_t)((r - a0 + 1) % C2_RQ) * C2_NA * 64; };
         auto issue = [&](int r) {
             if (r <= rlast) {
-                double* base = slot(r);
+                T* base = slot(r);
                 const int urow = refl(r, g.Y);
                 const int irow = min(max(r, HALO_PAD), ylast + 1);
 #pragma unroll
                 for (int k = 0; k < C2_NA; ++k) {
                     if (!src[k]) continue;
-                    cp_async_16(base + k * 64 + 2 * lane, src[k] + fidx(g, cc, k == C2_U ? urow : irow, 0));
+                    ring_copy_pair(base + k * 64 + 2 * lane, src[k] + fidx(g, cc, k == C2_U ? urow : irow, 0));
                 }
             }
             cp_async_commit();
@@ -1124,40 +1180,40 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
         cp_async_wait<C2_RP + 1>();
         __syncwarp();
         // u at rows t-1 (m) and t (c); iteration-1 u at rows t-2 (vm) and t-1 (vc); its p at t-1 (q).
-        double um0, um1, uc0, uc1;
+        T um0, um1, uc0, uc1;
         {
-            const double* b = slot(a0 - 1) + C2_U * 64 + 2 * lane;
+            const T* b = slot(a0 - 1) + C2_U * 64 + 2 * lane;
             um0 = b[0];
             um1 = b[1];
-            const double* d = slot(a0) + C2_U * 64 + 2 * lane;
+            const T* d = slot(a0) + C2_U * 64 + 2 * lane;
             uc0 = d[0];
             uc1 = d[1];
         }
-        double vm0 = 0.0, vm1 = 0.0, vc0 = 0.0, vc1 = 0.0, q0 = 0.0, q1 = 0.0;
+        T vm0 = zero, vm1 = zero, vc0 = zero, vc1 = zero, q0 = zero, q1 = zero;
         for (int t = a0; t <= j1; ++t) {
             cp_async_wait<C2_RP>();
             __syncwarp();
-            const double* rp = slot(t - 1);
-            const double* rc = slot(t);
-            const double* rn = slot(t + 1);
-            double un0 = rn[C2_U * 64 + 2 * lane], un1 = rn[C2_U * 64 + 2 * lane + 1];
+            const T* rp = slot(t - 1);
+            const T* rc = slot(t);
+            const T* rn = slot(t + 1);
+            const T un0 = rn[C2_U * 64 + 2 * lane], un1 = rn[C2_U * 64 + 2 * lane + 1];
             // Iteration 1 at row t.
-            double v0, v1, p0, p1;
+            T v0, v1, p0, p1;
             if (t <= ylast) {
-                const double kx0 = rc[C2_KX * 64 + 2 * lane], kx1 = rc[C2_KX * 64 + 2 * lane + 1];
-                const double kx2 = __shfl_down_sync(0xffffffffu, kx0, 1);
-                const double up = __shfl_up_sync(0xffffffffu, uc1, 1);
-                const double dn = __shfl_down_sync(0xffffffffu, uc0, 1);
-                NbT<double> nb;
-                nb.zm = nb.zp = 0.0;
+                const T kx0 = rc[C2_KX * 64 + 2 * lane], kx1 = rc[C2_KX * 64 + 2 * lane + 1];
+                const T kx2 = __shfl_down_sync(0xffffffffu, kx0, 1);
+                const T up = __shfl_up_sync(0xffffffffu, uc1, 1);
+                const T dn = __shfl_down_sync(0xffffffffu, uc0, 1);
+                NbT<T> nb;
+                nb.zm = nb.zp = zero;
                 nb.c = uc0;
                 nb.xm = c == HALO_PAD ? uc0 : up;
                 nb.xp = c == xlast ? uc0 : uc1;
                 nb.ym = um0;
                 nb.yp = un0;
                 {
-                    const double w = smvp_k(nb, kx0, kx1, rc[C2_KY * 64 + 2 * lane], rn[C2_KY * 64 + 2 * lane], 0.0, 0.0);
-                    const double r = rc[C2_U0 * 64 + 2 * lane] - w;
+                    const T w = smvp_k(nb, kx0, kx1, rc[C2_KY * 64 + 2 * lane], rn[C2_KY * 64 + 2 * lane], zero, zero);
+                    const T r = rc[C2_U0 * 64 + 2 * lane] - w;
                     p0 = al1 * rc[C2_P * 64 + 2 * lane] + be1 * (precond ? rc[C2_MI * 64 + 2 * lane] * r : r);
                     v0 = uc0 + p0;
                 }
@@ -1167,9 +1223,9 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
                 nb.ym = um1;
                 nb.yp = un1;
                 {
-                    const double w =
-                        smvp_k(nb, kx1, kx2, rc[C2_KY * 64 + 2 * lane + 1], rn[C2_KY * 64 + 2 * lane + 1], 0.0, 0.0);
-                    const double r = rc[C2_U0 * 64 + 2 * lane + 1] - w;
+                    const T w =
+                        smvp_k(nb, kx1, kx2, rc[C2_KY * 64 + 2 * lane + 1], rn[C2_KY * 64 + 2 * lane + 1], zero, zero);
+                    const T r = rc[C2_U0 * 64 + 2 * lane + 1] - w;
                     p1 = al1 * rc[C2_P * 64 + 2 * lane + 1] + be1 * (precond ? rc[C2_MI * 64 + 2 * lane + 1] * r : r);
                     v1 = uc1 + p1;
                 }
@@ -1177,7 +1233,7 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
                 // Row ylast + 1 is the halo: the reflection of row ylast.
                 v0 = vc0;
                 v1 = vc1;
-                p0 = p1 = 0.0;
+                p0 = p1 = zero;
             }
             if (t == HALO_PAD) {
                 // Row 1 is the halo: the reflection of row 2.
@@ -1187,21 +1243,21 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
             // Iteration 2 at row s = t - 1.
             const int srow = t - 1;
             if (srow >= j0) {
-                const double kx0 = rp[C2_KX * 64 + 2 * lane], kx1 = rp[C2_KX * 64 + 2 * lane + 1];
-                const double kx2 = __shfl_down_sync(0xffffffffu, kx0, 1);
-                const double up = __shfl_up_sync(0xffffffffu, vc1, 1);
-                const double dn = __shfl_down_sync(0xffffffffu, vc0, 1);
+                const T kx0 = rp[C2_KX * 64 + 2 * lane], kx1 = rp[C2_KX * 64 + 2 * lane + 1];
+                const T kx2 = __shfl_down_sync(0xffffffffu, kx0, 1);
+                const T up = __shfl_up_sync(0xffffffffu, vc1, 1);
+                const T dn = __shfl_down_sync(0xffffffffu, vc0, 1);
                 const long i = fidx(g, c, srow, 0);
-                NbT<double> nb;
-                nb.zm = nb.zp = 0.0;
+                NbT<T> nb;
+                nb.zm = nb.zp = zero;
                 nb.c = vc0;
                 nb.xm = c == HALO_PAD ? vc0 : up;
                 nb.xp = c == xlast ? vc0 : vc1;
                 nb.ym = vm0;
                 nb.yp = v0;
-                double u2a, p2a, u2b, p2b, ra, rb;
+                T u2a, p2a, u2b, p2b, ra, rb;
                 {
-                    const double w = smvp_k(nb, kx0, kx1, rp[C2_KY * 64 + 2 * lane], rc[C2_KY * 64 + 2 * lane], 0.0, 0.0);
+                    const T w = smvp_k(nb, kx0, kx1, rp[C2_KY * 64 + 2 * lane], rc[C2_KY * 64 + 2 * lane], zero, zero);
                     ra = rp[C2_U0 * 64 + 2 * lane] - w;
                     p2a = al2 * q0 + be2 * (precond ? rp[C2_MI * 64 + 2 * lane] * ra : ra);
                     u2a = vc0 + p2a;
@@ -1212,8 +1268,8 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
                 nb.ym = vm1;
                 nb.yp = v1;
                 {
-                    const double w =
-                        smvp_k(nb, kx1, kx2, rp[C2_KY * 64 + 2 * lane + 1], rc[C2_KY * 64 + 2 * lane + 1], 0.0, 0.0);
+                    const T w =
+                        smvp_k(nb, kx1, kx2, rp[C2_KY * 64 + 2 * lane + 1], rc[C2_KY * 64 + 2 * lane + 1], zero, zero);
                     rb = rp[C2_U0 * 64 + 2 * lane + 1] - w;
                     p2b = al2 * q1 + be2 * (precond ? rp[C2_MI * 64 + 2 * lane + 1] * rb : rb);
                     u2b = vc1 + p2b;
@@ -1221,15 +1277,15 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
                 const bool oka = out_lane && c <= xlast;
                 const bool okb = out_lane && c + 1 <= xlast;
                 if (oka && okb) {
-                    *reinterpret_cast<double2*>(unew + i) = make_double2(u2a, u2b);
-                    *reinterpret_cast<double2*>(pnew + i) = make_double2(p2a, p2b);
+                    st_pair(unew + i, u2a, u2b);
+                    st_pair(pnew + i, p2a, p2b);
                 } else if (oka) {
                     unew[i] = u2a;
                     pnew[i] = p2a;
                 }
                 if (check2) {
-                    if (oka) dd_add(acc.v[0], ra * ra);
-                    if (okb) dd_add(acc.v[0], rb * rb);
+                    if (oka) dd_add(acc.v[0], (double)ra * (double)ra);
+                    if (okb) dd_add(acc.v[0], (double)rb * (double)rb);
                 }
             }
             vm0 = vc0;
@@ -1248,17 +1304,7 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
         cp_async_wait<0>();
         __syncwarp();
     }
-    grid_reduce_then<1>(acc, a.red, [&](const double* v) {
-        if (a.timing) return;
-        SolveState& s = *a.st;
-        s.par_u ^= 1;
-        s.par_p ^= 1;
-        s.cheby_calc_steps = s.cheby_calc_steps + 1;
-        end_iteration(a, s, PHASE_CHEBY);  // cannot end the loop (see above)
-        if (check2) s.error = v[0];
-        s.cheby_calc_steps = s.cheby_calc_steps + 1;
-        end_iteration(a, s, PHASE_CHEBY);
-    });
+    grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.pair_control(a, v, check2); });
 }
 #endif
 
@@ -1424,9 +1470,10 @@ __global__ void __launch_bounds__(256) k_coef_to_fp32(FusedArgs a)
     }
 }
 
-// Outer residual in FP64 (CalculateResidual + Calculate2Norm), seeding the FP32 inner CG:
-// r32 = fl32(r), p32 = r32, d32 = 0; sums: r.r (FP64, decides outer convergence) and
-// r32.r32 (the inner rro).
+// Outer residual in FP64 (CalculateResidual + Calculate2Norm), seeding the FP32 inner
+// solve: r32 = fl32(r), and for CG p32 = r32, d32 = 0, for Chebyshev its first step
+// p32 = d32 = r32 / theta; sums: r.r (FP64, decides outer convergence) and r32.r32 (the
+// inner rro / reference norm).
 struct OpOuterResid {
     static constexpr bool kReduce = true;
     using T = double;
@@ -1440,8 +1487,14 @@ struct OpOuterResid {
     struct In {
         double u0;
     };
+    int cheby;      // seed the inner Chebyshev solve (else the inner CG)
+    float theta32;  // its first step d = p = r / theta
     __device__ bool skip(const FusedArgs&) { return false; }
-    __device__ void begin(const FusedArgs&) {}
+    __device__ void begin(const FusedArgs& a)
+    {
+        cheby = a.st->inner_cheby;
+        theta32 = (float)a.st->theta;
+    }
     __device__ Raw load_raw(const FusedArgs& a, long i) const
     {
         Raw r;
@@ -1477,8 +1530,14 @@ struct OpOuterResid {
         const double r = in.u0 - s;
         const float r32 = (float)r;
         a.r32[i] = r32;
-        a.p32[0][i] = r32;
-        a.d32[i] = 0.0f;
+        if (cheby) {
+            const float p = r32 / theta32;
+            a.p32[0][i] = p;
+            a.d32[i] = p;
+        } else {
+            a.p32[0][i] = r32;
+            a.d32[i] = 0.0f;
+        }
         dd_add(acc.v[0], r * r);
         dd_add(acc.v[1], (double)r32 * (double)r32);
     }
@@ -1491,7 +1550,8 @@ struct OpOuterResid {
         s.pending_p = 0;
         s.pending_u = 0;
         s.par_p = 0;
-        s.n_inner = 0;
+        s.par_u = 0;
+        s.n_inner = cheby ? 1 : 0;
         if (!isfinite(v[0])) s.nonfinite = 1;
     }
 };
@@ -1582,6 +1642,124 @@ struct OpSweepA32 {
     }
 };
 
+// FP32 Chebyshev iteration of the inner solve A d = r32 (the reference's ChebyIterate +
+// ChebyCalcU with u0 -> r32, u -> d), the standard coefficient sequence from the first
+// iteration on; the inner residual norm every 10 iterations decides the inner stop
+// (sum r^2 < tol2) beside inner_max.
+struct OpCheby32 {
+    static constexpr bool kReduce = true;
+    using T = float;
+    static constexpr int NV = 1;
+    __device__ const float* coef_x(const FusedArgs& a) const { return a.kx32; }
+    __device__ const float* coef_y(const FusedArgs& a) const { return a.ky32; }
+    __device__ const float* coef_z(const FusedArgs& a) const { return a.kz32; }
+    const float* ucur;  // the iterate d
+    float* unew;
+    float* pcur;
+    float* pnext;
+    float al, be;
+    int j, jmax, check;
+    __device__ bool skip(const FusedArgs&) { return false; }
+    __device__ void begin(const FusedArgs& a)
+    {
+        const SolveState& s = *a.st;
+        ucur = a.dc32[s.par_u];
+        unew = a.dc32[s.par_u ^ 1];
+        pcur = a.p32[s.par_p];
+        pnext = a.p32[s.par_p ^ 1];
+        j = s.n_inner;
+        jmax = s.inner_max;
+        al = (float)a.ch_alphas[j - 1];
+        be = (float)a.ch_betas[j - 1];
+        check = (j % 10 == 0);
+    }
+    struct Raw {
+        float d;
+    };
+    struct In {
+        float rhs, p;
+    };
+    __device__ Raw load_raw(const FusedArgs&, long i) const
+    {
+        Raw r;
+        r.d = ucur[i];
+        return r;
+    }
+    __device__ float stage_raw(const Raw& r) const { return r.d; }
+    __device__ In load_in(const FusedArgs& a, long i) const
+    {
+        In in;
+        in.rhs = a.r32[i];
+        in.p = pcur[i];
+        return in;
+    }
+    static constexpr int NR = 1, NI = 2;
+    __device__ const float* raw_ptr(const FusedArgs&, int) const { return ucur; }
+    __device__ const float* in_ptr(const FusedArgs& a, int k) const { return k == 0 ? a.r32 : pcur; }
+    __device__ Raw raw_from(const float* v) const
+    {
+        Raw r;
+        r.d = v[0];
+        return r;
+    }
+    __device__ In in_from(const float* v) const
+    {
+        In in;
+        in.rhs = v[0];
+        in.p = v[1];
+        return in;
+    }
+    __device__ void interior_k(const FusedArgs&, long i, const NbT<float>& nb, const Raw&, const In& in, float kx0,
+                               float kx1, float ky0, float ky1, float kz0, float kz1, DDVec<1>& acc) const
+    {
+        const float w = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
+        const float r = in.rhs - w;
+        const float p = al * in.p + be * r;
+        pcur[i] = p;
+        unew[i] = nb.c + p;
+        if (check) dd_add(acc.v[0], (double)r * (double)r);
+    }
+    __device__ static void finish(const FusedArgs& a, SolveState& s, bool checked, double rr)
+    {
+        if (checked) s.rrn = rr;
+        // Healthy Chebyshev: sum r^2 <= 4 rho^(2k) sum r0^2.  Far above that (1e4) after 50
+        // iterations, or growing, means the spectrum estimate missed low modes.
+        const bool diverged = checked && (!(rr <= 100.0 * s.rro) ||
+                                          (s.n_inner >= 50 && rr > 1e4 * s.rro * pow(s.cheby_rho2, (double)s.n_inner)));
+        if (diverged) s.inner_diverged = 1;
+        const bool stop = (checked && (rr < s.tol2 || diverged)) || s.n_inner >= s.inner_max;
+        s.cont = !stop;
+        if (a.use_handle) cudaGraphSetConditional(a.handle, stop ? 0u : 1u);
+    }
+    __device__ void control(const FusedArgs& a, const double* v)
+    {
+        if (a.timing) return;
+        SolveState& s = *a.st;
+        s.par_u ^= 1;
+        s.n_inner = j + 1;
+        finish(a, s, check != 0, v[0]);
+    }
+    // Two-iteration kernel: a pair unless iteration j is a check or the last allowed.
+    __device__ bool pair_ok(const FusedArgs&) const { return (j % 10 != 0) && j + 1 < jmax; }
+    __device__ void pair_coefs(const FusedArgs& a, float& al2, float& be2, bool& check2) const
+    {
+        al2 = (float)a.ch_alphas[j];
+        be2 = (float)a.ch_betas[j];
+        check2 = ((j + 1) % 10 == 0);
+    }
+    __device__ const float* pair_rhs(const FusedArgs& a) const { return a.r32; }
+    __device__ const float* pair_mi(const FusedArgs&) const { return nullptr; }
+    __device__ void pair_control(const FusedArgs& a, const double* v, bool check2) const
+    {
+        if (a.timing) return;
+        SolveState& s = *a.st;
+        s.par_u ^= 1;
+        s.par_p ^= 1;
+        s.n_inner = j + 2;
+        finish(a, s, check2, v[0]);
+    }
+};
+
 // FP32 CG sweep B: r -= alpha w, rr; beta, and the inner loop test: stop when the inner
 // residual has dropped below tol2 (inner_tol^2 times its start) or after inner_max.
 __global__ void __launch_bounds__(256) k_cg32_sweep_b(FusedArgs a)
@@ -1617,6 +1795,10 @@ __global__ void __launch_bounds__(256) k_cg32_sweep_b(FusedArgs a)
         st.pending_p = 1;
         st.pending_u = 1;
         st.n_inner = st.n_inner + 1;
+        // The inner CG's scalars feed the Lanczos eigenvalue estimate of the Chebyshev
+        // corrections (indexed 1.., as the FP64 loop stores them).
+        a.cg_alphas[st.n_inner] = st.alpha;
+        a.cg_betas[st.n_inner] = st.beta;
         if (!isfinite(v[0])) st.nonfinite = 1;
         const int cont = isfinite(v[0]) && v[0] >= st.tol2 && st.n_inner < st.inner_max;
         st.cont = cont;
@@ -1629,12 +1811,13 @@ __global__ void __launch_bounds__(256) k_dc_update(FusedArgs a)
 {
     const SolveState& s = *a.st;
     const float alpha = (float)s.last_alpha;
-    const int pend = s.pending_u;
+    const int pend = s.inner_cheby ? 0 : s.pending_u;
     const float* __restrict__ P = a.p32[s.par_p];
+    const float* __restrict__ D = s.inner_cheby ? a.dc32[s.par_u] : a.d32;
     walk_pairs(a.g, [&](long i, bool two) {
         const int n = two ? 2 : 1;
         for (int k = 0; k < n; ++k) {
-            float d = a.d32[i + k];
+            float d = D[i + k];
             if (pend) d = d + alpha * P[i + k];
             a.u[0][i + k] = a.u[0][i + k] + (double)d;
         }

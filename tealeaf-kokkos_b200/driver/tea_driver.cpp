@@ -859,6 +859,12 @@ extern "C" int tea_calc_eigenvalues_c(const double* cg_alphas, const double* cg_
     return tea::tea_calc_eigenvalues(cg_alphas, cg_betas, n, eigmin, eigmax);
 }
 
+extern "C" int tea_tridiag_extremes_c(const double* cg_alphas, const double* cg_betas, int n, double* eigmin,
+                                      double* eigmax)
+{
+    return tea::tea_tridiag_extremes(cg_alphas, cg_betas, n, eigmin, eigmax);
+}
+
 extern "C" void tea_calc_ch_coefs_c(double* ch_alphas, double* ch_betas, double eigmin, double eigmax,
                                     double* theta, int n)
 {

@@ -125,6 +125,52 @@ inline void tea_calc_ch_coefs(double* ch_alphas, double* ch_betas, double eigmin
     }
 }
 
+// Smallest and largest eigenvalue of the same Lanczos tridiagonal as tea_calc_eigenvalues
+// (from the first `n` CG alphas/betas) by Sturm-sequence bisection: O(n) per step instead
+// of the O(n^2) QL sweep, for estimates refreshed while CG runs (the FP32-refined form).
+// Not part of the reference's algorithm.  Returns 0 on success, 1 for n < 1.
+inline int tea_tridiag_extremes(const double* cg_alphas, const double* cg_betas, int n, double* eigmin,
+                                double* eigmax)
+{
+    if (n < 1) return 1;
+    std::vector<double> diag(n), off2(n, 0.0);  // off2[k] = offdiag(k)^2, coupling k-1 and k
+    double lo = 0.0, hi = 0.0;
+    for (int k = 0; k < n; ++k) {
+        diag[k] = 1.0 / cg_alphas[k];
+        if (k > 0) diag[k] = diag[k] + cg_betas[k - 1] / cg_alphas[k - 1];
+        if (k > 0) off2[k] = cg_betas[k - 1] / (cg_alphas[k - 1] * cg_alphas[k - 1]);
+    }
+    // Gershgorin interval.
+    for (int k = 0; k < n; ++k) {
+        const double r = (k > 0 ? std::sqrt(off2[k]) : 0.0) + (k + 1 < n ? std::sqrt(off2[k + 1]) : 0.0);
+        lo = k == 0 ? diag[k] - r : std::fmin(lo, diag[k] - r);
+        hi = k == 0 ? diag[k] + r : std::fmax(hi, diag[k] + r);
+    }
+    // Number of eigenvalues below x (Sturm count of the LDL^T pivots).
+    auto below = [&](double x) {
+        int count = 0;
+        double q = 1.0;
+        for (int k = 0; k < n; ++k) {
+            q = diag[k] - x - (k > 0 ? off2[k] / q : 0.0);
+            if (q == 0.0) q = -1e-300;
+            if (q < 0.0) ++count;
+        }
+        return count;
+    };
+    auto bisect = [&](int index) {  // the eigenvalue with `index` eigenvalues below it
+        double a = lo, b = hi;
+        for (int it = 0; it < 200 && b - a > 1e-13 * std::fmax(std::fabs(a), std::fabs(b)); ++it) {
+            const double m = 0.5 * (a + b);
+            if (below(m) > index) b = m;
+            else a = m;
+        }
+        return 0.5 * (a + b);
+    };
+    *eigmin = bisect(0);
+    *eigmax = bisect(n - 1);
+    return 0;
+}
+
 // NINT(LOG(it_alpha)/(2*LOG(gamm))) with it_alpha = EPSILON(1d0)*bb/(4*error).
 inline int tea_cheby_est_itc(double bb, double error, double cn)
 {

@@ -72,6 +72,7 @@ def _drv():
     lib.tea_calc_eigenvalues_c.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                            ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_double)]
+    lib.tea_tridiag_extremes_c.argtypes = lib.tea_calc_eigenvalues_c.argtypes
     lib.tea_calc_ch_coefs_c.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                         ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
                                         ctypes.c_int]
@@ -94,6 +95,23 @@ def test_eigenvalues_match_dense_solver(n, seed):
     ev = np.linalg.eigvalsh(np.diag(d) + np.diag(e, 1) + np.diag(e, -1))
     assert abs(lo.value - ev[0]) <= 1e-12 * abs(ev[-1])
     assert abs(hi.value - ev[-1]) <= 1e-12 * abs(ev[-1])
+
+
+@pytest.mark.parametrize("n,seed", [(1, 4), (7, 5), (64, 6), (1500, 7)])
+def test_tridiagonal_extremes_by_bisection(n, seed):
+    """The Sturm-bisection extremes (used while FP64 CG presteps run in the FP32-refined
+    form) agree with a dense solver on the same Lanczos tridiagonal."""
+    rng = np.random.default_rng(seed)
+    alphas = rng.uniform(0.2, 2.0, n)
+    betas = rng.uniform(0.01, 0.9, n)
+    lo, hi = ctypes.c_double(), ctypes.c_double()
+    P = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert _drv().tea_tridiag_extremes_c(P(alphas), P(betas), n, ctypes.byref(lo), ctypes.byref(hi)) == 0
+    d = np.array([1 / alphas[k] + (betas[k - 1] / alphas[k - 1] if k else 0.0) for k in range(n)])
+    e = np.array([np.sqrt(betas[k]) / alphas[k] for k in range(n - 1)])
+    ev = np.linalg.eigvalsh(np.diag(d) + np.diag(e, 1) + np.diag(e, -1))
+    assert abs(lo.value - ev[0]) <= 1e-11 * abs(ev[-1])
+    assert abs(hi.value - ev[-1]) <= 1e-11 * abs(ev[-1])
 
 
 def test_chebyshev_coefficients_recurrence():

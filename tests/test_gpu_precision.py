@@ -1,9 +1,10 @@
 """The FP32-refined precision form of ext_tea_leaf_solve_ against the FP64 oracle.
 
-FP32 inner CG inside FP64 defect correction: each timestep must reach the same
-convergence target as the FP64 solve (tested on the true FP64 residual), and the field
-summary must stay within 1e-9 relative of the FP64 oracle's (the bar the specification
-sets for the precision form), step by step.
+FP32 inner solves inside FP64 defect correction -- CG for CG and Jacobi decks; for
+Chebyshev and PPCG decks a first inner CG whose scalars give the eigenvalue bounds, then
+FP32 Chebyshev -- must reach the same convergence target as the FP64 solve (tested on the
+true FP64 residual), and the field summary must stay within 1e-9 relative of the FP64
+oracle's (the bar the specification sets for the precision form), step by step.
 """
 import pytest
 
@@ -29,6 +30,8 @@ def test_fp32_refined_matches_fp64_oracle(dim, solver, seed):
     _, got = tea.run_deck(deck, dim, fused=True, precision=tea.PRECISION_FP32_REFINED, summary_every_step=True)
     for a, b in zip(got, ref):
         assert a["corrections"] >= 1
+        if solver in ("chebyshev", "ppcg"):
+            assert a["cheby_steps"] > 0, a  # the FP32 Chebyshev corrections ran
         assert a["exact_error"] < a["eps_used"], (a["step"], a["exact_error"], a["eps_used"])
         for k in ("vol", "mass", "ie", "temp"):
             assert rel(a[k], b[k]) <= FIELD_SUMMARY_TOL, (a["step"], k, a[k], b[k], rel(a[k], b[k]))
