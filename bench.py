@@ -58,7 +58,7 @@ WORDS = {  # algorithmic FP64 words per interior cell of one launch
 }
 KERNEL_IDS = {"cg_sweep_a": 2, "cheby_pair": 6, "cg_sweep_b": 5}
 ALL_KERNEL_IDS = {"ppcg_inner": 1, "cg_sweep_a": 2, "cheby_iterate": 3, "jacobi": 4, "cg_sweep_b": 5,
-                  "cheby_pair": 6}
+                  "cheby_pair": 6, "cg32_sweep_a": 7, "cg32_sweep_b": 8, "cheby32_pair": 9}
 PROFILES = ROOT / "profiles"
 # Per-timestep iteration counts of this deck (CG iterations before the Chebyshev switch,
 # Chebyshev iterations after it) for simulation steps 1..20, measured with this build; the
@@ -491,8 +491,9 @@ def kernel_only(args):
     ms = ctypes.c_double(0.0)
     lib.tea_kernel_timing_(ch.cid, ctypes.byref(ctypes.c_int(ALL_KERNEL_IDS[args.kernel])),
                            ctypes.byref(ctypes.c_int(args.reps)), ctypes.byref(ms))
+    # FP32 kernels: their FP32 words counted as half FP64 words.
     words = {"ppcg_inner": 8, "cg_sweep_a": 8, "cheby_iterate": 7, "jacobi": 5, "cg_sweep_b": 3,
-             "cheby_pair": 7}[args.kernel]
+             "cheby_pair": 7, "cg32_sweep_a": 4, "cg32_sweep_b": 1.5, "cheby32_pair": 3.5}[args.kernel]
     gbs = words * 8 * CELLS * CELLS / (ms.value / 1e3) / 1e9 if ms.value > 0 else None
     print(json.dumps({"kernel": args.kernel, "ms_per_launch": ms.value, "algorithmic_gbs": gbs}))
     lib.ext_finalise_()

@@ -68,7 +68,9 @@ int tea_chunk_stream_(const int* chunk, void** stream);
  * path on the chunk's stream, between two CUDA events, on the chunk's current fields
  * (which it modifies).  kernel: 1 PPCG inner step, 2 CG/PPCG sweep A, 3 Chebyshev
  * iteration, 4 Jacobi sweep, 5 CG sweep B, 6 two Chebyshev iterations in one pass (2D;
- * in 3D the single iteration).  Writes the mean milliseconds per launch. */
+ * in 3D the single iteration), and the FP32 inner-solve kernels of the precision form:
+ * 7 CG sweep A, 8 CG sweep B, 9 two Chebyshev iterations (3D: one).  Writes the mean
+ * milliseconds per launch. */
 void tea_kernel_timing_(const int* chunk, const int* kernel, const int* reps, double* ms_per_launch);
 
 /* Host<->device bytes the library has moved for the chunk so far: state tables,
@@ -151,8 +153,10 @@ typedef struct {
     double eps_used;        /* the absolute threshold that was applied */
     double eigmin, eigmax;  /* scaled eigenvalue bounds at the switch (0 if none) */
     int corrections;        /* FP32_REFINED: outer corrections */
-    int reserved_i;
-    double reserved[7];
+    int warm_start_used;    /* 1 when the solve started from an attached network's guess */
+    double warm_r0_plain;   /* with a network attached: sum r^2 of the start u = u0 */
+    double warm_r0_guess;   /* ... and of the start u = u0 + the network's du */
+    double reserved[5];
 } tea_solve_result;
 
 /* Whole implicit solve of one timestep on the device: the control flow of
@@ -165,6 +169,46 @@ typedef struct {
  * makes; produces the same fields and iteration counts. */
 void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* params,
                          tea_solve_result* result);
+
+/* ---------------------------------------------------------------------------------
+ * Learned warm start (no counterpart in the reference; 2D).  A U-Net of `levels`
+ * levels and `base` channels at full resolution (doubling per level), bfloat16 weights
+ * and activations with float32 accumulation, predicts the timestep increment
+ * du = u(n+1) - u0 from u0 = density*energy, density, Kx and Ky.  A chunk with a network
+ * attached starts each ext_tea_leaf_solve_ from u0 + du when that start has the smaller
+ * FP64 residual (else from u0, as the reference does) and converges to the same
+ * tolerance.  All functions return a TEA_* status.
+ * --------------------------------------------------------------------------------- */
+
+/* New network with seeded He-initialised weights on the current device: levels 2..5,
+ * base 16, 32 or 64.  Writes its id (1-based). */
+int tea_ws_create_(const int* levels, const int* base, const int* seed, int* net);
+int tea_ws_destroy_(const int* net);
+/* Records a training pair from the chunk's last ext_tea_leaf_solve_ (its features and
+ * (u - u0) / max|u0|), kept in device memory by the network. */
+int tea_ws_record_(const int* net, const int* chunk);
+int tea_ws_pairs_(const int* net, int* count);
+/* Adam training: `steps` steps on `batch` random crop x crop windows of the recorded
+ * pairs (crop a multiple of 2^(levels-1)); targets are normalised to unit RMS over the
+ * recorded pairs at the first training.  Writes the MSE loss averaged over the first and
+ * over the last 10 steps, and the device milliseconds per step. */
+int tea_ws_train_(const int* net, const int* steps, const int* batch, const int* crop, const double* lr,
+                  const int* seed, double* loss_first, double* loss_last, double* ms_per_step);
+/* Attaches the network to a chunk (net 0 detaches); sides must be multiples of
+ * 2^(levels-1) for the guess to be used. */
+int tea_ws_attach_(const int* chunk, const int* net);
+/* The network's du for the chunk's current step, into a host array [ny][nx], and the
+ * device milliseconds of the prediction. */
+int tea_ws_predict_(const int* net, const int* chunk, double* du, double* ms);
+/* Test hooks: parameters in the order of the CPU oracle (per 3x3 layer w[co][9][cin],
+ * then b; head w, head b), the choice of convolution (0 tensor cores, 1 CUDA cores),
+ * and forward/backward on host images [n][H][W][4] (target null: forward only). */
+int tea_ws_param_count_(const int* net, long long* count);
+int tea_ws_get_params_(const int* net, float* params);
+int tea_ws_set_params_(const int* net, const float* params);
+int tea_ws_set_conv_(const int* net, const int* reference);
+int tea_ws_eval_host_(const int* net, const float* x, const float* target, const int* n, const int* H,
+                      const int* W, float* y, double* loss, float* grads);
 
 #ifdef __cplusplus
 }

@@ -80,7 +80,8 @@ class RunOptions(ctypes.Structure):
         ("dim", ctypes.c_int), ("backend", ctypes.c_char_p), ("use_fused_solve", ctypes.c_int),
         ("summary_every_step", ctypes.c_int), ("end_step_override", ctypes.c_int), ("quiet", ctypes.c_int),
         ("out_path", ctypes.c_char_p), ("eps_override", ctypes.c_double), ("eps_rel_override", ctypes.c_double),
-        ("keep_chunk", ctypes.c_int), ("precision", ctypes.c_int), ("reserved", ctypes.c_int * 6),
+        ("keep_chunk", ctypes.c_int), ("precision", ctypes.c_int), ("ws_net", ctypes.c_int),
+        ("ws_mode", ctypes.c_int), ("reserved", ctypes.c_int * 4),
     ]
 
 
@@ -91,7 +92,7 @@ class StepRecord(ctypes.Structure):
         ("error", ctypes.c_double), ("exact_error", ctypes.c_double), ("eps_used", ctypes.c_double),
         ("solve_seconds", ctypes.c_double), ("vol", ctypes.c_double), ("mass", ctypes.c_double),
         ("ie", ctypes.c_double), ("temp", ctypes.c_double), ("has_summary", ctypes.c_int),
-        ("switch_step", ctypes.c_int), ("est_itc", ctypes.c_int), ("pad", ctypes.c_int),
+        ("switch_step", ctypes.c_int), ("est_itc", ctypes.c_int), ("warm_start_used", ctypes.c_int),
         ("wall_end", ctypes.c_double), ("h2d_bytes", ctypes.c_longlong), ("d2h_bytes", ctypes.c_longlong),
         ("corrections", ctypes.c_int), ("pad2", ctypes.c_int),
     ]
@@ -122,7 +123,8 @@ def driver() -> ctypes.CDLL:
 
 def run_deck(deck_text: str, dim: int, backend=None, *, fused: bool = False, summary_every_step: bool = False,
              end_step: int = 0, quiet: bool = True, out_path=None, eps: float = 0.0, eps_rel: float = 0.0,
-             keep_chunk: bool = False, precision: int = 0, max_records: int = 100000):
+             keep_chunk: bool = False, precision: int = 0, max_records: int = 100000, ws_net: int = 0,
+             ws_mode: int = 0):
     """Run a tea.in deck through the C++ driver against ``backend`` (default: the CUDA
     library for ``dim``).  Returns ``(summary, records)`` as dicts."""
     backend = str(backend) if backend is not None else str(lib_path(dim))
@@ -140,6 +142,8 @@ def run_deck(deck_text: str, dim: int, backend=None, *, fused: bool = False, sum
     opt.eps_rel_override = float(eps_rel)
     opt.keep_chunk = 1 if keep_chunk else 0
     opt.precision = int(precision)
+    opt.ws_net = int(ws_net)
+    opt.ws_mode = int(ws_mode)
     summary = RunSummary()
     records = (StepRecord * max_records)()
     lib = driver()
@@ -169,7 +173,8 @@ class SolveResult(ctypes.Structure):
         ("cheby_steps", ctypes.c_int), ("switch_step", ctypes.c_int), ("est_itc", ctypes.c_int),
         ("error", ctypes.c_double), ("exact_error", ctypes.c_double), ("eps_used", ctypes.c_double),
         ("eigmin", ctypes.c_double), ("eigmax", ctypes.c_double), ("corrections", ctypes.c_int),
-        ("reserved_i", ctypes.c_int), ("reserved", ctypes.c_double * 7),
+        ("warm_start_used", ctypes.c_int), ("warm_r0_plain", ctypes.c_double), ("warm_r0_guess", ctypes.c_double),
+        ("reserved", ctypes.c_double * 5),
     ]
 
 
@@ -288,6 +293,72 @@ class ExtChunk:
 
 
 # ----------------------------------------------------------------------------- decks
+
+WS_RECORD, WS_ATTACH = 1, 2  # run_deck ws_mode values
+
+
+class WarmStart:
+    """A learned warm-start network of the 2D CUDA library (tea_ws_* entry points)."""
+
+    def __init__(self, levels: int = 3, base: int = 32, seed: int = 0):
+        self.lib = cuda_library(2)
+        nid = ctypes.c_int(0)
+        self._check(self.lib.tea_ws_create_(_i(levels), _i(base), _i(seed), ctypes.byref(nid)), "create")
+        self.id = nid.value
+        self.levels, self.base = levels, base
+
+    def _check(self, rc, what):
+        if rc != 0:
+            self.lib.tea_last_error.restype = ctypes.c_char_p
+            raise RuntimeError(f"tea_ws_{what}_: status {rc}: {self.lib.tea_last_error().decode()}")
+
+    def close(self):
+        if self.id:
+            self.lib.tea_ws_destroy_(_i(self.id))
+            self.id = 0
+
+    def param_count(self) -> int:
+        n = ctypes.c_longlong(0)
+        self._check(self.lib.tea_ws_param_count_(_i(self.id), ctypes.byref(n)), "param_count")
+        return n.value
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.param_count(), dtype=np.float32)
+        self._check(self.lib.tea_ws_get_params_(_i(self.id), out.ctypes.data_as(ctypes.c_void_p)), "get_params")
+        return out
+
+    def set_params(self, flat) -> None:
+        arr = np.ascontiguousarray(flat, dtype=np.float32)
+        self._check(self.lib.tea_ws_set_params_(_i(self.id), arr.ctypes.data_as(ctypes.c_void_p)), "set_params")
+
+    def set_reference_conv(self, on: bool) -> None:
+        self._check(self.lib.tea_ws_set_conv_(_i(self.id), _i(1 if on else 0)), "set_conv")
+
+    def eval(self, x, target=None):
+        """x [n][H][W][4] float32 -> (y [n][H][W], loss, flat gradients or None)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        n, H, W, _ = x.shape
+        y = np.zeros((n, H, W), dtype=np.float32)
+        loss = ctypes.c_double(0.0)
+        grads = np.zeros(self.param_count(), dtype=np.float32) if target is not None else None
+        t = np.ascontiguousarray(target, dtype=np.float32) if target is not None else None
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+        self._check(self.lib.tea_ws_eval_host_(_i(self.id), P(x), P(t), _i(n), _i(H), _i(W), P(y),
+                                               ctypes.byref(loss), P(grads)), "eval_host")
+        return y, loss.value, grads
+
+    def pairs(self) -> int:
+        n = ctypes.c_int(0)
+        self._check(self.lib.tea_ws_pairs_(_i(self.id), ctypes.byref(n)), "pairs")
+        return n.value
+
+    def train(self, steps: int, batch: int, crop: int, lr: float = 1e-3, seed: int = 0):
+        """Returns (first-step loss, last-step loss, device ms per step)."""
+        lf, ll, ms = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.tea_ws_train_(_i(self.id), _i(steps), _i(batch), _i(crop), _d(lr), _i(seed),
+                                           ctypes.byref(lf), ctypes.byref(ll), ctypes.byref(ms)), "train")
+        return lf.value, ll.value, ms.value
+
 
 @dataclass
 class DeckSpec:

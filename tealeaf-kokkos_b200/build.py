@@ -59,7 +59,7 @@ def cuda_sources():
 
 def build(verbose: bool = False, force: bool = False) -> None:
     nvcc = _nvcc()
-    cu = [CSRC / "tea_ext.cu", CSRC / "tea_fused.cu", CSRC / "tea_noalloc.cu"]
+    cu = [CSRC / "tea_ext.cu", CSRC / "tea_fused.cu", CSRC / "tea_noalloc.cu", CSRC / "tea_warmstart.cu"]
     deps = cuda_sources()
     for dim in (2, 3):
         out = HERE / f"libtea{dim}d_b200.so"

@@ -80,6 +80,7 @@ struct Chunk {
     int grid_blocks = 0;      // blocks for grid-stride per-call kernels
     int device = 0;
     void* fused = nullptr;    // whole-solve state (tea_fused.cuh)
+    void* ws = nullptr;       // attached warm-start network (tea_warmstart.cu), not owned
     long long h2d_bytes = 0;  // host<->device bytes moved for this chunk (inputs, results)
     long long d2h_bytes = 0;
 };

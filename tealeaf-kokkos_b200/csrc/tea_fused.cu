@@ -30,6 +30,7 @@
 namespace tea {
 
 Chunk* get_chunk(const int* chunk);
+int ws_predict_into(Chunk* c, double* u_out);  // tea_warmstart.cu
 void sync(Chunk* c);
 void update_halo(Chunk* c, const int* neighbours, const int* fields, int depth);
 
@@ -57,7 +58,7 @@ struct Fused {
     double *d_ch_alphas = nullptr, *d_ch_betas = nullptr;
     int cap = 0;  // entries of the coefficient arrays
     FusedArgs base{};
-    int stencil_blocks = 0, point_blocks = 0, pair_blocks = 0;
+    int stencil_blocks = 0, point_blocks = 0, pair_blocks = 0, quad_blocks = 0;
     RingLaunch ring[RING_OPS];  // grid and segment rows of k_ring2d per sweep (2D)
     RingLaunch pair;            // k_cheby2_ring2d<OpCheby> (2D); blocks 0: one iteration per launch
     RingLaunch pair32;          // k_cheby2_ring2d<OpCheby32> (2D)
@@ -67,6 +68,27 @@ struct Fused {
 };
 
 Fused* fused_of(Chunk* c) { return static_cast<Fused*>(c->fused); }
+
+// After a warm start replaced u (and r = u0 - A u was recomputed): the CG start
+// p = z = Mi r (preconditioned) or p = r, and rro = sum r.p -- CGCalcRRO's last part.
+__global__ void __launch_bounds__(BLOCK) k_ws_restart(Geom g, Box inner, Fields f, int precond, RedScratch rs,
+                                                      double* out)
+{
+    DDVec<1> acc;
+    acc.zero();
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        const double r = f.r[i];
+        double p = r;
+        if (precond) {
+            p = f.mi[i] * r;
+            f.z[i] = p;
+        }
+        f.p[i] = p;
+        dd_add(acc.v[0], r * p);
+    });
+    grid_reduce<1>(acc, rs, out);
+}
 
 void free_loops(Fused* F)
 {
@@ -154,7 +176,7 @@ template <class Op>
 void setup_ring(Fused* F, const Geom& g, int sms, int max_blocks)
 {
     const int occ = smem_occupancy(k_ring2d<Op>, (int)ring_smem_bytes<Op>());
-    F->ring[RingId<Op>::value] = ring_launch(g, sms, occ, 64, max_blocks);
+    F->ring[RingId<Op>::value] = ring_launch(g, sms, occ, RingGeomOf<Op>::STRIP, max_blocks);
 }
 #endif
 
@@ -295,10 +317,10 @@ Fused* ensure_fused(Chunk* c, int max_iters)
                 setup_ring<OpOuterResid>(F, g, sms, mb);
                 setup_ring<OpCheby32>(F, g, sms, mb);
                 const int occ2 = smem_occupancy(k_cheby2_ring2d<OpCheby>, (int)cheby2_smem_bytes<OpCheby>());
-                F->pair = ring_launch(g, sms, occ2, C2_OUT, mb);
+                F->pair = ring_launch(g, sms, occ2, Pair2Geom<double>::OUT, mb);
                 const int occ3 =
                     smem_occupancy(k_cheby2_ring2d<OpCheby32>, (int)cheby2_smem_bytes<OpCheby32>());
-                F->pair32 = ring_launch(g, sms, occ3, C2_OUT, mb);
+                F->pair32 = ring_launch(g, sms, occ3, Pair2Geom<float>::OUT, mb);
             }
         }
 #endif
@@ -307,6 +329,8 @@ Fused* ensure_fused(Chunk* c, int max_iters)
             const long warps = make_seg(g).nseg;  // one 64-cell segment per warp at most
             const long blocks = (warps + 7) / 8;
             F->pair_blocks = (int)std::max<long>(1, std::min<long>(blocks, c->red.max_blocks));
+            const long qwarps = (long)((g.nx + 127) / 128) * g.ny * g.nz;  // one 128-cell segment per warp
+            F->quad_blocks = (int)std::max<long>(1, std::min<long>((qwarps + 7) / 8, c->red.max_blocks));
         }
     }
     if (F->cap < max_iters + 2) {
@@ -405,7 +429,7 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         break;
     case LOOP_CG32:
         stencil<OpSweepA32>(F, a, s);
-        k_cg32_sweep_b<<<F->pair_blocks, 256, 0, s>>>(a);
+        k_cg32_sweep_b<<<F->quad_blocks, 256, 0, s>>>(a);
         break;
     }
 }
@@ -616,6 +640,31 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
         int zero = 0;
         ext_calculate_2norm_(chunk, &bb, &zero);
         eps = P->eps_rel * P->eps_rel * bb;
+    }
+    // Learned warm start (a network attached with tea_ws_attach_): keep u = u0 + du when its
+    // FP64 residual is smaller than that of u = u0, and restart CG from it.
+    int ws_used = 0;
+    double ws_r0_plain = 0.0, ws_r0_guess = 0.0;
+    if (c->ws && cg_like) {
+        int one = 1;
+        ext_calculate_2norm_(chunk, &ws_r0_plain, &one);  // r = u0 - A u0 after the set-up
+        if (ws_predict_into(c, c->f.u)) {
+            ext_calculate_residual_(chunk);
+            ext_calculate_2norm_(chunk, &ws_r0_guess, &one);
+            if (ws_r0_guess < ws_r0_plain) {
+                k_ws_restart<<<launch_blocks(c, c->inner.ntiles), dim3(TILE_X, TILE_Y), 0, c->stream>>>(
+                    c->g, c->inner, c->f, precond, c->red, c->d_out);
+                sync(c);
+                rro = ((volatile double*)c->h_out)[0];
+                c->d2h_bytes += sizeof(double);
+                ws_used = 1;
+            } else {
+                TEA_CK(cudaMemcpyAsync(c->alloc[F_U], c->alloc[F_U0], c->field_elems * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, c->stream));
+                ext_calculate_residual_(chunk);
+            }
+            halo(c, {4, 5}, 1);
+        }
     }
     // The second buffers start as copies, so halos the loops never write match u and p.
     const size_t bytes = c->field_elems * sizeof(double);
@@ -886,6 +935,9 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
     R->eigmin = eigmin;
     R->eigmax = eigmax;
     R->corrections = corrections;
+    R->warm_start_used = ws_used;
+    R->warm_r0_plain = ws_r0_plain;
+    R->warm_r0_guess = ws_r0_guess;
 }
 
 // Measurement hook: `reps` back-to-back launches of one fused kernel on the chunk's
@@ -897,6 +949,7 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
     Chunk* c = get_chunk(chunk);
     if (!c || *reps < 1) return;
     Fused* F = ensure_fused(c, 1);
+    if (*kernel >= 7 && !ensure_fp32(c, F)) return;
     FusedArgs a = F->base;
     a.step = 1;
     a.timing = 1;
@@ -911,6 +964,8 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
     F->h_st->est_itc = 1 << 30;
     F->h_st->max_iters = std::max(F->h_st->max_iters, 2);
     F->h_st->cheby_calc_steps = 1;
+    F->h_st->n_inner = 1;
+    F->h_st->inner_max = 1 << 30;
     push_state(c, F);
     cudaEvent_t e0, e1;
     TEA_CK(cudaEventCreate(&e0));
@@ -921,6 +976,22 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
         case 2: stencil<OpSweepA>(F, a, c->stream); break;
         case 3: stencil<OpCheby>(F, a, c->stream); break;
         case 5: k_cg_sweep_b<<<F->pair_blocks, 256, 0, c->stream>>>(a); break;
+        case 7: stencil<OpSweepA32>(F, a, c->stream); break;
+        case 8: k_cg32_sweep_b<<<F->quad_blocks, 256, 0, c->stream>>>(a); break;
+#if TEA_DIM == 2
+        case 9:
+            if (F->pair32.blocks > 0) {
+                FusedArgs ap = a;
+                ap.seg_rows = F->pair32.rows;
+                k_cheby2_ring2d<OpCheby32>
+                    <<<F->pair32.blocks, RWARPS * 32, cheby2_smem_bytes<OpCheby32>(), c->stream>>>(ap);
+            } else {
+                stencil<OpCheby32>(F, a, c->stream);
+            }
+            break;
+#else
+        case 9: stencil<OpCheby32>(F, a, c->stream); break;
+#endif
 #if TEA_DIM == 2
         case 6:
             if (F->pair.blocks > 0) {

@@ -413,13 +413,14 @@ __global__ void __launch_bounds__(P3BLOCK, 2) k_pipe3d(FusedArgs a)
 }
 
 // 2D streaming through a per-warp shared-memory ring filled by cp.async.  Each warp owns a
-// strip of 64 columns (two adjacent cells per lane, 16-byte copies for FP64) and marches
-// down a segment of a.seg_rows rows; the rows of every input array are copied asynchronously
-// RP rows ahead of the row being computed, so the data in flight lives in shared memory,
-// not in registers.  A ring row holds columns c0-1 .. c0+64 (the outer two for the
-// x-neighbours of the strip's edge cells).  Rows and columns outside the inner domain are
-// copied from their reflected interior cell; within the strip the right-hand boundary is
-// reflected when the operand is read.  No block barrier: warps are independent.
+// strip of 32 * VEC columns (VEC adjacent cells per lane: one 16-byte copy, 2 doubles or 4
+// floats) and marches down a segment of a.seg_rows rows; the rows of every input array are
+// copied asynchronously RP rows ahead of the row being computed, so the data in flight
+// lives in shared memory, not in registers.  A ring row also holds the two columns just
+// outside the strip (the x-neighbours of its edge cells).  Rows and columns outside the
+// inner domain are copied from their reflected interior cell; within the strip the
+// right-hand boundary is reflected when the operand is read.  No block barrier: warps are
+// independent.
 #ifndef TEA_RING_RP
 #define TEA_RING_RP 3
 #endif
@@ -431,7 +432,6 @@ __global__ void __launch_bounds__(P3BLOCK, 2) k_pipe3d(FusedArgs a)
 #endif
 constexpr int RP = TEA_RING_RP;  // rows in flight beyond row j+1
 constexpr int RQ = RP + 2;     // ring rows per warp
-constexpr int RW = 68;         // elements per ring row: pad, c0-1, c0..c0+63, c0+64, pad
 constexpr int RWARPS = TEA_RING_WARPS;  // warps per block
 
 __device__ __forceinline__ void cp_async_16(void* dst, const void* src)
@@ -466,10 +466,77 @@ __device__ __forceinline__ void ring_copy_one(T* dst, const T* src)
     else cp_async_4(dst, src);
 }
 
+// Strip geometry of the 2D ring kernels for element type T: each lane owns VEC adjacent
+// cells (one 16-byte copy), a warp a strip of 32 * VEC columns.  A ring row holds the
+// strip at offset OFF (16-byte aligned) with the left outside column at OFF - 1 and the
+// right one at OFF + STRIP.
+template <class T, int V = 16 / (int)sizeof(T)>
+struct RingGeom {
+    static constexpr int VEC = V;
+    static constexpr int STRIP = 32 * VEC;
+    static constexpr int OFF = 16 / (int)sizeof(T);  // keeps the strip 16-byte aligned
+    static constexpr int WIDTH = STRIP + 2 * OFF;
+};
+
+// Cells per lane of a sweep's ring kernel: one 16-byte copy by default; a sweep whose
+// per-cell stores are many narrow ones (FP32 CG sweep A: d, p and w) keeps two cells per
+// lane so that each store instruction covers whole sectors.
+template <class Op>
+struct RingVec {
+    static constexpr int value = 16 / (int)sizeof(typename Op::T);
+};
+struct OpSweepA32;
+template <>
+struct RingVec<OpSweepA32> {
+    static constexpr int value = 2;
+};
+template <class Op>
+using RingGeomOf = RingGeom<typename Op::T, RingVec<Op>::value>;
+
+template <class T>
+__device__ __forceinline__ void ld_vec(const T* p, T* out);
+template <>
+__device__ __forceinline__ void ld_vec<double>(const double* p, double* out)
+{
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    out[0] = v.x;
+    out[1] = v.y;
+}
+template <>
+__device__ __forceinline__ void ld_vec<float>(const float* p, float* out)
+{
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    out[0] = v.x;
+    out[1] = v.y;
+    out[2] = v.z;
+    out[3] = v.w;
+}
+
+// VEC consecutive elements (8 or 16 bytes, aligned to their size).
+template <int VEC, class T>
+__device__ __forceinline__ void ld_vecn(const T* p, T* out)
+{
+    if constexpr (VEC * sizeof(T) == 16) {
+        ld_vec(p, out);
+    } else {
+        static_assert(VEC == 2 && sizeof(T) == 4, "8-byte vectors are float pairs");
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        out[0] = v.x;
+        out[1] = v.y;
+    }
+}
+template <int VEC, class T>
+__device__ __forceinline__ void cp_async_vecn(T* dst, const T* src)
+{
+    if constexpr (VEC * sizeof(T) == 16) cp_async_16(dst, src);
+    else cp_async_8(dst, src);
+}
+
 template <class Op>
 constexpr size_t ring_smem_bytes()
 {
-    return (size_t)RWARPS * RQ * (Op::NR + Op::NI + 2) * RW * sizeof(typename Op::T);
+    using T = typename Op::T;
+    return (size_t)RWARPS * RQ * (Op::NR + Op::NI + 2) * RingGeomOf<Op>::WIDTH * sizeof(T);
 }
 
 // The body of k_ring2d after op.begin(), ending with the grid reduction and op.control().
@@ -477,16 +544,16 @@ template <class Op>
 __device__ __forceinline__ void ring2d_body(const FusedArgs& a, Op& op, unsigned char* s_ring_raw)
 {
     using T = typename Op::T;
-    using Raw = typename Op::Raw;
-    using In = typename Op::In;
     constexpr int NV = Op::NV;
     constexpr int NR = Op::NR, NI = Op::NI;
     constexpr int NA = NR + NI + 2;  // + Kx, Ky
     constexpr int AKX = NR + NI, AKY = NR + NI + 1;
+    constexpr int VEC = RingGeomOf<Op>::VEC, STRIP = RingGeomOf<Op>::STRIP, OFF = RingGeomOf<Op>::OFF;
+    constexpr int RWT = RingGeomOf<Op>::WIDTH;
     const Geom& g = a.g;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * RQ * NA * RW;
+    T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * RQ * NA * RWT;
     const T* src[NA];
 #pragma unroll
     for (int k = 0; k < NR; ++k) src[k] = op.raw_ptr(a, k);
@@ -498,25 +565,29 @@ __device__ __forceinline__ void ring2d_body(const FusedArgs& a, Op& op, unsigned
     acc.zero();
     const int xlast = g.X - HALO_PAD - 1;
     const int ylast = g.Y - HALO_PAD - 1;
-    const int per_x = (g.nx + 63) / 64;
+    const int per_x = (g.nx + STRIP - 1) / STRIP;
     const int per_y = (g.ny + a.seg_rows - 1) / a.seg_rows;
     const long nseg = (long)per_x * per_y;
     const long gw = (long)blockIdx.x * RWARPS + warp, nw = (long)gridDim.x * RWARPS;
-    const int cmax = (int)g.pitch - 2;  // last even column whose pair stays inside the row
+    // Last first-column of a lane whose VEC cells stay inside the row (same residue as the
+    // lanes' columns modulo VEC, so the copy stays 16-byte aligned); lanes beyond it own
+    // no inner cell.
+    const int cmax = (int)g.pitch - 2 * VEC + 2;
     for (long sgi = gw; sgi < nseg; sgi += nw) {
         const int xs = (int)(sgi % per_x), ys = (int)(sgi / per_x);
-        const int c0 = HALO_PAD + 64 * xs;
-        const int c = c0 + 2 * lane;
+        const int c0 = HALO_PAD + STRIP * xs;
+        const int c = c0 + VEC * lane;
         const int cc = min(c, cmax);
         const int j0 = HALO_PAD + a.seg_rows * ys;
         const int j1 = min(j0 + a.seg_rows, ylast + 1);
         const int left = refl(c0 - 1, g.X);
-        const int right_op = refl(min(c0 + 64, xlast + 1), g.X);
-        const int right_k = min(c0 + 64, xlast + 1);
-        // Copy ring row for grid row r (relative row rr = r - j0 + 1 selects the slot).
+        const int right_op = refl(min(c0 + STRIP, xlast + 1), g.X);
+        const int right_k = min(c0 + STRIP, xlast + 1);
+        auto slot = [&](int r) { return ring + (size_t)((r - j0 + 1) % RQ) * NA * RWT; };
+        // Copy the ring row of grid row r.
         auto issue = [&](int r) {
             if (r <= j1) {
-                T* base = ring + (size_t)((r - j0 + 1) % RQ) * NA * RW;
+                T* base = slot(r);
                 const int srow = refl(min(max(r, 1), ylast + 1), g.Y);
                 const int irow = min(max(r, HALO_PAD), ylast + 1);
 #pragma unroll
@@ -524,88 +595,84 @@ __device__ __forceinline__ void ring2d_body(const FusedArgs& a, Op& op, unsigned
                     const T* sp = src[k];
                     if (!sp) continue;
                     const int row = k < NR ? srow : irow;
-                    T* d = base + k * RW;
-                    ring_copy_pair(d + 2 + 2 * lane, sp + fidx(g, cc, row, 0));
-                    if (lane == 0 && k < NR) ring_copy_one(d + 1, sp + fidx(g, left, row, 0));
+                    T* d = base + k * RWT;
+                    cp_async_vecn<VEC>(d + OFF + VEC * lane, sp + fidx(g, cc, row, 0));
+                    if (lane == 0 && k < NR) ring_copy_one(d + OFF - 1, sp + fidx(g, left, row, 0));
                     if (lane == 31 && (k < NR || k == AKX))
-                        ring_copy_one(d + 66, sp + fidx(g, k < NR ? right_op : right_k, row, 0));
+                        ring_copy_one(d + OFF + STRIP, sp + fidx(g, k < NR ? right_op : right_k, row, 0));
                 }
             }
             cp_async_commit();
         };
-        // The operand of ring row `r` at the lane's two cells and at the strip's edge.
-        auto stage_row = [&](int r, T& v0, T& v1, T& ve) {
-            const T* base = ring + (size_t)((r - j0 + 1) % RQ) * NA * RW;
-            T x0[NR], x1[NR], xe[NR];
+        // The operand of ring row r at the lane's cells and at the strip's outside column
+        // (left for lane 0, right for lane 31).
+        auto stage_row = [&](int r, T* v, T& ve) {
+            const T* base = slot(r);
+            T x[NR][VEC], xq[NR], xe[NR];
 #pragma unroll
             for (int k = 0; k < NR; ++k) {
-                x0[k] = base[k * RW + 2 + 2 * lane];
-                x1[k] = base[k * RW + 3 + 2 * lane];
-                xe[k] = base[k * RW + (lane == 0 ? 1 : 66)];
+                ld_vecn<VEC>(base + k * RWT + OFF + VEC * lane, x[k]);
+                xe[k] = base[k * RWT + (lane == 0 ? OFF - 1 : OFF + STRIP)];
             }
-            v0 = op.stage_raw(op.raw_from(x0));
-            v1 = op.stage_raw(op.raw_from(x1));
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+#pragma unroll
+                for (int k = 0; k < NR; ++k) xq[k] = x[k][q];
+                v[q] = op.stage_raw(op.raw_from(xq));
+            }
             ve = op.stage_raw(op.raw_from(xe));
         };
         for (int r = j0 - 1; r <= j0 + RP; ++r) issue(r);
         cp_async_wait<RP>();
         __syncwarp();
-        T m0, m1, me, c0v, c1v, ce;
-        stage_row(j0 - 1, m0, m1, me);
-        stage_row(j0, c0v, c1v, ce);
+        T mv[VEC], cv[VEC], ce;
+        stage_row(j0 - 1, mv, ce);  // (the outside column of row j0 - 1 is not needed)
+        stage_row(j0, cv, ce);
         for (int jj = j0; jj < j1; ++jj) {
             cp_async_wait<RP - 1>();
             __syncwarp();
-            T p0, p1, pe;
-            stage_row(jj + 1, p0, p1, pe);
-            const T* cur = ring + (size_t)((jj - j0 + 1) % RQ) * NA * RW;
-            const T* nxt = ring + (size_t)((jj - j0 + 2) % RQ) * NA * RW;
-            // x-neighbours of the pair (reflection at the last inner column).
-            const T up = __shfl_up_sync(0xffffffffu, c1v, 1);
-            const T dn = __shfl_down_sync(0xffffffffu, c0v, 1);
-            const T kxa = cur[AKX * RW + 2 + 2 * lane], kxb = cur[AKX * RW + 3 + 2 * lane];
-            const T kxn = __shfl_down_sync(0xffffffffu, kxa, 1);
-            const T kxc = lane == 31 ? cur[AKX * RW + 66] : kxn;
-            const T kya = cur[AKY * RW + 2 + 2 * lane], kyb = cur[AKY * RW + 3 + 2 * lane];
-            const T kya1 = nxt[AKY * RW + 2 + 2 * lane], kyb1 = nxt[AKY * RW + 3 + 2 * lane];
-            T r0[NR > 0 ? NR : 1], r1[NR > 0 ? NR : 1], i0[NI], i1[NI];
+            T pv[VEC], pe;
+            stage_row(jj + 1, pv, pe);
+            const T* cur = slot(jj);
+            const T* nxt = slot(jj + 1);
+            const T up = __shfl_up_sync(0xffffffffu, cv[VEC - 1], 1);
+            const T dn = __shfl_down_sync(0xffffffffu, cv[0], 1);
+            T kx[VEC + 1], ky0[VEC], ky1[VEC];
+            ld_vecn<VEC>(cur + AKX * RWT + OFF + VEC * lane, kx);
+            const T kxn = __shfl_down_sync(0xffffffffu, kx[0], 1);
+            kx[VEC] = lane == 31 ? cur[AKX * RWT + OFF + STRIP] : kxn;
+            ld_vecn<VEC>(cur + AKY * RWT + OFF + VEC * lane, ky0);
+            ld_vecn<VEC>(nxt + AKY * RWT + OFF + VEC * lane, ky1);
+            T rv[NR > 0 ? NR : 1][VEC], iv[NI][VEC];
 #pragma unroll
-            for (int k = 0; k < NR; ++k) {
-                r0[k] = cur[k * RW + 2 + 2 * lane];
-                r1[k] = cur[k * RW + 3 + 2 * lane];
+            for (int k = 0; k < NR; ++k) ld_vecn<VEC>(cur + k * RWT + OFF + VEC * lane, rv[k]);
+#pragma unroll
+            for (int k = 0; k < NI; ++k) ld_vecn<VEC>(cur + (NR + k) * RWT + OFF + VEC * lane, iv[k]);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                const int cq = c + q;
+                if (cq <= xlast) {
+                    T rq[NR > 0 ? NR : 1], iq[NI];
+#pragma unroll
+                    for (int k = 0; k < NR; ++k) rq[k] = rv[k][q];
+#pragma unroll
+                    for (int k = 0; k < NI; ++k) iq[k] = iv[k][q];
+                    NbT<T> nb;
+                    nb.c = cv[q];
+                    nb.xm = q == 0 ? (lane == 0 ? ce : up) : cv[q > 0 ? q - 1 : 0];
+                    nb.xp = cq == xlast ? cv[q] : (q == VEC - 1 ? (lane == 31 ? ce : dn) : cv[q < VEC - 1 ? q + 1 : q]);
+                    nb.ym = mv[q];
+                    nb.yp = pv[q];
+                    nb.zm = nb.zp = (T)0;
+                    op.interior_k(a, fidx(g, cq, jj, 0), nb, op.raw_from(rq), op.in_from(iq), kx[q], kx[q + 1], ky0[q],
+                                  ky1[q], (T)0, (T)0, acc);
+                }
             }
 #pragma unroll
-            for (int k = 0; k < NI; ++k) {
-                i0[k] = cur[(NR + k) * RW + 2 + 2 * lane];
-                i1[k] = cur[(NR + k) * RW + 3 + 2 * lane];
+            for (int q = 0; q < VEC; ++q) {
+                mv[q] = cv[q];
+                cv[q] = pv[q];
             }
-            if (c <= xlast) {
-                NbT<T> nb;
-                nb.c = c0v;
-                nb.xm = lane == 0 ? ce : up;
-                nb.xp = c == xlast ? c0v : c1v;
-                nb.ym = m0;
-                nb.yp = p0;
-                nb.zm = nb.zp = (T)0;
-                op.interior_k(a, fidx(g, c, jj, 0), nb, op.raw_from(r0), op.in_from(i0), kxa, kxb, kya, kya1, (T)0,
-                              (T)0, acc);
-            }
-            if (c + 1 <= xlast) {
-                NbT<T> nb;
-                nb.c = c1v;
-                nb.xm = c0v;
-                nb.xp = c + 1 == xlast ? c1v : (lane == 31 ? ce : dn);
-                nb.ym = m1;
-                nb.yp = p1;
-                nb.zm = nb.zp = (T)0;
-                op.interior_k(a, fidx(g, c + 1, jj, 0), nb, op.raw_from(r1), op.in_from(i1), kxb, kxc, kyb, kyb1,
-                              (T)0, (T)0, acc);
-            }
-            m0 = c0v;
-            m1 = c1v;
-            me = ce;
-            c0v = p0;
-            c1v = p1;
             ce = pe;
             __syncwarp();
             issue(jj + RP + 1);  // into the slot of row jj - 1, which no lane reads any more
@@ -761,6 +828,27 @@ __device__ __forceinline__ void walk_pairs(const Geom& g, F&& f)
         const int ii = DIM == 3 ? HALO_PAD + (int)(row / g.ny) : 0;
         const int kk = HALO_PAD + xs * 64 + 2 * lane;
         if (kk <= xlast) f(fidx(g, kk, jj, ii), kk < xlast);
+    }
+}
+
+// FP32 variant of walk_pairs: 128-cell row segments, four adjacent cells per lane (one
+// 16-byte access); f(i, n) gets the first cell and how many of the four are inner (1..4).
+template <class F>
+__device__ __forceinline__ void walk_quads(const Geom& g, F&& f)
+{
+    const int per_row = (g.nx + 127) / 128;
+    const long nseg = (long)per_row * g.ny * g.nz;
+    const int lane = threadIdx.x & 31;
+    const long warp0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    const int xlast = g.X - HALO_PAD - 1;
+    for (long sgi = warp0; sgi < nseg; sgi += nwarps) {
+        const long row = sgi / per_row;
+        const int xs = (int)(sgi - row * per_row);
+        const int jj = HALO_PAD + (int)(row % g.ny);
+        const int ii = DIM == 3 ? HALO_PAD + (int)(row / g.ny) : 0;
+        const int kk = HALO_PAD + xs * 128 + 4 * lane;
+        if (kk <= xlast) f(fidx(g, kk, jj, ii), min(4, xlast - kk + 1));
     }
 }
 
@@ -1093,28 +1181,38 @@ struct OpCheby {
 constexpr int C2_RP = TEA_CHEBY2_RP;   // ring rows in flight beyond row t+1
 constexpr int C2_RQ = C2_RP + 3;       // ring rows per warp: t-1 .. t+1+C2_RP
 constexpr int C2_NA = 6;               // u, u0, p, mi, Kx, Ky
-constexpr int C2_OUT = 60;             // columns written per warp strip
 enum { C2_U = 0, C2_U0 = 1, C2_P = 2, C2_MI = 3, C2_KX = 4, C2_KY = 5 };
+
+// Strips of the two-iteration kernel: 32 * VEC loaded columns, of which lanes 1..30 write
+// OUT = 30 * VEC; the lane's first column is OUT * strip + VEC * lane - (VEC - 2), so that
+// lane 1 of strip 0 starts at the first inner column.
+template <class T>
+struct Pair2Geom {
+    static constexpr int VEC = RingGeom<T>::VEC;
+    static constexpr int STRIP = RingGeom<T>::STRIP;
+    static constexpr int OUT = 30 * VEC;
+};
 
 template <class Op>
 constexpr size_t cheby2_smem_bytes()
 {
-    return (size_t)RWARPS * C2_RQ * C2_NA * 64 * sizeof(typename Op::T) > ring_smem_bytes<Op>()
-        ? (size_t)RWARPS * C2_RQ * C2_NA * 64 * sizeof(typename Op::T)
+    using T = typename Op::T;
+    return (size_t)RWARPS * C2_RQ * C2_NA * Pair2Geom<T>::STRIP * sizeof(T) > ring_smem_bytes<Op>()
+        ? (size_t)RWARPS * C2_RQ * C2_NA * Pair2Geom<T>::STRIP * sizeof(T)
         : ring_smem_bytes<Op>();
 }
 
 template <class T>
-__device__ __forceinline__ void st_pair(T* p, T x, T y);
+__device__ __forceinline__ void st_vec(T* p, const T* v);
 template <>
-__device__ __forceinline__ void st_pair<double>(double* p, double x, double y)
+__device__ __forceinline__ void st_vec<double>(double* p, const double* v)
 {
-    *reinterpret_cast<double2*>(p) = make_double2(x, y);
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
 }
 template <>
-__device__ __forceinline__ void st_pair<float>(float* p, float x, float y)
+__device__ __forceinline__ void st_vec<float>(float* p, const float* v)
 {
-    *reinterpret_cast<float2*>(p) = make_float2(x, y);
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
 // Op: OpCheby (FP64, the reference's iteration) or OpCheby32 (the FP32 inner solve).
@@ -1122,6 +1220,7 @@ template <class Op>
 __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
 {
     using T = typename Op::T;
+    constexpr int VEC = Pair2Geom<T>::VEC, STRIP = Pair2Geom<T>::STRIP, OUT = Pair2Geom<T>::OUT;
     extern __shared__ __align__(16) unsigned char s_ring_raw[];
     Op op;
     op.begin(a);
@@ -1141,28 +1240,31 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
     const Geom& g = a.g;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * C2_RQ * C2_NA * 64;
+    T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * C2_RQ * C2_NA * STRIP;
     const T* src[C2_NA] = {ucur, op.pair_rhs(a), op.pcur, mi, op.coef_x(a), op.coef_y(a)};
     DDVec<1> acc;
     acc.zero();
     const int xlast = g.X - HALO_PAD - 1;
     const int ylast = g.Y - HALO_PAD - 1;
-    const int per_x = (g.nx + C2_OUT - 1) / C2_OUT;
+    const int per_x = (g.nx + OUT - 1) / OUT;
     const int per_y = (g.ny + a.seg_rows - 1) / a.seg_rows;
     const long nseg = (long)per_x * per_y;
     const long gw = (long)blockIdx.x * RWARPS + warp, nw = (long)gridDim.x * RWARPS;
-    const int cmax = (int)g.pitch - 2;
+    const int cmax = (int)g.pitch - 2 * VEC + 2;
     const bool out_lane = lane >= 1 && lane <= 30;
     const T zero = (T)0;
     for (long sgi = gw; sgi < nseg; sgi += nw) {
         const int xs = (int)(sgi % per_x), ys = (int)(sgi / per_x);
-        const int c = C2_OUT * xs + 2 * lane;  // the lane's first column (lane 1 of strip 0: column 2)
-        const int cc = min(c, cmax);
+        const int c = OUT * xs + VEC * lane - (VEC - 2);  // the lane's first column
+        // Lane 0 of the first strip starts left of column 0 (FP32: at column -2): it only feeds
+        // lane 1, whose first cell is the first inner column and reflects there, so any in-row
+        // data will do; it copies from c + VEC, which keeps the 16-byte alignment (c mod VEC).
+        const int cc = min(c < 0 ? c + VEC : c, cmax);
         const int j0 = HALO_PAD + a.seg_rows * ys;
         const int j1 = min(j0 + a.seg_rows, ylast + 1);
         const int a0 = j0 == HALO_PAD ? HALO_PAD : j0 - 1;  // first row of iteration 1
         const int rlast = min(j1 + 1, ylast + 1);             // last ring row
-        auto slot = [&](int r) { return ring + (size_t)((r - a0 + 1) % C2_RQ) * C2_NA * 64; };
+        auto slot = [&](int r) { return ring + (size_t)((r - a0 + 1) % C2_RQ) * C2_NA * STRIP; };
         auto issue = [&](int r) {
             if (r <= rlast) {
                 T* base = slot(r);
@@ -1171,7 +1273,7 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
 #pragma unroll
                 for (int k = 0; k < C2_NA; ++k) {
                     if (!src[k]) continue;
-                    ring_copy_pair(base + k * 64 + 2 * lane, src[k] + fidx(g, cc, k == C2_U ? urow : irow, 0));
+                    cp_async_16(base + k * STRIP + VEC * lane, src[k] + fidx(g, cc, k == C2_U ? urow : irow, 0));
                 }
             }
             cp_async_commit();
@@ -1179,125 +1281,109 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
         for (int r = a0 - 1; r <= a0 + C2_RP + 1; ++r) issue(r);
         cp_async_wait<C2_RP + 1>();
         __syncwarp();
-        // u at rows t-1 (m) and t (c); iteration-1 u at rows t-2 (vm) and t-1 (vc); its p at t-1 (q).
-        T um0, um1, uc0, uc1;
-        {
-            const T* b = slot(a0 - 1) + C2_U * 64 + 2 * lane;
-            um0 = b[0];
-            um1 = b[1];
-            const T* d = slot(a0) + C2_U * 64 + 2 * lane;
-            uc0 = d[0];
-            uc1 = d[1];
-        }
-        T vm0 = zero, vm1 = zero, vc0 = zero, vc1 = zero, q0 = zero, q1 = zero;
+        // u at rows t-1 (um) and t (uc); iteration-1 u at rows t-2 (vm) and t-1 (vc); its p at t-1 (qv).
+        T um[VEC], uc[VEC], vm[VEC], vc[VEC], qv[VEC];
+        ld_vec(slot(a0 - 1) + C2_U * STRIP + VEC * lane, um);
+        ld_vec(slot(a0) + C2_U * STRIP + VEC * lane, uc);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) vm[q] = vc[q] = qv[q] = zero;
         for (int t = a0; t <= j1; ++t) {
             cp_async_wait<C2_RP>();
             __syncwarp();
             const T* rp = slot(t - 1);
             const T* rc = slot(t);
             const T* rn = slot(t + 1);
-            const T un0 = rn[C2_U * 64 + 2 * lane], un1 = rn[C2_U * 64 + 2 * lane + 1];
+            T un[VEC];
+            ld_vec(rn + C2_U * STRIP + VEC * lane, un);
             // Iteration 1 at row t.
-            T v0, v1, p0, p1;
+            T v[VEC], pv[VEC];
             if (t <= ylast) {
-                const T kx0 = rc[C2_KX * 64 + 2 * lane], kx1 = rc[C2_KX * 64 + 2 * lane + 1];
-                const T kx2 = __shfl_down_sync(0xffffffffu, kx0, 1);
-                const T up = __shfl_up_sync(0xffffffffu, uc1, 1);
-                const T dn = __shfl_down_sync(0xffffffffu, uc0, 1);
-                NbT<T> nb;
-                nb.zm = nb.zp = zero;
-                nb.c = uc0;
-                nb.xm = c == HALO_PAD ? uc0 : up;
-                nb.xp = c == xlast ? uc0 : uc1;
-                nb.ym = um0;
-                nb.yp = un0;
-                {
-                    const T w = smvp_k(nb, kx0, kx1, rc[C2_KY * 64 + 2 * lane], rn[C2_KY * 64 + 2 * lane], zero, zero);
-                    const T r = rc[C2_U0 * 64 + 2 * lane] - w;
-                    p0 = al1 * rc[C2_P * 64 + 2 * lane] + be1 * (precond ? rc[C2_MI * 64 + 2 * lane] * r : r);
-                    v0 = uc0 + p0;
-                }
-                nb.c = uc1;
-                nb.xm = uc0;
-                nb.xp = c + 1 == xlast ? uc1 : dn;
-                nb.ym = um1;
-                nb.yp = un1;
-                {
-                    const T w =
-                        smvp_k(nb, kx1, kx2, rc[C2_KY * 64 + 2 * lane + 1], rn[C2_KY * 64 + 2 * lane + 1], zero, zero);
-                    const T r = rc[C2_U0 * 64 + 2 * lane + 1] - w;
-                    p1 = al1 * rc[C2_P * 64 + 2 * lane + 1] + be1 * (precond ? rc[C2_MI * 64 + 2 * lane + 1] * r : r);
-                    v1 = uc1 + p1;
+                T kx[VEC + 1], ky0[VEC], ky1[VEC], u0[VEC], p0[VEC], m0[VEC];
+                ld_vec(rc + C2_KX * STRIP + VEC * lane, kx);
+                kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
+                ld_vec(rc + C2_KY * STRIP + VEC * lane, ky0);
+                ld_vec(rn + C2_KY * STRIP + VEC * lane, ky1);
+                ld_vec(rc + C2_U0 * STRIP + VEC * lane, u0);
+                ld_vec(rc + C2_P * STRIP + VEC * lane, p0);
+                if (precond) ld_vec(rc + C2_MI * STRIP + VEC * lane, m0);
+                const T up = __shfl_up_sync(0xffffffffu, uc[VEC - 1], 1);
+                const T dn = __shfl_down_sync(0xffffffffu, uc[0], 1);
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    NbT<T> nb;
+                    nb.zm = nb.zp = zero;
+                    nb.c = uc[q];
+                    nb.xm = c + q == HALO_PAD ? uc[q] : (q == 0 ? up : uc[q > 0 ? q - 1 : 0]);
+                    nb.xp = c + q == xlast ? uc[q] : (q == VEC - 1 ? dn : uc[q < VEC - 1 ? q + 1 : q]);
+                    nb.ym = um[q];
+                    nb.yp = un[q];
+                    const T w = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], zero, zero);
+                    const T r = u0[q] - w;
+                    pv[q] = al1 * p0[q] + be1 * (precond ? m0[q] * r : r);
+                    v[q] = uc[q] + pv[q];
                 }
             } else {
                 // Row ylast + 1 is the halo: the reflection of row ylast.
-                v0 = vc0;
-                v1 = vc1;
-                p0 = p1 = zero;
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    v[q] = vc[q];
+                    pv[q] = zero;
+                }
             }
             if (t == HALO_PAD) {
                 // Row 1 is the halo: the reflection of row 2.
-                vc0 = v0;
-                vc1 = v1;
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) vc[q] = v[q];
             }
             // Iteration 2 at row s = t - 1.
             const int srow = t - 1;
             if (srow >= j0) {
-                const T kx0 = rp[C2_KX * 64 + 2 * lane], kx1 = rp[C2_KX * 64 + 2 * lane + 1];
-                const T kx2 = __shfl_down_sync(0xffffffffu, kx0, 1);
-                const T up = __shfl_up_sync(0xffffffffu, vc1, 1);
-                const T dn = __shfl_down_sync(0xffffffffu, vc0, 1);
+                T kx[VEC + 1], ky0[VEC], ky1[VEC], u0[VEC], m0[VEC], u2[VEC], p2[VEC];
+                ld_vec(rp + C2_KX * STRIP + VEC * lane, kx);
+                kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
+                ld_vec(rp + C2_KY * STRIP + VEC * lane, ky0);
+                ld_vec(rc + C2_KY * STRIP + VEC * lane, ky1);
+                ld_vec(rp + C2_U0 * STRIP + VEC * lane, u0);
+                if (precond) ld_vec(rp + C2_MI * STRIP + VEC * lane, m0);
+                const T up = __shfl_up_sync(0xffffffffu, vc[VEC - 1], 1);
+                const T dn = __shfl_down_sync(0xffffffffu, vc[0], 1);
                 const long i = fidx(g, c, srow, 0);
-                NbT<T> nb;
-                nb.zm = nb.zp = zero;
-                nb.c = vc0;
-                nb.xm = c == HALO_PAD ? vc0 : up;
-                nb.xp = c == xlast ? vc0 : vc1;
-                nb.ym = vm0;
-                nb.yp = v0;
-                T u2a, p2a, u2b, p2b, ra, rb;
-                {
-                    const T w = smvp_k(nb, kx0, kx1, rp[C2_KY * 64 + 2 * lane], rc[C2_KY * 64 + 2 * lane], zero, zero);
-                    ra = rp[C2_U0 * 64 + 2 * lane] - w;
-                    p2a = al2 * q0 + be2 * (precond ? rp[C2_MI * 64 + 2 * lane] * ra : ra);
-                    u2a = vc0 + p2a;
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    NbT<T> nb;
+                    nb.zm = nb.zp = zero;
+                    nb.c = vc[q];
+                    nb.xm = c + q == HALO_PAD ? vc[q] : (q == 0 ? up : vc[q > 0 ? q - 1 : 0]);
+                    nb.xp = c + q == xlast ? vc[q] : (q == VEC - 1 ? dn : vc[q < VEC - 1 ? q + 1 : q]);
+                    nb.ym = vm[q];
+                    nb.yp = v[q];
+                    const T w = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], zero, zero);
+                    const T r = u0[q] - w;
+                    p2[q] = al2 * qv[q] + be2 * (precond ? m0[q] * r : r);
+                    u2[q] = vc[q] + p2[q];
+                    if (check2 && out_lane && c + q <= xlast) dd_add(acc.v[0], (double)r * (double)r);
                 }
-                nb.c = vc1;
-                nb.xm = vc0;
-                nb.xp = c + 1 == xlast ? vc1 : dn;
-                nb.ym = vm1;
-                nb.yp = v1;
-                {
-                    const T w =
-                        smvp_k(nb, kx1, kx2, rp[C2_KY * 64 + 2 * lane + 1], rc[C2_KY * 64 + 2 * lane + 1], zero, zero);
-                    rb = rp[C2_U0 * 64 + 2 * lane + 1] - w;
-                    p2b = al2 * q1 + be2 * (precond ? rp[C2_MI * 64 + 2 * lane + 1] * rb : rb);
-                    u2b = vc1 + p2b;
-                }
-                const bool oka = out_lane && c <= xlast;
-                const bool okb = out_lane && c + 1 <= xlast;
-                if (oka && okb) {
-                    st_pair(unew + i, u2a, u2b);
-                    st_pair(pnew + i, p2a, p2b);
-                } else if (oka) {
-                    unew[i] = u2a;
-                    pnew[i] = p2a;
-                }
-                if (check2) {
-                    if (oka) dd_add(acc.v[0], (double)ra * (double)ra);
-                    if (okb) dd_add(acc.v[0], (double)rb * (double)rb);
+                if (out_lane && c + VEC - 1 <= xlast) {
+                    st_vec(unew + i, u2);
+                    st_vec(pnew + i, p2);
+                } else if (out_lane) {
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) {
+                        if (c + q <= xlast) {
+                            unew[i + q] = u2[q];
+                            pnew[i + q] = p2[q];
+                        }
+                    }
                 }
             }
-            vm0 = vc0;
-            vm1 = vc1;
-            vc0 = v0;
-            vc1 = v1;
-            q0 = p0;
-            q1 = p1;
-            um0 = uc0;
-            um1 = uc1;
-            uc0 = un0;
-            uc1 = un1;
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                vm[q] = vc[q];
+                vc[q] = v[q];
+                qv[q] = pv[q];
+                um[q] = uc[q];
+                uc[q] = un[q];
+            }
             __syncwarp();
             issue(t + C2_RP + 2);  // into the slot of row t - 1, which no lane reads any more
         }
@@ -1770,18 +1856,23 @@ __global__ void __launch_bounds__(256) k_cg32_sweep_b(FusedArgs a)
     const float* __restrict__ W = a.w32;
     DDVec<1> acc;
     acc.zero();
-    walk_pairs(a.g, [&](long i, bool two) {
-        if (two) {
-            const float2 r2 = *reinterpret_cast<const float2*>(R + i);
-            const float2 w2 = *reinterpret_cast<const float2*>(W + i);
-            const float r0 = r2.x - alpha * w2.x, r1 = r2.y - alpha * w2.y;
-            *reinterpret_cast<float2*>(R + i) = make_float2(r0, r1);
+    walk_quads(a.g, [&](long i, int n) {
+        if (n == 4) {
+            const float4 r4 = *reinterpret_cast<const float4*>(R + i);
+            const float4 w4 = *reinterpret_cast<const float4*>(W + i);
+            const float r0 = r4.x - alpha * w4.x, r1 = r4.y - alpha * w4.y;
+            const float r2 = r4.z - alpha * w4.z, r3 = r4.w - alpha * w4.w;
+            *reinterpret_cast<float4*>(R + i) = make_float4(r0, r1, r2, r3);
             dd_add(acc.v[0], (double)r0 * (double)r0);
             dd_add(acc.v[0], (double)r1 * (double)r1);
+            dd_add(acc.v[0], (double)r2 * (double)r2);
+            dd_add(acc.v[0], (double)r3 * (double)r3);
         } else {
-            const float r0 = R[i] - alpha * W[i];
-            R[i] = r0;
-            dd_add(acc.v[0], (double)r0 * (double)r0);
+            for (int k = 0; k < n; ++k) {
+                const float r0 = R[i + k] - alpha * W[i + k];
+                R[i + k] = r0;
+                dd_add(acc.v[0], (double)r0 * (double)r0);
+            }
         }
     });
     grid_reduce_then<1>(acc, a.red, [&](const double* v) {

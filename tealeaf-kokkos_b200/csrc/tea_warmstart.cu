@@ -1,0 +1,920 @@
+// Learned warm start of the implicit solve (no counterpart in the reference).
+//
+// A small U-Net (tea_ws_conv.cuh, tea_ws_kernels.cuh; the numpy restatement is
+// oracle/warmstart_oracle.py) predicts the timestep increment du = u(n+1) - u0 from the
+// step's inputs u0 = density * energy, density, Kx and Ky.  The solve starts from
+// u0 + du when that guess has a smaller FP64 initial residual than u0 itself, and
+// converges to the same tolerance either way, so no network error survives.  Training
+// pairs are recorded from the solver's own timesteps (tea_ws_record_), the network is
+// trained on the GPU by this file's forward and backward kernels (bfloat16 storage,
+// float32 accumulation, Adam on float32 master weights) and attached to a chunk
+// (tea_ws_attach_), whose whole-solve calls then warm-start from it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <vector>
+
+#include "../../include/tea_b200.h"
+#include "tea_chunk.cuh"
+#include "tea_common.cuh"
+#include "tea_ws_kernels.cuh"
+
+#define TEA_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace tea {
+
+Chunk* get_chunk(const int* chunk);
+
+namespace ws {
+
+constexpr int IN_PAD = 16;  // network input channels as stored (4 features, zero padding)
+constexpr int N_FEAT = 4;
+
+// ----------------------------------------------------------------------------- chunk <-> features
+
+// Largest |u0| over the inner cells (the scale of u): per-block maxima, then one block.
+__global__ void k_absmax(Geom g, const double* u0, double* partial, double* out, int nblocks_final)
+{
+    __shared__ double s[256];
+    double m = 0.0;
+    const long n = (long)g.nx * g.ny;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int kk = HALO_PAD + (int)(i % g.nx), jj = HALO_PAD + (int)(i / g.nx);
+        m = fmax(m, fabs(u0[fidx(g, kk, jj, 0)]));
+    }
+    s[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s[threadIdx.x] = fmax(s[threadIdx.x], s[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
+    (void)nblocks_final;
+    (void)out;
+}
+
+__global__ void k_absmax_final(const double* partial, int n, double* out)
+{
+    __shared__ double s[256];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, partial[i]);
+    s[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s[threadIdx.x] = fmax(s[threadIdx.x], s[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = s[0] > 0.0 ? s[0] : 1.0;
+}
+
+// Network input of the chunk's timestep: [ny][nx][IN_PAD] bfloat16, channels u0 / scale,
+// log10(density) / 2, log10(1 + Kx) / 4, log10(1 + Ky) / 4, then zeros.
+__global__ void k_features(Geom g, const double* u0, const double* dens, const double* kx, const double* ky,
+                           const double* scale, bf16* x)
+{
+    const long n = (long)g.nx * g.ny;
+    const double inv = 1.0 / scale[0];
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int kk = HALO_PAD + (int)(i % g.nx), jj = HALO_PAD + (int)(i / g.nx);
+        const long f = fidx(g, kk, jj, 0);
+        __align__(16) bf16 v[IN_PAD];
+        v[0] = __float2bfloat16((float)(u0[f] * inv));
+        v[1] = __float2bfloat16((float)(log10(dens[f]) * 0.5));
+        v[2] = __float2bfloat16((float)(log10(1.0 + kx[f]) * 0.25));
+        v[3] = __float2bfloat16((float)(log10(1.0 + ky[f]) * 0.25));
+        for (int c = N_FEAT; c < IN_PAD; ++c) v[c] = __float2bfloat16(0.f);
+        uint4* dst = reinterpret_cast<uint4*>(x + i * IN_PAD);
+        dst[0] = reinterpret_cast<const uint4*>(v)[0];
+        dst[1] = reinterpret_cast<const uint4*>(v)[1];
+    }
+}
+
+// A recorded pair: the four features and the target (u - u0) / scale.
+__global__ void k_record(Geom g, const bf16* x, const double* u, const double* u0, const double* scale, bf16* feat,
+                         float* tgt)
+{
+    const long n = (long)g.nx * g.ny;
+    const double inv = 1.0 / scale[0];
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int kk = HALO_PAD + (int)(i % g.nx), jj = HALO_PAD + (int)(i / g.nx);
+        const long f = fidx(g, kk, jj, 0);
+        for (int c = 0; c < N_FEAT; ++c) feat[i * N_FEAT + c] = x[i * IN_PAD + c];
+        tgt[i] = (float)((u[f] - u0[f]) * inv);
+    }
+}
+
+// u = u0 + y * scale over the inner cells.
+__global__ void k_apply_guess(Geom g, const float* y, const double* u0, const double* scale, double inv_out,
+                              double* u)
+{
+    const long n = (long)g.nx * g.ny;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int kk = HALO_PAD + (int)(i % g.nx), jj = HALO_PAD + (int)(i / g.nx);
+        const long f = fidx(g, kk, jj, 0);
+        u[f] = u0[f] + (double)y[i] * inv_out * scale[0];
+    }
+}
+
+struct Crop {
+    const bf16* feat;
+    const float* tgt;
+    int W, y0, x0;  // source width, crop origin
+};
+
+// Training batch: b crops of size s x s from recorded pairs.
+__global__ void k_crops(const Crop* crops, int s, bf16* x, float* t, int nb, float tscale)
+{
+    const long per = (long)s * s;
+    const long total = per * nb;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int b = (int)(i / per);
+        const int yy = (int)((i % per) / s), xx = (int)(i % s);
+        const Crop c = crops[b];
+        const long src = (long)(c.y0 + yy) * c.W + (c.x0 + xx);
+        for (int ch = 0; ch < IN_PAD; ++ch)
+            x[i * IN_PAD + ch] = ch < N_FEAT ? c.feat[src * N_FEAT + ch] : __float2bfloat16(0.f);
+        t[i] = c.tgt[src] * tscale;
+    }
+}
+
+// Sum of squares of n floats into *out (float32 atomics of block sums).
+__global__ void k_sumsq(const float* v, long n, float* out)
+{
+    __shared__ float s[256];
+    float a = 0.f;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) a += v[i] * v[i];
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(out, s[0]);
+}
+
+// ----------------------------------------------------------------------------- network
+
+struct Conv {
+    int cin, cout;
+    float *w = nullptr, *b = nullptr, *gw = nullptr, *gb = nullptr, *mw = nullptr, *vw = nullptr, *mb = nullptr,
+          *vb = nullptr;
+    bf16 *w16 = nullptr, *wt16 = nullptr;
+};
+
+struct Pair {
+    bf16* feat = nullptr;
+    float* tgt = nullptr;
+    int H = 0, W = 0;
+};
+
+struct Net {
+    int levels = 0, base = 0, device = 0;
+    std::vector<int> ch;
+    std::vector<Conv> conv;  // enc0a, enc0b, ..., enc(L-1)b, dec(L-2)a, dec(L-2)b, ..., dec0a, dec0b
+    float *hw = nullptr, *hb = nullptr, *ghw = nullptr, *ghb = nullptr, *mh = nullptr, *vh = nullptr;  // head: C0 + 1
+    long step = 0;
+    int use_ref = 0;  // 1: CUDA-core convolutions
+    cudaStream_t stream = nullptr;
+    int* d_err = nullptr;
+    float* d_sums = nullptr;
+    double* d_scale = nullptr;
+    double* d_partial = nullptr;
+    // Workspace for n images of H x W.
+    int wn = 0, wH = 0, wW = 0;
+    std::vector<void*> wsbuf;
+    bf16* x0 = nullptr;
+    std::vector<bf16*> A, cat, P, DA, DB, gcat;
+    bf16* bottom = nullptr;
+    bf16 *G[3] = {nullptr, nullptr, nullptr};
+    float *y = nullptr, *target = nullptr;
+    std::vector<Pair> pairs;
+    Crop* d_crops = nullptr;
+    int sms = 148;
+    float out_scale = 1.f;  // the network predicts du / max|u0| * out_scale (unit RMS on the pairs)
+};
+
+std::mutex g_mutex;
+std::vector<std::unique_ptr<Net>>& nets()
+{
+    static std::vector<std::unique_ptr<Net>> v;
+    return v;
+}
+
+Net* get_net(const int* id)
+{
+    auto& v = nets();
+    if (!id || *id < 1 || (size_t)*id > v.size() || !v[*id - 1]) {
+        set_status(TEA_ERR_BAD_ARGUMENT, "warm start: invalid network id %d", id ? *id : -1);
+        return nullptr;
+    }
+    return v[*id - 1].get();
+}
+
+#define WS_CK(call)                                                                                       \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess) {                                                                          \
+            set_status(TEA_ERR_CUDA, "warm start: %s failed: %s", #call, cudaGetErrorString(e_));       \
+            return TEA_ERR_CUDA;                                                                          \
+        }                                                                                                 \
+    } while (0)
+
+int grid_for(long work, int threads = 256)
+{
+    return (int)std::max<long>(1, std::min<long>((work + threads - 1) / threads, 148L * 16));
+}
+
+template <class T>
+int dalloc(T** p, size_t count)
+{
+    WS_CK(cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(count, 1)));
+    WS_CK(cudaMemset(*p, 0, sizeof(T) * std::max<size_t>(count, 1)));
+    return TEA_OK;
+}
+
+void free_workspace(Net* N)
+{
+    for (void* p : N->wsbuf) cudaFree(p);
+    N->wsbuf.clear();
+    N->A.clear();
+    N->cat.clear();
+    N->P.clear();
+    N->DA.clear();
+    N->DB.clear();
+    N->gcat.clear();
+    N->wn = N->wH = N->wW = 0;
+}
+
+int ensure_workspace(Net* N, int n, int H, int W)
+{
+    if (N->wn == n && N->wH == H && N->wW == W) return TEA_OK;
+    free_workspace(N);
+    const int L = N->levels;
+    auto take = [&](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
+        N->wsbuf.push_back(p);
+        return p;
+    };
+    const long pix = (long)n * H * W;
+    auto lv = [&](int l) { return pix >> (2 * l); };
+    bool ok = true;
+    N->x0 = (bf16*)take(sizeof(bf16) * pix * IN_PAD);
+    ok = ok && N->x0;
+    N->A.resize(L);
+    N->cat.resize(L);
+    N->gcat.resize(L);
+    N->P.resize(L);
+    N->DA.resize(L);
+    N->DB.resize(L);
+    for (int l = 0; l < L; ++l) {
+        N->A[l] = (bf16*)take(sizeof(bf16) * lv(l) * N->ch[l]);
+        ok = ok && N->A[l];
+        if (l < L - 1) {
+            const int cc = N->ch[l + 1] + N->ch[l];
+            N->cat[l] = (bf16*)take(sizeof(bf16) * lv(l) * cc);
+            N->gcat[l] = (bf16*)take(sizeof(bf16) * lv(l) * cc);
+            N->P[l] = (bf16*)take(sizeof(bf16) * lv(l + 1) * N->ch[l]);
+            N->DA[l] = (bf16*)take(sizeof(bf16) * lv(l) * N->ch[l]);
+            N->DB[l] = (bf16*)take(sizeof(bf16) * lv(l) * N->ch[l]);
+            ok = ok && N->cat[l] && N->gcat[l] && N->P[l] && N->DA[l] && N->DB[l];
+        }
+    }
+    N->bottom = (bf16*)take(sizeof(bf16) * lv(L - 1) * N->ch[L - 1]);
+    for (int k = 0; k < 3; ++k) {
+        N->G[k] = (bf16*)take(sizeof(bf16) * pix * N->ch[0]);
+        ok = ok && N->G[k];
+    }
+    N->y = (float*)take(sizeof(float) * pix);
+    N->target = (float*)take(sizeof(float) * pix);
+    ok = ok && N->bottom && N->y && N->target;
+    if (!ok) {
+        free_workspace(N);
+        set_status(TEA_ERR_CUDA, "warm start: out of device memory for %d x %d x %d", n, H, W);
+        return TEA_ERR_CUDA;
+    }
+    N->wn = n;
+    N->wH = H;
+    N->wW = W;
+    return TEA_OK;
+}
+
+// y = conv3x3(x) over n images of H x W.
+void conv(Net* N, View x, View y, const bf16* w, const float* bias, int relu, View mask, int n, int H, int W,
+          int cin, int cout)
+{
+    ConvArgs a;
+    a.x = x.p;
+    a.xcs = x.cs;
+    a.xco = x.co;
+    a.y = y.p;
+    a.ycs = y.cs;
+    a.yco = y.co;
+    a.w = w;
+    a.bias = bias;
+    a.mask = mask.p;
+    a.mcs = mask.cs;
+    a.mco = mask.co;
+    a.relu = relu;
+    a.n = n;
+    a.H = H;
+    a.W = W;
+    a.cin = cin;
+    a.cout = cout;
+    a.err = N->d_err;
+    const long npix = (long)n * H * W;
+    if (N->use_ref) {
+        k_conv_ref<<<grid_for(npix * cout), 256, 0, N->stream>>>(a);
+        return;
+    }
+    const long tiles = (npix + TC_M - 1) / TC_M;
+    const int bytes = (int)conv_tc_smem_bytes(cin, cout);
+    cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_tc, TC_THREADS, bytes);
+    occ = std::max(1, std::min(occ, 512 / tmem_cols(cout)));
+    const long grid = std::min<long>(tiles, (long)N->sms * occ);
+    k_conv_tc<<<(int)grid, TC_THREADS, bytes, N->stream>>>(a);
+}
+
+void wgrad(Net* N, View x, View gy, Conv& L, int n, int H, int W)
+{
+    const int tiles = 9 * ((L.cin + 31) / 32) * ((L.cout + 31) / 32);
+    const long npix = (long)n * H * W;
+    const int splits = (int)std::max<long>(1, std::min<long>((N->sms * 8 + tiles - 1) / tiles, (npix + 255) / 256));
+    k_wgrad<<<dim3(tiles, splits), 256, 0, N->stream>>>(x.p, x.cs, x.co, gy.p, gy.cs, gy.co, n, H, W, L.cin, L.cout,
+                                                        L.gw, L.gb);
+}
+
+View view(bf16* p, int cs, int co, int c)
+{
+    View v;
+    v.p = p;
+    v.cs = cs;
+    v.co = co;
+    v.c = c;
+    return v;
+}
+const View kNoView = {nullptr, 0, 0, 0};
+
+Conv& enc(Net* N, int l, int s) { return N->conv[2 * l + s]; }
+Conv& dec(Net* N, int l, int s) { return N->conv[2 * N->levels + 2 * (N->levels - 2 - l) + s]; }
+
+// Forward pass over the workspace's n images; x0 must hold the input.
+void forward(Net* N)
+{
+    const int L = N->levels, n = N->wn;
+    View h = view(N->x0, IN_PAD, 0, IN_PAD);
+    for (int l = 0; l < L; ++l) {
+        const int H = N->wH >> l, W = N->wW >> l, C = N->ch[l];
+        Conv& a = enc(N, l, 0);
+        Conv& b = enc(N, l, 1);
+        conv(N, h, view(N->A[l], C, 0, C), a.w16, a.b, 1, kNoView, n, H, W, a.cin, C);
+        const View out = l < L - 1 ? view(N->cat[l], N->ch[l + 1] + C, N->ch[l + 1], C) : view(N->bottom, C, 0, C);
+        conv(N, view(N->A[l], C, 0, C), out, b.w16, b.b, 1, kNoView, n, H, W, C, C);
+        if (l < L - 1) {
+            k_avgpool<<<grid_for((long)n * (H / 2) * (W / 2) * C), 256, 0, N->stream>>>(out, N->P[l], n, H, W);
+            h = view(N->P[l], C, 0, C);
+        }
+    }
+    for (int l = L - 2; l >= 0; --l) {
+        const int H = N->wH >> l, W = N->wW >> l, C = N->ch[l], Cu = N->ch[l + 1];
+        const View hin = l == L - 2 ? view(N->bottom, Cu, 0, Cu) : view(N->DB[l + 1], Cu, 0, Cu);
+        k_upsample<<<grid_for((long)n * H * W * Cu), 256, 0, N->stream>>>(hin, view(N->cat[l], Cu + C, 0, Cu), n, H, W);
+        Conv& a = dec(N, l, 0);
+        Conv& b = dec(N, l, 1);
+        conv(N, view(N->cat[l], Cu + C, 0, Cu + C), view(N->DA[l], C, 0, C), a.w16, a.b, 1, kNoView, n, H, W, Cu + C,
+             C);
+        conv(N, view(N->DA[l], C, 0, C), view(N->DB[l], C, 0, C), b.w16, b.b, 1, kNoView, n, H, W, C, C);
+    }
+}
+
+void head(Net* N, const float* target)
+{
+    const long npix = (long)N->wn * N->wH * N->wW;
+    const int C0 = N->ch[0];
+    const int grid = grid_for(npix);
+    if (C0 == 16)
+        k_head<16><<<grid, 256, 0, N->stream>>>(N->DB[0], N->hw, N->hb, N->y, npix, target, N->d_sums, N->G[0],
+                                                 N->ghw, N->ghb);
+    else if (C0 == 32)
+        k_head<32><<<grid, 256, 0, N->stream>>>(N->DB[0], N->hw, N->hb, N->y, npix, target, N->d_sums, N->G[0],
+                                                 N->ghw, N->ghb);
+    else
+        k_head<64><<<grid, 256, 0, N->stream>>>(N->DB[0], N->hw, N->hb, N->y, npix, target, N->d_sums, N->G[0],
+                                                 N->ghw, N->ghb);
+}
+
+// Backward pass after forward() and head(target): accumulates every parameter gradient.
+void backward(Net* N)
+{
+    const int L = N->levels, n = N->wn;
+    bf16* gcur = N->G[0];  // gradient w.r.t. the pre-activation of dec0b (from the head)
+    bf16* gnext = N->G[1];
+    bf16* gtmp = N->G[2];
+    for (int l = 0; l <= L - 2; ++l) {
+        const int H = N->wH >> l, W = N->wW >> l, C = N->ch[l], Cu = N->ch[l + 1];
+        Conv& a = dec(N, l, 0);
+        Conv& b = dec(N, l, 1);
+        wgrad(N, view(N->DA[l], C, 0, C), view(gcur, C, 0, C), b, n, H, W);
+        conv(N, view(gcur, C, 0, C), view(gnext, C, 0, C), b.wt16, nullptr, 0, view(N->DA[l], C, 0, C), n, H, W, C,
+             C);
+        wgrad(N, view(N->cat[l], Cu + C, 0, Cu + C), view(gnext, C, 0, C), a, n, H, W);
+        conv(N, view(gnext, C, 0, C), view(N->gcat[l], Cu + C, 0, Cu + C), a.wt16, nullptr, 0,
+             view(N->cat[l], Cu + C, 0, Cu + C), n, H, W, C, Cu + C);
+        k_upsample_bw<<<grid_for((long)n * (H / 2) * (W / 2) * Cu), 256, 0, N->stream>>>(
+            view(N->gcat[l], Cu + C, 0, Cu), gcur, n, H, W);
+    }
+    // gcur: gradient w.r.t. the pre-activation of enc(L-1)b.
+    for (int l = L - 1; l >= 0; --l) {
+        const int H = N->wH >> l, W = N->wW >> l, C = N->ch[l];
+        Conv& a = enc(N, l, 0);
+        Conv& b = enc(N, l, 1);
+        if (l < L - 1) {
+            // gcur holds the gradient w.r.t. the pooled tensor P[l] (coarse); add the skip's.
+            const int Cu = N->ch[l + 1];
+            k_avgpool_bw<<<grid_for((long)n * H * W * C), 256, 0, N->stream>>>(
+                gcur, view(N->cat[l], Cu + C, Cu, C), view(N->gcat[l], Cu + C, Cu, C), gtmp, n, H, W);
+            std::swap(gcur, gtmp);
+        }
+        wgrad(N, view(N->A[l], C, 0, C), view(gcur, C, 0, C), b, n, H, W);
+        conv(N, view(gcur, C, 0, C), view(gnext, C, 0, C), b.wt16, nullptr, 0, view(N->A[l], C, 0, C), n, H, W, C, C);
+        const View xin = l == 0 ? view(N->x0, IN_PAD, 0, IN_PAD) : view(N->P[l - 1], N->ch[l - 1], 0, N->ch[l - 1]);
+        wgrad(N, xin, view(gnext, C, 0, C), a, n, H, W);
+        if (l > 0) {
+            const int Cp = N->ch[l - 1];
+            conv(N, view(gnext, C, 0, C), view(gcur, Cp, 0, Cp), a.wt16, nullptr, 0, kNoView, n, H, W, C, Cp);
+        }
+    }
+}
+
+void refresh_bf16(Net* N)
+{
+    for (Conv& c : N->conv)
+        k_weights_bf16<<<grid_for((long)c.cout * 9 * c.cin), 256, 0, N->stream>>>(c.w, c.w16, c.wt16, c.cout, c.cin);
+}
+
+void adam_step(Net* N, float lr)
+{
+    N->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float c1 = 1.f - powf(b1, (float)N->step), c2 = 1.f - powf(b2, (float)N->step);
+    for (Conv& c : N->conv) {
+        const long nw = (long)c.cout * 9 * c.cin;
+        k_adam<<<grid_for(nw), 256, 0, N->stream>>>(c.w, c.gw, c.mw, c.vw, nw, lr, b1, b2, eps, c1, c2);
+        k_adam<<<grid_for(c.cout), 256, 0, N->stream>>>(c.b, c.gb, c.mb, c.vb, c.cout, lr, b1, b2, eps, c1, c2);
+    }
+    const int nh = N->ch[0] + 1;  // head weights and bias are contiguous
+    k_adam<<<1, 256, 0, N->stream>>>(N->hw, N->ghw, N->mh, N->vh, nh, lr, b1, b2, eps, c1, c2);
+    refresh_bf16(N);
+}
+
+int cin_of_oracle(const Net* N, int k) { return k == 0 ? N_FEAT : N->conv[k].cin; }
+
+// Parameters in the oracle's order (oracle/warmstart_oracle.py layer_shapes): per layer
+// w[co][9][cin] (cin of the first layer: the 4 real features) then b; head w, head b.
+long param_count(const Net* N)
+{
+    long n = 0;
+    for (size_t k = 0; k < N->conv.size(); ++k)
+        n += (long)N->conv[k].cout * 9 * cin_of_oracle(N, (int)k) + N->conv[k].cout;
+    return n + N->ch[0] + 1;
+}
+
+// Copy between host oracle-order arrays and the device (w: master weights, or gradients).
+int transfer_params(Net* N, float* host, bool to_device, bool grads)
+{
+    long off = 0;
+    std::vector<float> buf;
+    for (size_t k = 0; k < N->conv.size(); ++k) {
+        Conv& c = N->conv[k];
+        const int ci_o = cin_of_oracle(N, (int)k);
+        buf.assign((size_t)c.cout * 9 * c.cin, 0.f);
+        float* dw = grads ? c.gw : c.w;
+        float* db = grads ? c.gb : c.b;
+        if (to_device) {
+            for (int co = 0; co < c.cout; ++co)
+                for (int t = 0; t < 9; ++t)
+                    for (int ci = 0; ci < ci_o; ++ci)
+                        buf[((size_t)co * 9 + t) * c.cin + ci] = host[off + ((long)co * 9 + t) * ci_o + ci];
+            WS_CK(cudaMemcpy(dw, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice));
+            WS_CK(cudaMemcpy(db, host + off + (long)c.cout * 9 * ci_o, sizeof(float) * c.cout, cudaMemcpyHostToDevice));
+        } else {
+            WS_CK(cudaMemcpy(buf.data(), dw, sizeof(float) * buf.size(), cudaMemcpyDeviceToHost));
+            for (int co = 0; co < c.cout; ++co)
+                for (int t = 0; t < 9; ++t)
+                    for (int ci = 0; ci < ci_o; ++ci)
+                        host[off + ((long)co * 9 + t) * ci_o + ci] = buf[((size_t)co * 9 + t) * c.cin + ci];
+            WS_CK(cudaMemcpy(host + off + (long)c.cout * 9 * ci_o, db, sizeof(float) * c.cout, cudaMemcpyDeviceToHost));
+        }
+        off += (long)c.cout * 9 * ci_o + c.cout;
+    }
+    const int nh = N->ch[0] + 1;
+    float* dh = grads ? N->ghw : N->hw;
+    if (to_device)
+        WS_CK(cudaMemcpy(dh, host + off, sizeof(float) * nh, cudaMemcpyHostToDevice));
+    else
+        WS_CK(cudaMemcpy(host + off, dh, sizeof(float) * nh, cudaMemcpyDeviceToHost));
+    if (to_device && !grads) refresh_bf16(N);
+    return TEA_OK;
+}
+
+int check_err(Net* N, const char* what)
+{
+    WS_CK(cudaStreamSynchronize(N->stream));
+    int e = 0;
+    WS_CK(cudaMemcpy(&e, N->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        set_status(TEA_ERR_CUDA, "warm start: %s: a tensor-core wait timed out", what);
+        int z = 0;
+        cudaMemcpy(N->d_err, &z, sizeof(int), cudaMemcpyHostToDevice);
+        return TEA_ERR_CUDA;
+    }
+    return TEA_OK;
+}
+
+}  // namespace ws
+
+// ----------------------------------------------------------------------------- solve hook
+
+// Called by ext_tea_leaf_solve_ after the CG set-up (u = u0, r, p, rro): predicts
+// du, and keeps u = u0 + du when its initial residual is smaller.  Returns 1 when the
+// guess was kept (the caller then re-initialises r, p and rro from it), 0 otherwise.
+int ws_predict_into(Chunk* c, double* u_out)
+{
+    using namespace ws;
+    Net* N = static_cast<Net*>(c->ws);
+    if (!N || DIM != 2) return 0;
+    const Geom& g = c->g;
+    if (ensure_workspace(N, 1, g.ny, g.nx) != TEA_OK) return 0;
+    if (g.nx % (1 << (N->levels - 1)) || g.ny % (1 << (N->levels - 1))) return 0;
+    cudaStream_t saved = N->stream;
+    N->stream = c->stream;
+    const int blocks = 512;
+    k_absmax<<<blocks, 256, 0, c->stream>>>(g, c->f.u0, N->d_partial, N->d_scale, blocks);
+    k_absmax_final<<<1, 256, 0, c->stream>>>(N->d_partial, blocks, N->d_scale);
+    k_features<<<grid_for((long)g.nx * g.ny), 256, 0, c->stream>>>(g, c->f.u0, c->f.density, c->f.kx, c->f.ky,
+                                                                   N->d_scale, N->x0);
+    forward(N);
+    head(N, nullptr);
+    k_apply_guess<<<grid_for((long)g.nx * g.ny), 256, 0, c->stream>>>(g, N->y, c->f.u0, N->d_scale,
+                                                                       1.0 / (double)N->out_scale, u_out);
+    N->stream = saved;
+    return 1;
+}
+
+}  // namespace tea
+
+using namespace tea;
+using namespace tea::ws;
+
+TEA_EXPORT int tea_ws_create_(const int* levels, const int* base, const int* seed, int* net)
+{
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!levels || !base || !net || *levels < 2 || *levels > 5 || (*base != 16 && *base != 32 && *base != 64)) {
+        set_status(TEA_ERR_BAD_ARGUMENT, "tea_ws_create_: levels must be 2..5 and base 16, 32 or 64");
+        return TEA_ERR_BAD_ARGUMENT;
+    }
+    auto N = std::make_unique<Net>();
+    N->levels = *levels;
+    N->base = *base;
+    WS_CK(cudaGetDevice(&N->device));
+    WS_CK(cudaDeviceGetAttribute(&N->sms, cudaDevAttrMultiProcessorCount, N->device));
+    WS_CK(cudaStreamCreateWithFlags(&N->stream, cudaStreamNonBlocking));
+    for (int l = 0; l < N->levels; ++l) N->ch.push_back(N->base << l);
+    if (N->ch.back() + N->ch[N->levels - 2] > 256) {
+        set_status(TEA_ERR_BAD_ARGUMENT, "tea_ws_create_: too many channels for one tensor-core tile");
+        return TEA_ERR_BAD_ARGUMENT;
+    }
+    int prev = IN_PAD;
+    for (int l = 0; l < N->levels; ++l) {
+        N->conv.push_back({prev, N->ch[l]});
+        N->conv.push_back({N->ch[l], N->ch[l]});
+        prev = N->ch[l];
+    }
+    for (int l = N->levels - 2; l >= 0; --l) {
+        N->conv.push_back({N->ch[l + 1] + N->ch[l], N->ch[l]});
+        N->conv.push_back({N->ch[l], N->ch[l]});
+    }
+    // He initialisation (the first layer over its 4 real inputs), small biases; seeded.
+    std::mt19937_64 rng((unsigned long long)(seed ? *seed : 0));
+    std::normal_distribution<float> nd(0.f, 1.f);
+    for (size_t k = 0; k < N->conv.size(); ++k) {
+        Conv& c = N->conv[k];
+        const long nw = (long)c.cout * 9 * c.cin;
+        for (float** p : {&c.w, &c.gw, &c.mw, &c.vw})
+            if (dalloc(p, nw)) return TEA_ERR_CUDA;
+        for (float** p : {&c.b, &c.gb, &c.mb, &c.vb})
+            if (dalloc(p, c.cout)) return TEA_ERR_CUDA;
+        if (dalloc(&c.w16, nw) || dalloc(&c.wt16, nw)) return TEA_ERR_CUDA;
+        const int ci_real = k == 0 ? N_FEAT : c.cin;
+        const float sd = sqrtf(2.f / (9.f * ci_real));
+        std::vector<float> w(nw, 0.f), b(c.cout);
+        for (int co = 0; co < c.cout; ++co)
+            for (int t = 0; t < 9; ++t)
+                for (int ci = 0; ci < ci_real; ++ci) w[((long)co * 9 + t) * c.cin + ci] = sd * nd(rng);
+        for (auto& v : b) v = 0.01f * nd(rng);
+        WS_CK(cudaMemcpy(c.w, w.data(), sizeof(float) * nw, cudaMemcpyHostToDevice));
+        WS_CK(cudaMemcpy(c.b, b.data(), sizeof(float) * c.cout, cudaMemcpyHostToDevice));
+    }
+    const int nh = N->ch[0] + 1;
+    for (float** p : {&N->hw, &N->ghw, &N->mh, &N->vh})
+        if (dalloc(p, nh)) return TEA_ERR_CUDA;
+    N->hb = N->hw + N->ch[0];
+    N->ghb = N->ghw + N->ch[0];
+    {
+        std::vector<float> h(nh, 0.f);
+        for (int k = 0; k < N->ch[0]; ++k) h[k] = sqrtf(1.f / N->ch[0]) * nd(rng) * 0.1f;
+        WS_CK(cudaMemcpy(N->hw, h.data(), sizeof(float) * nh, cudaMemcpyHostToDevice));
+    }
+    if (dalloc(&N->d_err, 1) || dalloc(&N->d_sums, 4) || dalloc(&N->d_scale, 1) || dalloc(&N->d_partial, 512) ||
+        dalloc(&N->d_crops, 256))
+        return TEA_ERR_CUDA;
+    refresh_bf16(N.get());
+    WS_CK(cudaStreamSynchronize(N->stream));
+    nets().push_back(std::move(N));
+    *net = (int)nets().size();
+    return TEA_OK;
+}
+
+TEA_EXPORT int tea_ws_destroy_(const int* net)
+{
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Net* N = get_net(net);
+    if (!N) return TEA_ERR_BAD_ARGUMENT;
+    cudaStreamSynchronize(N->stream);
+    free_workspace(N);
+    for (Conv& c : N->conv)
+        for (void* p : {(void*)c.w, (void*)c.b, (void*)c.gw, (void*)c.gb, (void*)c.mw, (void*)c.vw, (void*)c.mb,
+                        (void*)c.vb, (void*)c.w16, (void*)c.wt16})
+            cudaFree(p);
+    for (void* p : {(void*)N->hw, (void*)N->ghw, (void*)N->mh, (void*)N->vh, (void*)N->d_err, (void*)N->d_sums,
+                    (void*)N->d_scale, (void*)N->d_partial, (void*)N->d_crops})
+        cudaFree(p);
+    for (Pair& p : N->pairs) {
+        cudaFree(p.feat);
+        cudaFree(p.tgt);
+    }
+    cudaStreamDestroy(N->stream);
+    nets()[*net - 1].reset();
+    return TEA_OK;
+}
+
+TEA_EXPORT int tea_ws_set_conv_(const int* net, const int* reference)
+{
+    Net* N = get_net(net);
+    if (!N) return TEA_ERR_BAD_ARGUMENT;
+    N->use_ref = *reference ? 1 : 0;
+    return TEA_OK;
+}
+
+TEA_EXPORT int tea_ws_param_count_(const int* net, long long* count)
+{
+    Net* N = get_net(net);
+    if (!N) return TEA_ERR_BAD_ARGUMENT;
+    *count = param_count(N);
+    return TEA_OK;
+}
+
+TEA_EXPORT int tea_ws_get_params_(const int* net, float* params)
+{
+    Net* N = get_net(net);
+    if (!N) return TEA_ERR_BAD_ARGUMENT;
+    return transfer_params(N, params, false, false);
+}
+
+TEA_EXPORT int tea_ws_set_params_(const int* net, const float* params)
+{
+    Net* N = get_net(net);
+    if (!N) return TEA_ERR_BAD_ARGUMENT;
+    const int rc = transfer_params(N, const_cast<float*>(params), true, false);
+    if (rc == TEA_OK) WS_CK(cudaStreamSynchronize(N->stream));
+    return rc;
+}
+
+// Forward (and, with a target, backward) over n host images of 4 features [n][H][W][4];
+// writes the prediction [n][H][W], the loss and the parameter gradients (oracle order).
+TEA_EXPORT int tea_ws_eval_host_(const int* net, const float* x, const float* target, const int* n, const int* H,
+                                 const int* W, float* y, double* loss, float* grads)
+{
+    Net* N = get_net(net);
+    if (!N || !x || !y || *n < 1 || *H < 2 || *W < 2) return TEA_ERR_BAD_ARGUMENT;
+    const int div = 1 << (N->levels - 1);
+    if (*H % div || *W % div) {
+        set_status(TEA_ERR_BAD_ARGUMENT, "warm start: image sides must be multiples of %d", div);
+        return TEA_ERR_BAD_ARGUMENT;
+    }
+    int rc = ensure_workspace(N, *n, *H, *W);
+    if (rc) return rc;
+    const long pix = (long)*n * *H * *W;
+    std::vector<bf16> hx(pix * IN_PAD, __float2bfloat16(0.f));
+    for (long p = 0; p < pix; ++p)
+        for (int c = 0; c < N_FEAT; ++c) hx[p * IN_PAD + c] = __float2bfloat16(x[p * N_FEAT + c]);
+    WS_CK(cudaMemcpyAsync(N->x0, hx.data(), sizeof(bf16) * hx.size(), cudaMemcpyHostToDevice, N->stream));
+    if (target) {
+        WS_CK(cudaMemcpyAsync(N->target, target, sizeof(float) * pix, cudaMemcpyHostToDevice, N->stream));
+        WS_CK(cudaMemsetAsync(N->d_sums, 0, sizeof(float) * 4, N->stream));
+        for (Conv& c : N->conv) {
+            WS_CK(cudaMemsetAsync(c.gw, 0, sizeof(float) * c.cout * 9 * c.cin, N->stream));
+            WS_CK(cudaMemsetAsync(c.gb, 0, sizeof(float) * c.cout, N->stream));
+        }
+        WS_CK(cudaMemsetAsync(N->ghw, 0, sizeof(float) * (N->ch[0] + 1), N->stream));
+    }
+    forward(N);
+    head(N, target ? N->target : nullptr);
+    if (target) backward(N);
+    if ((rc = check_err(N, "eval"))) return rc;
+    WS_CK(cudaMemcpy(y, N->y, sizeof(float) * pix, cudaMemcpyDeviceToHost));
+    if (target) {
+        float s = 0.f;
+        WS_CK(cudaMemcpy(&s, N->d_sums, sizeof(float), cudaMemcpyDeviceToHost));
+        if (loss) *loss = (double)s / (double)pix;
+        if (grads && (rc = transfer_params(N, grads, false, true))) return rc;
+    }
+    return TEA_OK;
+}
+
+// Records a training pair from the chunk's last solve: the step's features and
+// (u - u0) / scale.  Call after ext_tea_leaf_solve_ (u holds the solution, u0 the step's
+// right-hand side).
+TEA_EXPORT int tea_ws_record_(const int* net, const int* chunk)
+{
+    Net* N = get_net(net);
+    Chunk* c = get_chunk(chunk);
+    if (!N || !c) return TEA_ERR_BAD_ARGUMENT;
+    if (DIM != 2) {
+        set_status(TEA_ERR_BAD_ARGUMENT, "tea_ws_record_: the warm-start network is two-dimensional");
+        return TEA_ERR_BAD_ARGUMENT;
+    }
+    const Geom& g = c->g;
+    int rc = ensure_workspace(N, 1, g.ny, g.nx);
+    if (rc) return rc;
+    Pair p;
+    p.H = g.ny;
+    p.W = g.nx;
+    const long pix = (long)g.nx * g.ny;
+    if (dalloc(&p.feat, pix * N_FEAT) || dalloc(&p.tgt, pix)) return TEA_ERR_CUDA;
+    WS_CK(cudaStreamSynchronize(c->stream));
+    const int blocks = 512;
+    k_absmax<<<blocks, 256, 0, N->stream>>>(g, c->f.u0, N->d_partial, N->d_scale, blocks);
+    k_absmax_final<<<1, 256, 0, N->stream>>>(N->d_partial, blocks, N->d_scale);
+    k_features<<<grid_for(pix), 256, 0, N->stream>>>(g, c->f.u0, c->f.density, c->f.kx, c->f.ky, N->d_scale, N->x0);
+    k_record<<<grid_for(pix), 256, 0, N->stream>>>(g, N->x0, c->f.u, c->f.u0, N->d_scale, p.feat, p.tgt);
+    WS_CK(cudaStreamSynchronize(N->stream));
+    N->pairs.push_back(p);
+    return TEA_OK;
+}
+
+TEA_EXPORT int tea_ws_pairs_(const int* net, int* count)
+{
+    Net* N = get_net(net);
+    if (!N) return TEA_ERR_BAD_ARGUMENT;
+    *count = (int)N->pairs.size();
+    return TEA_OK;
+}
+
+// `steps` Adam steps on batches of `batch` random crop x crop windows of the recorded pairs.
+TEA_EXPORT int tea_ws_train_(const int* net, const int* steps, const int* batch, const int* crop, const double* lr,
+                             const int* seed, double* loss_first, double* loss_last, double* ms_per_step)
+{
+    Net* N = get_net(net);
+    if (!N) return TEA_ERR_BAD_ARGUMENT;
+    const int div = 1 << (N->levels - 1);
+    if (N->pairs.empty() || *steps < 1 || *batch < 1 || *batch > 256 || *crop < div || *crop % div) {
+        set_status(TEA_ERR_BAD_ARGUMENT, "tea_ws_train_: needs recorded pairs, 1..256 crops a multiple of %d", div);
+        return TEA_ERR_BAD_ARGUMENT;
+    }
+    for (const Pair& p : N->pairs)
+        if (p.H < *crop || p.W < *crop) {
+            set_status(TEA_ERR_BAD_ARGUMENT, "tea_ws_train_: crop larger than a recorded pair");
+            return TEA_ERR_BAD_ARGUMENT;
+        }
+    int rc = ensure_workspace(N, *batch, *crop, *crop);
+    if (rc) return rc;
+    std::mt19937_64 rng((unsigned long long)(seed ? *seed : 0));
+    std::vector<Crop> crops(*batch);
+    const long pix = (long)*batch * *crop * *crop;
+    if (N->step == 0) {
+        // Targets normalised to unit RMS over the recorded pairs (fixed at the first training).
+        WS_CK(cudaMemsetAsync(N->d_sums + 1, 0, sizeof(float), N->stream));
+        long total = 0;
+        for (const Pair& p : N->pairs) {
+            const long n = (long)p.H * p.W;
+            k_sumsq<<<grid_for(n), 256, 0, N->stream>>>(p.tgt, n, N->d_sums + 1);
+            total += n;
+        }
+        float ss = 0.f;
+        WS_CK(cudaMemcpyAsync(&ss, N->d_sums + 1, sizeof(float), cudaMemcpyDeviceToHost, N->stream));
+        WS_CK(cudaStreamSynchronize(N->stream));
+        const double rms = std::sqrt((double)ss / (double)std::max<long>(total, 1));
+        N->out_scale = rms > 0.0 ? (float)(1.0 / rms) : 1.f;
+    }
+    const int win = std::max(1, std::min(10, *steps / 2));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double first = 0.0, last = 0.0;
+    for (int s = 0; s < *steps; ++s) {
+        for (int b = 0; b < *batch; ++b) {
+            const Pair& p = N->pairs[rng() % N->pairs.size()];
+            crops[b].feat = p.feat;
+            crops[b].tgt = p.tgt;
+            crops[b].W = p.W;
+            crops[b].y0 = (int)(rng() % (unsigned long long)(p.H - *crop + 1));
+            crops[b].x0 = (int)(rng() % (unsigned long long)(p.W - *crop + 1));
+        }
+        WS_CK(cudaMemcpyAsync(N->d_crops, crops.data(), sizeof(Crop) * crops.size(), cudaMemcpyHostToDevice,
+                              N->stream));
+        if (s == 1) cudaEventRecord(e0, N->stream);
+        k_crops<<<grid_for(pix), 256, 0, N->stream>>>(N->d_crops, *crop, N->x0, N->target, *batch, N->out_scale);
+        // The loss sums run over the first and the last `win` steps.
+        if (s == 0 || s == *steps - win) WS_CK(cudaMemsetAsync(N->d_sums, 0, sizeof(float), N->stream));
+        forward(N);
+        head(N, N->target);
+        backward(N);
+        adam_step(N, (float)*lr);
+        if (s == win - 1 || s == *steps - 1) {
+            float v = 0.f;
+            WS_CK(cudaMemcpyAsync(&v, N->d_sums, sizeof(float), cudaMemcpyDeviceToHost, N->stream));
+            WS_CK(cudaStreamSynchronize(N->stream));
+            (s == win - 1 ? first : last) = (double)v / (double)pix / win;
+        }
+    }
+    if (*steps == 1) last = first;
+    cudaEventRecord(e1, N->stream);
+    if ((rc = check_err(N, "train"))) return rc;
+    float ms = 0.f;
+    if (*steps > 1) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (loss_first) *loss_first = first;
+    if (loss_last) *loss_last = last;
+    if (ms_per_step) *ms_per_step = *steps > 1 ? ms / (*steps - 1) : 0.0;
+    return TEA_OK;
+}
+
+// Attaches a network to a chunk (net 0 detaches): the chunk's whole-solve calls then start
+// from the network's prediction when it has the smaller initial residual.
+TEA_EXPORT int tea_ws_attach_(const int* chunk, const int* net)
+{
+    Chunk* c = get_chunk(chunk);
+    if (!c) return TEA_ERR_BAD_ARGUMENT;
+    if (!net || *net == 0) {
+        c->ws = nullptr;
+        return TEA_OK;
+    }
+    Net* N = get_net(net);
+    if (!N) return TEA_ERR_BAD_ARGUMENT;
+    c->ws = N;
+    return TEA_OK;
+}
+
+// Prediction on the chunk's current step (features from u0, density, Kx, Ky) into a host
+// array [ny][nx] of du, and the milliseconds the network took on the device.
+TEA_EXPORT int tea_ws_predict_(const int* net, const int* chunk, double* du, double* ms)
+{
+    Net* N = get_net(net);
+    Chunk* c = get_chunk(chunk);
+    if (!N || !c || DIM != 2) return TEA_ERR_BAD_ARGUMENT;
+    void* saved = c->ws;  // (du below is in units of u: the output normalisation is undone)
+    c->ws = N;
+    const Geom& g = c->g;
+    double* tmp = nullptr;
+    const long pix = (long)g.nx * g.ny;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    WS_CK(cudaMalloc(&tmp, sizeof(double) * c->field_elems));
+    cudaEventRecord(e0, c->stream);
+    const int used = ws_predict_into(c, tmp + kLeadPad);
+    cudaEventRecord(e1, c->stream);
+    c->ws = saved;
+    WS_CK(cudaStreamSynchronize(c->stream));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (ms) *ms = t;
+    int rc = TEA_OK;
+    if (!used) {
+        set_status(TEA_ERR_BAD_ARGUMENT, "tea_ws_predict_: chunk sides must be multiples of %d",
+                   1 << (N->levels - 1));
+        rc = TEA_ERR_BAD_ARGUMENT;
+    } else if (du) {
+        std::vector<double> u(c->field_elems), u0(c->field_elems);
+        cudaMemcpy(u.data(), tmp, sizeof(double) * c->field_elems, cudaMemcpyDeviceToHost);
+        cudaMemcpy(u0.data(), c->alloc[F_U0], sizeof(double) * c->field_elems, cudaMemcpyDeviceToHost);
+        for (long i = 0; i < pix; ++i) {
+            const long f = kLeadPad + fidx(g, HALO_PAD + (int)(i % g.nx), HALO_PAD + (int)(i / g.nx), 0);
+            du[i] = u[f] - u0[f];
+        }
+    }
+    cudaFree(tmp);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == TEA_OK) rc = check_err(N, "predict");
+    return rc;
+}

@@ -1,0 +1,309 @@
+// Convolutions of the learned warm-start network (no counterpart in the reference).
+//
+// Activations are bfloat16 NHWC tensors whose channel dimension may be a slice of a wider
+// buffer (channel stride `cs`, first channel `co`), so that a decoder's concatenation is
+// written in place.  3x3 weights are stored [Cout][9][Cin] (tap t = 3*dy + dx), bfloat16,
+// with float32 biases.
+//
+// k_conv_tc is the implicit GEMM on the 5th-generation tensor cores: D[128 pixels x Cout]
+// (float32, in tensor memory) += A[128 pixels x Cin] * B[Cout x Cin]^T for each of the 9
+// taps, A gathered from the input shifted by the tap (zero padding) and B the tap's weights,
+// both staged by cp.async into shared memory in the K-major, non-swizzled canonical layout
+// (8-row x 16-byte core matrices; the descriptor fields follow CUTLASS 4.5's
+// cute/arch/mma_sm100_desc.hpp and cute/atom/mma_traits_sm100.hpp).  One thread issues
+// tcgen05.mma (kind::f16, M = 128, N = Cout, K = 16 per instruction) and commits them to an
+// mbarrier; taps are double-buffered so that the gather of tap t+1 overlaps the MMAs of
+// tap t.  The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes
+// 32w..32w+31 = pixels), adds the bias, applies ReLU and/or a ReLU-derivative mask, and
+// stores bfloat16.  Every mbarrier wait is bounded: past the limit the kernel records an
+// error, stops issuing work, and still frees its tensor memory.
+//
+// k_conv_ref is the same function on CUDA cores (float32 accumulation): the reference the
+// tests hold the tensor-core kernel to.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tea {
+namespace ws {
+
+using bf16 = __nv_bfloat16;
+
+struct ConvArgs {
+    const bf16* x;  // [n][H][W][xcs], channels xco .. xco+cin
+    int xcs, xco;
+    bf16* y;  // [n][H][W][ycs], channels yco .. yco+cout
+    int ycs, yco;
+    const bf16* w;      // [cout][9][cin]
+    const float* bias;  // [cout] or null
+    const bf16* mask;   // optional: y *= (mask > 0), mask [n][H][W][mcs] channels mco..
+    int mcs, mco;
+    int relu;
+    int n, H, W, cin, cout;
+    int* err;  // set to 1 when a bounded wait gave up
+};
+
+// ----------------------------------------------------------------------------- reference
+
+__global__ void __launch_bounds__(256) k_conv_ref(ConvArgs a)
+{
+    const long npix = (long)a.n * a.H * a.W;
+    const long total = npix * a.cout;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+        const int co = (int)(idx % a.cout);
+        const long p = idx / a.cout;
+        const int xx = (int)(p % a.W);
+        const int yy = (int)((p / a.W) % a.H);
+        const long img = p / ((long)a.W * a.H);
+        float acc = a.bias ? a.bias[co] : 0.0f;
+        for (int t = 0; t < 9; ++t) {
+            const int sy = yy + t / 3 - 1, sx = xx + t % 3 - 1;
+            if (sy < 0 || sy >= a.H || sx < 0 || sx >= a.W) continue;
+            const bf16* xp = a.x + ((img * a.H + sy) * a.W + sx) * a.xcs + a.xco;
+            const bf16* wp = a.w + ((long)co * 9 + t) * a.cin;
+            for (int ci = 0; ci < a.cin; ++ci) acc += __bfloat162float(xp[ci]) * __bfloat162float(wp[ci]);
+        }
+        if (a.relu) acc = fmaxf(acc, 0.0f);
+        if (a.mask && !(__bfloat162float(a.mask[p * a.mcs + a.mco + co]) > 0.0f)) acc = 0.0f;
+        a.y[p * a.ycs + a.yco + co] = __float2bfloat16(acc);
+    }
+}
+
+// ----------------------------------------------------------------------------- tcgen05 helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, K-major without swizzle: LBO = byte distance between the
+// two 16-byte K halves of one MMA's K = 16, SBO = byte distance between 8-row groups.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+    return d;                // base offset 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor of kind::f16: A, B bfloat16, D float32, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n)
+{
+    return (1u << 4)                       // D format: F32
+         | (1u << 7)                       // A format: BF16
+         | (1u << 10)                      // B format: BF16
+         | ((uint32_t)(n >> 3) << 17)      // N / 8
+         | ((uint32_t)(m >> 4) << 24);     // M / 16
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Bounded wait for the completion of the phase with parity `parity`.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity)
+{
+    const uint32_t addr = smem_u32(bar);
+    for (long it = 0; it < (1L << 24); ++it) {
+        uint32_t ok = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void cp_async_16z(void* dst, const void* src, bool valid)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+// ----------------------------------------------------------------------------- tensor-core conv
+
+constexpr int TC_THREADS = 128;
+constexpr int TC_M = 128;  // pixels per tile
+
+// Shared memory: two stages of A (128 x cin) and B (cout x cin) bfloat16, plus barriers.
+__host__ __device__ constexpr size_t conv_tc_smem_bytes(int cin, int cout)
+{
+    return 2 * ((size_t)TC_M * cin * 2 + (size_t)cout * cin * 2) + 1024 + 64;
+}
+
+__host__ __device__ constexpr int tmem_cols(int cout) { return cout <= 32 ? 32 : (cout <= 64 ? 64 : (cout <= 128 ? 128 : 256)); }
+
+__global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char s_raw[];
+    // 1024-align the operand area.
+    unsigned char* base = s_raw + ((1024 - (smem_u32(s_raw) & 1023u)) & 1023u);
+    const int cin = a.cin, cout = a.cout;
+    const size_t a_bytes = (size_t)TC_M * cin * 2, b_bytes = (size_t)cout * cin * 2;
+    bf16* sA[2] = {reinterpret_cast<bf16*>(base), reinterpret_cast<bf16*>(base + a_bytes + b_bytes)};
+    bf16* sB[2] = {reinterpret_cast<bf16*>(base + a_bytes), reinterpret_cast<bf16*>(base + 2 * a_bytes + b_bytes)};
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * (a_bytes + b_bytes));
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+    int* s_abort = reinterpret_cast<int*>(tmem_slot + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ncols = tmem_cols(cout);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        *s_abort = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    const uint32_t idesc = umma_idesc_bf16(TC_M, cout);
+    const uint32_t sbo = (uint32_t)cin * 16;  // bytes between 8-row groups
+    const int kchunks = cin / 8;              // 16-byte chunks per row
+    const long npix = (long)a.n * a.H * a.W;
+    const long ntiles = (npix + TC_M - 1) / TC_M;
+    long fill = 0;  // fills issued by this CTA (stage = fill & 1)
+    bool ok = true;
+
+    for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const long p0 = tile * TC_M;
+        for (int t = 0; t < 9 && ok; ++t, ++fill) {
+            const int st = (int)(fill & 1);
+            if (fill >= 2) {
+                // The MMAs that last read this stage (fill - 2) must be complete; the decision
+                // to give up is made by the whole block at once.
+                const bool done = mbar_wait(&bar[st], (unsigned)(((fill - 2) >> 1) & 1));
+                if (!__syncthreads_and(done)) {
+                    ok = false;
+                    break;
+                }
+            }
+            const int dy = t / 3 - 1, dx = t % 3 - 1;
+            // A: 128 rows (pixels) x kchunks 16-byte chunks.
+            for (int idx = tid; idx < TC_M * kchunks; idx += TC_THREADS) {
+                const int m = idx / kchunks, c = idx % kchunks;
+                const long p = p0 + m;
+                bool valid = p < npix;
+                const bf16* src = a.x;
+                if (valid) {
+                    const int xx = (int)(p % a.W);
+                    const int yy = (int)((p / a.W) % a.H);
+                    const long img = p / ((long)a.W * a.H);
+                    const int sy = yy + dy, sx = xx + dx;
+                    valid = sy >= 0 && sy < a.H && sx >= 0 && sx < a.W;
+                    if (valid) src = a.x + ((img * a.H + sy) * a.W + sx) * a.xcs + a.xco + c * 8;
+                }
+                bf16* dst = sA[st] + (size_t)(m >> 3) * (sbo / 2) + (size_t)c * 64 + (m & 7) * 8;
+                cp_async_16z(dst, src, valid);
+            }
+            // B: cout rows x kchunks chunks of tap t.
+            for (int idx = tid; idx < cout * kchunks; idx += TC_THREADS) {
+                const int r = idx / kchunks, c = idx % kchunks;
+                const bf16* src = a.w + ((size_t)r * 9 + t) * cin + c * 8;
+                bf16* dst = sB[st] + (size_t)(r >> 3) * (sbo / 2) + (size_t)c * 64 + (r & 7) * 8;
+                cp_async_16z(dst, src, true);
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a_addr = smem_u32(sA[st]), b_addr = smem_u32(sB[st]);
+                for (int s = 0; s < cin / 16; ++s) {
+                    const uint64_t da = umma_desc(a_addr + s * 256, 128, sbo);
+                    const uint64_t db = umma_desc(b_addr + s * 256, 128, sbo);
+                    const uint32_t acc = (t > 0 || s > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                        : "memory");
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&bar[st]))
+                             : "memory");
+            }
+        }
+        if (!ok) break;
+        // All nine taps issued; wait for the last commit (MMAs complete in order).
+        const long last = fill - 1;
+        const bool done = mbar_wait(&bar[last & 1], (unsigned)((last >> 1) & 1));
+        if (!__syncthreads_and(done)) {
+            ok = false;
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // Epilogue: warp w reads TMEM lanes 32w..32w+31 (pixels), 16 columns at a time.
+        const long p = p0 + warp * 32 + lane;
+        for (int c0 = 0; c0 < cout; c0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (p < npix) {
+                __align__(16) bf16 out[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    float v = __uint_as_float(r[j]);
+                    if (a.bias) v += a.bias[c0 + j];
+                    if (a.relu) v = fmaxf(v, 0.0f);
+                    if (a.mask && !(__bfloat162float(a.mask[p * a.mcs + a.mco + c0 + j]) > 0.0f)) v = 0.0f;
+                    out[j] = __float2bfloat16(v);
+                }
+                bf16* dst = a.y + p * a.ycs + a.yco + c0;
+                if ((((uintptr_t)dst) & 15u) == 0) {
+                    reinterpret_cast<uint4*>(dst)[0] = reinterpret_cast<const uint4*>(out)[0];
+                    reinterpret_cast<uint4*>(dst)[1] = reinterpret_cast<const uint4*>(out)[1];
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) dst[j] = out[j];
+                }
+            }
+        }
+        // The next tile's MMAs overwrite the accumulator: every lane's reads come first.
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    if (!ok) {
+        *s_abort = 1;
+        if (a.err) atomicExch(a.err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (*s_abort) {
+        // Let MMAs still in flight finish (bounded) before the memory they use is released:
+        // the last fill committed on each stage.
+        for (int s = 0; s < 2; ++s) {
+            const long f = ((fill - 1) & 1) == s ? fill - 1 : fill - 2;
+            if (f >= 0) mbar_wait(&bar[s], (unsigned)((f >> 1) & 1));
+        }
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+    }
+}
+
+}  // namespace ws
+}  // namespace tea

@@ -1,0 +1,238 @@
+// Element-wise, pooling, reduction and optimiser kernels of the learned warm-start network
+// (no counterpart in the reference).  Shapes and conventions as in tea_ws_conv.cuh.
+#pragma once
+
+#include "tea_ws_conv.cuh"
+
+namespace tea {
+namespace ws {
+
+struct View {  // a channel slice of an NHWC buffer
+    bf16* p;
+    int cs, co, c;  // channel stride, first channel, channels
+};
+
+// ----------------------------------------------------------------------------- weight gradient
+
+// gW[co][t][ci] += sum_p gy[p][co] x[p + tap t][ci] and gb[co] += sum_p gy[p][co], float32
+// accumulation on CUDA cores.  Block: one tap, a 32 x 32 (co, ci) tile and a slice of the
+// pixels (blockIdx.y); 256 threads, each four (co, ci) products.
+constexpr int WG_PIX = 64;
+
+__global__ void __launch_bounds__(256) k_wgrad(const bf16* x, int xcs, int xco, const bf16* gy, int gcs, int gco,
+                                                int n, int H, int W, int cin, int cout, float* gw, float* gb)
+{
+    __shared__ float s_g[WG_PIX][33];
+    __shared__ float s_x[WG_PIX][33];
+    const int ci_tiles = (cin + 31) / 32, co_tiles = (cout + 31) / 32;
+    int b = blockIdx.x;
+    const int t = b % 9;
+    b /= 9;
+    const int cit = b % ci_tiles;
+    const int cot = b / ci_tiles;
+    if (cot >= co_tiles) return;
+    const int dy = t / 3 - 1, dx = t % 3 - 1;
+    const long npix = (long)n * H * W;
+    const long per = (npix + gridDim.y - 1) / gridDim.y;
+    const long pbeg = blockIdx.y * per, pend = min(npix, pbeg + per);
+    const int tid = threadIdx.x;
+    const int tco = tid >> 3;        // 0..31
+    const int tci = (tid & 7) * 4;   // 0..28
+    float acc[4] = {0.f, 0.f, 0.f, 0.f}, accb = 0.f;
+    for (long p0 = pbeg; p0 < pend; p0 += WG_PIX) {
+        for (int idx = tid; idx < WG_PIX * 32; idx += 256) {
+            const int pp = idx / 32, c = idx % 32;
+            const long p = p0 + pp;
+            float gv = 0.f, xv = 0.f;
+            if (p < pend) {
+                const int co = cot * 32 + c;
+                if (co < cout) gv = __bfloat162float(gy[p * gcs + gco + co]);
+                const int ci = cit * 32 + c;
+                const int xx = (int)(p % W), yy = (int)((p / W) % H);
+                const long img = p / ((long)W * H);
+                const int sy = yy + dy, sx = xx + dx;
+                if (ci < cin && sy >= 0 && sy < H && sx >= 0 && sx < W)
+                    xv = __bfloat162float(x[((img * H + sy) * W + sx) * xcs + xco + ci]);
+            }
+            s_g[pp][c] = gv;
+            s_x[pp][c] = xv;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int pp = 0; pp < WG_PIX; ++pp) {
+            const float g = s_g[pp][tco];
+            acc[0] += g * s_x[pp][tci];
+            acc[1] += g * s_x[pp][tci + 1];
+            acc[2] += g * s_x[pp][tci + 2];
+            acc[3] += g * s_x[pp][tci + 3];
+            accb += g;
+        }
+        __syncthreads();
+    }
+    const int co = cot * 32 + tco;
+    if (co < cout) {
+        for (int k = 0; k < 4; ++k) {
+            const int ci = cit * 32 + tci + k;
+            if (ci < cin) atomicAdd(&gw[((long)co * 9 + t) * cin + ci], acc[k]);
+        }
+        if (gb && t == 0 && cit == 0 && tci == 0) atomicAdd(&gb[co], accb);
+    }
+}
+
+// ----------------------------------------------------------------------------- pooling
+
+__global__ void k_avgpool(View x, bf16* y, int n, int H, int W)
+{
+    const int h2 = H / 2, w2 = W / 2;
+    const long total = (long)n * h2 * w2 * x.c;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % x.c);
+        const long q = i / x.c;
+        const int xx = (int)(q % w2), yy = (int)((q / w2) % h2);
+        const long img = q / ((long)w2 * h2);
+        float s = 0.f;
+        for (int d = 0; d < 4; ++d) {
+            const long p = (img * H + 2 * yy + d / 2) * W + 2 * xx + d % 2;
+            s += __bfloat162float(x.p[p * x.cs + x.co + c]);
+        }
+        y[q * x.c + c] = __float2bfloat16(0.25f * s);
+    }
+}
+
+// g_fine = (g_coarse / 4) * (act > 0) + g_skip, the gradient with respect to the
+// pre-activation of an encoder level's last convolution.
+__global__ void k_avgpool_bw(const bf16* gc, View act, View gskip, bf16* gf, int n, int H, int W)
+{
+    const int C = act.c;
+    const long total = (long)n * H * W * C;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long p = i / C;
+        const int xx = (int)(p % W), yy = (int)((p / W) % H);
+        const long img = p / ((long)W * H);
+        const long q = (img * (H / 2) + yy / 2) * (W / 2) + xx / 2;
+        float g = 0.25f * __bfloat162float(gc[q * C + c]);
+        if (!(__bfloat162float(act.p[p * act.cs + act.co + c]) > 0.f)) g = 0.f;
+        g += __bfloat162float(gskip.p[p * gskip.cs + gskip.co + c]);
+        gf[p * C + c] = __float2bfloat16(g);
+    }
+}
+
+__global__ void k_upsample(View h, View cat, int n, int H, int W)  // H, W: fine size
+{
+    const int C = h.c;
+    const long total = (long)n * H * W * C;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long p = i / C;
+        const int xx = (int)(p % W), yy = (int)((p / W) % H);
+        const long img = p / ((long)W * H);
+        const long q = (img * (H / 2) + yy / 2) * (W / 2) + xx / 2;
+        cat.p[p * cat.cs + cat.co + c] = h.p[q * h.cs + h.co + c];
+    }
+}
+
+__global__ void k_upsample_bw(View gcat, bf16* gh, int n, int H, int W)  // H, W: fine size
+{
+    const int C = gcat.c, h2 = H / 2, w2 = W / 2;
+    const long total = (long)n * h2 * w2 * C;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long q = i / C;
+        const int xx = (int)(q % w2), yy = (int)((q / w2) % h2);
+        const long img = q / ((long)w2 * h2);
+        float s = 0.f;
+        for (int d = 0; d < 4; ++d) {
+            const long p = (img * H + 2 * yy + d / 2) * W + 2 * xx + d % 2;
+            s += __bfloat162float(gcat.p[p * gcat.cs + gcat.co + c]);
+        }
+        gh[q * C + c] = __float2bfloat16(s);
+    }
+}
+
+// ----------------------------------------------------------------------------- head and loss
+
+// y = h . w + b per pixel (float32 out).  With a target: sums[0] += (y - t)^2 and the
+// backward pass: gy = 2 (y - t) / N, gh = gy w (h > 0), gw += gy h, gb += gy.
+template <int C>
+__global__ void __launch_bounds__(256) k_head(const bf16* h, const float* w, const float* b, float* y, long npix,
+                                               const float* target, float* sums, bf16* gh, float* gw, float* gb)
+{
+    __shared__ float s_w[C];
+    __shared__ float s_red[C + 2];
+    for (int c = threadIdx.x; c < C; c += blockDim.x) s_w[c] = w[c];
+    for (int c = threadIdx.x; c < C + 2; c += blockDim.x) s_red[c] = 0.f;
+    __syncthreads();
+    float gwl[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) gwl[c] = 0.f;
+    float lossl = 0.f, gbl = 0.f;
+    const float inv = 2.0f / (float)npix;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
+        float hv[C];
+        float acc = b[0];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            hv[c] = __bfloat162float(h[p * C + c]);
+            acc += hv[c] * s_w[c];
+        }
+        y[p] = acc;
+        if (target) {
+            const float d = acc - target[p];
+            lossl += d * d;
+            const float g = inv * d;
+            gbl += g;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                gwl[c] += g * hv[c];
+                gh[p * C + c] = __float2bfloat16(hv[c] > 0.f ? g * s_w[c] : 0.f);
+            }
+        }
+    }
+    if (!target) return;
+#pragma unroll
+    for (int c = 0; c < C; ++c) atomicAdd(&s_red[c], gwl[c]);
+    atomicAdd(&s_red[C], gbl);
+    atomicAdd(&s_red[C + 1], lossl);
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&gw[c], s_red[c]);
+    if (threadIdx.x == 0) {
+        atomicAdd(gb, s_red[C]);
+        atomicAdd(&sums[0], s_red[C + 1]);
+    }
+}
+
+// ----------------------------------------------------------------------------- optimiser
+
+// Adam on float32 master weights; clears the gradient.
+__global__ void k_adam(float* w, float* g, float* m, float* v, long count, float lr, float b1, float b2, float eps,
+                       float c1, float c2)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < count; i += (long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        g[i] = 0.f;
+    }
+}
+
+// bfloat16 copies of a 3x3 layer: w16[co][t][ci] and, for the input gradient, the
+// transposed, tap-flipped wt16[ci][t][co] = w[co][8 - t][ci].
+__global__ void k_weights_bf16(const float* w, bf16* w16, bf16* wt16, int cout, int cin)
+{
+    const long total = (long)cout * 9 * cin;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int ci = (int)(i % cin);
+        const int t = (int)((i / cin) % 9);
+        const int co = (int)(i / (9L * cin));
+        const bf16 v = __float2bfloat16(w[i]);
+        w16[i] = v;
+        if (wt16) wt16[((long)ci * 9 + (8 - t)) * cout + co] = v;
+    }
+}
+
+}  // namespace ws
+}  // namespace tea

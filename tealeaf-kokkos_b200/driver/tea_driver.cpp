@@ -312,6 +312,8 @@ struct Backend {
     void (*whole_solve)(const int*, const tea_solve_params*, tea_solve_result*) = nullptr;
     void (*get_status)(int*) = nullptr;
     int (*transfer_bytes)(const int*, long long*, long long*) = nullptr;
+    int (*ws_record)(const int*, const int*) = nullptr;
+    int (*ws_attach)(const int*, const int*) = nullptr;
 
     template <class F>
     void bind(F& fp, const char* name, bool required = true)
@@ -352,6 +354,8 @@ struct Backend {
         bind(whole_solve, "ext_tea_leaf_solve_", false);
         bind(get_status, "ext_get_status_", false);
         bind(transfer_bytes, "tea_transfer_bytes_", false);
+        bind(ws_record, "tea_ws_record_", false);
+        bind(ws_attach, "tea_ws_attach_", false);
     }
 
     void close()
@@ -519,6 +523,9 @@ struct Runner {
         be.check_status("ext_generate_chunk_");
         halo({FIELD_DENSITY, FIELD_ENERGY0, FIELD_ENERGY1}, 2);
         field_summary(sum, false, nullptr);
+        if (opt->ws_net && opt->ws_mode == 2) {
+            if (!be.ws_attach || be.ws_attach(&chunk, &opt->ws_net) != 0) fail("warm start: cannot attach network");
+        }
     }
 
     // tea_leaf(), tealeaf_2d/tea_solve.f90:36-605, one implicit solve per timestep.
@@ -575,6 +582,10 @@ struct Runner {
             rec->switch_step = r.switch_step;
             rec->est_itc = r.est_itc;
             rec->corrections = r.corrections;
+            rec->warm_start_used = r.warm_start_used;
+            if (opt->ws_net && opt->ws_mode == 1) {
+                if (!be.ws_record || be.ws_record(&opt->ws_net, &chunk) != 0) fail("warm start: cannot record pair");
+            }
             return;
         }
 

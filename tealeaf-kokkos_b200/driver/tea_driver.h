@@ -27,7 +27,10 @@ typedef struct {
     double eps_rel_override; /* > 0: replace tl_eps_rel */
     int keep_chunk;          /* 1: skip ext_finalise_ so the caller can inspect the fields */
     int precision;           /* > 0: TEA_PRECISION_* for the whole-solve path (deck: tl_precision) */
-    int reserved[6];
+    int ws_net;              /* a learned warm-start network id (tea_ws_create_), or 0 */
+    int ws_mode;             /* with ws_net: 1 record a training pair after every solve,
+                                2 warm-start every solve from the network */
+    int reserved[4];
 } tea_run_options;
 
 typedef struct {
@@ -45,7 +48,7 @@ typedef struct {
     int has_summary;
     int switch_step;
     int est_itc;
-    int pad;
+    int warm_start_used;     /* 1 when the solve started from the network's guess */
     double wall_end;         /* seconds since the start of the timestep loop, at the step's end */
     long long h2d_bytes;     /* backend host->device bytes so far (0 if not reported) */
     long long d2h_bytes;     /* backend device->host bytes so far */

@@ -1,0 +1,134 @@
+"""The learned warm start on the GPU: the network's kernels against the CPU oracle, the
+tensor-core convolution against the CUDA-core one, training, and what the trained
+network gains in the solve.
+
+There is no reference counterpart (TeaLeaf has no learned component); the numerics are
+held to oracle/warmstart_oracle.py (float64, itself pinned by finite differences in
+tests/test_warmstart_oracle.py) within bfloat16 tolerances, and the solve is judged by
+converging to the same tolerance with fewer iterations.
+"""
+import importlib.util
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rel, tea
+
+pytestmark = pytest.mark.gpu
+
+_spec = importlib.util.spec_from_file_location("warmstart_oracle", ROOT / "oracle" / "warmstart_oracle.py")
+wo = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(wo)
+
+# bfloat16 storage (8 significant bits) through a few layers: relative L2 errors of a few
+# per cent against the float64 oracle.
+FWD_TOL = 3e-2
+GRAD_COS = 0.99
+
+
+def _flat(p, levels, base):
+    parts = []
+    for name, _, _ in wo.layer_shapes(levels, base):
+        parts += [p[name + ".w"].reshape(-1), p[name + ".b"].reshape(-1)]
+    parts += [p["head.w"], p["head.b"]]
+    return np.concatenate(parts).astype(np.float32)
+
+
+def _split(flat, levels, base):
+    out, off = {}, 0
+    for name, co, ci in wo.layer_shapes(levels, base):
+        out[name + ".w"] = flat[off:off + co * 9 * ci].reshape(co, 9, ci)
+        off += co * 9 * ci
+        out[name + ".b"] = flat[off:off + co]
+        off += co
+    c0 = wo.channels(levels, base)[0]
+    out["head.w"] = flat[off:off + c0]
+    out["head.b"] = flat[off + c0:off + c0 + 1]
+    return out
+
+
+def _rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def _case(levels, base, n, hw, seed):
+    rng = np.random.default_rng(seed)
+    p = wo.init_params(levels, base, seed=seed)
+    x = rng.normal(size=(n, hw, hw, wo.IN_CHANNELS)) * 0.5
+    t = rng.normal(size=(n, hw, hw)) * 0.1
+    return p, x, t
+
+
+@pytest.mark.parametrize("reference_conv", [True, False], ids=["cuda_cores", "tensor_cores"])
+@pytest.mark.parametrize("levels,base", [(2, 16), (3, 32)])
+def test_forward_and_gradients_match_oracle(reference_conv, levels, base):
+    p, x, t = _case(levels, base, 2, 32, seed=levels * 7 + base)
+    net = tea.WarmStart(levels, base, seed=0)
+    try:
+        net.set_reference_conv(reference_conv)
+        net.set_params(_flat(p, levels, base))
+        y, loss, grads = net.eval(x, t)
+        ys, gsum, lsum = [], None, 0.0
+        for i in range(x.shape[0]):
+            yi, cache = wo.forward(p, x[i], levels, base)
+            gi = wo.backward(p, cache, yi, t[i], levels, base)
+            ys.append(yi)
+            lsum += wo.loss(yi, t[i])
+            gsum = gi if gsum is None else {k: gsum[k] + gi[k] for k in gi}
+        y_ref = np.stack(ys)
+        assert _rel_l2(y, y_ref) <= FWD_TOL, _rel_l2(y, y_ref)
+        assert rel(loss, lsum / x.shape[0]) <= 0.05
+        # The GPU averages the loss over all n images at once: scale the oracle's per-image
+        # gradients the same way.
+        g = _split(grads, levels, base)
+        for k, ref in gsum.items():
+            ref = ref / x.shape[0]
+            a, b = g[k].reshape(-1).astype(np.float64), ref.reshape(-1)
+            cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
+            assert cos >= GRAD_COS, (k, cos)
+            assert 0.9 <= np.linalg.norm(a) / (np.linalg.norm(b) + 1e-30) <= 1.1, k
+    finally:
+        net.close()
+
+
+def test_tensor_core_convolution_equals_cuda_cores():
+    levels, base = 3, 32
+    p, x, _ = _case(levels, base, 1, 256, seed=5)  # 65536 pixels: many 128-pixel tiles
+    net = tea.WarmStart(levels, base, seed=0)
+    try:
+        net.set_params(_flat(p, levels, base))
+        net.set_reference_conv(True)
+        y_ref, _, _ = net.eval(x)
+        net.set_reference_conv(False)
+        y_tc, _, _ = net.eval(x)
+        assert _rel_l2(y_tc, y_ref) <= 1e-2, _rel_l2(y_tc, y_ref)
+    finally:
+        net.close()
+
+
+def _deck(seed, steps=8, cells=128):
+    spec = tea.DeckSpec(dim=2, cells=cells, states=8, seed=seed, solver="cg", end_step=steps, dt=0.004, eps=1e-15,
+                        eps_rel=1e-10, max_iters=20000, summary_frequency=1, check_result=True)
+    return tea.seeded_deck(spec)
+
+
+def test_training_reduces_loss_and_warm_start_saves_iterations():
+    net = tea.WarmStart(3, 32, seed=1)
+    try:
+        for seed in (101, 102, 103):  # training layouts
+            tea.run_deck(_deck(seed), 2, fused=True, ws_net=net.id, ws_mode=tea.WS_RECORD)
+        assert net.pairs() == 24
+        first, last, ms = net.train(steps=400, batch=8, crop=64, lr=2e-3, seed=7)
+        assert last < 0.3 * first, (first, last)
+        # An unseen layout: same tolerance, fewer iterations from the network's start.
+        deck = _deck(204)
+        _, plain = tea.run_deck(deck, 2, fused=True, summary_every_step=True)
+        _, warm = tea.run_deck(deck, 2, fused=True, summary_every_step=True, ws_net=net.id, ws_mode=tea.WS_ATTACH)
+        assert sum(r["warm_start_used"] for r in warm) >= len(warm) // 2
+        assert sum(r["iterations"] for r in warm) < sum(r["iterations"] for r in plain)
+        for a, b in zip(warm, plain):
+            assert a["exact_error"] < a["eps_used"]
+            for k in ("vol", "mass", "ie", "temp"):
+                assert rel(a[k], b[k]) <= 1e-9, (a["step"], k)
+    finally:
+        net.close()
