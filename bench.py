@@ -257,12 +257,14 @@ def solve_params(spec, precision=0):
     return p
 
 
-def gpu_arm(args, world, precision=0, kernels=True):
+def gpu_arm(args, world, precision=0, kernels=True, ws_net=0):
     import torch
 
     lib = tea.cuda_library(2)
     spec = workload_spec()
     ch = setup_chunk(lib, spec)
+    if ws_net:
+        lib.tea_ws_attach_(ch.cid, ctypes.byref(ctypes.c_int(ws_net)))
     stream_ptr = ctypes.c_void_p()
     lib.tea_chunk_stream_(ch.cid, ctypes.byref(stream_ptr))
     stream = torch.cuda.ExternalStream(stream_ptr.value)
@@ -329,6 +331,8 @@ def gpu_arm(args, world, precision=0, kernels=True):
         "warmup_iterations": [r["iterations"] for r in warm], "bad_status": [r["status"] for r in bad],
         "corrections": [r["corrections"] for r in results], "summary": summaries,
         "exact_errors": [r["exact_error"] for r in results],
+        "warm_start_used": [r["warm_start_used"] for r in results],
+        "warm_r0_ratio": [r["warm_r0_guess"] / r["warm_r0_plain"] if r["warm_r0_plain"] else None for r in results],
     }
 
 
@@ -484,6 +488,29 @@ def workload_3d(args):
     print(json.dumps(out))
 
 
+def learned_arm(args, world):
+    """FP32-refined + learned warm start on the same workload: a U-Net (3 levels, 32 base
+    channels) trained on pairs the solver generates from four other seeded 1024^2 layouts
+    (6 timesteps each), then attached to the workload's chunk.  Returns the timing and the
+    training cost."""
+    t0 = time.perf_counter()
+    net = tea.WarmStart(3, 32, seed=SEED)
+    for k in range(4):
+        spec = tea.DeckSpec(dim=2, cells=1024, states=STATES, seed=SEED + 1 + k, solver=SOLVER, end_step=6, dt=0.004,
+                            eps=1e-15, eps_rel=EPS_REL, max_iters=20000, presteps=30, summary_frequency=0,
+                            check_result=False)
+        tea.run_deck(tea.seeded_deck(spec), 2, fused=True, ws_net=net.id, ws_mode=tea.WS_RECORD)
+    t_record = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    loss_first, loss_last, ms_step = net.train(steps=1000, batch=8, crop=128, lr=1e-4, seed=SEED)
+    t_train = time.perf_counter() - t1
+    r = gpu_arm(args, world, precision=1, kernels=False, ws_net=net.id)
+    net.close()
+    r.update({"record_s": t_record, "train_s": t_train, "train_ms_per_step": ms_step, "loss_first": loss_first,
+              "loss_last": loss_last, "pairs": 24})
+    return r
+
+
 def kernel_only(args):
     """Set up the 4096^2 workload and launch one fused kernel 1 + reps times (no solve)."""
     lib = tea.cuda_library(2)
@@ -510,6 +537,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-refined", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS),
                     help="only launch one fused kernel --reps times on the 4096^2 workload (for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
@@ -531,6 +559,7 @@ def main():
 
     g = gpu_arm(args, world)
     refined = None if args.no_refined else gpu_arm(args, world, precision=1, kernels=False)
+    learned = None if args.no_refined or args.no_learned else learned_arm(args, world)
     e2e = None if args.no_e2e else e2e_arm(args)
     if rank != 0:
         dist_done(world)
@@ -591,6 +620,23 @@ def main():
                                 "fp32_chebyshev_steps": refined["cheby_steps"], "corrections": refined["corrections"],
                                 "exact_errors": refined["exact_errors"],
                                 "field_summary_max_rel_diff_vs_fp64": diff, "clocks": refined["clocks"]}
+    if learned:
+        # FP32-refined + learned warm start: the same timesteps with the network attached;
+        # training cost (pair recording + training) stated beside it.
+        diff = max(tea.rel_diff(a, b) for a, b in zip(learned["summary"], g["summary"]))
+        saved = refined["sec_per_step"] - learned["sec_per_step"] if refined else None
+        cost = learned["record_s"] + learned["train_s"]
+        line["fp32_refined_learned"] = {
+            "value": learned["sec_per_step"], "unit": "s", "speedup_vs_fp64": g["sec_per_step"] / learned["sec_per_step"],
+            "iterations": learned["iterations"], "warm_start_used": learned["warm_start_used"],
+            "warm_r0_ratio": learned["warm_r0_ratio"], "corrections": learned["corrections"],
+            "field_summary_max_rel_diff_vs_fp64": diff,
+            "training": {"pairs": learned["pairs"], "layouts": "4 seeded 1024^2 layouts x 6 timesteps",
+                         "record_s": learned["record_s"], "train_s": learned["train_s"],
+                         "train_ms_per_step": learned["train_ms_per_step"], "steps": 1000,
+                         "loss_first": learned["loss_first"], "loss_last": learned["loss_last"]},
+            "amortised_after_steps": (cost / saved) if saved and saved > 0 else None,
+            "clocks": learned["clocks"]}
     if g["bad_status"]:
         line["status_warnings"] = g["bad_status"]
     print(json.dumps(line))

@@ -174,10 +174,12 @@ void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* params,
  * Learned warm start (no counterpart in the reference; 2D).  A U-Net of `levels`
  * levels and `base` channels at full resolution (doubling per level), bfloat16 weights
  * and activations with float32 accumulation, predicts the timestep increment
- * du = u(n+1) - u0 from u0 = density*energy, density, Kx and Ky.  A chunk with a network
- * attached starts each ext_tea_leaf_solve_ from u0 + du when that start has the smaller
- * FP64 residual (else from u0, as the reference does) and converges to the same
- * tolerance.  All functions return a TEA_* status.
+ * du = u(n+1) - u0 from u0 = density*energy, density, Kx and Ky (through the plain start's
+ * residual r0 = u0 - A u0, which scales input and output).  A chunk with a network
+ * attached starts each ext_tea_leaf_solve_ from u0 + du, smoothed by 8 damped Jacobi
+ * sweeps in FP64, when that start has the smaller FP64 residual (else from u0, as the
+ * reference does) and converges to the same tolerance.  All functions return a TEA_*
+ * status.
  * --------------------------------------------------------------------------------- */
 
 /* New network with seeded He-initialised weights on the current device: levels 2..5,
@@ -189,9 +191,11 @@ int tea_ws_destroy_(const int* net);
 int tea_ws_record_(const int* net, const int* chunk);
 int tea_ws_pairs_(const int* net, int* count);
 /* Adam training: `steps` steps on `batch` random crop x crop windows of the recorded
- * pairs (crop a multiple of 2^(levels-1)); targets are normalised to unit RMS over the
- * recorded pairs at the first training.  Writes the MSE loss averaged over the first and
- * over the last 10 steps, and the device milliseconds per step. */
+ * pairs (crop a multiple of 2^(levels-1)).  The loss is, per crop, the energy norm of the
+ * smoothed guess's error relative to that of the plain start, e.A e / du.A du with
+ * e = M^8 (du_pred - du), A the solver's operator on the crop and M the smoothing sweep.
+ * Writes that loss averaged over the first and over the last 10 steps (below 1: the guess
+ * beats u0 on average), and the device milliseconds per step. */
 int tea_ws_train_(const int* net, const int* steps, const int* batch, const int* crop, const double* lr,
                   const int* seed, double* loss_first, double* loss_last, double* ms_per_step);
 /* Attaches the network to a chunk (net 0 detaches); sides must be multiples of
@@ -202,13 +206,14 @@ int tea_ws_attach_(const int* chunk, const int* net);
 int tea_ws_predict_(const int* net, const int* chunk, double* du, double* ms);
 /* Test hooks: parameters in the order of the CPU oracle (per 3x3 layer w[co][9][cin],
  * then b; head w, head b), the choice of convolution (0 tensor cores, 1 CUDA cores),
- * and forward/backward on host images [n][H][W][4] (target null: forward only). */
+ * and forward/backward on host images [n][H][W][4] (target null: forward only; kxy null:
+ * mean squared error, else the residual loss with face coefficients [n][H][W][2]). */
 int tea_ws_param_count_(const int* net, long long* count);
 int tea_ws_get_params_(const int* net, float* params);
 int tea_ws_set_params_(const int* net, const float* params);
 int tea_ws_set_conv_(const int* net, const int* reference);
-int tea_ws_eval_host_(const int* net, const float* x, const float* target, const int* n, const int* H,
-                      const int* W, float* y, double* loss, float* grads);
+int tea_ws_eval_host_(const int* net, const float* x, const float* target, const float* kxy, const int* n,
+                      const int* H, const int* W, float* y, double* loss, float* grads);
 
 #ifdef __cplusplus
 }

@@ -25,7 +25,7 @@ from __future__ import annotations
 
 import numpy as np
 
-IN_CHANNELS = 4  # u0 / scale, log10(density) / 2, log10(1 + Kx) / 4, log10(1 + Ky) / 4
+IN_CHANNELS = 4  # r0 / scale, log10(density) / 2, log10(1 + Kx) / 4, log10(1 + Ky) / 4
 
 
 def channels(levels: int, base: int):
@@ -137,11 +137,73 @@ def loss(y, target):
     return float(np.mean((y - target) ** 2))
 
 
-def backward(p, cache, y, target, levels: int, base: int):
-    """Gradients of loss(y, target) with respect to every parameter."""
+def apply_a(v, kx, ky):
+    """The solver's operator on one (H, W) image: kx, ky are each cell's face coefficients
+    to its left and below; faces through the image's edges carry no flux."""
+    kxl = kx.copy()
+    kxl[:, 0] = 0.0
+    kxr = np.zeros_like(kx)
+    kxr[:, :-1] = kx[:, 1:]
+    kyd = ky.copy()
+    kyd[0, :] = 0.0
+    kyu = np.zeros_like(ky)
+    kyu[:-1, :] = ky[1:, :]
+    a = (1.0 + kxl + kxr + kyd + kyu) * v
+    a[:, 1:] -= kxl[:, 1:] * v[:, :-1]
+    a[:, :-1] -= kxr[:, :-1] * v[:, 1:]
+    a[1:, :] -= kyd[1:, :] * v[:-1, :]
+    a[:-1, :] -= kyu[:-1, :] * v[1:, :]
+    return a
+
+
+SMOOTH_SWEEPS, OMEGA = 8, 0.8  # the warm start's damped Jacobi sweeps of the guess
+
+
+def diag_a(kx, ky):
+    H, W = kx.shape
+    d = np.ones((H, W))
+    d[:, 1:] += kx[:, 1:]
+    d[:, :-1] += kx[:, 1:]
+    d[1:, :] += ky[1:, :]
+    d[:-1, :] += ky[1:, :]
+    return d
+
+
+def smooth(e, kx, ky):
+    """The sweeps acting on the guess's error: e <- (I - omega D^-1 A) e."""
+    d = diag_a(kx, ky)
+    for _ in range(SMOOTH_SWEEPS):
+        e = e - OMEGA * apply_a(e, kx, ky) / d
+    return e
+
+
+def smooth_transpose(g, kx, ky):
+    d = diag_a(kx, ky)
+    for _ in range(SMOOTH_SWEEPS):
+        g = g - OMEGA * apply_a(g / d, kx, ky)
+    return g
+
+
+def residual_loss(y, target, kx, ky):
+    """The training loss of the warm start: the energy norm of the smoothed guess's error,
+    relative to that of the plain start (du = 0), when target is the true du."""
+    es = smooth(y - target, kx, ky)
+    return float(np.sum(es * apply_a(es, kx, ky)) / np.sum(target * apply_a(target, kx, ky)))
+
+
+def residual_loss_grad(y, target, kx, ky):
+    es = smooth(y - target, kx, ky)
+    g = 2.0 * apply_a(es, kx, ky) / np.sum(target * apply_a(target, kx, ky))  # A is symmetric
+    return smooth_transpose(g, kx, ky)
+
+
+def backward(p, cache, y, target, levels: int, base: int, gy=None):
+    """Gradients with respect to every parameter of loss(y, target), or, given gy = dL/dy,
+    of that loss."""
     ch = channels(levels, base)
     g = {}
-    gy = 2.0 * (y - target) / y.size
+    if gy is None:
+        gy = 2.0 * (y - target) / y.size
     h = cache["head.in"]
     g["head.w"] = np.einsum("hw,hwc->c", gy, h)
     g["head.b"] = np.array([gy.sum()])
@@ -165,10 +227,12 @@ def backward(p, cache, y, target, levels: int, base: int):
     return g
 
 
-def features(u0, density, kx, ky):
-    """Network input of a timestep (inner cells, (H, W) arrays) and the scale of u."""
-    scale = float(np.max(np.abs(u0)))
+def features(r0, density, kx, ky):
+    """Network input of a timestep (inner cells, (H, W) arrays): r0 = u0 - A u0, the residual
+    of the plain start, scaled by its largest magnitude (also the scale of the target du),
+    and the coefficients."""
+    scale = float(np.max(np.abs(r0)))
     scale = scale if scale > 0.0 else 1.0
-    x = np.stack([u0 / scale, np.log10(density) / 2.0, np.log10(1.0 + kx) / 4.0, np.log10(1.0 + ky) / 4.0],
+    x = np.stack([r0 / scale, np.log10(density) / 2.0, np.log10(1.0 + kx) / 4.0, np.log10(1.0 + ky) / 4.0],
                  axis=2)
     return x, scale

@@ -334,16 +334,18 @@ class WarmStart:
     def set_reference_conv(self, on: bool) -> None:
         self._check(self.lib.tea_ws_set_conv_(_i(self.id), _i(1 if on else 0)), "set_conv")
 
-    def eval(self, x, target=None):
-        """x [n][H][W][4] float32 -> (y [n][H][W], loss, flat gradients or None)."""
+    def eval(self, x, target=None, kxy=None):
+        """x [n][H][W][4] float32 -> (y [n][H][W], loss, flat gradients or None); with kxy
+        ([n][H][W][2] face coefficients) the loss is the residual loss of training."""
         x = np.ascontiguousarray(x, dtype=np.float32)
         n, H, W, _ = x.shape
         y = np.zeros((n, H, W), dtype=np.float32)
         loss = ctypes.c_double(0.0)
         grads = np.zeros(self.param_count(), dtype=np.float32) if target is not None else None
         t = np.ascontiguousarray(target, dtype=np.float32) if target is not None else None
+        k = np.ascontiguousarray(kxy, dtype=np.float32) if kxy is not None else None
         P = lambda a: a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
-        self._check(self.lib.tea_ws_eval_host_(_i(self.id), P(x), P(t), _i(n), _i(H), _i(W), P(y),
+        self._check(self.lib.tea_ws_eval_host_(_i(self.id), P(x), P(t), P(k), _i(n), _i(H), _i(W), P(y),
                                                ctypes.byref(loss), P(grads)), "eval_host")
         return y, loss.value, grads
 

@@ -90,6 +90,15 @@ __global__ void __launch_bounds__(BLOCK) k_ws_restart(Geom g, Box inner, Fields 
     grid_reduce<1>(acc, rs, out);
 }
 
+// Back to the plain start after a rejected guess: inner u = u0 (the set-up's u, bit for bit).
+__global__ void __launch_bounds__(BLOCK) k_ws_restore(Geom g, Box inner, Fields f)
+{
+    walk(inner, [&](int kk, int jj, int ii) {
+        const long i = fidx(g, kk, jj, ii);
+        f.u[i] = f.u0[i];
+    });
+}
+
 void free_loops(Fused* F)
 {
     for (Loop& l : F->loops) {
@@ -649,6 +658,8 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
         int one = 1;
         ext_calculate_2norm_(chunk, &ws_r0_plain, &one);  // r = u0 - A u0 after the set-up
         if (ws_predict_into(c, c->f.u)) {
+            // The residual reads u's halo: reflect the guess first.
+            halo(c, {4}, 1);
             ext_calculate_residual_(chunk);
             ext_calculate_2norm_(chunk, &ws_r0_guess, &one);
             if (ws_r0_guess < ws_r0_plain) {
@@ -658,12 +669,15 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
                 rro = ((volatile double*)c->h_out)[0];
                 c->d2h_bytes += sizeof(double);
                 ws_used = 1;
+                halo(c, {5}, 1);
             } else {
-                TEA_CK(cudaMemcpyAsync(c->alloc[F_U], c->alloc[F_U0], c->field_elems * sizeof(double),
-                                       cudaMemcpyDeviceToDevice, c->stream));
+                // The set-up's state: inner u = u0 with its reflected halo, r = u0 - A u
+                // (the same operations as the set-up's r = u - A u), p and rro untouched.
+                k_ws_restore<<<launch_blocks(c, c->inner.ntiles), dim3(TILE_X, TILE_Y), 0, c->stream>>>(
+                    c->g, c->inner, c->f);
+                halo(c, {4}, 1);
                 ext_calculate_residual_(chunk);
             }
-            halo(c, {4, 5}, 1);
         }
     }
     // The second buffers start as copies, so halos the loops never write match u and p.

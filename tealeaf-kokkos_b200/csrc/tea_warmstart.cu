@@ -2,7 +2,9 @@
 //
 // A small U-Net (tea_ws_conv.cuh, tea_ws_kernels.cuh; the numpy restatement is
 // oracle/warmstart_oracle.py) predicts the timestep increment du = u(n+1) - u0 from the
-// step's inputs u0 = density * energy, density, Kx and Ky.  The solve starts from
+// step's inputs u0 = density * energy, density, Kx and Ky -- through r0 = u0 - A u0, the
+// residual of the plain start (A du = r0, so the network learns an approximate inverse of
+// the operator; normalising r0 and du by max |r0| keeps every timestep at unit scale).  The solve starts from
 // u0 + du when that guess has a smaller FP64 initial residual than u0 itself, and
 // converges to the same tolerance either way, so no network error survives.  Training
 // pairs are recorded from the solver's own timesteps (tea_ws_record_), the network is
@@ -37,16 +39,31 @@ constexpr int N_FEAT = 4;
 
 // ----------------------------------------------------------------------------- chunk <-> features
 
-// Largest |u0| over the inner cells (the scale of u): per-block maxima, then one block.
-__global__ void k_absmax(Geom g, const double* u0, double* partial, double* out, int nblocks_final)
+// The plain start's residual r0 = u0 - A u0 (FP64) over the inner cells, [ny][nx]; the
+// neighbours outside the domain are the reflected cells, as the halo update makes them.
+__global__ void k_r0(Geom g, const double* u0, const double* kx, const double* ky, double* r0)
+{
+    const long n = (long)g.nx * g.ny;
+    const int xlast = g.X - HALO_PAD - 1, ylast = g.Y - HALO_PAD - 1;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int kk = HALO_PAD + (int)(i % g.nx), jj = HALO_PAD + (int)(i / g.nx);
+        const long f = fidx(g, kk, jj, 0);
+        const double c = u0[f];
+        const double xm = kk > HALO_PAD ? u0[f - 1] : c, xp = kk < xlast ? u0[f + 1] : c;
+        const double ym = jj > HALO_PAD ? u0[f - g.pitch] : c, yp = jj < ylast ? u0[f + g.pitch] : c;
+        const double kx0 = kx[f], kx1 = kx[f + 1], ky0 = ky[f], ky1 = ky[f + g.pitch];
+        const double au = (1.0 + (kx1 + kx0) + (ky1 + ky0)) * c - (kx1 * xp + kx0 * xm) - (ky1 * yp + ky0 * ym);
+        r0[i] = c - au;
+    }
+}
+
+// Largest |v| over n values: per-block maxima (partial), then one block (k_absmax_final).
+__global__ void k_absmax(const double* v, long n, double* partial)
 {
     __shared__ double s[256];
     double m = 0.0;
-    const long n = (long)g.nx * g.ny;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const int kk = HALO_PAD + (int)(i % g.nx), jj = HALO_PAD + (int)(i / g.nx);
-        m = fmax(m, fabs(u0[fidx(g, kk, jj, 0)]));
-    }
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(v[i]));
     s[threadIdx.x] = m;
     __syncthreads();
     for (int o = 128; o > 0; o >>= 1) {
@@ -54,8 +71,6 @@ __global__ void k_absmax(Geom g, const double* u0, double* partial, double* out,
         __syncthreads();
     }
     if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
-    (void)nblocks_final;
-    (void)out;
 }
 
 __global__ void k_absmax_final(const double* partial, int n, double* out)
@@ -72,9 +87,9 @@ __global__ void k_absmax_final(const double* partial, int n, double* out)
     if (threadIdx.x == 0) out[0] = s[0] > 0.0 ? s[0] : 1.0;
 }
 
-// Network input of the chunk's timestep: [ny][nx][IN_PAD] bfloat16, channels u0 / scale,
-// log10(density) / 2, log10(1 + Kx) / 4, log10(1 + Ky) / 4, then zeros.
-__global__ void k_features(Geom g, const double* u0, const double* dens, const double* kx, const double* ky,
+// Network input of the chunk's timestep: [ny][nx][IN_PAD] bfloat16, channels r0 / scale
+// (scale = max |r0|), log10(density) / 2, log10(1 + Kx) / 4, log10(1 + Ky) / 4, then zeros.
+__global__ void k_features(Geom g, const double* r0, const double* dens, const double* kx, const double* ky,
                            const double* scale, bf16* x)
 {
     const long n = (long)g.nx * g.ny;
@@ -83,7 +98,7 @@ __global__ void k_features(Geom g, const double* u0, const double* dens, const d
         const int kk = HALO_PAD + (int)(i % g.nx), jj = HALO_PAD + (int)(i / g.nx);
         const long f = fidx(g, kk, jj, 0);
         __align__(16) bf16 v[IN_PAD];
-        v[0] = __float2bfloat16((float)(u0[f] * inv));
+        v[0] = __float2bfloat16((float)(r0[i] * inv));
         v[1] = __float2bfloat16((float)(log10(dens[f]) * 0.5));
         v[2] = __float2bfloat16((float)(log10(1.0 + kx[f]) * 0.25));
         v[3] = __float2bfloat16((float)(log10(1.0 + ky[f]) * 0.25));
@@ -94,9 +109,10 @@ __global__ void k_features(Geom g, const double* u0, const double* dens, const d
     }
 }
 
-// A recorded pair: the four features and the target (u - u0) / scale.
-__global__ void k_record(Geom g, const bf16* x, const double* u, const double* u0, const double* scale, bf16* feat,
-                         float* tgt)
+// A recorded pair: the four features, the target (u - u0) / scale (scale = max |r0|), and
+// the cell's face coefficients (Kx, Ky) for the residual loss.
+__global__ void k_record(Geom g, const bf16* x, const double* u, const double* u0, const double* kx, const double* ky,
+                         const double* scale, bf16* feat, float* tgt, float* kxy)
 {
     const long n = (long)g.nx * g.ny;
     const double inv = 1.0 / scale[0];
@@ -105,6 +121,29 @@ __global__ void k_record(Geom g, const bf16* x, const double* u, const double* u
         const long f = fidx(g, kk, jj, 0);
         for (int c = 0; c < N_FEAT; ++c) feat[i * N_FEAT + c] = x[i * IN_PAD + c];
         tgt[i] = (float)((u[f] - u0[f]) * inv);
+        kxy[2 * i] = (float)kx[f];
+        kxy[2 * i + 1] = (float)ky[f];
+    }
+}
+
+// One damped Jacobi sweep of the guess in FP64: out = u + omega (u0 - A u) / diag(A), the
+// neighbours outside the domain reflected.
+__global__ void k_ws_smooth(Geom g, const double* u, const double* u0, const double* kx, const double* ky,
+                            double* out)
+{
+    const long n = (long)g.nx * g.ny;
+    const int xlast = g.X - HALO_PAD - 1, ylast = g.Y - HALO_PAD - 1;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int kk = HALO_PAD + (int)(i % g.nx), jj = HALO_PAD + (int)(i / g.nx);
+        const long f = fidx(g, kk, jj, 0);
+        const double c = u[f];
+        const double xm = kk > HALO_PAD ? u[f - 1] : c, xp = kk < xlast ? u[f + 1] : c;
+        const double ym = jj > HALO_PAD ? u[f - g.pitch] : c, yp = jj < ylast ? u[f + g.pitch] : c;
+        const double kx0 = kk > HALO_PAD ? kx[f] : 0.0, kx1 = kk < xlast ? kx[f + 1] : 0.0;
+        const double ky0 = jj > HALO_PAD ? ky[f] : 0.0, ky1 = jj < ylast ? ky[f + g.pitch] : 0.0;
+        const double d = 1.0 + (kx1 + kx0) + (ky1 + ky0);
+        const double au = d * c - (kx1 * xp + kx0 * xm) - (ky1 * yp + ky0 * ym);
+        out[f] = c + (double)WS_OMEGA * (u0[f] - au) / d;
     }
 }
 
@@ -123,11 +162,12 @@ __global__ void k_apply_guess(Geom g, const float* y, const double* u0, const do
 struct Crop {
     const bf16* feat;
     const float* tgt;
+    const float* kk;
     int W, y0, x0;  // source width, crop origin
 };
 
 // Training batch: b crops of size s x s from recorded pairs.
-__global__ void k_crops(const Crop* crops, int s, bf16* x, float* t, int nb, float tscale)
+__global__ void k_crops(const Crop* crops, int s, bf16* x, float* t, float* kk, int nb, float tscale)
 {
     const long per = (long)s * s;
     const long total = per * nb;
@@ -139,6 +179,8 @@ __global__ void k_crops(const Crop* crops, int s, bf16* x, float* t, int nb, flo
         for (int ch = 0; ch < IN_PAD; ++ch)
             x[i * IN_PAD + ch] = ch < N_FEAT ? c.feat[src * N_FEAT + ch] : __float2bfloat16(0.f);
         t[i] = c.tgt[src] * tscale;
+        kk[2 * i] = c.kk[2 * src];
+        kk[2 * i + 1] = c.kk[2 * src + 1];
     }
 }
 
@@ -169,6 +211,7 @@ struct Conv {
 struct Pair {
     bf16* feat = nullptr;
     float* tgt = nullptr;
+    float* kk = nullptr;  // (Kx, Ky) per cell
     int H = 0, W = 0;
 };
 
@@ -184,6 +227,11 @@ struct Net {
     float* d_sums = nullptr;
     double* d_scale = nullptr;
     double* d_partial = nullptr;
+    float* d_img = nullptr;  // per-image residual sums of the training loss [2 * 256]
+    double* r0buf = nullptr;  // the chunk's r0, [ny][nx]
+    long r0cap = 0;
+    double* ubuf = nullptr;  // a pitched u-sized buffer for the smoothing sweeps
+    long ucap = 0;
     // Workspace for n images of H x W.
     int wn = 0, wH = 0, wW = 0;
     std::vector<void*> wsbuf;
@@ -192,6 +240,7 @@ struct Net {
     bf16* bottom = nullptr;
     bf16 *G[3] = {nullptr, nullptr, nullptr};
     float *y = nullptr, *target = nullptr;
+    float *kk = nullptr, *dbuf = nullptr, *ebuf = nullptr, *gy = nullptr;  // residual loss
     std::vector<Pair> pairs;
     Crop* d_crops = nullptr;
     int sms = 148;
@@ -292,7 +341,11 @@ int ensure_workspace(Net* N, int n, int H, int W)
     }
     N->y = (float*)take(sizeof(float) * pix);
     N->target = (float*)take(sizeof(float) * pix);
-    ok = ok && N->bottom && N->y && N->target;
+    N->kk = (float*)take(sizeof(float) * pix * 2);
+    N->dbuf = (float*)take(sizeof(float) * pix);
+    N->ebuf = (float*)take(sizeof(float) * pix);
+    N->gy = (float*)take(sizeof(float) * pix);
+    ok = ok && N->bottom && N->y && N->target && N->kk && N->dbuf && N->ebuf && N->gy;
     if (!ok) {
         free_workspace(N);
         set_status(TEA_ERR_CUDA, "warm start: out of device memory for %d x %d x %d", n, H, W);
@@ -410,7 +463,50 @@ void head(Net* N, const float* target)
                                                  N->ghw, N->ghb);
 }
 
-// Backward pass after forward() and head(target): accumulates every parameter gradient.
+// Training loss: the energy norm (the norm CG minimises) of the smoothed guess's error
+// relative to that of the plain start, per crop,
+// L = (1/n) sum_b (M^k e_b).A(M^k e_b) / t_b.(A t_b), e_b = y_b - t_b (A the solver's operator
+// with the crop's own Kx, Ky, no flux through the crop's edges; M^k the warm start's k damped
+// Jacobi sweeps, which take care of the error's high frequencies and hence of most of the
+// residual norm that decides whether a solve uses the guess); every timestep alike.  Writes dL/dh into G[0] and the head's gradients;
+// d_img[2b], d_img[2b + 1] receive |A (y_b - t_b)|^2 and |A t_b|^2.
+void residual_loss_backward(Net* N)
+{
+    const int n = N->wn, H = N->wH, W = N->wW;
+    const long npix = (long)n * H * W;
+    const int grid = grid_for(npix);
+    const dim3 g2(std::max(1, grid_for((long)H * W) / std::max(1, n / 8 + 1)), n);
+    cudaMemsetAsync(N->d_img, 0, sizeof(float) * 2 * n, N->stream);
+    // d = y - t, then WS_SMOOTH damped Jacobi sweeps of the error (ping-pong d <-> gy).
+    k_res_loss<<<g2, 256, 0, N->stream>>>(N->y, N->target, N->kk, N->dbuf, N->ebuf, H, W, N->d_img, 0);
+    float* a = N->dbuf;
+    float* b = N->gy;
+    for (int k = 0; k < WS_SMOOTH; ++k) {
+        k_smooth_err<<<grid, 256, 0, N->stream>>>(a, nullptr, b, N->kk, n, H, W, 0);
+        std::swap(a, b);
+    }
+    if (a != N->dbuf) cudaMemcpyAsync(N->dbuf, a, sizeof(float) * npix, cudaMemcpyDeviceToDevice, N->stream);
+    // e = A M^k (y - t); sums; g = 2 A M^k (y - t) / (n t.A t), then back through the sweeps.
+    k_res_loss<<<g2, 256, 0, N->stream>>>(N->y, N->target, N->kk, N->dbuf, N->ebuf, H, W, N->d_img, 1);
+    k_res_grad<<<g2, 256, 0, N->stream>>>(N->ebuf, N->kk, N->d_img, N->gy, n, H, W);
+    a = N->gy;
+    b = N->dbuf;
+    for (int k = 0; k < WS_SMOOTH; ++k) {
+        k_dinv<<<grid, 256, 0, N->stream>>>(a, N->ebuf, N->kk, n, H, W);
+        k_smooth_err<<<grid, 256, 0, N->stream>>>(a, N->ebuf, b, N->kk, n, H, W, 1);
+        std::swap(a, b);
+    }
+    if (a != N->gy) cudaMemcpyAsync(N->gy, a, sizeof(float) * npix, cudaMemcpyDeviceToDevice, N->stream);
+    const int C0 = N->ch[0];
+    if (C0 == 16)
+        k_head_bw<16><<<grid, 256, 0, N->stream>>>(N->DB[0], N->hw, N->gy, npix, N->G[0], N->ghw, N->ghb);
+    else if (C0 == 32)
+        k_head_bw<32><<<grid, 256, 0, N->stream>>>(N->DB[0], N->hw, N->gy, npix, N->G[0], N->ghw, N->ghb);
+    else
+        k_head_bw<64><<<grid, 256, 0, N->stream>>>(N->DB[0], N->hw, N->gy, npix, N->G[0], N->ghw, N->ghb);
+}
+
+// Backward pass after forward() and the head's backward: accumulates every parameter gradient.
 void backward(Net* N)
 {
     const int L = N->levels, n = N->wn;
@@ -538,6 +634,26 @@ int check_err(Net* N, const char* what)
     return TEA_OK;
 }
 
+// Features of the chunk's step into x0 (and the scale max |r0| into d_scale), on `stream`.
+int chunk_features(Net* N, Chunk* c, cudaStream_t stream)
+{
+    const Geom& g = c->g;
+    const long pix = (long)g.nx * g.ny;
+    if (N->r0cap < pix) {
+        if (N->r0buf) cudaFree(N->r0buf);
+        N->r0buf = nullptr;
+        N->r0cap = 0;
+        if (dalloc(&N->r0buf, pix)) return TEA_ERR_CUDA;
+        N->r0cap = pix;
+    }
+    const int blocks = 512;
+    k_r0<<<grid_for(pix), 256, 0, stream>>>(g, c->f.u0, c->f.kx, c->f.ky, N->r0buf);
+    k_absmax<<<blocks, 256, 0, stream>>>(N->r0buf, pix, N->d_partial);
+    k_absmax_final<<<1, 256, 0, stream>>>(N->d_partial, blocks, N->d_scale);
+    k_features<<<grid_for(pix), 256, 0, stream>>>(g, N->r0buf, c->f.density, c->f.kx, c->f.ky, N->d_scale, N->x0);
+    return TEA_OK;
+}
+
 }  // namespace ws
 
 // ----------------------------------------------------------------------------- solve hook
@@ -555,15 +671,33 @@ int ws_predict_into(Chunk* c, double* u_out)
     if (g.nx % (1 << (N->levels - 1)) || g.ny % (1 << (N->levels - 1))) return 0;
     cudaStream_t saved = N->stream;
     N->stream = c->stream;
-    const int blocks = 512;
-    k_absmax<<<blocks, 256, 0, c->stream>>>(g, c->f.u0, N->d_partial, N->d_scale, blocks);
-    k_absmax_final<<<1, 256, 0, c->stream>>>(N->d_partial, blocks, N->d_scale);
-    k_features<<<grid_for((long)g.nx * g.ny), 256, 0, c->stream>>>(g, c->f.u0, c->f.density, c->f.kx, c->f.ky,
-                                                                   N->d_scale, N->x0);
+    if (chunk_features(N, c, c->stream) != TEA_OK) {
+        N->stream = saved;
+        return 0;
+    }
     forward(N);
     head(N, nullptr);
+    // Guess into u, then WS_SMOOTH (even) damped Jacobi sweeps ping-ponged through a second
+    // pitched buffer, ending in u; only inner cells are written.
+    if (N->ucap < (long)c->field_elems) {
+        if (N->ubuf) cudaFree(N->ubuf);
+        N->ubuf = nullptr;
+        N->ucap = 0;
+        if (dalloc(&N->ubuf, c->field_elems)) {
+            N->stream = saved;
+            return 0;
+        }
+        N->ucap = (long)c->field_elems;
+    }
+    static_assert(WS_SMOOTH % 2 == 0, "the sweeps must end in u");
     k_apply_guess<<<grid_for((long)g.nx * g.ny), 256, 0, c->stream>>>(g, N->y, c->f.u0, N->d_scale,
                                                                        1.0 / (double)N->out_scale, u_out);
+    double* src = u_out;
+    double* dst = N->ubuf + kLeadPad;
+    for (int k = 0; k < WS_SMOOTH; ++k) {
+        k_ws_smooth<<<grid_for((long)g.nx * g.ny), 256, 0, c->stream>>>(g, src, c->f.u0, c->f.kx, c->f.ky, dst);
+        std::swap(src, dst);
+    }
     N->stream = saved;
     return 1;
 }
@@ -627,13 +761,9 @@ TEA_EXPORT int tea_ws_create_(const int* levels, const int* base, const int* see
         if (dalloc(p, nh)) return TEA_ERR_CUDA;
     N->hb = N->hw + N->ch[0];
     N->ghb = N->ghw + N->ch[0];
-    {
-        std::vector<float> h(nh, 0.f);
-        for (int k = 0; k < N->ch[0]; ++k) h[k] = sqrtf(1.f / N->ch[0]) * nd(rng) * 0.1f;
-        WS_CK(cudaMemcpy(N->hw, h.data(), sizeof(float) * nh, cudaMemcpyHostToDevice));
-    }
+    // The head starts at zero: the untrained guess is du = 0, the plain start itself.
     if (dalloc(&N->d_err, 1) || dalloc(&N->d_sums, 4) || dalloc(&N->d_scale, 1) || dalloc(&N->d_partial, 512) ||
-        dalloc(&N->d_crops, 256))
+        dalloc(&N->d_crops, 256) || dalloc(&N->d_img, 512))
         return TEA_ERR_CUDA;
     refresh_bf16(N.get());
     WS_CK(cudaStreamSynchronize(N->stream));
@@ -654,11 +784,13 @@ TEA_EXPORT int tea_ws_destroy_(const int* net)
                         (void*)c.vb, (void*)c.w16, (void*)c.wt16})
             cudaFree(p);
     for (void* p : {(void*)N->hw, (void*)N->ghw, (void*)N->mh, (void*)N->vh, (void*)N->d_err, (void*)N->d_sums,
-                    (void*)N->d_scale, (void*)N->d_partial, (void*)N->d_crops})
+                    (void*)N->d_scale, (void*)N->d_partial, (void*)N->d_crops, (void*)N->d_img, (void*)N->r0buf,
+                    (void*)N->ubuf})
         cudaFree(p);
     for (Pair& p : N->pairs) {
         cudaFree(p.feat);
         cudaFree(p.tgt);
+        cudaFree(p.kk);
     }
     cudaStreamDestroy(N->stream);
     nets()[*net - 1].reset();
@@ -699,8 +831,10 @@ TEA_EXPORT int tea_ws_set_params_(const int* net, const float* params)
 
 // Forward (and, with a target, backward) over n host images of 4 features [n][H][W][4];
 // writes the prediction [n][H][W], the loss and the parameter gradients (oracle order).
-TEA_EXPORT int tea_ws_eval_host_(const int* net, const float* x, const float* target, const int* n, const int* H,
-                                 const int* W, float* y, double* loss, float* grads)
+// The loss is the mean squared error, or with kxy ([n][H][W][2] face coefficients) the
+// training's residual loss mean |A (y - target)|^2.
+TEA_EXPORT int tea_ws_eval_host_(const int* net, const float* x, const float* target, const float* kxy,
+                                 const int* n, const int* H, const int* W, float* y, double* loss, float* grads)
 {
     Net* N = get_net(net);
     if (!N || !x || !y || *n < 1 || *H < 2 || *W < 2) return TEA_ERR_BAD_ARGUMENT;
@@ -726,14 +860,28 @@ TEA_EXPORT int tea_ws_eval_host_(const int* net, const float* x, const float* ta
         WS_CK(cudaMemsetAsync(N->ghw, 0, sizeof(float) * (N->ch[0] + 1), N->stream));
     }
     forward(N);
-    head(N, target ? N->target : nullptr);
+    if (target && kxy) {
+        WS_CK(cudaMemcpyAsync(N->kk, kxy, sizeof(float) * pix * 2, cudaMemcpyHostToDevice, N->stream));
+        head(N, nullptr);
+        residual_loss_backward(N);
+    } else {
+        head(N, target ? N->target : nullptr);
+    }
     if (target) backward(N);
     if ((rc = check_err(N, "eval"))) return rc;
     WS_CK(cudaMemcpy(y, N->y, sizeof(float) * pix, cudaMemcpyDeviceToHost));
     if (target) {
-        float s = 0.f;
-        WS_CK(cudaMemcpy(&s, N->d_sums, sizeof(float), cudaMemcpyDeviceToHost));
-        if (loss) *loss = (double)s / (double)pix;
+        if (kxy) {
+            std::vector<float> v(2 * (size_t)*n);
+            WS_CK(cudaMemcpy(v.data(), N->d_img, sizeof(float) * v.size(), cudaMemcpyDeviceToHost));
+            double r = 0.0;
+            for (int b = 0; b < *n; ++b) r += v[2 * b + 1] > 0.f ? (double)v[2 * b] / v[2 * b + 1] : 0.0;
+            if (loss) *loss = r / *n;
+        } else {
+            float s = 0.f;
+            WS_CK(cudaMemcpy(&s, N->d_sums, sizeof(float), cudaMemcpyDeviceToHost));
+            if (loss) *loss = (double)s / (double)pix;
+        }
         if (grads && (rc = transfer_params(N, grads, false, true))) return rc;
     }
     return TEA_OK;
@@ -758,13 +906,11 @@ TEA_EXPORT int tea_ws_record_(const int* net, const int* chunk)
     p.H = g.ny;
     p.W = g.nx;
     const long pix = (long)g.nx * g.ny;
-    if (dalloc(&p.feat, pix * N_FEAT) || dalloc(&p.tgt, pix)) return TEA_ERR_CUDA;
+    if (dalloc(&p.feat, pix * N_FEAT) || dalloc(&p.tgt, pix) || dalloc(&p.kk, pix * 2)) return TEA_ERR_CUDA;
     WS_CK(cudaStreamSynchronize(c->stream));
-    const int blocks = 512;
-    k_absmax<<<blocks, 256, 0, N->stream>>>(g, c->f.u0, N->d_partial, N->d_scale, blocks);
-    k_absmax_final<<<1, 256, 0, N->stream>>>(N->d_partial, blocks, N->d_scale);
-    k_features<<<grid_for(pix), 256, 0, N->stream>>>(g, c->f.u0, c->f.density, c->f.kx, c->f.ky, N->d_scale, N->x0);
-    k_record<<<grid_for(pix), 256, 0, N->stream>>>(g, N->x0, c->f.u, c->f.u0, N->d_scale, p.feat, p.tgt);
+    if ((rc = chunk_features(N, c, N->stream))) return rc;
+    k_record<<<grid_for(pix), 256, 0, N->stream>>>(g, N->x0, c->f.u, c->f.u0, c->f.kx, c->f.ky, N->d_scale, p.feat,
+                                                   p.tgt, p.kk);
     WS_CK(cudaStreamSynchronize(N->stream));
     N->pairs.push_back(p);
     return TEA_OK;
@@ -824,6 +970,7 @@ TEA_EXPORT int tea_ws_train_(const int* net, const int* steps, const int* batch,
             const Pair& p = N->pairs[rng() % N->pairs.size()];
             crops[b].feat = p.feat;
             crops[b].tgt = p.tgt;
+            crops[b].kk = p.kk;
             crops[b].W = p.W;
             crops[b].y0 = (int)(rng() % (unsigned long long)(p.H - *crop + 1));
             crops[b].x0 = (int)(rng() % (unsigned long long)(p.W - *crop + 1));
@@ -831,21 +978,27 @@ TEA_EXPORT int tea_ws_train_(const int* net, const int* steps, const int* batch,
         WS_CK(cudaMemcpyAsync(N->d_crops, crops.data(), sizeof(Crop) * crops.size(), cudaMemcpyHostToDevice,
                               N->stream));
         if (s == 1) cudaEventRecord(e0, N->stream);
-        k_crops<<<grid_for(pix), 256, 0, N->stream>>>(N->d_crops, *crop, N->x0, N->target, *batch, N->out_scale);
-        // The loss sums run over the first and the last `win` steps.
-        if (s == 0 || s == *steps - win) WS_CK(cudaMemsetAsync(N->d_sums, 0, sizeof(float), N->stream));
+        k_crops<<<grid_for(pix), 256, 0, N->stream>>>(N->d_crops, *crop, N->x0, N->target, N->kk, *batch,
+                                                       N->out_scale);
         forward(N);
-        head(N, N->target);
+        head(N, nullptr);
+        residual_loss_backward(N);
         backward(N);
         adam_step(N, (float)*lr);
-        if (s == win - 1 || s == *steps - 1) {
-            float v = 0.f;
-            WS_CK(cudaMemcpyAsync(&v, N->d_sums, sizeof(float), cudaMemcpyDeviceToHost, N->stream));
+        // The reported losses average the first and the last `win` steps.
+        if (s < win || s >= *steps - win) {
+            std::vector<float> v(2 * (size_t)*batch);
+            WS_CK(cudaMemcpyAsync(v.data(), N->d_img, sizeof(float) * v.size(), cudaMemcpyDeviceToHost, N->stream));
             WS_CK(cudaStreamSynchronize(N->stream));
-            (s == win - 1 ? first : last) = (double)v / (double)pix / win;
+            float dmax = 0.f;
+            for (int b = 0; b < *batch; ++b) dmax = std::max(dmax, v[2 * b + 1]);
+            double r = 0.0;
+            for (int b = 0; b < *batch; ++b) r += (double)v[2 * b] / std::max(std::max(v[2 * b + 1], 1e-3f * dmax), 1e-30f);
+            r /= *batch;
+            if (s < win) first += r / win;
+            if (s >= *steps - win) last += r / win;
         }
     }
-    if (*steps == 1) last = first;
     cudaEventRecord(e1, N->stream);
     if ((rc = check_err(N, "train"))) return rc;
     float ms = 0.f;

@@ -202,6 +202,156 @@ __global__ void __launch_bounds__(256) k_head(const bf16* h, const float* w, con
     }
 }
 
+// ----------------------------------------------------------------------------- residual loss
+
+// The solver's operator on an n x H x W crop stack, A v = (1 + sum of the cell's face
+// coefficients) v - sum K_face v_neighbour, with kk[p] = (Kx, Ky) of pixel p (the faces
+// to its left and below) and the crop's outer faces taken as zero (no flux), which keeps A
+// symmetric.
+__device__ __forceinline__ float apply_a(const float* v, const float* kk, long p, int xx, int yy, int H, int W)
+{
+    const float kxl = xx > 0 ? kk[2 * p] : 0.f;
+    const float kxr = xx + 1 < W ? kk[2 * (p + 1)] : 0.f;
+    const float kyd = yy > 0 ? kk[2 * p + 1] : 0.f;
+    const float kyu = yy + 1 < H ? kk[2 * (p + W) + 1] : 0.f;
+    float a = (1.f + kxl + kxr + kyd + kyu) * v[p];
+    if (xx > 0) a -= kxl * v[p - 1];
+    if (xx + 1 < W) a -= kxr * v[p + 1];
+    if (yy > 0) a -= kyd * v[p - W];
+    if (yy + 1 < H) a -= kyu * v[p + W];
+    return a;
+}
+
+// Pass 0: d = y - t.  Pass 1 (d now the smoothed error): e = A d; per image b (blockIdx.y),
+// sums[2b] += d.(A d) and sums[2b + 1] += t.(A t): the energy norm of the guess's error and
+// that of the plain start's (du = 0).
+__global__ void k_res_loss(const float* y, const float* t, const float* kk, float* d, float* e, int H, int W,
+                           float* sums, int pass)
+{
+    const long per = (long)H * W;
+    const long off = (long)blockIdx.y * per;
+    float s0 = 0.f, s1 = 0.f;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < per; q += (long)gridDim.x * blockDim.x) {
+        const long p = off + q;
+        if (pass == 0) {
+            d[p] = y[p] - t[p];
+        } else {
+            const int xx = (int)(q % W), yy = (int)(q / W);
+            const float ev = apply_a(d, kk, p, xx, yy, H, W);
+            e[p] = ev;
+            s0 += d[p] * ev;
+            s1 += t[p] * apply_a(t, kk, p, xx, yy, H, W);
+        }
+    }
+    if (pass == 0) return;
+    __shared__ float r0[256], r1[256];
+    r0[threadIdx.x] = s0;
+    r1[threadIdx.x] = s1;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            r0[threadIdx.x] += r0[threadIdx.x + o];
+            r1[threadIdx.x] += r1[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&sums[2 * blockIdx.y], r0[0]);
+        atomicAdd(&sums[2 * blockIdx.y + 1], r1[0]);
+    }
+}
+
+// dL/d(smoothed error) of L = (1/n) sum_b d_b.(A d_b) / t_b.(A t_b): 2 A d_b / (n t_b.(A t_b)),
+// with e = A d from pass 1.
+__global__ void k_res_grad(const float* e, const float* kk, const float* sums, float* gy, int n, int H, int W)
+{
+    const long per = (long)H * W;
+    const long off = (long)blockIdx.y * per;
+    // Crops with almost no activity (t.A t tiny) would dominate: their denominator is floored
+    // at 1e-3 of the batch's largest.
+    float dmax = 0.f;
+    for (int b = 0; b < n; ++b) dmax = fmaxf(dmax, sums[2 * b + 1]);
+    const float sc = 2.f / ((float)n * fmaxf(fmaxf(sums[2 * blockIdx.y + 1], 1e-3f * dmax), 1e-30f));
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < per; q += (long)gridDim.x * blockDim.x) {
+        const long p = off + q;
+        gy[p] = sc * e[p];
+    }
+    (void)kk;
+    (void)W;
+}
+
+// The warm start smooths the network's guess with damped Jacobi sweeps in FP64 before the
+// solve; training sees the same linear smoothing on the error e = y - t:
+//   e <- M e,  M = I - omega D^-1 A        (forward),
+//   g <- M^T g = g - omega A (D^-1 g)      (backward; A symmetric, D its diagonal).
+constexpr int WS_SMOOTH = 8;
+constexpr float WS_OMEGA = 0.8f;
+
+__device__ __forceinline__ float diag_a(const float* kk, long p, int xx, int yy, int H, int W)
+{
+    const float kxl = xx > 0 ? kk[2 * p] : 0.f;
+    const float kxr = xx + 1 < W ? kk[2 * (p + 1)] : 0.f;
+    const float kyd = yy > 0 ? kk[2 * p + 1] : 0.f;
+    const float kyu = yy + 1 < H ? kk[2 * (p + W) + 1] : 0.f;
+    return 1.f + kxl + kxr + kyd + kyu;
+}
+
+// out = in - omega D^-1 A in (transpose = 0), or out = in - omega A tmp with tmp = D^-1 in
+// precomputed (transpose = 1); over n images of H x W.
+__global__ void k_smooth_err(const float* in, const float* tmp, float* out, const float* kk, int n, int H, int W,
+                             int transpose)
+{
+    const long total = (long)n * H * W;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < total; p += (long)gridDim.x * blockDim.x) {
+        const int xx = (int)(p % W), yy = (int)((p / W) % H);
+        if (!transpose)
+            out[p] = in[p] - WS_OMEGA * apply_a(in, kk, p, xx, yy, H, W) / diag_a(kk, p, xx, yy, H, W);
+        else
+            out[p] = in[p] - WS_OMEGA * apply_a(tmp, kk, p, xx, yy, H, W);
+    }
+}
+
+__global__ void k_dinv(const float* in, float* out, const float* kk, int n, int H, int W)
+{
+    const long total = (long)n * H * W;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < total; p += (long)gridDim.x * blockDim.x) {
+        const int xx = (int)(p % W), yy = (int)((p / W) % H);
+        out[p] = in[p] / diag_a(kk, p, xx, yy, H, W);
+    }
+}
+
+// Head backward from a given dL/dy: gh = gy w (h > 0), gw += gy h, gb += gy.
+template <int C>
+__global__ void __launch_bounds__(256) k_head_bw(const bf16* h, const float* w, const float* gy, long npix, bf16* gh,
+                                                  float* gw, float* gb)
+{
+    __shared__ float s_w[C];
+    __shared__ float s_red[C + 1];
+    for (int c = threadIdx.x; c < C; c += blockDim.x) s_w[c] = w[c];
+    for (int c = threadIdx.x; c < C + 1; c += blockDim.x) s_red[c] = 0.f;
+    __syncthreads();
+    float gwl[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) gwl[c] = 0.f;
+    float gbl = 0.f;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
+        const float g = gy[p];
+        gbl += g;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const float hv = __bfloat162float(h[p * C + c]);
+            gwl[c] += g * hv;
+            gh[p * C + c] = __float2bfloat16(hv > 0.f ? g * s_w[c] : 0.f);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) atomicAdd(&s_red[c], gwl[c]);
+    atomicAdd(&s_red[C], gbl);
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&gw[c], s_red[c]);
+    if (threadIdx.x == 0) atomicAdd(gb, s_red[C]);
+}
+
 // ----------------------------------------------------------------------------- optimiser
 
 // Adam on float32 master weights; clears the gradient.

@@ -47,3 +47,20 @@ def test_layer_shapes_follow_the_unet():
     assert dict((n, (co, ci)) for n, co, ci in shapes)["dec1a"] == (64, 128 + 64)
     params = sum(co * 9 * ci + co for _, co, ci in shapes) + 32 + 1
     assert 400_000 < params < 600_000  # about half a million parameters
+
+
+def test_residual_loss_gradient_matches_finite_differences():
+    rng = np.random.default_rng(9)
+    H, W = 6, 7
+    y, t = rng.normal(size=(H, W)), rng.normal(size=(H, W))
+    kx, ky = rng.uniform(0.1, 5.0, (H, W)), rng.uniform(0.1, 5.0, (H, W))
+    g = wo.residual_loss_grad(y, t, kx, ky)
+    h = 1e-6
+    for idx in [(0, 0), (2, 3), (5, 6), (3, 0)]:
+        yp, ym = y.copy(), y.copy()
+        yp[idx] += h
+        ym[idx] -= h
+        fd = (wo.residual_loss(yp, t, kx, ky) - wo.residual_loss(ym, t, kx, ky)) / (2 * h)
+        assert abs(fd - g[idx]) <= 1e-6 * max(1.0, abs(fd)), (idx, fd, g[idx])
+    # A is the operator with zero-flux edges: constants are its eigenvectors (eigenvalue 1).
+    assert np.allclose(wo.apply_a(np.ones((H, W)), kx, ky), 1.0)
