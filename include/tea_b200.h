@@ -94,6 +94,17 @@ int tea_transfer_bytes_(const int* chunk, long long* h2d, long long* d2h);
 int tea_2norm_noalloc_(const double* field, const int* nx, const int* ny, const int* nz, double* norm,
                        void* stream);
 
+/* Face packing for a halo exchange between ranks: the arguments and meaning of the 2D
+ * ext_pack_message_ (tealeaf_2d/ext_core.cpp:151; the 3D library takes the same seven
+ * arguments, without fieldType) with one difference: in 2D the bottom (3) and top (4) faces
+ * are packed from, and unpacked into, the inner columns 2..nx+1.  The reference's 2D
+ * packer (TopBottomPacker, tealeaf_2d/ext_pack_kernel.hpp:17-44) starts those rows at padded
+ * column 0, so the last two inner columns of each exchanged halo row are never sent;
+ * ext_pack_message_ keeps that behaviour for parity, and the slab driver uses this one.
+ * Every other face, and every 3D face, is packed exactly as ext_pack_message_ packs it. */
+void tea_pack_face_(const int* chunk, const int* fields, const int* offsets, const int* depth, const int* face,
+                    double* buffer, const void* pack);
+
 /* Solver ids for the whole-solve entry point. */
 enum {
     TEA_SOLVER_JACOBI = 1,

@@ -494,7 +494,7 @@ EXPORT void ext_update_halo_kernel_(const int* chunk, const int* chunkNeighbours
 /* Packers, tealeaf_2d/ext_pack_kernel.hpp:8-97 and tealeaf_3d/ext_pack_kernel.hpp.
  * The field index of buffer element `index` is restated from each packer's offset
  * expression; 3D front/back follow tealeaf_3d/ext_pack_kernel.hpp:137-190. */
-static long pack_index(const Chunk* c, int face, int depth, int pack, long index)
+static long pack_index(const Chunk* c, int face, int depth, int pack, long index, int exact)
 {
     const long X = c->dims.x, Y = c->dims.y;
 #if TEA_DIM == 2
@@ -511,9 +511,10 @@ static long pack_index(const Chunk* c, int face, int depth, int pack, long index
         if (face == 4) off = pack ? X * (Y - HALO_PAD - depth) + lines * 2 * HALO_PAD
                                   : X * (Y - HALO_PAD) + lines * 2 * HALO_PAD;
         else off = pack ? X * HALO_PAD + lines * 2 * HALO_PAD : X * (HALO_PAD - depth) + lines * 2 * HALO_PAD;
-        return off + index;
+        return off + index + (exact ? HALO_PAD : 0);
     }
 #else
+    (void)exact;
     const long Z = c->dims.z;
     const long HP2 = 2 * HALO_PAD;
     const long page = X * Y;
@@ -544,7 +545,7 @@ static long pack_index(const Chunk* c, int face, int depth, int pack, long index
 }
 
 static void pack_message(Chunk* c, const int* fields, const int* offsets, int depth, int face,
-                         double* buffer, int pack)
+                         double* buffer, int pack, int exact)
 {
     long len;
 #if TEA_DIM == 2
@@ -563,7 +564,7 @@ static void pack_message(Chunk* c, const int* fields, const int* offsets, int de
         double* b = halo_field(c, f + 1);
         double* ext = buffer + offsets[f];
         for (long index = 0; index < len; ++index) {
-            long fi = pack_index(c, face, depth, pack, index);
+            long fi = pack_index(c, face, depth, pack, index, exact);
             if (pack) ext[index] = b[fi];
             else b[fi] = ext[index];
         }
@@ -576,7 +577,7 @@ EXPORT void ext_pack_message_(const int* chunk, const int* fields, const int* of
                               const void* pack)
 {
     pack_message(get_chunk(chunk), fields, offsets, *depth, *face, buffer,
-                 *(const unsigned char*)pack != 0);
+                 *(const unsigned char*)pack != 0, 0);
 }
 #else
 EXPORT void ext_pack_message_(const int* chunk, const int* fields, const int* offsets,
@@ -585,9 +586,19 @@ EXPORT void ext_pack_message_(const int* chunk, const int* fields, const int* of
 {
     (void)fieldType;
     pack_message(get_chunk(chunk), fields, offsets, *depth, *face, buffer,
-                 *(const unsigned char*)pack != 0);
+                 *(const unsigned char*)pack != 0, 0);
 }
 #endif
+
+/* The exchange packer of the slab driver: ext_pack_message_ with the 2D bottom/top faces
+ * on the inner columns (the reference's 2D packer starts at column 0,
+ * tealeaf_2d/ext_pack_kernel.hpp:17-44); 3D faces are identical to it. */
+EXPORT void tea_pack_face_(const int* chunk, const int* fields, const int* offsets, const int* depth,
+                           const int* face, double* buffer, const void* pack)
+{
+    pack_message(get_chunk(chunk), fields, offsets, *depth, *face, buffer, *(const unsigned char*)pack != 0, 1);
+}
+
 
 /* ---------------------------------------------------------------- shared methods */
 

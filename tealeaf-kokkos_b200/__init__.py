@@ -124,7 +124,7 @@ def driver() -> ctypes.CDLL:
 def run_deck(deck_text: str, dim: int, backend=None, *, fused: bool = False, summary_every_step: bool = False,
              end_step: int = 0, quiet: bool = True, out_path=None, eps: float = 0.0, eps_rel: float = 0.0,
              keep_chunk: bool = False, precision: int = 0, max_records: int = 100000, ws_net: int = 0,
-             ws_mode: int = 0):
+             ws_mode: int = 0, comm=None):
     """Run a tea.in deck through the C++ driver against ``backend`` (default: the CUDA
     library for ``dim``).  Returns ``(summary, records)`` as dicts."""
     backend = str(backend) if backend is not None else str(lib_path(dim))
@@ -147,11 +147,58 @@ def run_deck(deck_text: str, dim: int, backend=None, *, fused: bool = False, sum
     summary = RunSummary()
     records = (StepRecord * max_records)()
     lib = driver()
-    rc = lib.tea_run_deck(deck_text.encode(), ctypes.byref(opt), ctypes.byref(summary), records, max_records)
+    if comm is None:
+        rc = lib.tea_run_deck(deck_text.encode(), ctypes.byref(opt), ctypes.byref(summary), records, max_records)
+    else:
+        rc = lib.tea_run_deck_comm(deck_text.encode(), ctypes.byref(opt), ctypes.byref(comm), ctypes.byref(summary),
+                                   records, max_records)
     if rc != 0:
         raise RuntimeError("tea driver: " + lib.tea_driver_last_error().decode())
     n = min(summary.steps, max_records)
     return _struct_dict(summary), [_struct_dict(records[i]) for i in range(n)]
+
+
+_ALLREDUCE = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_void_p)
+_SENDRECV = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                             ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int, ctypes.c_void_p)
+
+
+class Comm(ctypes.Structure):
+    _fields_ = [("rank", ctypes.c_int), ("size", ctypes.c_int), ("allreduce_sum", _ALLREDUCE),
+                ("sendrecv", _SENDRECV), ("ctx", ctypes.c_void_p)]
+
+
+def run_deck_dist(deck_text: str, dim: int, backend=None, *, group=None, device=None, **kw):
+    """run_deck over the ranks of a torch.distributed process group: rank r owns the r-th
+    slab of the slowest axis; halo faces and global sums go through the group (gloo on the
+    host, or NCCL with ``device`` a CUDA device).  Per-call path only."""
+    import torch
+    import torch.distributed as dist
+
+    def to_dev(t):
+        return t.to(device) if device is not None else t
+
+    def allreduce(ptr, n, _ctx):
+        a = np.ctypeslib.as_array(ptr, shape=(n,))
+        t = to_dev(torch.from_numpy(a.copy()))
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        a[:] = t.cpu().numpy()
+
+    def sendrecv(sp, ns, to, rp, nr, frm, _ctx):
+        snd = to_dev(torch.from_numpy(np.ctypeslib.as_array(sp, shape=(ns,)).copy()))
+        rcv = to_dev(torch.empty(nr, dtype=torch.float64))
+        reqs = [dist.isend(snd, to, group=group), dist.irecv(rcv, frm, group=group)]
+        for q in reqs:
+            q.wait()
+        np.ctypeslib.as_array(rp, shape=(nr,))[:] = rcv.cpu().numpy()
+
+    comm = Comm()
+    comm.rank = dist.get_rank(group)
+    comm.size = dist.get_world_size(group)
+    comm.allreduce_sum = _ALLREDUCE(allreduce)
+    comm.sendrecv = _SENDRECV(sendrecv)
+    comm.ctx = None
+    return run_deck(deck_text, dim, backend, comm=comm, **kw)
 
 
 # ----------------------------------------------------------------------------- chunks

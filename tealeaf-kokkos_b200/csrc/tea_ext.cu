@@ -427,7 +427,7 @@ TEA_EXPORT void ext_field_summary_kernel_(const int* chunk, double* vol, double*
 // ===================================================================== halo / pack
 
 static void pack_message(const int* chunk, const int* fields, const int* offsets, const int* depth,
-                         const int* face, double* buffer, const void* pack)
+                         const int* face, double* buffer, const void* pack, bool exact = false)
 {
     Chunk* c = get_chunk(chunk);
     if (!c) return;
@@ -452,7 +452,7 @@ static void pack_message(const int* chunk, const int* fields, const int* offsets
         }
         const int blocks = (int)std::min<long>((len + 255) / 256, 4096);
         k_pack<<<std::max(blocks, 1), 256, 0, c->stream>>>(c->g, halo_field(c, fid), dbuf, len, *face, *depth,
-                                                           do_pack ? 1 : 0);
+                                                           do_pack ? 1 : 0, exact ? 1 : 0);
         sync(c);
         if (do_pack) {
             TEA_CK(cudaMemcpy(ext, dbuf, sizeof(double) * len, cudaMemcpyDeviceToHost));
@@ -476,6 +476,14 @@ TEA_EXPORT void ext_pack_message_(const int* chunk, const int* fields, const int
     pack_message(chunk, fields, offsets, depth, face, buffer, pack);
 }
 #endif
+
+// Face packing for an exchange between ranks: ext_pack_message_ with the 2D bottom/top faces
+// on the inner columns (see pack_flat_index); 3D faces are identical to it.
+TEA_EXPORT void tea_pack_face_(const int* chunk, const int* fields, const int* offsets, const int* depth,
+                               const int* face, double* buffer, const void* pack)
+{
+    pack_message(chunk, fields, offsets, depth, face, buffer, pack, true);
+}
 
 TEA_EXPORT void ext_update_halo_kernel_(const int* chunk, const int* chunkNeighbours, const int* fields,
                                         const int* depth)

@@ -207,7 +207,10 @@ __global__ void k_update_halo(Geom g, HaloJob job)
 // Packers, tealeaf_2d/ext_pack_kernel.hpp:8-97 and tealeaf_3d/ext_pack_kernel.hpp: the
 // padded flat index of buffer element `index`, restated from each packer's offset
 // expression, then mapped to the pitched layout.
-__device__ __forceinline__ long pack_flat_index(const Geom& g, int face, int depth, bool pack, long index)
+// exact: the 2D bottom/top faces cover the inner columns 2..nx+1 (the reference's packer
+// starts at column 0, tealeaf_2d/ext_pack_kernel.hpp:17-44; every other face is the same).
+__device__ __forceinline__ long pack_flat_index(const Geom& g, int face, int depth, bool pack, long index,
+                                                bool exact = false)
 {
     const long X = g.X, Y = g.Y;
 #if TEA_DIM == 2
@@ -223,7 +226,7 @@ __device__ __forceinline__ long pack_flat_index(const Geom& g, int face, int dep
     long off;
     if (face == 4) off = pack ? X * (Y - HALO_PAD - depth) + lines * 2 * HALO_PAD : X * (Y - HALO_PAD) + lines * 2 * HALO_PAD;
     else off = pack ? X * HALO_PAD + lines * 2 * HALO_PAD : X * (HALO_PAD - depth) + lines * 2 * HALO_PAD;
-    return off + index;
+    return off + index + (exact ? HALO_PAD : 0);
 #else
     const long Z = g.Z, HP2 = 2 * HALO_PAD, page = X * Y;
     if (face == 1 || face == 2) {
@@ -252,10 +255,10 @@ __device__ __forceinline__ long pack_flat_index(const Geom& g, int face, int dep
 #endif
 }
 
-__global__ void k_pack(Geom g, double* field, double* buf, long len, int face, int depth, int pack)
+__global__ void k_pack(Geom g, double* field, double* buf, long len, int face, int depth, int pack, int exact)
 {
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < len; idx += (long)gridDim.x * blockDim.x) {
-        const long flat = pack_flat_index(g, face, depth, pack != 0, idx);
+        const long flat = pack_flat_index(g, face, depth, pack != 0, idx, exact != 0);
         const long kk = flat % g.X;
         const long rest = flat / g.X;
         const long jj = rest % g.Y;

@@ -298,6 +298,9 @@ struct Backend {
     void (*calc_2norm)(const int*, double*, const void*) = nullptr;
     void (*finalise_solve)(const int*) = nullptr;
     void (*update_halo)(const int*, const int*, const int*, const int*) = nullptr;
+    void* pack = nullptr;  // ext_pack_message_ (2D and 3D signatures differ)
+    // tea_pack_face_: the same packing with the 2D bottom/top faces on the inner columns
+    void (*pack_face)(const int*, const int*, const int*, const int*, const int*, double*, const void*) = nullptr;
     void (*jacobi_init)(const int*, const int*, const double*) = nullptr;
     void (*jacobi_solve)(const int*, double*) = nullptr;
     void (*cg_init)(const int*, const int*, const int*, double*, double*) = nullptr;
@@ -340,6 +343,8 @@ struct Backend {
         bind(calc_2norm, "ext_calculate_2norm_");
         bind(finalise_solve, "ext_solver_finalise_");
         bind(update_halo, "ext_update_halo_kernel_");
+        pack = dlsym(handle, "ext_pack_message_");
+        bind(pack_face, "tea_pack_face_", false);
         bind(jacobi_init, "ext_jacobi_kernel_init_");
         bind(jacobi_solve, "ext_jacobi_kernel_solve_");
         bind(cg_init, "ext_cg_solver_init_");
@@ -428,8 +433,75 @@ struct Runner {
     Backend be;
     Log log;
     const tea_run_options* opt;
+    const tea_comm* comm = nullptr;  // several ranks: slabs (tea_run_deck_comm)
     int chunk = 1;
     int neighbours[6] = {-1, -1, -1, -1, -1, -1};  // every face EXTERNAL_FACE on one rank
+    int lx = 0, ly = 0, lz = 0;                    // this rank's chunk, inner cells
+    std::vector<double> snd, rcv;
+
+    bool split() const { return comm && comm->size > 1; }
+
+    // tea_allsum (tealeaf_2d/tea.f90:1249-1267): every global scalar is a sum over ranks.
+    void allsum(double* v, int n)
+    {
+        if (split()) comm->allreduce_sum(v, n, comm->ctx);
+    }
+
+    // tea_exchange (tealeaf_2d/tea.f90:246-407, tealeaf_3d/tea.f90): pack the selected
+    // fields' faces towards each internal neighbour, swap, unpack.  Slabs have internal
+    // faces only across the split axis (bottom/top in 2D, back/front in 3D).  The 2D
+    // bottom/top packer of the reference (tealeaf_2d/ext_pack_kernel.hpp:17-44) starts at
+    // padded column 0, so it sends columns 0..nx-1 and the last two inner columns of every
+    // exchanged halo row stay stale; a backend that exports tea_pack_face_ packs the inner
+    // columns and is used instead.
+    void exchange(const int* fields, int depth)
+    {
+        if (!split()) return;
+        if (be.pack_face) {
+            exchange_with(fields, depth, [&](int face, double* buf, int pk) {
+                be.pack_face(&chunk, fields, cur_offsets, &depth, &face, buf, &pk);
+                be.check_status("tea_pack_face_");
+            });
+            return;
+        }
+        if (!be.pack) fail("backend lacks ext_pack_message_");
+        exchange_with(fields, depth, [&](int face, double* buf, int pk) {
+            const int cell_data = 1;
+            if (cfg.dim == 2)
+                reinterpret_cast<void (*)(const int*, const int*, const int*, const int*, const int*, double*,
+                                          const void*)>(be.pack)(&chunk, fields, cur_offsets, &depth, &face, buf, &pk);
+            else
+                reinterpret_cast<void (*)(const int*, const int*, const int*, const int*, const int*, const int*,
+                                          double*, const void*)>(be.pack)(&chunk, fields, cur_offsets, &depth, &face,
+                                                                          &cell_data, buf, &pk);
+            be.check_status("ext_pack_message_");
+        });
+    }
+
+    int cur_offsets[NUM_FIELDS] = {};
+
+    template <class Pack>
+    void exchange_with(const int* fields, int depth, Pack&& pack)
+    {
+        const int face_lo = cfg.dim == 2 ? 3 : 5, face_hi = face_lo + 1;  // CHUNK_BOTTOM/TOP, BACK/FRONT
+        const int per_depth = cfg.dim == 2 ? lx + 5 : (lx + 5) * (ly + 5);
+        int end = 0;
+        for (int f = 0; f < NUM_FIELDS; ++f) {
+            cur_offsets[f] = fields[f] ? end : (cfg.dim == 2 ? 0 : -1);
+            if (fields[f]) end += depth * per_depth;
+        }
+        if (end == 0) return;
+        snd.assign(end, 0.0);
+        rcv.assign(end, 0.0);
+        for (int face : {face_lo, face_hi}) {
+            const int nb = neighbours[face - 1];
+            if (nb < 0) continue;  // external
+            const int peer = comm->rank + (face == face_lo ? -1 : 1);
+            pack(face, snd.data(), 1);
+            comm->sendrecv(snd.data(), end, peer, rcv.data(), end, peer, comm->ctx);
+            pack(face, rcv.data(), 0);
+        }
+    }
     double time = 0.0, dt = 0.0;
     int step = 0;
     bool complete = false;
@@ -437,8 +509,9 @@ struct Runner {
 
     void update_halo(const int* fields, int depth)
     {
-        // update_halo (tealeaf_2d/update_halo.f90:27-66): tea_exchange is a no-op with one
-        // rank, leaving the reflective boundary update.
+        // update_halo (tealeaf_2d/update_halo.f90:27-66): tea_exchange (a no-op on one rank),
+        // then the reflective update of the external faces.
+        exchange(fields, depth);
         be.update_halo(&chunk, neighbours, fields, &depth);
     }
 
@@ -454,6 +527,14 @@ struct Runner {
         // tealeaf_2d/field_summary.f90:27-161.
         double vol = 0, mass = 0, ie = 0, temp = 0;
         be.field_summary(&chunk, &vol, &mass, &ie, &temp);
+        {
+            double v4[4] = {vol, mass, ie, temp};
+            allsum(v4, 4);
+            vol = v4[0];
+            mass = v4[1];
+            ie = v4[2];
+            temp = v4[3];
+        }
         log.line("");
         log.line(" Time %.16g", time);
         log.line("                       Volume            Mass         Density          Energy               U");
@@ -481,15 +562,35 @@ struct Runner {
         time = 0.0;
         step = 0;
         dt = cfg.dtinit;
-        int x = cfg.x_cells, y = cfg.y_cells, z = cfg.z_cells, rank = 0;
+        int x = cfg.x_cells, y = cfg.y_cells, z = cfg.z_cells, rank = split() ? comm->rank : 0;
+        // tea_decompose (tealeaf_2d/tea.f90:115-212) restricted to slabs of the slowest axis:
+        // first cell and count of this rank, the remainder going to the first ranks.
+        int first = 1;
+        if (split()) {
+            const int total = cfg.dim == 2 ? y : z, n = comm->size, r = comm->rank;
+            const int delta = total / n, mod = total % n;
+            first = r * delta + 1 + std::min(r, mod);
+            const int count = delta + (r < mod ? 1 : 0);
+            if (count < 1) fail("%d ranks for %d cells along the split axis", n, total);
+            (cfg.dim == 2 ? y : z) = count;
+            const int lo = cfg.dim == 2 ? 2 : 4;  // CHUNK_BOTTOM / CHUNK_BACK, 0-based
+            neighbours[lo] = r > 0 ? r : -1;          // the neighbour's chunk id (1-based)
+            neighbours[lo + 1] = r < n - 1 ? r + 2 : -1;
+        }
+        lx = x;
+        ly = y;
+        lz = z;
         if (cfg.dim == 2) reinterpret_cast<void (*)(int*, int*, int*)>(be.init)(&x, &y, &rank);
         else reinterpret_cast<void (*)(int*, int*, int*, int*)>(be.init)(&x, &y, &z, &rank);
         be.check_status("ext_init_");
-        // initialise_chunk.f90:33-36 (left = bottom = 1 on one rank).
+        // initialise_chunk.f90:33-36 (x/ymin + d * (left/bottom - 1)).
         double dx = (cfg.xmax - cfg.xmin) / (double)(float)cfg.x_cells;
         double dy = (cfg.ymax - cfg.ymin) / (double)(float)cfg.y_cells;
         double dz = (cfg.zmax - cfg.zmin) / (double)(float)cfg.z_cells;
-        double xmin = cfg.xmin + dx * 0.0, ymin = cfg.ymin + dy * 0.0, zmin = cfg.zmin + dz * 0.0;
+        const double off = (double)(first - 1);
+        double xmin = cfg.xmin + dx * 0.0;
+        double ymin = cfg.ymin + dy * (cfg.dim == 2 ? off : 0.0);
+        double zmin = cfg.zmin + dz * (cfg.dim == 3 ? off : 0.0);
         if (cfg.dim == 2)
             reinterpret_cast<void (*)(const int*, const double*, const double*, const double*, const double*)>(
                 be.initialise_chunk)(&chunk, &xmin, &ymin, &dx, &dy);
@@ -601,6 +702,7 @@ struct Runner {
         halo({FIELD_ENERGY1, FIELD_DENSITY}, 2);
         if (cg_like) {
             be.cg_init(&chunk, &coefficient, &precond, &dt, &rro);
+            allsum(&rro, 1);
             std::fill(fields, fields + NUM_FIELDS, 0);
             fields[FIELD_U - 1] = 1;
             fields[FIELD_P - 1] = 1;
@@ -615,7 +717,7 @@ struct Runner {
             // Additive relative target: sum r^2 < tl_eps_rel^2 * sum u0^2.
             double bb = 0.0;
             int zero = 0;
-            be.calc_2norm(&chunk, &bb, &zero);
+            be.calc_2norm(&chunk, &bb, &zero); allsum(&bb, 1);
             eps = cfg.tl_eps_rel * cfg.tl_eps_rel * bb;
         }
         be.check_status("solver init");
@@ -660,12 +762,12 @@ struct Runner {
                         // tea_leaf_cheby_first_step, :658-750.
                         double bb = 0.0;
                         int zero = 0, one = 1;
-                        be.calc_2norm(&chunk, &bb, &zero);
+                        be.calc_2norm(&chunk, &bb, &zero); allsum(&bb, 1);
                         be.cheby_init(&chunk, ch_alphas.data(), ch_betas.data(), &theta, &precond,
                                       &max_cheby_iters);
                         update_halo(fields, 1);
                         be.cheby_iterate(&chunk, &max_cheby_iters);
-                        be.calc_2norm(&chunk, &error, &one);
+                        be.calc_2norm(&chunk, &error, &one); allsum(&error, 1);
                         est_itc = tea::tea_cheby_est_itc(bb, error, cn);
                         log.line("    est itc");
                         log.line("%11d", est_itc);
@@ -675,7 +777,7 @@ struct Runner {
                         be.cheby_iterate(&chunk, &cheby_calc_steps);
                         if ((n >= est_itc) && (n % 10 == 0)) {
                             int one = 1;
-                            be.calc_2norm(&chunk, &error, &one);
+                            be.calc_2norm(&chunk, &error, &one); allsum(&error, 1);
                         }
                     }
                 } else {
@@ -686,9 +788,9 @@ struct Runner {
                         be.calc_residual(&chunk);
                         update_halo(fields, 1);
                     }
-                    be.cg_calc_w(&chunk, &pw);
+                    be.cg_calc_w(&chunk, &pw); allsum(&pw, 1);
                     alpha = rro / pw;
-                    be.cg_calc_ur(&chunk, &alpha, &rrn);
+                    be.cg_calc_ur(&chunk, &alpha, &rrn); allsum(&rrn, 1);
                     // tea_leaf_run_ppcg_inner_steps, :607-656.
                     be.ppcg_init_sd(&chunk);
                     int sd_fields[NUM_FIELDS] = {0, 0, 0, 0, 0, 1};
@@ -697,7 +799,7 @@ struct Runner {
                         be.ppcg_inner(&chunk, &k);
                     }
                     int one = 1;
-                    be.calc_2norm(&chunk, &rrn, &one);
+                    be.calc_2norm(&chunk, &rrn, &one); allsum(&rrn, 1);
                     beta = rrn / rro;
                     be.cg_calc_p(&chunk, &beta);
                     error = rrn;
@@ -706,22 +808,22 @@ struct Runner {
                 cheby_calc_steps = cheby_calc_steps + 1;
             } else if (cg_like) {
                 fields[FIELD_P - 1] = 1;
-                be.cg_calc_w(&chunk, &pw);
+                be.cg_calc_w(&chunk, &pw); allsum(&pw, 1);
                 alpha = rro / pw;
                 if (use_cheby || use_ppcg) cg_alphas[n] = alpha;
-                be.cg_calc_ur(&chunk, &alpha, &rrn);
+                be.cg_calc_ur(&chunk, &alpha, &rrn); allsum(&rrn, 1);
                 beta = rrn / rro;
                 if (use_cheby || use_ppcg) cg_betas[n] = beta;
                 be.cg_calc_p(&chunk, &beta);
                 error = rrn;
                 rro = rrn;
             } else {
-                be.jacobi_solve(&chunk, &error);
+                be.jacobi_solve(&chunk, &error); allsum(&error, 1);
                 if (n % 50 == 0) {
                     update_halo(fields, 1);
                     int one = 1;
                     be.calc_residual(&chunk);
-                    be.calc_2norm(&chunk, &error, &one);
+                    be.calc_2norm(&chunk, &error, &one); allsum(&error, 1);
                 }
             }
             update_halo(fields, 1);
@@ -731,7 +833,7 @@ struct Runner {
         if (cfg.tl_check_result) {
             int one = 1;
             be.calc_residual(&chunk);
-            be.calc_2norm(&chunk, &exact_error, &one);
+            be.calc_2norm(&chunk, &exact_error, &one); allsum(&exact_error, 1);
         }
         be.check_status("solve");
         log.line("Conduction error %14.7E", error);
@@ -828,6 +930,12 @@ struct Runner {
 extern "C" int tea_run_deck(const char* deck_text, const tea_run_options* options, tea_run_summary* summary,
                             tea_step_record* steps, int max_steps)
 {
+    return tea_run_deck_comm(deck_text, options, nullptr, summary, steps, max_steps);
+}
+
+extern "C" int tea_run_deck_comm(const char* deck_text, const tea_run_options* options, const tea_comm* comm,
+                                 tea_run_summary* summary, tea_step_record* steps, int max_steps)
+{
     g_last_error.clear();
     tea_run_summary local;
     if (!summary) summary = &local;
@@ -837,15 +945,21 @@ extern "C" int tea_run_deck(const char* deck_text, const tea_run_options* option
         if (!options || !options->backend) fail("no backend given");
         if (options->dim != 2 && options->dim != 3) fail("dim must be 2 or 3");
         r.opt = options;
+        r.comm = comm;
+        if (comm && (comm->size < 1 || comm->rank < 0 || comm->rank >= comm->size ||
+                     (comm->size > 1 && (!comm->allreduce_sum || !comm->sendrecv))))
+            fail("invalid communicator");
         r.cfg = parse_deck(deck_text ? deck_text : "", options->dim);
         if (options->use_fused_solve) r.cfg.use_fused_solve = true;
         if (options->precision > 0) r.cfg.precision = options->precision;
         if (r.cfg.precision != TEA_PRECISION_FP64 && !r.cfg.use_fused_solve)
             fail("tl_precision fp32 needs the whole-solve path (use_fused_solve)");
+        if (r.split() && r.cfg.use_fused_solve)
+            fail("the whole-solve path runs one chunk: several ranks use the per-call path");
         if (options->eps_override > 0.0) r.cfg.eps = options->eps_override;
         if (options->eps_rel_override > 0.0) r.cfg.tl_eps_rel = options->eps_rel_override;
-        r.log.echo = !options->quiet;
-        if (options->out_path) {
+        r.log.echo = !options->quiet && !(comm && comm->rank != 0);
+        if (options->out_path && !(comm && comm->rank != 0)) {
             r.log.file = fopen(options->out_path, "w");
             if (!r.log.file) fail("cannot open %s", options->out_path);
         }

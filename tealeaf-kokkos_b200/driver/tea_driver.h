@@ -77,6 +77,25 @@ typedef struct {
 int tea_run_deck(const char* deck_text, const tea_run_options* options,
                  tea_run_summary* summary, tea_step_record* steps, int max_steps);
 
+/* A run split into slabs over `size` ranks -- the reference's MPI layer (tea_decompose,
+ * tea_exchange, tea_allsum of tealeaf_2d/tea.f90, tealeaf_3d/tea.f90) with the transport
+ * supplied by the caller (e.g. torch.distributed over NCCL or gloo).  Rank r owns the
+ * r-th slab of the slowest axis (y in 2D, z in 3D; the remainder cells go to the first
+ * ranks, as in tea_decompose).  allreduce_sum sums n doubles over all ranks in place;
+ * sendrecv sends `send` to rank `to` and receives into `recv` from rank `from`, both
+ * completing before it returns.  Faces are exchanged with the backend's tea_pack_face_
+ * when it exports one (else ext_pack_message_, whose 2D bottom/top faces miss two inner
+ * columns, as the reference's do).  The per-call path only (use_fused_solve must be 0). */
+typedef struct {
+    int rank, size;
+    void (*allreduce_sum)(double* values, int n, void* ctx);
+    void (*sendrecv)(const double* send, int nsend, int to, double* recv, int nrecv, int from, void* ctx);
+    void* ctx;
+} tea_comm;
+
+int tea_run_deck_comm(const char* deck_text, const tea_run_options* options, const tea_comm* comm,
+                      tea_run_summary* summary, tea_step_record* steps, int max_steps);
+
 const char* tea_driver_last_error(void);
 
 #ifdef __cplusplus

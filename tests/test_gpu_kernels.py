@@ -184,10 +184,12 @@ def test_jacobi_and_methods(pair, coef):
     assert g == c
 
 
-def test_pack_message(pair):
+@pytest.mark.parametrize("packer", ["ext_pack_message_", "tea_pack_face_"])
+def test_pack_message(pair, packer):
     d = pair.dim
     faces = [1, 2, 3, 4] + ([5, 6] if d == 3 else [])
     nx, ny, nz = pair.gpu.X - 4, pair.gpu.Y - 4, max(pair.gpu.Z - 4, 1)
+    field_type = [I(1)] if d == 3 and packer == "ext_pack_message_" else []
     for face in faces:
         for depth in (1, 2):
             if face <= 2:
@@ -201,12 +203,12 @@ def test_pack_message(pair):
             bufs = {}
             for name, ch in (("gpu", pair.gpu), ("cpu", pair.cpu)):
                 buf = np.zeros(6 * n)
-                args = [fields, offsets, I(depth), I(face)] + ([I(1)] if d == 3 else [])
-                ch.call("ext_pack_message_", *args, buf.ctypes.data_as(ctypes.c_void_p), I(1))
+                args = [fields, offsets, I(depth), I(face)] + field_type
+                ch.call(packer, *args, buf.ctypes.data_as(ctypes.c_void_p), I(1))
                 bufs[name] = buf
             assert np.array_equal(bufs["gpu"], bufs["cpu"]), (face, depth)
             src = np.arange(6 * n, dtype=np.float64) * 0.5
             for ch in (pair.gpu, pair.cpu):
-                args = [fields, offsets, I(depth), I(face)] + ([I(1)] if d == 3 else [])
-                ch.call("ext_pack_message_", *args, src.ctypes.data_as(ctypes.c_void_p), I(0))
+                args = [fields, offsets, I(depth), I(face)] + field_type
+                ch.call(packer, *args, src.ctypes.data_as(ctypes.c_void_p), I(0))
             pair.check(f"unpack face {face} depth {depth}")
