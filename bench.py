@@ -511,8 +511,39 @@ def learned_arm(args, world):
     return r
 
 
+# Algorithmic FP64-equivalent words per cell of each fused kernel in 3D (FP32 words count
+# half): the 7-point sweeps read one more coefficient array than their 2D forms.
+WORDS_3D = {"ppcg_inner": 9, "cg_sweep_a": 9, "cheby_iterate": 8, "jacobi": 6, "cg_sweep_b": 3, "cheby_pair": 8,
+            "cg32_sweep_a": 4.5, "cg32_sweep_b": 1.5, "cheby32_pair": 4}
+
+
+def kernel_only_3d(args):
+    """--workload NAME --kernel K: one timestep of the 3D configuration through the driver
+    (the FP32-refined form for the FP32 kernels, so that their arrays exist), then K launched
+    1 + reps times back to back on the chunk's live fields."""
+    w = WORKLOADS_3D[args.workload]
+    fp32 = args.kernel.startswith(("cg32", "cheby32"))
+    spec = tea.DeckSpec(dim=3, cells=w["cells"], states=w["states"], seed=w["seed"], solver=w["solver"], end_step=1,
+                        dt=0.004, eps=1e-15, eps_rel=EPS_REL, max_iters=20000, presteps=30, inner_steps=10,
+                        check_result=False, summary_frequency=0)
+    tea.run_deck(tea.seeded_deck(spec), 3, fused=True, keep_chunk=True,
+                 precision=tea.PRECISION_FP32_REFINED if fp32 else tea.PRECISION_FP64)
+    lib = tea.cuda_library(3)
+    ms = ctypes.c_double(0.0)
+    lib.tea_kernel_timing_(ctypes.byref(ctypes.c_int(1)), ctypes.byref(ctypes.c_int(ALL_KERNEL_IDS[args.kernel])),
+                           ctypes.byref(ctypes.c_int(args.reps)), ctypes.byref(ms))
+    cells = w["cells"] ** 3
+    gbs = WORDS_3D[args.kernel] * 8 * cells / (ms.value / 1e3) / 1e9 if ms.value > 0 else None
+    print(json.dumps({"workload": args.workload, "kernel": args.kernel, "ms_per_launch": ms.value,
+                      "algorithmic_gbs": gbs}))
+    lib.ext_finalise_()
+
+
 def kernel_only(args):
     """Set up the 4096^2 workload and launch one fused kernel 1 + reps times (no solve)."""
+    if args.workload:
+        kernel_only_3d(args)
+        return
     lib = tea.cuda_library(2)
     ch = setup_chunk(lib, workload_spec())
     ms = ctypes.c_double(0.0)
@@ -539,7 +570,8 @@ def main():
     ap.add_argument("--no-refined", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS),
-                    help="only launch one fused kernel --reps times on the 4096^2 workload (for ncu captures)")
+                    help="only launch one fused kernel --reps times on the 4096^2 workload, or after one "
+                         "timestep of --workload (for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--workload", choices=sorted(WORKLOADS_3D),
                     help="time a 3D configuration instead (plain FP64 and FP32-refined, through the driver)")

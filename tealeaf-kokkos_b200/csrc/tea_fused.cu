@@ -62,6 +62,7 @@ struct Fused {
     RingLaunch ring[RING_OPS];  // grid and segment rows of k_ring2d per sweep (2D)
     RingLaunch pair;            // k_cheby2_ring2d<OpCheby> (2D); blocks 0: one iteration per launch
     RingLaunch pair32;          // k_cheby2_ring2d<OpCheby32> (2D)
+    RingLaunch ring3[RING_OPS]; // grid and z-segment planes of k_ring3d per sweep (3D)
     int stencil_mode = 0;  // 0: the faster kernel per sweep, 1: register pipeline only, 2: ring only
     Loop loops[LOOP_COUNT];
     bool use_graph = true;
@@ -116,16 +117,17 @@ int occupancy(K kernel, int threads)
     return n;
 }
 
-#if TEA_DIM == 2
 // Opt a ring kernel into its dynamic shared memory; blocks per SM it then reaches.
 template <class K>
-int smem_occupancy(K kernel, int bytes)
+int smem_occupancy(K kernel, int bytes, int threads = RWARPS * 32)
 {
     TEA_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, RWARPS * 32, bytes) != cudaSuccess || n < 1) n = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, bytes) != cudaSuccess || n < 1) n = 1;
     return n;
 }
+
+#if TEA_DIM == 2
 
 // One wave: every resident warp gets one segment of a strip `strip` columns wide, the
 // segment length chosen so that the strips' segments fill the resident warps.
@@ -141,6 +143,8 @@ RingLaunch ring_launch(const Geom& g, int sms, int occ, int strip, int max_block
     L.blocks = (int)std::max<long>(1, std::min<long>(blocks, max_blocks));
     return L;
 }
+
+#endif
 
 template <class Op>
 struct RingId;
@@ -181,11 +185,82 @@ struct RingId<OpCheby32> {
     static constexpr int value = 8;
 };
 
+#if TEA_DIM == 2
 template <class Op>
 void setup_ring(Fused* F, const Geom& g, int sms, int max_blocks)
 {
     const int occ = smem_occupancy(k_ring2d<Op>, (int)ring_smem_bytes<Op>());
     F->ring[RingId<Op>::value] = ring_launch(g, sms, occ, RingGeomOf<Op>::STRIP, max_blocks);
+}
+#else
+// Grid and z-segment length of k_ring3d: units (x-y tile, z segment) are dealt to the
+// resident blocks round-robin; the segment length minimises the waves times the planes a
+// unit streams (its own plus about two of pipeline start-up).
+RingLaunch ring3_launch(const Geom& g, int sms, int occ, int strip, int ty, int max_blocks)
+{
+    const long slots = std::max<long>(1, std::min<long>((long)sms * occ, max_blocks));
+    const long txy = (long)((g.nx + strip - 1) / strip) * ((g.ny + ty - 1) / ty);
+    RingLaunch L;
+    long best = -1;
+    for (int nseg = 1; nseg <= g.nz; ++nseg) {
+        const int len = (g.nz + nseg - 1) / nseg;
+        if (nseg > 1 && len == (g.nz + nseg - 2) / (nseg - 1)) continue;  // same length as before
+        const long units = txy * ((g.nz + len - 1) / len);
+        const long waves = (units + slots - 1) / slots;
+        const long cost = waves * (len + 2);
+        if (best < 0 || cost < best) {
+            best = cost;
+            L.rows = len;
+            L.blocks = (int)std::min(units, slots);
+        }
+    }
+    return L;
+}
+
+// Rows per tile (warps per block) and planes in flight of each sweep's k_ring3d, measured
+// on B200 at 512^3 over TY in {2, 4, 6, 8} and RP in {1, 2, 3, 4, 6}.
+template <class Op>
+struct Ring3Cfg {
+    static constexpr int TY = 4, RP = 2;
+};
+template <bool P>
+struct Ring3Cfg<OpPPCGInner<P>> {
+    static constexpr int TY = 4, RP = 3;
+};
+template <>
+struct Ring3Cfg<OpJacobi> {
+    static constexpr int TY = 8, RP = 2;
+};
+template <>
+struct Ring3Cfg<OpJacobiResidual> {
+    static constexpr int TY = 8, RP = 2;
+};
+template <>
+struct Ring3Cfg<OpOuterResid> {
+    static constexpr int TY = 8, RP = 2;
+};
+template <>
+struct Ring3Cfg<OpCheby32> {
+    static constexpr int TY = 8, RP = 1;
+};
+
+template <class Op>
+constexpr auto ring3_kernel()
+{
+    return k_ring3d<Op, Ring3Cfg<Op>::TY, Ring3Cfg<Op>::RP>;
+}
+template <class Op>
+constexpr size_t ring3_bytes()
+{
+    return ring3_smem_bytes<Op, Ring3Cfg<Op>::TY, Ring3Cfg<Op>::RP>();
+}
+
+template <class Op>
+void setup_ring3(Fused* F, const Geom& g, int sms, int max_blocks)
+{
+    constexpr int ty = Ring3Cfg<Op>::TY;
+    const int occ = smem_occupancy(ring3_kernel<Op>(), (int)ring3_bytes<Op>(), ty * 32);
+    F->ring3[RingId<Op>::value] = ring3_launch(g, sms, occ, RingGeomOf<Op>::STRIP, ty, max_blocks);
 }
 #endif
 
@@ -225,6 +300,12 @@ template <>
 struct RingPreferred<OpJacobiResidual> {
     static constexpr bool value = true;
 };
+#else
+// Every 3D sweep runs the plane ring by default.
+template <class Op>
+struct RingPreferred {
+    static constexpr bool value = true;
+};
 #endif
 
 // Launch the streaming stencil kernel of Op over the inner domain.
@@ -237,6 +318,14 @@ void stencil(const Fused* F, const FusedArgs& a, cudaStream_t s)
         FusedArgs ar = a;
         ar.seg_rows = L.rows;
         k_ring2d<Op><<<L.blocks, RWARPS * 32, ring_smem_bytes<Op>(), s>>>(ar);
+        return;
+    }
+#else
+    if (F->stencil_mode == 2 || (F->stencil_mode == 0 && RingPreferred<Op>::value)) {
+        const RingLaunch& L = F->ring3[RingId<Op>::value];
+        FusedArgs ar = a;
+        ar.seg_rows = L.rows;
+        ring3_kernel<Op>()<<<L.blocks, Ring3Cfg<Op>::TY * 32, ring3_bytes<Op>(), s>>>(ar);
         return;
     }
 #endif
@@ -309,11 +398,26 @@ Fused* ensure_fused(Chunk* c, int max_iters)
         F->stencil_blocks = (int)std::min<long>(a.ntiles, (long)sms * occ);
         F->stencil_blocks = std::min(F->stencil_blocks, c->red.max_blocks);
         F->stencil_blocks = std::max(F->stencil_blocks, 1);
-#if TEA_DIM == 2
         {
             // TEA_B200_STENCIL=pipe|ring forces one kernel family for every sweep (A/B timing).
             const char* kind = getenv("TEA_B200_STENCIL");
             F->stencil_mode = !kind ? 0 : (strcmp(kind, "pipe") == 0 ? 1 : (strcmp(kind, "ring") == 0 ? 2 : 0));
+        }
+#if TEA_DIM == 3
+        if (F->stencil_mode != 1) {
+            const int mb = c->red.max_blocks;
+            setup_ring3<OpSweepA>(F, g, sms, mb);
+            setup_ring3<OpCheby>(F, g, sms, mb);
+            setup_ring3<OpPPCGInner<false>>(F, g, sms, mb);
+            setup_ring3<OpPPCGInner<true>>(F, g, sms, mb);
+            setup_ring3<OpJacobi>(F, g, sms, mb);
+            setup_ring3<OpJacobiResidual>(F, g, sms, mb);
+            setup_ring3<OpSweepA32>(F, g, sms, mb);
+            setup_ring3<OpOuterResid>(F, g, sms, mb);
+            setup_ring3<OpCheby32>(F, g, sms, mb);
+        }
+#else
+        {
             if (F->stencil_mode != 1) {
                 const int mb = c->red.max_blocks;
                 setup_ring<OpSweepA>(F, g, sms, mb);

@@ -693,6 +693,234 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ring2d(FusedArgs a)
     ring2d_body(a, op, s_ring_raw);
 }
 
+#if TEA_DIM == 3
+// 3D streaming through a block-shared ring of planes filled by cp.async.  A block of TY
+// warps owns an x-y tile of 32 * VEC columns by TY rows (warp w: row y0 + w) and marches
+// through a segment of a.seg_rows planes.  A ring slot holds one plane of the tile: per
+// operand array the tile's rows plus the rows just below and above it, per interior input
+// the tile's rows, Kx (with the column right of the strip), Ky (with the row above the
+// tile) and Kz; operand rows also carry the two columns just outside the strip.  RP planes
+// are in flight beyond plane z+1 (RP + 2 slots).  The operand of planes z-1, z, z+1 at the
+// warp's own row stays in registers (z-neighbours), y-neighbours are staged from the slot's
+// neighbouring rows (the staging arithmetic is the same, so the values are identical),
+// x-neighbours come by shuffle.  One block barrier per plane: after it every warp's copies
+// of plane z+1 have landed and no warp still reads the slot that the next copy overwrites.
+// Work units (tile, z segment) are ordered segment-major, so tiles that are y-neighbours
+// run at the same time and their shared rows are read from L2.  TY and RP are chosen per
+// sweep: more resident blocks per SM (short tiles, few slots) hide the per-plane barrier
+// better than deeper prefetch does.
+
+// Row offsets of one ring slot.
+template <class Op, int TY>
+struct Ring3Rows {
+    static constexpr int RAW = 0;                               // Op::NR x (TY + 2)
+    static constexpr int IN = Op::NR * (TY + 2);                // Op::NI x TY
+    static constexpr int KX = IN + Op::NI * TY;                 // TY
+    static constexpr int KY = KX + TY;                          // TY + 1
+    static constexpr int KZ = KY + TY + 1;                      // TY
+    static constexpr int ROWS = KZ + TY;
+};
+
+template <class Op, int TY, int RP>
+constexpr size_t ring3_smem_bytes()
+{
+    return (size_t)(RP + 2) * Ring3Rows<Op, TY>::ROWS * RingGeomOf<Op>::WIDTH * sizeof(typename Op::T);
+}
+
+template <class Op, int TY3R, int RP3>
+__global__ void __launch_bounds__(TY3R * 32) k_ring3d(FusedArgs a)
+{
+    extern __shared__ __align__(16) unsigned char s_ring_raw[];
+    constexpr int RQ3 = RP3 + 2;
+    using T = typename Op::T;
+    using R = Ring3Rows<Op, TY3R>;
+    constexpr int NV = Op::NV;
+    constexpr int NR = Op::NR, NI = Op::NI;
+    constexpr int VEC = RingGeomOf<Op>::VEC, STRIP = RingGeomOf<Op>::STRIP, OFF = RingGeomOf<Op>::OFF;
+    constexpr int RWT = RingGeomOf<Op>::WIDTH;
+    constexpr int SLOT = R::ROWS * RWT;
+    Op op;
+    if (op.skip(a)) return;
+    op.begin(a);
+    const Geom& g = a.g;
+    T* ring = reinterpret_cast<T*>(s_ring_raw);
+    const T* src_raw[NR];
+    const T* src_in[NI > 0 ? NI : 1];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) src_raw[k] = op.raw_ptr(a, k);
+#pragma unroll
+    for (int k = 0; k < NI; ++k) src_in[k] = op.in_ptr(a, k);
+    const T* __restrict__ KX = op.coef_x(a);
+    const T* __restrict__ KY = op.coef_y(a);
+    const T* __restrict__ KZ = op.coef_z(a);
+    DDVec<NV> acc;
+    acc.zero();
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const int xlast = g.X - HALO_PAD - 1;
+    const int ylast = g.Y - HALO_PAD - 1;
+    const int zlast = g.Z - HALO_PAD - 1;
+    const int zlen = a.seg_rows;
+    const int per_x = (g.nx + STRIP - 1) / STRIP;
+    const int per_y = (g.ny + TY3R - 1) / TY3R;
+    const long txy = (long)per_x * per_y;
+    const long nunits = txy * ((g.nz + zlen - 1) / zlen);
+    const int cmax = (int)g.pitch - 2 * VEC + 2;  // as in the 2D ring: copies stay inside the row
+    for (long unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
+        const int zs = (int)(unit / txy);
+        const long rxy = unit % txy;
+        const int xs = (int)(rxy % per_x), ys = (int)(rxy / per_x);
+        const int c0 = HALO_PAD + STRIP * xs;
+        const int c = c0 + VEC * lane;
+        const int cc = min(c, cmax);
+        const int y0 = HALO_PAD + TY3R * ys;
+        const int j = y0 + w;
+        const bool row_active = j <= ylast;
+        const int z0 = HALO_PAD + zlen * zs;
+        const int z1 = min(z0 + zlen, zlast + 1);
+        const int left = refl(c0 - 1, g.X);
+        const int right_op = refl(min(c0 + STRIP, xlast + 1), g.X);
+        const int right_k = min(c0 + STRIP, xlast + 1);
+        // Operand rows are reflected into the inner domain, input rows clamped to the
+        // boundary face row (Ky there is the face coefficient).
+        const int rj = refl(min(j, ylast + 1), g.Y);
+        const int ij = min(j, ylast + 1);
+        const int r_below = refl(y0 - 1, g.Y);
+        const int r_above = refl(min(y0 + TY3R, ylast + 1), g.Y);
+        const int i_above = min(y0 + TY3R, ylast + 1);
+        auto slot = [&](int z) { return ring + (size_t)((z - z0 + 1) % RQ3) * SLOT; };
+        // Copy plane z of the tile: the operand rows for planes z0-1 .. z1, the rest for the
+        // segment's planes, Kz also for plane z1 (the upper face of plane z1 - 1).
+        auto issue = [&](int z) {
+            if (z <= z1) {
+                T* base = slot(z);
+                const bool seg = z >= z0 && z < z1;
+                const int zr = refl(min(z, zlast + 1), g.Z);
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    const T* sp = src_raw[k];
+                    if (!sp) continue;
+                    T* d = base + (R::RAW + k * (TY3R + 2)) * RWT;
+                    cp_async_vecn<VEC>(d + (w + 1) * RWT + OFF + VEC * lane, sp + fidx(g, cc, rj, zr));
+                    if (z >= z0) {
+                        if (lane == 0) ring_copy_one(d + (w + 1) * RWT + OFF - 1, sp + fidx(g, left, rj, zr));
+                        if (lane == 31)
+                            ring_copy_one(d + (w + 1) * RWT + OFF + STRIP, sp + fidx(g, right_op, rj, zr));
+                    }
+                    if (seg && w == 0) cp_async_vecn<VEC>(d + OFF + VEC * lane, sp + fidx(g, cc, r_below, zr));
+                    if (seg && w == TY3R - 1)
+                        cp_async_vecn<VEC>(d + (TY3R + 1) * RWT + OFF + VEC * lane, sp + fidx(g, cc, r_above, zr));
+                }
+                if (seg) {
+#pragma unroll
+                    for (int k = 0; k < NI; ++k) {
+                        if (!src_in[k]) continue;
+                        cp_async_vecn<VEC>(base + (R::IN + k * TY3R + w) * RWT + OFF + VEC * lane,
+                                           src_in[k] + fidx(g, cc, ij, z));
+                    }
+                    T* dx = base + (R::KX + w) * RWT;
+                    cp_async_vecn<VEC>(dx + OFF + VEC * lane, KX + fidx(g, cc, ij, z));
+                    if (lane == 31) ring_copy_one(dx + OFF + STRIP, KX + fidx(g, right_k, ij, z));
+                    cp_async_vecn<VEC>(base + (R::KY + w) * RWT + OFF + VEC * lane, KY + fidx(g, cc, ij, z));
+                    if (w == TY3R - 1)
+                        cp_async_vecn<VEC>(base + (R::KY + TY3R) * RWT + OFF + VEC * lane, KY + fidx(g, cc, i_above, z));
+                }
+                if (z >= z0) cp_async_vecn<VEC>(base + (R::KZ + w) * RWT + OFF + VEC * lane, KZ + fidx(g, cc, ij, z));
+            }
+            cp_async_commit();
+        };
+        // The operand at slot row `row` (0 = the row below the tile) for the lane's cells.
+        auto stage_row = [&](const T* base, int row, T* v) {
+            T x[NR][VEC], xq[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) ld_vecn<VEC>(base + (R::RAW + k * (TY3R + 2) + row) * RWT + OFF + VEC * lane, x[k]);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+#pragma unroll
+                for (int k = 0; k < NR; ++k) xq[k] = x[k][q];
+                v[q] = op.stage_raw(op.raw_from(xq));
+            }
+        };
+        // The operand at the strip's outside column of the warp's row (left for lane 0,
+        // right for lane 31).
+        auto stage_edge = [&](const T* base) {
+            T xe[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k)
+                xe[k] = base[(R::RAW + k * (TY3R + 2) + w + 1) * RWT + (lane == 0 ? OFF - 1 : OFF + STRIP)];
+            return op.stage_raw(op.raw_from(xe));
+        };
+        for (int z = z0 - 1; z <= z0 + RP3; ++z) issue(z);
+        cp_async_wait<RP3>();
+        __syncthreads();
+        T mv[VEC], cv[VEC];
+        stage_row(slot(z0 - 1), w + 1, mv);
+        stage_row(slot(z0), w + 1, cv);
+        T ce = stage_edge(slot(z0));
+        for (int z = z0; z < z1; ++z) {
+            cp_async_wait<RP3 - 1>();
+            __syncthreads();
+            issue(z + RP3 + 1);  // into the slot of plane z - 1, which no warp reads any more
+            const T* cur = slot(z);
+            const T* nxt = slot(z + 1);
+            T pv[VEC], ym[VEC], yp[VEC];
+            stage_row(nxt, w + 1, pv);
+            const T pe = stage_edge(nxt);
+            stage_row(cur, w, ym);
+            stage_row(cur, w + 2, yp);
+            const T up = __shfl_up_sync(0xffffffffu, cv[VEC - 1], 1);
+            const T dn = __shfl_down_sync(0xffffffffu, cv[0], 1);
+            T kx[VEC + 1], ky0[VEC], ky1[VEC], kz0[VEC], kz1[VEC];
+            ld_vecn<VEC>(cur + (R::KX + w) * RWT + OFF + VEC * lane, kx);
+            const T kxn = __shfl_down_sync(0xffffffffu, kx[0], 1);
+            kx[VEC] = lane == 31 ? cur[(R::KX + w) * RWT + OFF + STRIP] : kxn;
+            ld_vecn<VEC>(cur + (R::KY + w) * RWT + OFF + VEC * lane, ky0);
+            ld_vecn<VEC>(cur + (R::KY + w + 1) * RWT + OFF + VEC * lane, ky1);
+            ld_vecn<VEC>(cur + (R::KZ + w) * RWT + OFF + VEC * lane, kz0);
+            ld_vecn<VEC>(nxt + (R::KZ + w) * RWT + OFF + VEC * lane, kz1);
+            T rv[NR][VEC], iv[NI > 0 ? NI : 1][VEC];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) ld_vecn<VEC>(cur + (R::RAW + k * (TY3R + 2) + w + 1) * RWT + OFF + VEC * lane, rv[k]);
+#pragma unroll
+            for (int k = 0; k < NI; ++k) ld_vecn<VEC>(cur + (R::IN + k * TY3R + w) * RWT + OFF + VEC * lane, iv[k]);
+            if (row_active) {
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    const int cq = c + q;
+                    if (cq <= xlast) {
+                        T rq[NR], iq[NI > 0 ? NI : 1];
+#pragma unroll
+                        for (int k = 0; k < NR; ++k) rq[k] = rv[k][q];
+#pragma unroll
+                        for (int k = 0; k < NI; ++k) iq[k] = iv[k][q];
+                        NbT<T> nb;
+                        nb.c = cv[q];
+                        nb.xm = q == 0 ? (lane == 0 ? ce : up) : cv[q > 0 ? q - 1 : 0];
+                        nb.xp = cq == xlast ? cv[q]
+                                            : (q == VEC - 1 ? (lane == 31 ? ce : dn) : cv[q < VEC - 1 ? q + 1 : q]);
+                        nb.ym = ym[q];
+                        nb.yp = yp[q];
+                        nb.zm = mv[q];
+                        nb.zp = pv[q];
+                        op.interior_k(a, fidx(g, cq, j, z), nb, op.raw_from(rq), op.in_from(iq), kx[q], kx[q + 1],
+                                      ky0[q], ky1[q], kz0[q], kz1[q], acc);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                mv[q] = cv[q];
+                cv[q] = pv[q];
+            }
+            ce = pe;
+        }
+        cp_async_wait<0>();
+        __syncthreads();  // the next unit's copies reuse slots other warps may still read
+    }
+    if (Op::kReduce) grid_reduce_then<NV>(acc, a.red, [&](const double* v) { op.control(a, v); });
+}
+#endif
+
 #if TEA_DIM == 2
 #define TEA_STENCIL k_pipe2d
 #define TEA_STENCIL_BLOCK dim3(SBLOCK)
