@@ -108,6 +108,49 @@ __device__ __forceinline__ void warp_merge(DDVec<NV>& a)
     }
 }
 
+// Last block of a grid reduction: every thread merges a strided share of the block
+// partials (up to four loads in flight per thread), then a fixed-order warp merge and a
+// merge of the warps in order through `s` (nwarps x NV, shared).  The order depends only on
+// the grid and block sizes.  Called by every thread of the last block; the result is valid
+// in thread 0.
+template <int NV>
+__device__ __forceinline__ DDVec<NV> merge_partials(const RedScratch& rs, DD* s, int tid, int nthreads)
+{
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nthreads >> 5;
+    DDVec<NV> b;
+    b.zero();
+    const int nblk = (int)gridDim.x;
+    for (int blk0 = tid; blk0 < nblk; blk0 += 4 * nthreads) {
+        DD p[4][NV];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int blk = blk0 + u * nthreads;
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                p[u][k].hi = blk < nblk ? __ldcg(&rs.partials[(long)blk * MAX_RED + k].hi) : 0.0;
+                p[u][k].lo = blk < nblk ? __ldcg(&rs.partials[(long)blk * MAX_RED + k].lo) : 0.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) b.v[k] = dd_merge(b.v[k], p[u][k]);
+    }
+    warp_merge<NV>(b);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s[warp * NV + k] = b.v[k];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        b.zero();
+        for (int w = 0; w < nwarps; ++w)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) b.v[k] = dd_merge(b.v[k], s[w * NV + k]);
+    }
+    return b;
+}
+
 // Block-reduce `acc`, then the last block to arrive merges every block's partial in
 // block order and writes the rounded results to out[0..NV).  Deterministic for a given
 // grid size; no block waits on another.  Must be called by every thread of the block.
@@ -140,25 +183,13 @@ __device__ void grid_reduce(DDVec<NV> acc, const RedScratch& rs, double* out)
     }
     __syncthreads();
     if (!s_last) return;
-    // Last block: lanes of warp 0 merge strided partials, then a fixed-order warp merge.
+    // Last block: every thread merges a share of the partials (fixed order).
     __threadfence();
-    if (warp == 0) {
-        DDVec<NV> b;
-        b.zero();
-        for (int blk = lane; blk < (int)gridDim.x; blk += 32)
+    const DDVec<NV> b = merge_partials<NV>(rs, &s_warp[0][0], tid, nwarps * 32);
+    if (tid == 0) {
 #pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                DD p;
-                p.hi = __ldcg(&rs.partials[(long)blk * MAX_RED + k].hi);
-                p.lo = __ldcg(&rs.partials[(long)blk * MAX_RED + k].lo);
-                b.v[k] = dd_merge(b.v[k], p);
-            }
-        warp_merge<NV>(b);
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) out[k] = dd_value(b.v[k]);
-            *rs.counter = 0u;
-        }
+        for (int k = 0; k < NV; ++k) out[k] = dd_value(b.v[k]);
+        *rs.counter = 0u;
     }
 }
 
@@ -194,25 +225,13 @@ __device__ void grid_reduce_then(DDVec<NV> acc, const RedScratch& rs, F&& f)
     __syncthreads();
     if (!s_last2) return;
     __threadfence();
-    if (warp == 0) {
-        DDVec<NV> b;
-        b.zero();
-        for (int blk = lane; blk < (int)gridDim.x; blk += 32)
+    const DDVec<NV> b = merge_partials<NV>(rs, &s_warp2[0][0], tid, nwarps * 32);
+    if (tid == 0) {
+        double vals[NV];
 #pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                DD p;
-                p.hi = __ldcg(&rs.partials[(long)blk * MAX_RED + k].hi);
-                p.lo = __ldcg(&rs.partials[(long)blk * MAX_RED + k].lo);
-                b.v[k] = dd_merge(b.v[k], p);
-            }
-        warp_merge<NV>(b);
-        if (lane == 0) {
-            double vals[NV];
-#pragma unroll
-            for (int k = 0; k < NV; ++k) vals[k] = dd_value(b.v[k]);
-            *rs.counter = 0u;
-            f(vals);
-        }
+        for (int k = 0; k < NV; ++k) vals[k] = dd_value(b.v[k]);
+        *rs.counter = 0u;
+        f(vals);
     }
 }
 
