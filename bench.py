@@ -58,7 +58,7 @@ WORDS = {  # algorithmic FP64 words per interior cell of one launch
 }
 KERNEL_IDS = {"cg_sweep_a": 2, "cheby_pair": 6, "cg_sweep_b": 5}
 ALL_KERNEL_IDS = {"ppcg_inner": 1, "cg_sweep_a": 2, "cheby_iterate": 3, "jacobi": 4, "cg_sweep_b": 5,
-                  "cheby_pair": 6, "cg32_sweep_a": 7, "cg32_sweep_b": 8, "cheby32_pair": 9}
+                  "cheby_pair": 6, "cg32_sweep_a": 7, "cg32_sweep_b": 8, "cheby32_pair": 9, "ppcg_pair": 10}
 PROFILES = ROOT / "profiles"
 # Per-timestep iteration counts of this deck (CG iterations before the Chebyshev switch,
 # Chebyshev iterations after it) for simulation steps 1..20, measured with this build; the
@@ -358,6 +358,18 @@ def e2e_arm(args):
     }
 
 
+def per_call_arm():
+    """The drop-in path as the reference's own driver drives it: tea_run_deck without the
+    whole-solve entry point, so every iteration is the reference's per-call ext_* sequence
+    (ext_cg_calc_w_, ext_cg_calc_ur_, ext_cg_calc_p_, halo updates, ...) with each reduction
+    read back to the host.  One warm-up timestep, then timestep 2 timed by the driver."""
+    spec = workload_spec(steps=2)
+    summary, recs = tea.run_deck(tea.seeded_deck(spec), 2, fused=False, summary_every_step=True)
+    r = recs[1]
+    return {"value": r["wall_end"] - recs[0]["wall_end"], "unit": "s", "timestep": 2,
+            "iterations": r["iterations"], "temp": summary["temp"]}
+
+
 # ----------------------------------------------------------------------------- CPU (reference) arm
 
 def reference_costs(threads: int, n_cg=40, n_cheby=40):
@@ -514,7 +526,7 @@ def learned_arm(args, world):
 # Algorithmic FP64-equivalent words per cell of each fused kernel in 3D (FP32 words count
 # half): the 7-point sweeps read one more coefficient array than their 2D forms.
 WORDS_3D = {"ppcg_inner": 9, "cg_sweep_a": 9, "cheby_iterate": 8, "jacobi": 6, "cg_sweep_b": 3, "cheby_pair": 8,
-            "cg32_sweep_a": 4.5, "cg32_sweep_b": 1.5, "cheby32_pair": 4}
+            "cg32_sweep_a": 4.5, "cg32_sweep_b": 1.5, "cheby32_pair": 4, "ppcg_pair": 9}
 
 
 def kernel_only_3d(args):
@@ -569,6 +581,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-refined", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-per-call", action="store_true", help="skip timing the per-call ext_* path")
     ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS),
                     help="only launch one fused kernel --reps times on the 4096^2 workload, or after one "
                          "timestep of --workload (for ncu captures)")
@@ -593,6 +606,7 @@ def main():
     refined = None if args.no_refined else gpu_arm(args, world, precision=1, kernels=False)
     learned = None if args.no_refined or args.no_learned else learned_arm(args, world)
     e2e = None if args.no_e2e else e2e_arm(args)
+    per_call = None if args.no_per_call else per_call_arm()
     if rank != 0:
         dist_done(world)
         return
@@ -669,6 +683,10 @@ def main():
                          "loss_first": learned["loss_first"], "loss_last": learned["loss_last"]},
             "amortised_after_steps": (cost / saved) if saved and saved > 0 else None,
             "clocks": learned["clocks"]}
+    if per_call:
+        # The same deck through the per-call ext_* entry points (what an unchanged Fortran
+        # driver calls), timestep 2; the fused arm's timesteps are later ones.
+        line["per_call"] = per_call
     if g["bad_status"]:
         line["status_warnings"] = g["bad_status"]
     print(json.dumps(line))

@@ -63,6 +63,7 @@ struct Fused {
     RingLaunch pair;            // k_cheby2_ring2d<OpCheby> (2D); blocks 0: one iteration per launch
     RingLaunch pair32;          // k_cheby2_ring2d<OpCheby32> (2D)
     RingLaunch ring3[RING_OPS]; // grid and z-segment planes of k_ring3d per sweep (3D)
+    RingLaunch ppcg2;           // k_ppcg2_ring3d (3D); blocks 0: single inner steps only
     int stencil_mode = 0;  // 0: the faster kernel per sweep, 1: register pipeline only, 2: ring only
     Loop loops[LOOP_COUNT];
     bool use_graph = true;
@@ -255,6 +256,20 @@ constexpr size_t ring3_bytes()
     return ring3_smem_bytes<Op, Ring3Cfg<Op>::TY, Ring3Cfg<Op>::RP>();
 }
 
+// Rows per tile and planes in flight of the two-step PPCG pass (3D), measured on B200 at
+// 512^3 over (TY, RP) in {(4, 1), (6, 1), (6, 2), (8, 1), (8, 2), (10, 1)}.
+#ifndef TEA_PPCG2_TY
+#define TEA_PPCG2_TY 8
+#endif
+#ifndef TEA_PPCG2_RP
+#define TEA_PPCG2_RP 2
+#endif
+constexpr int PPCG2_TY = TEA_PPCG2_TY, PPCG2_RP = TEA_PPCG2_RP;
+
+// PPCG inner steps that run as two-step passes: an even number of pairs, none holding the
+// last step (which forms the 2-norm).
+inline int ppcg_pair_steps(int inner_steps) { return 4 * ((inner_steps - 1) / 4); }
+
 template <class Op>
 void setup_ring3(Fused* F, const Geom& g, int sms, int max_blocks)
 {
@@ -415,6 +430,9 @@ Fused* ensure_fused(Chunk* c, int max_iters)
             setup_ring3<OpSweepA32>(F, g, sms, mb);
             setup_ring3<OpOuterResid>(F, g, sms, mb);
             setup_ring3<OpCheby32>(F, g, sms, mb);
+            const int occ = smem_occupancy(k_ppcg2_ring3d<PPCG2_TY, PPCG2_RP>,
+                                           (int)ppcg2_smem_bytes<PPCG2_TY, PPCG2_RP>(), PPCG2_TY * 32);
+            F->ppcg2 = ring3_launch(g, sms, occ, 30 * RingGeom<double>::VEC, PPCG2_TY - 2, mb);
         }
 #else
         {
@@ -528,7 +546,19 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
     case LOOP_PPCG: {
         stencil<OpSweepA>(F, a, s);
         k_ppcg_sweep_b<<<F->point_blocks, pb, 0, s>>>(a, c->inner);
-        for (int k = 1; k <= inner_steps; ++k) {
+        int k0 = 1;
+#if TEA_DIM == 3
+        if (F->ppcg2.blocks > 0) {
+            for (; k0 <= ppcg_pair_steps(inner_steps); k0 += 2) {
+                FusedArgs ak = a;
+                ak.step = k0;
+                ak.seg_rows = F->ppcg2.rows;
+                k_ppcg2_ring3d<PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
+                                                    ppcg2_smem_bytes<PPCG2_TY, PPCG2_RP>(), s>>>(ak);
+            }
+        }
+#endif
+        for (int k = k0; k <= inner_steps; ++k) {
             FusedArgs ak = a;
             ak.step = k;
             if (k < inner_steps) stencil<OpPPCGInner<false>>(F, ak, s);
@@ -1060,7 +1090,8 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
 
 // Measurement hook: `reps` back-to-back launches of one fused kernel on the chunk's
 // stream between two CUDA events, on the chunk's current fields (their values change).
-// kernel: 1 PPCG inner step, 2 CG/PPCG sweep A, 3 Chebyshev iteration, 4 Jacobi sweep.
+// kernel: 1 PPCG inner step, 2 CG/PPCG sweep A, 3 Chebyshev iteration, 4 Jacobi sweep,
+// 10 two PPCG inner steps in one pass (3D).
 TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const int* reps, double* ms_per_launch)
 {
     *ms_per_launch = 0.0;
@@ -1118,6 +1149,16 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
                 k_cheby2_ring2d<OpCheby><<<F->pair.blocks, RWARPS * 32, cheby2_smem_bytes<OpCheby>(), c->stream>>>(ap);
             } else {
                 stencil<OpCheby>(F, a, c->stream);
+            }
+            break;
+#endif
+#if TEA_DIM == 3
+        case 10:
+            if (F->ppcg2.blocks > 0) {
+                FusedArgs ap = a;
+                ap.seg_rows = F->ppcg2.rows;
+                k_ppcg2_ring3d<PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
+                                                    ppcg2_smem_bytes<PPCG2_TY, PPCG2_RP>(), c->stream>>>(ap);
             }
             break;
 #endif

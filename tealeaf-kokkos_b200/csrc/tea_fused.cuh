@@ -512,6 +512,20 @@ __device__ __forceinline__ void ld_vec<float>(const float* p, float* out)
     out[3] = v.w;
 }
 
+// One 16-byte vector store (2 doubles or 4 floats, 16-byte aligned).
+template <class T>
+__device__ __forceinline__ void st_vec(T* p, const T* v);
+template <>
+__device__ __forceinline__ void st_vec<double>(double* p, const double* v)
+{
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+}
+template <>
+__device__ __forceinline__ void st_vec<float>(float* p, const float* v)
+{
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
 // VEC consecutive elements (8 or 16 bytes, aligned to their size).
 template <int VEC, class T>
 __device__ __forceinline__ void ld_vecn(const T* p, T* out)
@@ -1263,6 +1277,251 @@ struct OpPPCGInner {
     }
 };
 
+#if TEA_DIM == 3
+// Two PPCG inner steps k, k+1 in one pass over the 3D field (temporal blocking).  The
+// reference refreshes sd's halo by reflection before every inner step
+// (tealeaf_2d/tea_solve.f90:631-636) and the steps between the outer iteration's sweeps
+// have no reduction except on the last one, so two of them share one read of sd, r, u, mi
+// and K and one write of r, u and sd: about 9 words per cell for two steps instead of
+// eighteen.  Per cell the operations and their order are those of two single steps, so the
+// results are bit-identical.
+//
+// The plane ring of k_ring3d (a block of TY warps, a 64-column x TY-row tile marching
+// through a z segment) computes step k for every loaded cell one plane ahead of step k+1.
+// Step k+1 needs step k's sd at its neighbours: z-neighbours stay in registers, y-neighbours
+// go through a two-plane shared buffer, x-neighbours by shuffle.  So a tile writes only its
+// inner 60 columns (lanes 1..30) and rows (warps 1..TY-2): tiles overlap by four columns and
+// two rows, z segments by one plane of step k.  At the domain's faces step k's sd is
+// reflected as the reference's halo update reflects it (the cell's own value).  Tiles read
+// r at cells that a neighbouring tile writes, so r goes to the other of r and w (w is free
+// during the inner steps) and sd to the other sd buffer; pairs come in even numbers so that
+// both end where single steps leave them.  Pair m (steps 2m-1, 2m) reads sd[(m-1)&1] and r
+// (m odd) or w (m even).  A pair never holds the last inner step (the one that reduces).
+template <int TY, int RP>
+constexpr size_t ppcg2_smem_bytes()
+{
+    return (size_t)(RP + 3) * Ring3Rows<OpPPCGInner<false>, TY>::ROWS * RingGeom<double>::WIDTH * sizeof(double)
+        + (size_t)2 * TY * RingGeom<double>::STRIP * sizeof(double);
+}
+
+template <int TY, int RP>
+__global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    using R = Ring3Rows<OpPPCGInner<false>, TY>;
+    constexpr int VEC = RingGeom<double>::VEC, STRIP = RingGeom<double>::STRIP, OFF = RingGeom<double>::OFF;
+    constexpr int RWT = RingGeom<double>::WIDTH;
+    constexpr int OUT = 30 * VEC;
+    constexpr int RQ = RP + 3;
+    constexpr int SLOT = R::ROWS * RWT;
+    constexpr int IN_R = R::IN, IN_U = R::IN + TY, IN_MI = R::IN + 2 * TY;
+    double* ring = reinterpret_cast<double*>(s_raw);
+    double* s1 = ring + (size_t)RQ * SLOT;  // step k's sd: [plane parity][TY rows][STRIP]
+    const Geom& g = a.g;
+    const int k = a.step;
+    const int m = (k + 1) >> 1;
+    const double* __restrict__ sdk = a.sd[(m - 1) & 1];
+    double* __restrict__ sdo = a.sd[m & 1];
+    const double* __restrict__ rin = (m & 1) ? a.r : a.w;
+    double* __restrict__ rout = (m & 1) ? a.w : a.r;
+    double* __restrict__ U = a.u[0];
+    const bool precond = a.st->precond != 0;
+    const double* __restrict__ MI = precond ? a.mi : nullptr;
+    const double al1 = a.ch_alphas[k - 1], be1 = a.ch_betas[k - 1];
+    const double al2 = a.ch_alphas[k], be2 = a.ch_betas[k];
+    const double* __restrict__ KX = a.kx;
+    const double* __restrict__ KY = a.ky;
+    const double* __restrict__ KZ = a.kz;
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const int xlast = g.X - HALO_PAD - 1;
+    const int ylast = g.Y - HALO_PAD - 1;
+    const int zlast = g.Z - HALO_PAD - 1;
+    const int zlen = a.seg_rows;
+    const int per_x = (g.nx + OUT - 1) / OUT;
+    const int per_y = (g.ny + TY - 3) / (TY - 2);
+    const long txy = (long)per_x * per_y;
+    const long nunits = txy * ((g.nz + zlen - 1) / zlen);
+    const int cmax = (int)g.pitch - 2 * VEC + 2;
+    const bool lane_out = lane >= 1 && lane <= 30;
+    for (long unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
+        const int zs = (int)(unit / txy);
+        const long rxy = unit % txy;
+        const int xs = (int)(rxy % per_x), ys = (int)(rxy / per_x);
+        const int c = HALO_PAD - VEC + OUT * xs + VEC * lane;  // >= 0: lane 0 of strip 0 sits on the halo
+        const int cc = min(c, cmax);
+        const int y0 = HALO_PAD - 1 + (TY - 2) * ys;
+        const int j = y0 + w;
+        const bool row_in = j >= HALO_PAD && j <= ylast;              // step k computed
+        const bool row_out = w >= 1 && w <= TY - 2 && j <= ylast;     // step k+1 written
+        const int z0 = HALO_PAD + zlen * zs;
+        const int z1 = min(z0 + zlen, zlast + 1);
+        const int zf = z0 > HALO_PAD ? z0 - 1 : z0;  // first plane of step k
+        const int zl = min(z1, zlast);              // last plane of step k
+        const int rj = refl(min(j, ylast + 1), g.Y);
+        const int ij = min(max(j, HALO_PAD), ylast + 1);
+        const int r_below = refl(y0 - 1, g.Y);
+        const int r_above = refl(min(y0 + TY, ylast + 1), g.Y);
+        const int i_above = min(y0 + TY, ylast + 1);
+        auto slot = [&](int p) { return ring + (size_t)((p - zf + 1) % RQ) * SLOT; };
+        // Plane p of the tile: sd at the warps' rows for planes zf-1 .. zl+1, the rest for
+        // step k's planes, Kz also for plane zl+1.
+        auto issue = [&](int p) {
+            if (p <= zl + 1) {
+                double* base = slot(p);
+                const int pr = refl(min(p, zlast + 1), g.Z);
+                const int pi = min(p, zlast + 1);
+                const int col = OFF + VEC * lane;
+                cp_async_16(base + (R::RAW + w + 1) * RWT + col, sdk + fidx(g, cc, rj, pr));
+                if (p >= zf && p <= zl) {
+                    if (w == 0) cp_async_16(base + R::RAW * RWT + col, sdk + fidx(g, cc, r_below, pr));
+                    if (w == TY - 1) cp_async_16(base + (R::RAW + TY + 1) * RWT + col, sdk + fidx(g, cc, r_above, pr));
+                    cp_async_16(base + (IN_R + w) * RWT + col, rin + fidx(g, cc, ij, pi));
+                    if (row_out && lane_out) cp_async_16(base + (IN_U + w) * RWT + col, U + fidx(g, cc, ij, pi));
+                    if (MI) cp_async_16(base + (IN_MI + w) * RWT + col, MI + fidx(g, cc, ij, pi));
+                    cp_async_16(base + (R::KX + w) * RWT + col, KX + fidx(g, cc, ij, pi));
+                    cp_async_16(base + (R::KY + w) * RWT + col, KY + fidx(g, cc, ij, pi));
+                    if (w == TY - 1) cp_async_16(base + (R::KY + TY) * RWT + col, KY + fidx(g, cc, i_above, pi));
+                }
+                if (p >= zf) cp_async_16(base + (R::KZ + w) * RWT + col, KZ + fidx(g, cc, ij, pi));
+            }
+            cp_async_commit();
+        };
+        auto own = [&](const double* base, int row, double* v) { ld_vec(base + row * RWT + OFF + VEC * lane, v); };
+        // Step k at plane p from sd at planes p-1 (A), p (B), p+1 (C): r1, u1 and sd1 at the
+        // lane's cells; sd1 also into the shared plane buffer.
+        auto step1 = [&](int p, const double* A, const double* B, const double* C, double* r1, double* u1,
+                         double* t1) {
+            const double* cur = slot(p);
+            const double* nxt = slot(p + 1);
+            const double up = __shfl_up_sync(0xffffffffu, B[VEC - 1], 1);
+            const double dn = __shfl_down_sync(0xffffffffu, B[0], 1);
+            double kx[VEC + 1];
+            own(cur, R::KX + w, kx);
+            kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
+            if (p <= zl && row_in) {
+                double ky0[VEC], ky1[VEC], kz0[VEC], kz1[VEC], ym[VEC], yp[VEC], rr[VEC], uu[VEC], mi[VEC];
+                own(cur, R::KY + w, ky0);
+                own(cur, R::KY + w + 1, ky1);
+                own(cur, R::KZ + w, kz0);
+                own(nxt, R::KZ + w, kz1);
+                own(cur, R::RAW + w, ym);
+                own(cur, R::RAW + w + 2, yp);
+                own(cur, IN_R + w, rr);
+                own(cur, IN_U + w, uu);
+                if (precond) own(cur, IN_MI + w, mi);
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    Nb nb;
+                    nb.c = B[q];
+                    nb.xm = c + q == HALO_PAD ? B[q] : (q == 0 ? up : B[q > 0 ? q - 1 : 0]);
+                    nb.xp = c + q == xlast ? B[q] : (q == VEC - 1 ? dn : B[q < VEC - 1 ? q + 1 : q]);
+                    nb.ym = ym[q];
+                    nb.yp = yp[q];
+                    nb.zm = A[q];
+                    nb.zp = C[q];
+                    const double s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], kz0[q], kz1[q]);
+                    const double r = rr[q] - s;
+                    r1[q] = r;
+                    u1[q] = uu[q] + B[q];
+                    t1[q] = al1 * B[q] + be1 * (precond ? mi[q] * r : r);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) r1[q] = u1[q] = t1[q] = 0.0;
+            }
+            st_vec(s1 + ((size_t)(p & 1) * TY + w) * STRIP + VEC * lane, t1);
+        };
+        for (int p = zf - 1; p < zf - 1 + RQ; ++p) issue(p);
+        cp_async_wait<RQ - 3>();
+        __syncthreads();
+        double sA[VEC], sB[VEC], sC[VEC];  // sd at planes z, z+1, z+2 (the warp's row)
+        double tm[VEC], tc[VEC], tn[VEC];  // step k's sd at planes z-1, z, z+1
+        double r1c[VEC], u1c[VEC], r1n[VEC], u1n[VEC];
+        {
+            double sM[VEC];
+            own(slot(zf - 1), R::RAW + w + 1, sM);
+            own(slot(zf), R::RAW + w + 1, sA);
+            own(slot(zf + 1), R::RAW + w + 1, sB);
+            step1(zf, sM, sA, sB, r1c, u1c, tc);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) tm[q] = tc[q];
+        }
+        for (int z = zf; z < z1; ++z) {
+            cp_async_wait<RP - 1>();
+            __syncthreads();
+            issue(z + RP + 2);  // into the slot of plane z - 1, which no warp reads any more
+            own(slot(z + 2), R::RAW + w + 1, sC);
+            step1(z + 1, sA, sB, sC, r1n, u1n, tn);
+            if (z >= z0) {
+                // Step k+1 at plane z.
+                const double* cur = slot(z);
+                const double* nxt = slot(z + 1);
+                const double up = __shfl_up_sync(0xffffffffu, tc[VEC - 1], 1);
+                const double dn = __shfl_down_sync(0xffffffffu, tc[0], 1);
+                double kx[VEC + 1];
+                own(cur, R::KX + w, kx);
+                kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
+                if (row_out && lane_out) {
+                    double ky0[VEC], ky1[VEC], kz0[VEC], kz1[VEC], ym[VEC], yp[VEC], mi[VEC];
+                    own(cur, R::KY + w, ky0);
+                    own(cur, R::KY + w + 1, ky1);
+                    own(cur, R::KZ + w, kz0);
+                    own(nxt, R::KZ + w, kz1);
+                    if (precond) own(cur, IN_MI + w, mi);
+                    const double* sp = s1 + (size_t)(z & 1) * TY * STRIP + VEC * lane;
+                    if (j > HALO_PAD) ld_vec(sp + (w - 1) * STRIP, ym);
+                    if (j < ylast) ld_vec(sp + (w + 1) * STRIP, yp);
+                    double r2[VEC], u2[VEC], d2[VEC];
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) {
+                        Nb nb;
+                        nb.c = tc[q];
+                        nb.xm = c + q == HALO_PAD ? tc[q] : (q == 0 ? up : tc[q > 0 ? q - 1 : 0]);
+                        nb.xp = c + q == xlast ? tc[q] : (q == VEC - 1 ? dn : tc[q < VEC - 1 ? q + 1 : q]);
+                        nb.ym = j == HALO_PAD ? tc[q] : ym[q];
+                        nb.yp = j == ylast ? tc[q] : yp[q];
+                        nb.zm = z == HALO_PAD ? tc[q] : tm[q];
+                        nb.zp = z == zlast ? tc[q] : tn[q];
+                        const double s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], kz0[q], kz1[q]);
+                        const double r = r1c[q] - s;
+                        r2[q] = r;
+                        u2[q] = u1c[q] + tc[q];
+                        d2[q] = al2 * tc[q] + be2 * (precond ? mi[q] * r : r);
+                    }
+                    const long i = fidx(g, c, j, z);
+                    if (c + VEC - 1 <= xlast) {
+                        st_vec(rout + i, r2);
+                        st_vec(U + i, u2);
+                        st_vec(sdo + i, d2);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) {
+                            if (c + q <= xlast) {
+                                rout[i + q] = r2[q];
+                                U[i + q] = u2[q];
+                                sdo[i + q] = d2[q];
+                            }
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                sA[q] = sB[q];
+                sB[q] = sC[q];
+                tm[q] = tc[q];
+                tc[q] = tn[q];
+                r1c[q] = r1n[q];
+                u1c[q] = u1n[q];
+            }
+        }
+        cp_async_wait<0>();
+        __syncthreads();  // the next unit's copies reuse slots other warps may still read
+    }
+}
+#endif
+
 // ------------------------------------------------------------------ Chebyshev
 
 // ChebyIterate + ChebyCalcU (tealeaf_2d/ext_cheby_kernel.hpp:50-115) in one sweep: the
@@ -1428,19 +1687,6 @@ constexpr size_t cheby2_smem_bytes()
     return (size_t)RWARPS * C2_RQ * C2_NA * Pair2Geom<T>::STRIP * sizeof(T) > ring_smem_bytes<Op>()
         ? (size_t)RWARPS * C2_RQ * C2_NA * Pair2Geom<T>::STRIP * sizeof(T)
         : ring_smem_bytes<Op>();
-}
-
-template <class T>
-__device__ __forceinline__ void st_vec(T* p, const T* v);
-template <>
-__device__ __forceinline__ void st_vec<double>(double* p, const double* v)
-{
-    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
-}
-template <>
-__device__ __forceinline__ void st_vec<float>(float* p, const float* v)
-{
-    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
 // Op: OpCheby (FP64, the reference's iteration) or OpCheby32 (the FP32 inner solve).
