@@ -469,6 +469,7 @@ def reference_arm(args, rank, world):
 WORKLOADS_3D = {
     "3d256_cg": dict(cells=256, solver="cg", states=12, seed=256),
     "3d256_ppcg": dict(cells=256, solver="ppcg", states=12, seed=256),
+    "3d256_cheby": dict(cells=256, solver="chebyshev", states=12, seed=256),
     "3d512_ppcg": dict(cells=512, solver="ppcg", states=24, seed=512),
 }
 

@@ -68,9 +68,9 @@ int tea_chunk_stream_(const int* chunk, void** stream);
  * path on the chunk's stream, between two CUDA events, on the chunk's current fields
  * (which it modifies).  kernel: 1 PPCG inner step, 2 CG/PPCG sweep A, 3 Chebyshev
  * iteration, 4 Jacobi sweep, 5 CG sweep B, 6 two Chebyshev iterations in one pass (2D;
- * in 3D the single iteration), and the FP32 inner-solve kernels of the precision form:
- * 7 CG sweep A, 8 CG sweep B, 9 two Chebyshev iterations (3D: one); 10 two PPCG inner
- * steps in one pass (3D; a no-op in 2D).  Writes the mean milliseconds per launch. */
+ * in 3D one iteration), and the FP32 inner-solve kernels of the precision form: 7 CG
+ * sweep A, 8 CG sweep B, 9 two Chebyshev iterations (3D: one); 10 two PPCG inner steps
+ * in one pass (3D; a no-op in 2D).  Writes the mean milliseconds per launch. */
 void tea_kernel_timing_(const int* chunk, const int* kernel, const int* reps, double* ms_per_launch);
 
 /* Host<->device bytes the library has moved for the chunk so far: state tables,

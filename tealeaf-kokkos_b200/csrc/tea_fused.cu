@@ -1140,6 +1140,7 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
             break;
 #else
         case 9: stencil<OpCheby32>(F, a, c->stream); break;
+        case 6: stencil<OpCheby>(F, a, c->stream); break;
 #endif
 #if TEA_DIM == 2
         case 6:
