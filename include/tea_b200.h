@@ -70,7 +70,7 @@ int tea_chunk_stream_(const int* chunk, void** stream);
  * iteration, 4 Jacobi sweep, 5 CG sweep B, 6 two Chebyshev iterations in one pass (2D;
  * in 3D one iteration), and the FP32 inner-solve kernels of the precision form: 7 CG
  * sweep A, 8 CG sweep B, 9 two Chebyshev iterations (3D: one); 10 two PPCG inner steps
- * in one pass (3D; a no-op in 2D).  Writes the mean milliseconds per launch. */
+ * in one pass.  Writes the mean milliseconds per launch. */
 void tea_kernel_timing_(const int* chunk, const int* kernel, const int* reps, double* ms_per_launch);
 
 /* Host<->device bytes the library has moved for the chunk so far: state tables,

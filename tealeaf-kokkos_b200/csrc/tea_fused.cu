@@ -63,7 +63,7 @@ struct Fused {
     RingLaunch pair;            // k_cheby2_ring2d<OpCheby> (2D); blocks 0: one iteration per launch
     RingLaunch pair32;          // k_cheby2_ring2d<OpCheby32> (2D)
     RingLaunch ring3[RING_OPS]; // grid and z-segment planes of k_ring3d per sweep (3D)
-    RingLaunch ppcg2;           // k_ppcg2_ring3d (3D); blocks 0: single inner steps only
+    RingLaunch ppcg2;           // k_ppcg2_ring3d (3D) / k_ppcg2_ring2d (2D); blocks 0: single steps only
     int stencil_mode = 0;  // 0: the faster kernel per sweep, 1: register pipeline only, 2: ring only
     Loop loops[LOOP_COUNT];
     bool use_graph = true;
@@ -117,6 +117,14 @@ int occupancy(K kernel, int threads)
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess || n < 1) n = 1;
     return n;
 }
+
+#if TEA_DIM == 2
+constexpr size_t ppcg2_2d_smem_bytes = (size_t)RWARPS * C2_RQ * C2_NA * Pair2Geom<double>::STRIP * sizeof(double);
+#endif
+
+// PPCG inner steps that run as two-step passes: an even number of pairs, none holding the
+// last step (which forms the 2-norm).
+inline int ppcg_pair_steps(int inner_steps) { return 4 * ((inner_steps - 1) / 4); }
 
 // Opt a ring kernel into its dynamic shared memory; blocks per SM it then reaches.
 template <class K>
@@ -265,10 +273,6 @@ constexpr size_t ring3_bytes()
 #define TEA_PPCG2_RP 2
 #endif
 constexpr int PPCG2_TY = TEA_PPCG2_TY, PPCG2_RP = TEA_PPCG2_RP;
-
-// PPCG inner steps that run as two-step passes: an even number of pairs, none holding the
-// last step (which forms the 2-norm).
-inline int ppcg_pair_steps(int inner_steps) { return 4 * ((inner_steps - 1) / 4); }
 
 template <class Op>
 void setup_ring3(Fused* F, const Geom& g, int sms, int max_blocks)
@@ -452,6 +456,8 @@ Fused* ensure_fused(Chunk* c, int max_iters)
                 const int occ3 =
                     smem_occupancy(k_cheby2_ring2d<OpCheby32>, (int)cheby2_smem_bytes<OpCheby32>());
                 F->pair32 = ring_launch(g, sms, occ3, Pair2Geom<float>::OUT, mb);
+                const int occ4 = smem_occupancy(k_ppcg2_ring2d, (int)ppcg2_2d_smem_bytes);
+                F->ppcg2 = ring_launch(g, sms, occ4, Pair2Geom<double>::OUT, mb);
             }
         }
 #endif
@@ -547,7 +553,16 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         stencil<OpSweepA>(F, a, s);
         k_ppcg_sweep_b<<<F->point_blocks, pb, 0, s>>>(a, c->inner);
         int k0 = 1;
-#if TEA_DIM == 3
+#if TEA_DIM == 2
+        if (F->ppcg2.blocks > 0) {
+            for (; k0 <= ppcg_pair_steps(inner_steps); k0 += 2) {
+                FusedArgs ak = a;
+                ak.step = k0;
+                ak.seg_rows = F->ppcg2.rows;
+                k_ppcg2_ring2d<<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, s>>>(ak);
+            }
+        }
+#else
         if (F->ppcg2.blocks > 0) {
             for (; k0 <= ppcg_pair_steps(inner_steps); k0 += 2) {
                 FusedArgs ak = a;
@@ -1153,7 +1168,15 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
             }
             break;
 #endif
-#if TEA_DIM == 3
+#if TEA_DIM == 2
+        case 10:
+            if (F->ppcg2.blocks > 0) {
+                FusedArgs ap = a;
+                ap.seg_rows = F->ppcg2.rows;
+                k_ppcg2_ring2d<<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, c->stream>>>(ap);
+            }
+            break;
+#else
         case 10:
             if (F->ppcg2.blocks > 0) {
                 FusedArgs ap = a;

@@ -1866,6 +1866,186 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
     }
     grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.pair_control(a, v, check2); });
 }
+
+// Two PPCG inner steps in one pass over the 2D field (temporal blocking), the 2D form of
+// k_ppcg2_ring3d on the strips and row rings of k_cheby2_ring2d: step k is computed for
+// every loaded cell one row ahead of step k+1, the strips' outer lanes and a segment's
+// first row only feed their neighbours, and at the domain's edges step k's sd is
+// reflected as the reference's halo update reflects it.  Per cell the operations and their
+// order are those of two single steps, so results are bit-identical.  r moves between r
+// and w and sd between its two buffers, as in 3D (pair m reads sd[(m-1)&1] and r for odd m,
+// w for even m); u is read and written only at the cells a warp writes.
+enum { P2_SD = 0, P2_R = 1, P2_U = 2, P2_MI = 3, P2_KX = 4, P2_KY = 5 };
+
+__global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
+{
+    using T = double;
+    constexpr int VEC = Pair2Geom<T>::VEC, STRIP = Pair2Geom<T>::STRIP, OUT = Pair2Geom<T>::OUT;
+    extern __shared__ __align__(16) unsigned char s_ring_raw[];
+    const int k = a.step;
+    const int m = (k + 1) >> 1;
+    const double* __restrict__ sdk = a.sd[(m - 1) & 1];
+    double* __restrict__ sdo = a.sd[m & 1];
+    const double* __restrict__ rin = (m & 1) ? a.r : a.w;
+    double* __restrict__ rout = (m & 1) ? a.w : a.r;
+    double* __restrict__ U = a.u[0];
+    const bool precond = a.st->precond != 0;
+    const double* __restrict__ mi = precond ? a.mi : nullptr;
+    const double al1 = a.ch_alphas[k - 1], be1 = a.ch_betas[k - 1];
+    const double al2 = a.ch_alphas[k], be2 = a.ch_betas[k];
+    const Geom& g = a.g;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * C2_RQ * C2_NA * STRIP;
+    const T* src[C2_NA] = {sdk, rin, U, mi, a.kx, a.ky};
+    const int xlast = g.X - HALO_PAD - 1;
+    const int ylast = g.Y - HALO_PAD - 1;
+    const int per_x = (g.nx + OUT - 1) / OUT;
+    const int per_y = (g.ny + a.seg_rows - 1) / a.seg_rows;
+    const long nseg = (long)per_x * per_y;
+    const long gw = (long)blockIdx.x * RWARPS + warp, nw = (long)gridDim.x * RWARPS;
+    const int cmax = (int)g.pitch - 2 * VEC + 2;
+    const bool out_lane = lane >= 1 && lane <= 30;
+    for (long sgi = gw; sgi < nseg; sgi += nw) {
+        const int xs = (int)(sgi % per_x), ys = (int)(sgi / per_x);
+        const int c = OUT * xs + VEC * lane - (VEC - 2);  // the lane's first column (>= 0)
+        const int cc = min(c, cmax);
+        const int j0 = HALO_PAD + a.seg_rows * ys;
+        const int j1 = min(j0 + a.seg_rows, ylast + 1);
+        const int a0 = j0 == HALO_PAD ? HALO_PAD : j0 - 1;  // first row of step k
+        const int rlast = min(j1 + 1, ylast + 1);             // last ring row
+        auto slot = [&](int r) { return ring + (size_t)((r - a0 + 1) % C2_RQ) * C2_NA * STRIP; };
+        auto issue = [&](int r) {
+            if (r <= rlast) {
+                T* base = slot(r);
+                const int srow = refl(r, g.Y);
+                const int irow = min(max(r, HALO_PAD), ylast + 1);
+#pragma unroll
+                for (int q = 0; q < C2_NA; ++q) {
+                    if (!src[q]) continue;
+                    if (q == P2_U && !(out_lane && r >= j0 && r < j1)) continue;  // u: written cells only
+                    cp_async_16(base + q * STRIP + VEC * lane, src[q] + fidx(g, cc, q == P2_SD ? srow : irow, 0));
+                }
+            }
+            cp_async_commit();
+        };
+        for (int r = a0 - 1; r <= a0 + C2_RP + 1; ++r) issue(r);
+        cp_async_wait<C2_RP + 1>();
+        __syncwarp();
+        // sd at rows t-1 (um) and t (uc); step k's sd at rows t-2 (vm) and t-1 (vc), its r
+        // and u at row t-1 (r1c, u1c).
+        T um[VEC], uc[VEC], vm[VEC], vc[VEC], r1c[VEC], u1c[VEC];
+        ld_vec(slot(a0 - 1) + P2_SD * STRIP + VEC * lane, um);
+        ld_vec(slot(a0) + P2_SD * STRIP + VEC * lane, uc);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) vm[q] = vc[q] = r1c[q] = u1c[q] = 0.0;
+        for (int t = a0; t <= j1; ++t) {
+            cp_async_wait<C2_RP>();
+            __syncwarp();
+            const T* rp = slot(t - 1);
+            const T* rc = slot(t);
+            const T* rn = slot(t + 1);
+            T un[VEC];
+            ld_vec(rn + P2_SD * STRIP + VEC * lane, un);
+            // Step k at row t.
+            T v[VEC], r1v[VEC], u1v[VEC];
+            if (t <= ylast) {
+                T kx[VEC + 1], ky0[VEC], ky1[VEC], rr[VEC], uu[VEC], m0[VEC];
+                ld_vec(rc + P2_KX * STRIP + VEC * lane, kx);
+                kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
+                ld_vec(rc + P2_KY * STRIP + VEC * lane, ky0);
+                ld_vec(rn + P2_KY * STRIP + VEC * lane, ky1);
+                ld_vec(rc + P2_R * STRIP + VEC * lane, rr);
+                ld_vec(rc + P2_U * STRIP + VEC * lane, uu);
+                if (precond) ld_vec(rc + P2_MI * STRIP + VEC * lane, m0);
+                const T up = __shfl_up_sync(0xffffffffu, uc[VEC - 1], 1);
+                const T dn = __shfl_down_sync(0xffffffffu, uc[0], 1);
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    Nb nb;
+                    nb.zm = nb.zp = 0.0;
+                    nb.c = uc[q];
+                    nb.xm = c + q == HALO_PAD ? uc[q] : (q == 0 ? up : uc[q > 0 ? q - 1 : 0]);
+                    nb.xp = c + q == xlast ? uc[q] : (q == VEC - 1 ? dn : uc[q < VEC - 1 ? q + 1 : q]);
+                    nb.ym = um[q];
+                    nb.yp = un[q];
+                    const T s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], 0.0, 0.0);
+                    const T r = rr[q] - s;
+                    r1v[q] = r;
+                    u1v[q] = uu[q] + uc[q];
+                    v[q] = al1 * uc[q] + be1 * (precond ? m0[q] * r : r);
+                }
+            } else {
+                // Row ylast + 1 is the halo: the reflection of row ylast.
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    v[q] = vc[q];
+                    r1v[q] = u1v[q] = 0.0;
+                }
+            }
+            if (t == HALO_PAD) {
+                // Row 1 is the halo: the reflection of row 2.
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) vc[q] = v[q];
+            }
+            // Step k+1 at row s = t - 1.
+            const int srow = t - 1;
+            if (srow >= j0) {
+                T kx[VEC + 1], ky0[VEC], ky1[VEC], m0[VEC], r2[VEC], u2[VEC], d2[VEC];
+                ld_vec(rp + P2_KX * STRIP + VEC * lane, kx);
+                kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
+                ld_vec(rp + P2_KY * STRIP + VEC * lane, ky0);
+                ld_vec(rc + P2_KY * STRIP + VEC * lane, ky1);
+                if (precond) ld_vec(rp + P2_MI * STRIP + VEC * lane, m0);
+                const T up = __shfl_up_sync(0xffffffffu, vc[VEC - 1], 1);
+                const T dn = __shfl_down_sync(0xffffffffu, vc[0], 1);
+                const long i = fidx(g, c, srow, 0);
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    Nb nb;
+                    nb.zm = nb.zp = 0.0;
+                    nb.c = vc[q];
+                    nb.xm = c + q == HALO_PAD ? vc[q] : (q == 0 ? up : vc[q > 0 ? q - 1 : 0]);
+                    nb.xp = c + q == xlast ? vc[q] : (q == VEC - 1 ? dn : vc[q < VEC - 1 ? q + 1 : q]);
+                    nb.ym = vm[q];
+                    nb.yp = v[q];
+                    const T s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], 0.0, 0.0);
+                    const T r = r1c[q] - s;
+                    r2[q] = r;
+                    u2[q] = u1c[q] + vc[q];
+                    d2[q] = al2 * vc[q] + be2 * (precond ? m0[q] * r : r);
+                }
+                if (out_lane && c + VEC - 1 <= xlast) {
+                    st_vec(rout + i, r2);
+                    st_vec(U + i, u2);
+                    st_vec(sdo + i, d2);
+                } else if (out_lane) {
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) {
+                        if (c + q <= xlast) {
+                            rout[i + q] = r2[q];
+                            U[i + q] = u2[q];
+                            sdo[i + q] = d2[q];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                vm[q] = vc[q];
+                vc[q] = v[q];
+                r1c[q] = r1v[q];
+                u1c[q] = u1v[q];
+                um[q] = uc[q];
+                uc[q] = un[q];
+            }
+            __syncwarp();
+            issue(t + C2_RP + 2);  // into the slot of row t - 1, which no lane reads any more
+        }
+        cp_async_wait<0>();
+        __syncwarp();
+    }
+}
 #endif
 
 // ------------------------------------------------------------------ Jacobi
