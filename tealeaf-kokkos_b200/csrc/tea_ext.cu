@@ -497,6 +497,15 @@ TEA_EXPORT void ext_update_halo_kernel_(const int* chunk, const int* chunkNeighb
 #define LAUNCH(kernel, box, ...)                                                                   \
     kernel<<<launch_blocks(c, (box).ntiles), dim3(TILE_X, TILE_Y), 0, c->stream>>>(__VA_ARGS__)
 
+// Pointwise kernels (walk_cell_pairs): one warp per 64-cell row segment, 256-thread blocks,
+// at most as many blocks as the reduction scratch holds partials for.
+static int pair_blocks(const Chunk* c)
+{
+    const long nseg = (long)((c->g.nx + 63) / 64) * c->g.ny * c->g.nz;
+    return (int)std::max<long>(1, std::min<long>((nseg + 7) / 8, c->red.max_blocks));
+}
+#define LAUNCH_PAIRS(kernel, ...) kernel<<<pair_blocks(c), BLOCK, 0, c->stream>>>(__VA_ARGS__)
+
 TEA_EXPORT void ext_set_field_kernel_(const int* chunk)
 {
     Chunk* c = get_chunk(chunk);
@@ -509,7 +518,7 @@ TEA_EXPORT void ext_solver_copy_u_(const int* chunk)
 {
     Chunk* c = get_chunk(chunk);
     if (!c) return;
-    LAUNCH(k_copy_u, c->inner, c->g, c->inner, c->f);
+    LAUNCH_PAIRS(k_copy_u, c->g, c->f);
     sync(c);
 }
 
@@ -517,7 +526,7 @@ TEA_EXPORT void ext_calculate_residual_(const int* chunk)
 {
     Chunk* c = get_chunk(chunk);
     if (!c) return;
-    LAUNCH(k_residual, c->inner, c->g, c->inner, c->f);
+    LAUNCH_PAIRS(k_residual, c->g, c->f);
     sync(c);
 }
 
@@ -526,7 +535,7 @@ TEA_EXPORT void ext_calculate_2norm_(const int* chunk, double* norm, const void*
     Chunk* c = get_chunk(chunk);
     if (!c) return;
     const double* b = *(const unsigned char*)normArray ? c->f.r : c->f.u0;
-    LAUNCH(k_2norm, c->inner, c->g, c->inner, b, c->red, c->d_out);
+    LAUNCH_PAIRS(k_2norm, c->g, b, c->red, c->d_out);
     *norm = result(c, 0);
 }
 
@@ -534,7 +543,7 @@ TEA_EXPORT void ext_solver_finalise_(const int* chunk)
 {
     Chunk* c = get_chunk(chunk);
     if (!c) return;
-    LAUNCH(k_finalise, c->inner, c->g, c->inner, c->f);
+    LAUNCH_PAIRS(k_finalise, c->g, c->f);
     sync(c);
 }
 
@@ -593,7 +602,7 @@ TEA_EXPORT void ext_cg_calc_w_(const int* chunk, double* pw)
 {
     Chunk* c = get_chunk(chunk);
     if (!c) return;
-    LAUNCH(k_cg_calc_w, c->inner, c->g, c->inner, c->f, c->red, c->d_out);
+    LAUNCH_PAIRS(k_cg_calc_w, c->g, c->f, c->red, c->d_out);
     *pw = result(c, 0);
 }
 
@@ -601,7 +610,7 @@ TEA_EXPORT void ext_cg_calc_ur_(const int* chunk, const double* alpha, double* r
 {
     Chunk* c = get_chunk(chunk);
     if (!c) return;
-    LAUNCH(k_cg_calc_ur, c->inner, c->g, c->inner, c->f, *alpha, c->preconditioner, c->red, c->d_out);
+    LAUNCH_PAIRS(k_cg_calc_ur, c->g, c->f, *alpha, c->preconditioner, c->red, c->d_out);
     *rrn = result(c, 0);
 }
 
@@ -609,7 +618,7 @@ TEA_EXPORT void ext_cg_calc_p_(const int* chunk, const double* beta)
 {
     Chunk* c = get_chunk(chunk);
     if (!c) return;
-    LAUNCH(k_cg_calc_p, c->inner, c->g, c->inner, c->f, *beta, c->preconditioner);
+    LAUNCH_PAIRS(k_cg_calc_p, c->g, c->f, *beta, c->preconditioner);
     sync(c);
 }
 
@@ -623,7 +632,7 @@ TEA_EXPORT void ext_cheby_solver_init_(const int* chunk, double* alphas, double*
     c->preconditioner = *preconditioner != 0;
     store_coefs(c, alphas, betas, *maxChebyIters);
     LAUNCH(k_cheby_init, c->inner, c->g, c->inner, c->f, *theta, c->preconditioner);
-    LAUNCH(k_cheby_calc_u, c->inner, c->g, c->inner, c->f);
+    LAUNCH_PAIRS(k_cheby_calc_u, c->g, c->f);
     sync(c);
 }
 
@@ -637,9 +646,9 @@ TEA_EXPORT void ext_cheby_solver_iterate_(const int* chunk, const int* chebyCalc
                    c->h_alphas.size());
         return;
     }
-    LAUNCH(k_cheby_iterate, c->inner, c->g, c->inner, c->f, c->h_alphas[step], c->h_betas[step],
+    LAUNCH_PAIRS(k_cheby_iterate, c->g, c->f, c->h_alphas[step], c->h_betas[step],
            c->preconditioner);
-    LAUNCH(k_cheby_calc_u, c->inner, c->g, c->inner, c->f);
+    LAUNCH_PAIRS(k_cheby_calc_u, c->g, c->f);
     sync(c);
 }
 
@@ -658,7 +667,7 @@ TEA_EXPORT void ext_ppcg_init_sd_(const int* chunk)
 {
     Chunk* c = get_chunk(chunk);
     if (!c) return;
-    LAUNCH(k_ppcg_init_sd, c->inner, c->g, c->inner, c->f, c->theta, c->preconditioner);
+    LAUNCH_PAIRS(k_ppcg_init_sd, c->g, c->f, c->theta, c->preconditioner);
     sync(c);
 }
 
@@ -671,8 +680,8 @@ TEA_EXPORT void ext_ppcg_inner_(const int* chunk, int* currentStep)
         set_status(2, "ext_ppcg_inner_: step %d outside the %zu stored coefficients", step + 1, c->h_alphas.size());
         return;
     }
-    LAUNCH(k_ppcg_calc_u, c->inner, c->g, c->inner, c->f);
-    LAUNCH(k_ppcg_calc_sd, c->inner, c->g, c->inner, c->f, c->h_alphas[step], c->h_betas[step], c->preconditioner);
+    LAUNCH_PAIRS(k_ppcg_calc_u, c->g, c->f);
+    LAUNCH_PAIRS(k_ppcg_calc_sd, c->g, c->f, c->h_alphas[step], c->h_betas[step], c->preconditioner);
     sync(c);
 }
 

@@ -47,6 +47,98 @@ __device__ __forceinline__ double diag(const double* __restrict__ kx, const doub
 #endif
 }
 
+// Pointwise kernels walk the inner domain in row segments of 64 cells: a warp per segment,
+// two adjacent cells per lane with one 16-byte access per array (the first inner cell of a
+// row is 256-byte aligned, so column 2 + 2*lane is 16-byte aligned).  f(i, two) gets the
+// lane's first cell and whether the second one is inner too.  Launched with 256-thread
+// blocks (pair_blocks on the host).
+template <class F>
+__device__ __forceinline__ void walk_cell_pairs(const Geom& g, F&& f)
+{
+    const int per_row = (g.nx + 63) / 64;
+    const long nseg = (long)per_row * g.ny * g.nz;
+    const int lane = threadIdx.x & 31;
+    const long warp0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    const int xlast = g.X - HALO_PAD - 1;
+    for (long sgi = warp0; sgi < nseg; sgi += nwarps) {
+        const long row = sgi / per_row;
+        const int xs = (int)(sgi - row * per_row);
+        const int jj = HALO_PAD + (int)(row % g.ny);
+        const int ii = TEA_DIM == 3 ? HALO_PAD + (int)(row / g.ny) : 0;
+        const int kk = HALO_PAD + xs * 64 + 2 * lane;
+        if (kk <= xlast) f(fidx(g, kk, jj, ii), kk < xlast);
+    }
+}
+
+__device__ __forceinline__ double2 ldp(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ void stp(double* p, double a, double b) { *reinterpret_cast<double2*>(p) = make_double2(a, b); }
+
+// The operator at a lane's pair of cells (walk_cell_pairs): the operand at the cells and
+// their neighbours, read from memory (halos included), and the face coefficients, with the
+// pair's rows loaded as 16-byte vectors.  smvp_at(q) evaluates smvp() of cell i + q with the
+// same operations in the same order.
+struct Stencil2 {
+    double c[2], xm[2], xp[2], ym[2], yp[2], zm[2], zp[2];
+    double kx0[2], kx1[2], ky0[2], ky1[2], kz0[2], kz1[2];
+    __device__ __forceinline__ void load(const Geom& g, const double* __restrict__ a, const double* __restrict__ kx,
+                                         const double* __restrict__ ky, const double* __restrict__ kz, long i, bool two)
+    {
+        const long P = g.pitch;
+        if (two) {
+            const double2 cc = ldp(a + i), m = ldp(a + i - P), pp = ldp(a + i + P);
+            const double l = a[i - 1], r = a[i + 2];
+            c[0] = cc.x; c[1] = cc.y;
+            xm[0] = l; xm[1] = cc.x;
+            xp[0] = cc.y; xp[1] = r;
+            ym[0] = m.x; ym[1] = m.y;
+            yp[0] = pp.x; yp[1] = pp.y;
+            const double2 k = ldp(kx + i);
+            kx0[0] = k.x; kx0[1] = k.y;
+            kx1[0] = k.y; kx1[1] = kx[i + 2];
+            const double2 k0 = ldp(ky + i), k1 = ldp(ky + i + P);
+            ky0[0] = k0.x; ky0[1] = k0.y;
+            ky1[0] = k1.x; ky1[1] = k1.y;
+#if TEA_DIM == 3
+            const long Q = g.page;
+            const double2 zm2 = ldp(a + i - Q), zp2 = ldp(a + i + Q), z0 = ldp(kz + i), z1 = ldp(kz + i + Q);
+            zm[0] = zm2.x; zm[1] = zm2.y;
+            zp[0] = zp2.x; zp[1] = zp2.y;
+            kz0[0] = z0.x; kz0[1] = z0.y;
+            kz1[0] = z1.x; kz1[1] = z1.y;
+#endif
+        } else {
+            c[0] = a[i];
+            xm[0] = a[i - 1];
+            xp[0] = a[i + 1];
+            ym[0] = a[i - P];
+            yp[0] = a[i + P];
+            kx0[0] = kx[i];
+            kx1[0] = kx[i + 1];
+            ky0[0] = ky[i];
+            ky1[0] = ky[i + P];
+#if TEA_DIM == 3
+            const long Q = g.page;
+            zm[0] = a[i - Q];
+            zp[0] = a[i + Q];
+            kz0[0] = kz[i];
+            kz1[0] = kz[i + Q];
+#endif
+        }
+    }
+    __device__ __forceinline__ double smvp_at(int q) const
+    {
+#if TEA_DIM == 2
+        return (1.0 + (kx1[q] + kx0[q]) + (ky1[q] + ky0[q])) * c[q] - (kx1[q] * xp[q] + kx0[q] * xm[q])
+            - (ky1[q] * yp[q] + ky0[q] * ym[q]);
+#else
+        return (1.0 + (kx1[q] + kx0[q]) + (ky1[q] + ky0[q]) + (kz1[q] + kz0[q])) * c[q]
+            - (kx1[q] * xp[q] + kx0[q] * xm[q]) - (ky1[q] * yp[q] + ky0[q] * ym[q])
+            - (kz1[q] * zp[q] + kz0[q] * zm[q]);
+#endif
+    }
+};
+
 // ---------------------------------------------------------------- set-up
 
 // InitialiseChunkAreas, tealeaf_2d/ext_initialise_chunk.hpp:63-90 (3D :66-99): volume only
@@ -281,43 +373,61 @@ __global__ void __launch_bounds__(BLOCK) k_set_field(Geom g, Box full, Fields f)
 }
 
 // CopyU, tealeaf_2d/ext_solver_methods.hpp:12-35.
-__global__ void __launch_bounds__(BLOCK) k_copy_u(Geom g, Box inner, Fields f)
+__global__ void __launch_bounds__(BLOCK) k_copy_u(Geom g, Fields f)
 {
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        f.u0[i] = f.u[i];
+    walk_cell_pairs(g, [&](long i, bool two) {
+        if (two) {
+            const double2 u = ldp(f.u + i);
+            stp(f.u0 + i, u.x, u.y);
+        } else {
+            f.u0[i] = f.u[i];
+        }
     });
 }
 
 // CalculateResidual, tealeaf_2d/ext_solver_methods.hpp:38-66.
-__global__ void __launch_bounds__(BLOCK) k_residual(Geom g, Box inner, Fields f)
+__global__ void __launch_bounds__(BLOCK) k_residual(Geom g, Fields f)
 {
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        const double s = smvp(f.u, f.kx, f.ky, f.kz, i, g.pitch, g.page);
-        f.r[i] = f.u0[i] - s;
+    walk_cell_pairs(g, [&](long i, bool two) {
+        Stencil2 n;
+        n.load(g, f.u, f.kx, f.ky, f.kz, i, two);
+        if (two) {
+            const double2 u0 = ldp(f.u0 + i);
+            stp(f.r + i, u0.x - n.smvp_at(0), u0.y - n.smvp_at(1));
+        } else {
+            f.r[i] = f.u0[i] - n.smvp_at(0);
+        }
     });
 }
 
 // Calculate2Norm, tealeaf_2d/ext_solver_methods.hpp:70-92.
-__global__ void __launch_bounds__(BLOCK) k_2norm(Geom g, Box inner, const double* __restrict__ b,
-                                                 RedScratch rs, double* out)
+__global__ void __launch_bounds__(BLOCK) k_2norm(Geom g, const double* __restrict__ b, RedScratch rs, double* out)
 {
     DDVec<1> acc;
     acc.zero();
-    walk(inner, [&](int kk, int jj, int ii) {
-        const double v = b[fidx(g, kk, jj, ii)];
-        dd_add(acc.v[0], v * v);
+    walk_cell_pairs(g, [&](long i, bool two) {
+        if (two) {
+            const double2 v = ldp(b + i);
+            dd_add(acc.v[0], v.x * v.x);
+            dd_add(acc.v[0], v.y * v.y);
+        } else {
+            const double v = b[i];
+            dd_add(acc.v[0], v * v);
+        }
     });
     grid_reduce<1>(acc, rs, out);
 }
 
 // Finalise, tealeaf_2d/ext_solver_methods.hpp:96-121.
-__global__ void __launch_bounds__(BLOCK) k_finalise(Geom g, Box inner, Fields f)
+__global__ void __launch_bounds__(BLOCK) k_finalise(Geom g, Fields f)
 {
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        f.energy[i] = f.u[i] / f.density[i];
+    walk_cell_pairs(g, [&](long i, bool two) {
+        if (two) {
+            const double2 u = ldp(f.u + i), d = ldp(f.density + i);
+            stp(f.energy + i, u.x / d.x, u.y / d.y);
+        } else {
+            f.energy[i] = f.u[i] / f.density[i];
+        }
     });
 }
 
@@ -458,47 +568,75 @@ __global__ void __launch_bounds__(BLOCK) k_cg_calc_rro(Geom g, Box inner, Fields
 }
 
 // CGCalcW, tealeaf_2d/ext_cg_kernel.hpp:148-197 (non-team operator, :177-189).
-__global__ void __launch_bounds__(BLOCK) k_cg_calc_w(Geom g, Box inner, Fields f, RedScratch rs, double* out)
+__global__ void __launch_bounds__(BLOCK) k_cg_calc_w(Geom g, Fields f, RedScratch rs, double* out)
 {
     DDVec<1> acc;
     acc.zero();
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        const double w = smvp(f.p, f.kx, f.ky, f.kz, i, g.pitch, g.page);
-        f.w[i] = w;
-        dd_add(acc.v[0], w * f.p[i]);
+    walk_cell_pairs(g, [&](long i, bool two) {
+        Stencil2 n;
+        n.load(g, f.p, f.kx, f.ky, f.kz, i, two);
+        const double w0 = n.smvp_at(0);
+        dd_add(acc.v[0], w0 * n.c[0]);
+        if (two) {
+            const double w1 = n.smvp_at(1);
+            stp(f.w + i, w0, w1);
+            dd_add(acc.v[0], w1 * n.c[1]);
+        } else {
+            f.w[i] = w0;
+        }
     });
     grid_reduce<1>(acc, rs, out);
 }
 
 // CGCalcUr, tealeaf_2d/ext_cg_kernel.hpp:200-275 (non-team operator, :244-264).
-__global__ void __launch_bounds__(BLOCK) k_cg_calc_ur(Geom g, Box inner, Fields f, double alpha, int precond,
-                                                      RedScratch rs, double* out)
+__global__ void __launch_bounds__(BLOCK) k_cg_calc_ur(Geom g, Fields f, double alpha, int precond, RedScratch rs,
+                                                      double* out)
 {
     DDVec<1> acc;
     acc.zero();
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        f.u[i] = f.u[i] + alpha * f.p[i];
-        const double r = f.r[i] - alpha * f.w[i];
-        f.r[i] = r;
-        if (precond) {
-            const double z = f.mi[i] * r;
-            f.z[i] = z;
-            dd_add(acc.v[0], r * z);
+    walk_cell_pairs(g, [&](long i, bool two) {
+        if (two) {
+            const double2 u = ldp(f.u + i), p = ldp(f.p + i), r = ldp(f.r + i), w = ldp(f.w + i);
+            stp(f.u + i, u.x + alpha * p.x, u.y + alpha * p.y);
+            const double r0 = r.x - alpha * w.x, r1 = r.y - alpha * w.y;
+            stp(f.r + i, r0, r1);
+            if (precond) {
+                const double2 m = ldp(f.mi + i);
+                const double z0 = m.x * r0, z1 = m.y * r1;
+                stp(f.z + i, z0, z1);
+                dd_add(acc.v[0], r0 * z0);
+                dd_add(acc.v[0], r1 * z1);
+            } else {
+                dd_add(acc.v[0], r0 * r0);
+                dd_add(acc.v[0], r1 * r1);
+            }
         } else {
-            dd_add(acc.v[0], r * r);
+            f.u[i] = f.u[i] + alpha * f.p[i];
+            const double r = f.r[i] - alpha * f.w[i];
+            f.r[i] = r;
+            if (precond) {
+                const double z = f.mi[i] * r;
+                f.z[i] = z;
+                dd_add(acc.v[0], r * z);
+            } else {
+                dd_add(acc.v[0], r * r);
+            }
         }
     });
     grid_reduce<1>(acc, rs, out);
 }
 
 // CGCalcP, tealeaf_2d/ext_cg_kernel.hpp:278-319 (non-team operator, :301-310).
-__global__ void __launch_bounds__(BLOCK) k_cg_calc_p(Geom g, Box inner, Fields f, double beta, int precond)
+__global__ void __launch_bounds__(BLOCK) k_cg_calc_p(Geom g, Fields f, double beta, int precond)
 {
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        f.p[i] = beta * f.p[i] + (precond ? f.z[i] : f.r[i]);
+    const double* __restrict__ q = precond ? f.z : f.r;
+    walk_cell_pairs(g, [&](long i, bool two) {
+        if (two) {
+            const double2 p = ldp(f.p + i), v = ldp(q + i);
+            stp(f.p + i, beta * p.x + v.x, beta * p.y + v.y);
+        } else {
+            f.p[i] = beta * f.p[i] + q[i];
+        }
     });
 }
 
@@ -518,57 +656,90 @@ __global__ void __launch_bounds__(BLOCK) k_cheby_init(Geom g, Box inner, Fields 
 }
 
 // ChebyCalcU, tealeaf_2d/ext_cheby_kernel.hpp:50-72.
-__global__ void __launch_bounds__(BLOCK) k_cheby_calc_u(Geom g, Box inner, Fields f)
+__global__ void __launch_bounds__(BLOCK) k_cheby_calc_u(Geom g, Fields f)
 {
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        f.u[i] = f.u[i] + f.p[i];
+    walk_cell_pairs(g, [&](long i, bool two) {
+        if (two) {
+            const double2 u = ldp(f.u + i), p = ldp(f.p + i);
+            stp(f.u + i, u.x + p.x, u.y + p.y);
+        } else {
+            f.u[i] = f.u[i] + f.p[i];
+        }
     });
 }
 
 // ChebyIterate, tealeaf_2d/ext_cheby_kernel.hpp:75-115.
-__global__ void __launch_bounds__(BLOCK) k_cheby_iterate(Geom g, Box inner, Fields f, double alpha,
-                                                         double beta, int precond)
+__global__ void __launch_bounds__(BLOCK) k_cheby_iterate(Geom g, Fields f, double alpha, double beta, int precond)
 {
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        const double w = smvp(f.u, f.kx, f.ky, f.kz, i, g.pitch, g.page);
-        f.w[i] = w;
-        const double r = f.u0[i] - w;
-        f.r[i] = r;
-        f.p[i] = alpha * f.p[i] + beta * (precond ? f.mi[i] * r : r);
+    walk_cell_pairs(g, [&](long i, bool two) {
+        Stencil2 n;
+        n.load(g, f.u, f.kx, f.ky, f.kz, i, two);
+        if (two) {
+            const double2 u0 = ldp(f.u0 + i), p = ldp(f.p + i);
+            double2 m = make_double2(0.0, 0.0);
+            if (precond) m = ldp(f.mi + i);
+            const double w0 = n.smvp_at(0), w1 = n.smvp_at(1);
+            stp(f.w + i, w0, w1);
+            const double r0 = u0.x - w0, r1 = u0.y - w1;
+            stp(f.r + i, r0, r1);
+            stp(f.p + i, alpha * p.x + beta * (precond ? m.x * r0 : r0), alpha * p.y + beta * (precond ? m.y * r1 : r1));
+        } else {
+            const double w = n.smvp_at(0);
+            f.w[i] = w;
+            const double r = f.u0[i] - w;
+            f.r[i] = r;
+            f.p[i] = alpha * f.p[i] + beta * (precond ? f.mi[i] * r : r);
+        }
     });
 }
 
 // ---------------------------------------------------------------- PPCG
 
 // PPCGInitSd, tealeaf_2d/ext_ppcg_kernel.hpp:8-34.
-__global__ void __launch_bounds__(BLOCK) k_ppcg_init_sd(Geom g, Box inner, Fields f, double theta, int precond)
+__global__ void __launch_bounds__(BLOCK) k_ppcg_init_sd(Geom g, Fields f, double theta, int precond)
 {
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        f.sd[i] = (precond ? f.mi[i] * f.r[i] : f.r[i]) / theta;
+    walk_cell_pairs(g, [&](long i, bool two) {
+        if (two) {
+            const double2 r = ldp(f.r + i);
+            double2 m = make_double2(0.0, 0.0);
+            if (precond) m = ldp(f.mi + i);
+            stp(f.sd + i, (precond ? m.x * r.x : r.x) / theta, (precond ? m.y * r.y : r.y) / theta);
+        } else {
+            f.sd[i] = (precond ? f.mi[i] * f.r[i] : f.r[i]) / theta;
+        }
     });
 }
 
 // PPCGCalcU, tealeaf_2d/ext_ppcg_kernel.hpp:37-65.
-__global__ void __launch_bounds__(BLOCK) k_ppcg_calc_u(Geom g, Box inner, Fields f)
+__global__ void __launch_bounds__(BLOCK) k_ppcg_calc_u(Geom g, Fields f)
 {
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        const double s = smvp(f.sd, f.kx, f.ky, f.kz, i, g.pitch, g.page);
-        f.r[i] = f.r[i] - s;
-        f.u[i] = f.u[i] + f.sd[i];
+    walk_cell_pairs(g, [&](long i, bool two) {
+        Stencil2 n;
+        n.load(g, f.sd, f.kx, f.ky, f.kz, i, two);
+        if (two) {
+            const double2 r = ldp(f.r + i), u = ldp(f.u + i);
+            stp(f.r + i, r.x - n.smvp_at(0), r.y - n.smvp_at(1));
+            stp(f.u + i, u.x + n.c[0], u.y + n.c[1]);
+        } else {
+            f.r[i] = f.r[i] - n.smvp_at(0);
+            f.u[i] = f.u[i] + n.c[0];
+        }
     });
 }
 
 // PPCGCalcSd, tealeaf_2d/ext_ppcg_kernel.hpp:68-100.
-__global__ void __launch_bounds__(BLOCK) k_ppcg_calc_sd(Geom g, Box inner, Fields f, double alpha, double beta,
-                                                        int precond)
+__global__ void __launch_bounds__(BLOCK) k_ppcg_calc_sd(Geom g, Fields f, double alpha, double beta, int precond)
 {
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        f.sd[i] = alpha * f.sd[i] + beta * (precond ? f.mi[i] * f.r[i] : f.r[i]);
+    walk_cell_pairs(g, [&](long i, bool two) {
+        if (two) {
+            const double2 sd = ldp(f.sd + i), r = ldp(f.r + i);
+            double2 m = make_double2(0.0, 0.0);
+            if (precond) m = ldp(f.mi + i);
+            stp(f.sd + i, alpha * sd.x + beta * (precond ? m.x * r.x : r.x),
+                alpha * sd.y + beta * (precond ? m.y * r.y : r.y));
+        } else {
+            f.sd[i] = alpha * f.sd[i] + beta * (precond ? f.mi[i] * f.r[i] : f.r[i]);
+        }
     });
 }
 
