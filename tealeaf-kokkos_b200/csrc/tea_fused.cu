@@ -519,7 +519,6 @@ bool ensure_fp32(Chunk* c, Fused* F)
 // Enqueue one iteration of loop `kind` on the chunk's stream.
 void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs& a)
 {
-    const dim3 pb(TILE_X, TILE_Y);
     cudaStream_t s = c->stream;
     switch (kind) {
     case LOOP_CG:
@@ -551,7 +550,7 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         break;
     case LOOP_PPCG: {
         stencil<OpSweepA>(F, a, s);
-        k_ppcg_sweep_b<<<F->point_blocks, pb, 0, s>>>(a, c->inner);
+        k_ppcg_sweep_b<<<F->pair_blocks, 256, 0, s>>>(a);
         int k0 = 1;
 #if TEA_DIM == 2
         if (F->ppcg2.blocks > 0) {

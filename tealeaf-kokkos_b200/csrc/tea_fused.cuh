@@ -1159,24 +1159,41 @@ __global__ void __launch_bounds__(256) k_cg_sweep_b(FusedArgs a)
 // CGCalcUr (u += alpha p, r -= alpha w, z = Mi r; its rrn is unused,
 // tealeaf_2d/tea_solve.f90:340) fused with PPCGInitSd (tealeaf_2d/ext_ppcg_kernel.hpp:8-34)
 // writing sd into buffer 0.
-__global__ void __launch_bounds__(BLOCK) k_ppcg_sweep_b(FusedArgs a, Box inner)
+__global__ void __launch_bounds__(256) k_ppcg_sweep_b(FusedArgs a)
 {
     const SolveState& s = *a.st;
     const double alpha = s.alpha, theta = s.theta;
     const int precond = s.precond;
     const double* __restrict__ p = a.p[s.par_p];
-    const Geom& g = a.g;
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        a.u[0][i] = a.u[0][i] + alpha * p[i];
-        const double r = a.r[i] - alpha * a.w[i];
-        a.r[i] = r;
-        double m = r;
-        if (precond) {
-            m = a.mi[i] * r;
-            a.z[i] = m;
+    double* __restrict__ U = a.u[0];
+    double* __restrict__ R = a.r;
+    const double* __restrict__ W = a.w;
+    double* __restrict__ SD = a.sd[0];
+    walk_pairs(a.g, [&](long i, bool two) {
+        if (two) {
+            const double2 u2 = ld2(U + i), p2 = ld2(p + i), r2 = ld2(R + i), w2 = ld2(W + i);
+            st2(U + i, u2.x + alpha * p2.x, u2.y + alpha * p2.y);
+            const double r0 = r2.x - alpha * w2.x, r1 = r2.y - alpha * w2.y;
+            st2(R + i, r0, r1);
+            double m0 = r0, m1 = r1;
+            if (precond) {
+                const double2 mi = ld2(a.mi + i);
+                m0 = mi.x * r0;
+                m1 = mi.y * r1;
+                st2(a.z + i, m0, m1);
+            }
+            st2(SD + i, m0 / theta, m1 / theta);
+        } else {
+            U[i] = U[i] + alpha * p[i];
+            const double r = R[i] - alpha * W[i];
+            R[i] = r;
+            double m = r;
+            if (precond) {
+                m = a.mi[i] * r;
+                a.z[i] = m;
+            }
+            SD[i] = m / theta;
         }
-        a.sd[0][i] = m / theta;
     });
 }
 
