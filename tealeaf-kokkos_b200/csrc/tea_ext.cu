@@ -575,8 +575,8 @@ TEA_EXPORT void ext_jacobi_kernel_solve_(const int* chunk, double* error)
 {
     Chunk* c = get_chunk(chunk);
     if (!c) return;
-    LAUNCH(k_jacobi_copy, c->full, c->g, c->full, c->f);
-    LAUNCH(k_jacobi_solve, c->inner, c->g, c->inner, c->f, c->red, c->d_out);
+    k_jacobi_copy<<<pair_blocks(c), BLOCK, 0, c->stream>>>(c->g, c->f);
+    LAUNCH_PAIRS(k_jacobi_solve, c->g, c->f, c->red, c->d_out);
     *error = result(c, 0);
 }
 

@@ -466,40 +466,49 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi_init(Geom g, Box full, Fields 
 }
 
 // JacobiCopyU, tealeaf_2d/ext_jacobi_kernel.hpp:66-82: r = u over the padded array.
-__global__ void __launch_bounds__(BLOCK) k_jacobi_copy(Geom g, Box full, Fields f)
+__global__ void __launch_bounds__(BLOCK) k_jacobi_copy(Geom g, Fields f)
 {
-    walk(full, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
-        f.r[i] = f.u[i];
-    });
+    // The whole padded array as one flat run of page * Z doubles (the pitch padding at the
+    // end of each row is copied too; nothing reads it).  The array starts 16-byte aligned
+    // and page is a multiple of 32, so every access is a 16-byte one.
+    const long n2 = g.page * g.Z / 2;
+    const double2* __restrict__ src = reinterpret_cast<const double2*>(f.u);
+    double2* __restrict__ dst = reinterpret_cast<double2*>(f.r);
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n2; k += (long)gridDim.x * blockDim.x)
+        dst[k] = src[k];
 }
 
 // JacobiSolve, tealeaf_2d/ext_jacobi_kernel.hpp:86-117 (3D :90-126).
-__global__ void __launch_bounds__(BLOCK) k_jacobi_solve(Geom g, Box inner, Fields f, RedScratch rs,
-                                                        double* out)
+__global__ void __launch_bounds__(BLOCK) k_jacobi_solve(Geom g, Fields f, RedScratch rs, double* out)
 {
     DDVec<1> acc;
     acc.zero();
-    const double* __restrict__ kx = f.kx;
-    const double* __restrict__ ky = f.ky;
-    const double* __restrict__ r = f.r;
-    const long px = g.pitch;
-    walk(inner, [&](int kk, int jj, int ii) {
-        const long i = fidx(g, kk, jj, ii);
+    walk_cell_pairs(g, [&](long i, bool two) {
+        Stencil2 n;
+        n.load(g, f.r, f.kx, f.ky, f.kz, i, two);
+        double u0[2], un[2];
+        if (two) {
+            const double2 v = ldp(f.u0 + i);
+            u0[0] = v.x;
+            u0[1] = v.y;
+        } else {
+            u0[0] = f.u0[i];
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (q == 1 && !two) break;
 #if TEA_DIM == 2
-        const double un = (f.u0[i] + (kx[i + 1] * r[i + 1] + kx[i] * r[i - 1])
-                           + (ky[i + px] * r[i + px] + ky[i] * r[i - px]))
-            / (1.0 + (kx[i] + kx[i + 1]) + (ky[i] + ky[i + px]));
+            un[q] = (u0[q] + (n.kx1[q] * n.xp[q] + n.kx0[q] * n.xm[q]) + (n.ky1[q] * n.yp[q] + n.ky0[q] * n.ym[q]))
+                / (1.0 + (n.kx0[q] + n.kx1[q]) + (n.ky0[q] + n.ky1[q]));
 #else
-        const double* __restrict__ kz = f.kz;
-        const long pg = g.page;
-        const double un = (f.u0[i] + (kx[i + 1] * r[i + 1] + kx[i] * r[i - 1])
-                           + (ky[i + px] * r[i + px] + ky[i] * r[i - px])
-                           + (kz[i + pg] * r[i + pg] + kz[i] * r[i - pg]))
-            / (1.0 + (kx[i] + kx[i + 1]) + (ky[i] + ky[i + px]) + (kz[i] + kz[i + pg]));
+            un[q] = (u0[q] + (n.kx1[q] * n.xp[q] + n.kx0[q] * n.xm[q]) + (n.ky1[q] * n.yp[q] + n.ky0[q] * n.ym[q])
+                     + (n.kz1[q] * n.zp[q] + n.kz0[q] * n.zm[q]))
+                / (1.0 + (n.kx0[q] + n.kx1[q]) + (n.ky0[q] + n.ky1[q]) + (n.kz0[q] + n.kz1[q]));
 #endif
-        f.u[i] = un;
-        dd_add(acc.v[0], fabs(un - r[i]));
+            dd_add(acc.v[0], fabs(un[q] - n.c[q]));
+        }
+        if (two) stp(f.u + i, un[0], un[1]);
+        else f.u[i] = un[0];
     });
     grid_reduce<1>(acc, rs, out);
 }
