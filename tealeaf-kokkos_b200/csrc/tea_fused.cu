@@ -124,7 +124,15 @@ constexpr size_t ppcg2_2d_smem_bytes = (size_t)RWARPS * C2_RQ * C2_NA * Pair2Geo
 
 // PPCG inner steps that run as two-step passes: an even number of pairs, none holding the
 // last step (which forms the 2-norm).
-inline int ppcg_pair_steps(int inner_steps) { return 4 * ((inner_steps - 1) / 4); }
+// Two-step PPCG passes per outer iteration: every step in pairs when the count is even (the
+// last pair also forms the 2-norm), else an even number of pairs and single steps after
+// them, so that the single steps find sd in the buffer they expect.
+inline int ppcg_pairs(int inner_steps)
+{
+    int pairs = inner_steps / 2;
+    if ((inner_steps & 1) && (pairs & 1)) pairs -= 1;
+    return pairs;
+}
 
 // Opt a ring kernel into its dynamic shared memory; blocks per SM it then reaches.
 template <class K>
@@ -388,6 +396,7 @@ Fused* ensure_fused(Chunk* c, int max_iters)
         a.use_handle = 0;
         a.step = 0;
         a.timing = 0;
+        a.r_in_w = 0;
         a.seg_rows = 64;  // every ring launch sets its own
         int sms = 148;
         TEA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
@@ -550,28 +559,24 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         break;
     case LOOP_PPCG: {
         stencil<OpSweepA>(F, a, s);
-        k_ppcg_sweep_b<<<F->pair_blocks, 256, 0, s>>>(a);
+        // r alternates between r and w over the pairs; with an odd number of pairs sweep B
+        // leaves r in w, so that the last pair writes it back into r.
+        const int pairs = F->ppcg2.blocks > 0 ? ppcg_pairs(inner_steps) : 0;
+        FusedArgs ab = a;
+        ab.r_in_w = pairs & 1;
+        k_ppcg_sweep_b<<<F->pair_blocks, 256, 0, s>>>(ab);
         int k0 = 1;
+        for (int m = 1; m <= pairs; ++m, k0 += 2) {
+            FusedArgs ak = ab;
+            ak.step = k0;
+            ak.seg_rows = F->ppcg2.rows;
 #if TEA_DIM == 2
-        if (F->ppcg2.blocks > 0) {
-            for (; k0 <= ppcg_pair_steps(inner_steps); k0 += 2) {
-                FusedArgs ak = a;
-                ak.step = k0;
-                ak.seg_rows = F->ppcg2.rows;
-                k_ppcg2_ring2d<<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, s>>>(ak);
-            }
-        }
+            k_ppcg2_ring2d<<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, s>>>(ak);
 #else
-        if (F->ppcg2.blocks > 0) {
-            for (; k0 <= ppcg_pair_steps(inner_steps); k0 += 2) {
-                FusedArgs ak = a;
-                ak.step = k0;
-                ak.seg_rows = F->ppcg2.rows;
-                k_ppcg2_ring3d<PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
-                                                    ppcg2_smem_bytes<PPCG2_TY, PPCG2_RP>(), s>>>(ak);
-            }
-        }
+            k_ppcg2_ring3d<PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
+                                                ppcg2_smem_bytes<PPCG2_TY, PPCG2_RP>(), s>>>(ak);
 #endif
+        }
         for (int k = k0; k <= inner_steps; ++k) {
             FusedArgs ak = a;
             ak.step = k;

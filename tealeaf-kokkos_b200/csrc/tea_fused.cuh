@@ -67,6 +67,7 @@ struct FusedArgs {
     int step;    // PPCG inner step (1-based) of this launch
     int seg_rows;  // rows per warp segment of the 2D ring kernels (set per launch)
     int timing;  // measurement launches: the last block leaves the solve state untouched
+    int r_in_w;  // PPCG: sweep B leaves r in the w array and the two-step passes start there
     // FP32 arrays of the defect-correction form (same pitched layout, float elements).
     float *kx32, *ky32, *kz32, *r32, *w32, *d32;
     float* p32[2];
@@ -1166,15 +1167,16 @@ __global__ void __launch_bounds__(256) k_ppcg_sweep_b(FusedArgs a)
     const int precond = s.precond;
     const double* __restrict__ p = a.p[s.par_p];
     double* __restrict__ U = a.u[0];
-    double* __restrict__ R = a.r;
-    const double* __restrict__ W = a.w;
+    const double* R = a.r;
+    const double* W = a.w;
+    double* RD = a.r_in_w ? a.w : a.r;  // where r goes: w when the two-step passes start there
     double* __restrict__ SD = a.sd[0];
     walk_pairs(a.g, [&](long i, bool two) {
         if (two) {
             const double2 u2 = ld2(U + i), p2 = ld2(p + i), r2 = ld2(R + i), w2 = ld2(W + i);
             st2(U + i, u2.x + alpha * p2.x, u2.y + alpha * p2.y);
             const double r0 = r2.x - alpha * w2.x, r1 = r2.y - alpha * w2.y;
-            st2(R + i, r0, r1);
+            st2(RD + i, r0, r1);
             double m0 = r0, m1 = r1;
             if (precond) {
                 const double2 mi = ld2(a.mi + i);
@@ -1186,7 +1188,7 @@ __global__ void __launch_bounds__(256) k_ppcg_sweep_b(FusedArgs a)
         } else {
             U[i] = U[i] + alpha * p[i];
             const double r = R[i] - alpha * W[i];
-            R[i] = r;
+            RD[i] = r;
             double m = r;
             if (precond) {
                 m = a.mi[i] * r;
@@ -1311,9 +1313,11 @@ struct OpPPCGInner {
 // two rows, z segments by one plane of step k.  At the domain's faces step k's sd is
 // reflected as the reference's halo update reflects it (the cell's own value).  Tiles read
 // r at cells that a neighbouring tile writes, so r goes to the other of r and w (w is free
-// during the inner steps) and sd to the other sd buffer; pairs come in even numbers so that
-// both end where single steps leave them.  Pair m (steps 2m-1, 2m) reads sd[(m-1)&1] and r
-// (m odd) or w (m even).  A pair never holds the last inner step (the one that reduces).
+// during the inner steps) and sd to the other sd buffer.  Pair m (steps 2m-1, 2m) reads
+// sd[(m-1)&1] and writes sd[m&1]; it reads r from r when m - 1 + a.r_in_w is even, else from
+// w, and writes it to the other.  With an odd number of pairs sweep B leaves r in w
+// (r_in_w), so the last pair writes r back into r.  A pair whose second step is the last
+// inner step also forms that step's sum r.r and ends the outer iteration.
 template <int TY, int RP>
 constexpr size_t ppcg2_smem_bytes()
 {
@@ -1339,10 +1343,13 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
     const int m = (k + 1) >> 1;
     const double* __restrict__ sdk = a.sd[(m - 1) & 1];
     double* __restrict__ sdo = a.sd[m & 1];
-    const double* __restrict__ rin = (m & 1) ? a.r : a.w;
-    double* __restrict__ rout = (m & 1) ? a.w : a.r;
+    const double* __restrict__ rin = ((m - 1 + a.r_in_w) & 1) ? a.w : a.r;
+    double* __restrict__ rout = ((m + a.r_in_w) & 1) ? a.w : a.r;
     double* __restrict__ U = a.u[0];
     const bool precond = a.st->precond != 0;
+    const bool last = k + 1 == a.st->inner_steps;  // step k+1 ends the outer iteration
+    DDVec<1> acc;
+    acc.zero();
     const double* __restrict__ MI = precond ? a.mi : nullptr;
     const double al1 = a.ch_alphas[k - 1], be1 = a.ch_betas[k - 1];
     const double al2 = a.ch_alphas[k], be2 = a.ch_betas[k];
@@ -1505,6 +1512,7 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
                         r2[q] = r;
                         u2[q] = u1c[q] + tc[q];
                         d2[q] = al2 * tc[q] + be2 * (precond ? mi[q] * r : r);
+                        if (last && c + q <= xlast) dd_add(acc.v[0], r * r);
                     }
                     const long i = fidx(g, c, j, z);
                     if (c + VEC - 1 <= xlast) {
@@ -1536,6 +1544,8 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
         cp_async_wait<0>();
         __syncthreads();  // the next unit's copies reuse slots other warps may still read
     }
+    // The last inner step's sum r.r and the end of the outer iteration, as OpPPCGInner<true>.
+    if (last) grid_reduce_then<1>(acc, a.red, [&](const double* v) { OpPPCGInner<true>().control(a, v); });
 }
 #endif
 
@@ -1890,8 +1900,8 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
 // first row only feed their neighbours, and at the domain's edges step k's sd is
 // reflected as the reference's halo update reflects it.  Per cell the operations and their
 // order are those of two single steps, so results are bit-identical.  r moves between r
-// and w and sd between its two buffers, as in 3D (pair m reads sd[(m-1)&1] and r for odd m,
-// w for even m); u is read and written only at the cells a warp writes.
+// and w and sd between its two buffers, and a pair may hold the last, reducing step, all as
+// in 3D; u is read and written only at the cells a warp writes.
 enum { P2_SD = 0, P2_R = 1, P2_U = 2, P2_MI = 3, P2_KX = 4, P2_KY = 5 };
 
 __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
@@ -1903,10 +1913,13 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
     const int m = (k + 1) >> 1;
     const double* __restrict__ sdk = a.sd[(m - 1) & 1];
     double* __restrict__ sdo = a.sd[m & 1];
-    const double* __restrict__ rin = (m & 1) ? a.r : a.w;
-    double* __restrict__ rout = (m & 1) ? a.w : a.r;
+    const double* __restrict__ rin = ((m - 1 + a.r_in_w) & 1) ? a.w : a.r;
+    double* __restrict__ rout = ((m + a.r_in_w) & 1) ? a.w : a.r;
     double* __restrict__ U = a.u[0];
     const bool precond = a.st->precond != 0;
+    const bool last = k + 1 == a.st->inner_steps;  // step k+1 ends the outer iteration
+    DDVec<1> acc;
+    acc.zero();
     const double* __restrict__ mi = precond ? a.mi : nullptr;
     const double al1 = a.ch_alphas[k - 1], be1 = a.ch_betas[k - 1];
     const double al2 = a.ch_alphas[k], be2 = a.ch_betas[k];
@@ -2031,6 +2044,7 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
                     r2[q] = r;
                     u2[q] = u1c[q] + vc[q];
                     d2[q] = al2 * vc[q] + be2 * (precond ? m0[q] * r : r);
+                    if (last && out_lane && c + q <= xlast) dd_add(acc.v[0], r * r);
                 }
                 if (out_lane && c + VEC - 1 <= xlast) {
                     st_vec(rout + i, r2);
@@ -2062,6 +2076,8 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
         cp_async_wait<0>();
         __syncwarp();
     }
+    // The last inner step's sum r.r and the end of the outer iteration, as OpPPCGInner<true>.
+    if (last) grid_reduce_then<1>(acc, a.red, [&](const double* v) { OpPPCGInner<true>().control(a, v); });
 }
 #endif
 

@@ -60,3 +60,24 @@ def test_fused_known_answer(dim):
     s_p, r_p = tea.run_deck(kat["deck"], dim)
     assert [r["iterations"] for r in r_f] == [r["iterations"] for r in r_p]
     assert s_f["temp"] == s_p["temp"] and s_f["kat_passed"] == 1
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("inner", [4, 5, 6, 7])
+def test_fused_ppcg_inner_step_splits(dim, inner):
+    """The whole-solve path runs PPCG inner steps two per pass: every step in pairs when the
+    count is even (the last pair also forms the 2-norm), else an even number of pairs and
+    single steps after them; r moves between r and w.  4, 5, 6 and 7 inner steps cover
+    each split (even and odd numbers of pairs, with and without single steps), against
+    the per-call path bit for bit."""
+    spec = tea.DeckSpec(dim=dim, cells=48 if dim == 2 else 20, states=6, seed=60 + inner, solver="ppcg", end_step=2,
+                        inner_steps=inner, eps=1e-15, eps_rel=1e-10, max_iters=5000, summary_frequency=1,
+                        check_result=True)
+    deck = tea.seeded_deck(spec)
+    _, fused = tea.run_deck(deck, dim, fused=True, summary_every_step=True)
+    _, percall = tea.run_deck(deck, dim, summary_every_step=True)
+    assert len(fused) == len(percall) == 2
+    assert all(r["cheby_steps"] > 0 for r in fused)  # the PPCG phase ran
+    for a, b in zip(fused, percall):
+        for k in FIELDS:
+            assert same(a[k], b[k]), f"{dim}D {inner} inner steps, step {a['step']} {k}: {a[k]!r} vs {b[k]!r}"
