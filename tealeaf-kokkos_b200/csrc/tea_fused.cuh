@@ -479,9 +479,7 @@ struct RingGeom {
     static constexpr int WIDTH = STRIP + 2 * OFF;
 };
 
-// Cells per lane of a sweep's ring kernel: one 16-byte copy by default; a sweep whose
-// per-cell stores are many narrow ones (FP32 CG sweep A: d, p and w) keeps two cells per
-// lane so that each store instruction covers whole sectors.
+// Cells per lane of a sweep's ring kernel: one 16-byte copy (2 doubles or 4 floats).
 template <class Op>
 struct RingVec {
     static constexpr int value = 16 / (int)sizeof(typename Op::T);
@@ -489,10 +487,22 @@ struct RingVec {
 struct OpSweepA32;
 template <>
 struct RingVec<OpSweepA32> {
-    static constexpr int value = 2;
+    static constexpr int value = 4;
 };
 template <class Op>
 using RingGeomOf = RingGeom<typename Op::T, RingVec<Op>::value>;
+
+// Sweeps whose ring kernels compute a lane's VEC cells first and then store each output
+// array with one vector store (Op::Out, interior_out, store_vec, store_one) instead of one
+// scalar store per cell and array.
+template <class Op>
+struct RingVecStore {
+    static constexpr bool value = false;
+};
+template <>
+struct RingVecStore<OpSweepA32> {
+    static constexpr bool value = true;
+};
 
 template <class T>
 __device__ __forceinline__ void ld_vec(const T* p, T* out);
@@ -663,24 +673,50 @@ __device__ __forceinline__ void ring2d_body(const FusedArgs& a, Op& op, unsigned
             for (int k = 0; k < NR; ++k) ld_vecn<VEC>(cur + k * RWT + OFF + VEC * lane, rv[k]);
 #pragma unroll
             for (int k = 0; k < NI; ++k) ld_vecn<VEC>(cur + (NR + k) * RWT + OFF + VEC * lane, iv[k]);
-#pragma unroll
-            for (int q = 0; q < VEC; ++q) {
+            auto cell_nb = [&](int q) {
                 const int cq = c + q;
-                if (cq <= xlast) {
+                NbT<T> nb;
+                nb.c = cv[q];
+                nb.xm = q == 0 ? (lane == 0 ? ce : up) : cv[q > 0 ? q - 1 : 0];
+                nb.xp = cq == xlast ? cv[q] : (q == VEC - 1 ? (lane == 31 ? ce : dn) : cv[q < VEC - 1 ? q + 1 : q]);
+                nb.ym = mv[q];
+                nb.yp = pv[q];
+                nb.zm = nb.zp = (T)0;
+                return nb;
+            };
+            if constexpr (RingVecStore<Op>::value) {
+                typename Op::Out o[VEC];
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
                     T rq[NR > 0 ? NR : 1], iq[NI];
 #pragma unroll
                     for (int k = 0; k < NR; ++k) rq[k] = rv[k][q];
 #pragma unroll
                     for (int k = 0; k < NI; ++k) iq[k] = iv[k][q];
-                    NbT<T> nb;
-                    nb.c = cv[q];
-                    nb.xm = q == 0 ? (lane == 0 ? ce : up) : cv[q > 0 ? q - 1 : 0];
-                    nb.xp = cq == xlast ? cv[q] : (q == VEC - 1 ? (lane == 31 ? ce : dn) : cv[q < VEC - 1 ? q + 1 : q]);
-                    nb.ym = mv[q];
-                    nb.yp = pv[q];
-                    nb.zm = nb.zp = (T)0;
-                    op.interior_k(a, fidx(g, cq, jj, 0), nb, op.raw_from(rq), op.in_from(iq), kx[q], kx[q + 1], ky0[q],
-                                  ky1[q], (T)0, (T)0, acc);
+                    o[q] = op.interior_out(cell_nb(q), op.raw_from(rq), op.in_from(iq), kx[q], kx[q + 1], ky0[q], ky1[q],
+                                           (T)0, (T)0, acc, c + q <= xlast);
+                }
+                const long i0 = fidx(g, c, jj, 0);
+                if (c + VEC - 1 <= xlast) {
+                    op.store_vec(a, i0, o);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q)
+                        if (c + q <= xlast) op.store_one(a, i0 + q, o[q]);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    const int cq = c + q;
+                    if (cq <= xlast) {
+                        T rq[NR > 0 ? NR : 1], iq[NI];
+#pragma unroll
+                        for (int k = 0; k < NR; ++k) rq[k] = rv[k][q];
+#pragma unroll
+                        for (int k = 0; k < NI; ++k) iq[k] = iv[k][q];
+                        op.interior_k(a, fidx(g, cq, jj, 0), cell_nb(q), op.raw_from(rq), op.in_from(iq), kx[q],
+                                      kx[q + 1], ky0[q], ky1[q], (T)0, (T)0, acc);
+                    }
                 }
             }
 #pragma unroll
@@ -898,27 +934,52 @@ __global__ void __launch_bounds__(TY3R * 32) k_ring3d(FusedArgs a)
             for (int k = 0; k < NR; ++k) ld_vecn<VEC>(cur + (R::RAW + k * (TY3R + 2) + w + 1) * RWT + OFF + VEC * lane, rv[k]);
 #pragma unroll
             for (int k = 0; k < NI; ++k) ld_vecn<VEC>(cur + (R::IN + k * TY3R + w) * RWT + OFF + VEC * lane, iv[k]);
+            auto cell_nb = [&](int q) {
+                const int cq = c + q;
+                NbT<T> nb;
+                nb.c = cv[q];
+                nb.xm = q == 0 ? (lane == 0 ? ce : up) : cv[q > 0 ? q - 1 : 0];
+                nb.xp = cq == xlast ? cv[q] : (q == VEC - 1 ? (lane == 31 ? ce : dn) : cv[q < VEC - 1 ? q + 1 : q]);
+                nb.ym = ym[q];
+                nb.yp = yp[q];
+                nb.zm = mv[q];
+                nb.zp = pv[q];
+                return nb;
+            };
             if (row_active) {
+                if constexpr (RingVecStore<Op>::value) {
+                    typename Op::Out o[VEC];
 #pragma unroll
-                for (int q = 0; q < VEC; ++q) {
-                    const int cq = c + q;
-                    if (cq <= xlast) {
+                    for (int q = 0; q < VEC; ++q) {
                         T rq[NR], iq[NI > 0 ? NI : 1];
 #pragma unroll
                         for (int k = 0; k < NR; ++k) rq[k] = rv[k][q];
 #pragma unroll
                         for (int k = 0; k < NI; ++k) iq[k] = iv[k][q];
-                        NbT<T> nb;
-                        nb.c = cv[q];
-                        nb.xm = q == 0 ? (lane == 0 ? ce : up) : cv[q > 0 ? q - 1 : 0];
-                        nb.xp = cq == xlast ? cv[q]
-                                            : (q == VEC - 1 ? (lane == 31 ? ce : dn) : cv[q < VEC - 1 ? q + 1 : q]);
-                        nb.ym = ym[q];
-                        nb.yp = yp[q];
-                        nb.zm = mv[q];
-                        nb.zp = pv[q];
-                        op.interior_k(a, fidx(g, cq, j, z), nb, op.raw_from(rq), op.in_from(iq), kx[q], kx[q + 1],
-                                      ky0[q], ky1[q], kz0[q], kz1[q], acc);
+                        o[q] = op.interior_out(cell_nb(q), op.raw_from(rq), op.in_from(iq), kx[q], kx[q + 1], ky0[q],
+                                               ky1[q], kz0[q], kz1[q], acc, c + q <= xlast);
+                    }
+                    const long i0 = fidx(g, c, j, z);
+                    if (c + VEC - 1 <= xlast) {
+                        op.store_vec(a, i0, o);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q)
+                            if (c + q <= xlast) op.store_one(a, i0 + q, o[q]);
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) {
+                        const int cq = c + q;
+                        if (cq <= xlast) {
+                            T rq[NR], iq[NI > 0 ? NI : 1];
+#pragma unroll
+                            for (int k = 0; k < NR; ++k) rq[k] = rv[k][q];
+#pragma unroll
+                            for (int k = 0; k < NI; ++k) iq[k] = iv[k][q];
+                            op.interior_k(a, fidx(g, cq, j, z), cell_nb(q), op.raw_from(rq), op.in_from(iq), kx[q],
+                                          kx[q + 1], ky0[q], ky1[q], kz0[q], kz1[q], acc);
+                        }
                     }
                 }
             }
@@ -2401,6 +2462,36 @@ struct OpSweepA32 {
         const float w = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
         a.w32[i] = w;
         dd_add(acc.v[0], (double)w * (double)nb.c);
+    }
+    // Ring kernels' vector-store form of interior_k: the same values, the lane's four cells
+    // stored with one 16-byte store per array (d only when its update is pending).
+    struct Out {
+        float d, p, w;
+    };
+    __device__ Out interior_out(const NbT<float>& nb, const Raw& rc, const In& in, float kx0, float kx1, float ky0,
+                                float ky1, float kz0, float kz1, DDVec<1>& acc, bool inner) const
+    {
+        Out o;
+        o.d = in.d + alpha * rc.p;
+        o.p = nb.c;
+        o.w = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
+        if (inner) dd_add(acc.v[0], (double)o.w * (double)nb.c);
+        return o;
+    }
+    __device__ void store_vec(const FusedArgs& a, long i, const Out* o) const
+    {
+        static_assert(RingVec<OpSweepA32>::value == 4, "one float4 per array");
+        const float d4[4] = {o[0].d, o[1].d, o[2].d, o[3].d}, p4[4] = {o[0].p, o[1].p, o[2].p, o[3].p},
+                    w4[4] = {o[0].w, o[1].w, o[2].w, o[3].w};
+        if (pend_u) st_vec(a.d32 + i, d4);
+        st_vec(pnew + i, p4);
+        st_vec(a.w32 + i, w4);
+    }
+    __device__ void store_one(const FusedArgs& a, long i, const Out& o) const
+    {
+        if (pend_u) a.d32[i] = o.d;
+        pnew[i] = o.p;
+        a.w32[i] = o.w;
     }
     __device__ void control(const FusedArgs& a, const double* v)
     {
