@@ -485,10 +485,7 @@ struct RingVec {
     static constexpr int value = 16 / (int)sizeof(typename Op::T);
 };
 struct OpSweepA32;
-template <>
-struct RingVec<OpSweepA32> {
-    static constexpr int value = 4;
-};
+struct OpCheby32;
 template <class Op>
 using RingGeomOf = RingGeom<typename Op::T, RingVec<Op>::value>;
 
@@ -501,6 +498,10 @@ struct RingVecStore {
 };
 template <>
 struct RingVecStore<OpSweepA32> {
+    static constexpr bool value = true;
+};
+template <>
+struct RingVecStore<OpCheby32> {
     static constexpr bool value = true;
 };
 
@@ -2582,6 +2583,33 @@ struct OpCheby32 {
         pcur[i] = p;
         unew[i] = nb.c + p;
         if (check) dd_add(acc.v[0], (double)r * (double)r);
+    }
+    // Ring kernels' vector-store form of interior_k: the lane's four cells of p and of the
+    // new iterate stored with one 16-byte store each.
+    struct Out {
+        float p, u;
+    };
+    __device__ Out interior_out(const NbT<float>& nb, const Raw&, const In& in, float kx0, float kx1, float ky0,
+                                float ky1, float kz0, float kz1, DDVec<1>& acc, bool inner) const
+    {
+        const float w = smvp_k(nb, kx0, kx1, ky0, ky1, kz0, kz1);
+        const float r = in.rhs - w;
+        Out o;
+        o.p = al * in.p + be * r;
+        o.u = nb.c + o.p;
+        if (check && inner) dd_add(acc.v[0], (double)r * (double)r);
+        return o;
+    }
+    __device__ void store_vec(const FusedArgs&, long i, const Out* o) const
+    {
+        const float p4[4] = {o[0].p, o[1].p, o[2].p, o[3].p}, u4[4] = {o[0].u, o[1].u, o[2].u, o[3].u};
+        st_vec(pcur + i, p4);
+        st_vec(unew + i, u4);
+    }
+    __device__ void store_one(const FusedArgs&, long i, const Out& o) const
+    {
+        pcur[i] = o.p;
+        unew[i] = o.u;
     }
     __device__ static void finish(const FusedArgs& a, SolveState& s, bool checked, double rr)
     {
