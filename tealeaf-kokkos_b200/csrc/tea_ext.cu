@@ -497,12 +497,24 @@ TEA_EXPORT void ext_update_halo_kernel_(const int* chunk, const int* chunkNeighb
 #define LAUNCH(kernel, box, ...)                                                                   \
     kernel<<<launch_blocks(c, (box).ntiles), dim3(TILE_X, TILE_Y), 0, c->stream>>>(__VA_ARGS__)
 
-// Pointwise kernels (walk_cell_pairs): one warp per 64-cell row segment, 256-thread blocks,
-// at most as many blocks as the reduction scratch holds partials for.
+// Segment-walk kernels (walk_cell_pairs): one warp per 64-cell row segment at most,
+// 256-thread blocks, at most one wave of resident blocks (no partial second wave) and no
+// more blocks than the reduction scratch holds partials for.
 static int pair_blocks(const Chunk* c)
 {
+    static int wave = 0;  // blocks of one wave of the heaviest segment-walk kernel
+    if (wave == 0) {
+        int sms = 148, occ = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        int n = 8;
+        for (const void* k : {(const void*)k_cg_calc_w, (const void*)k_cheby_iterate, (const void*)k_ppcg_calc_u,
+                              (const void*)k_jacobi_solve, (const void*)k_cg_calc_ur})
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, BLOCK, 0) == cudaSuccess && occ > 0)
+                n = std::min(n, occ);
+        wave = sms * n;
+    }
     const long nseg = (long)((c->g.nx + 63) / 64) * c->g.ny * c->g.nz;
-    return (int)std::max<long>(1, std::min<long>((nseg + 7) / 8, c->red.max_blocks));
+    return (int)std::max<long>(1, std::min<long>(std::min<long>((nseg + 7) / 8, wave), c->red.max_blocks));
 }
 #define LAUNCH_PAIRS(kernel, ...) kernel<<<pair_blocks(c), BLOCK, 0, c->stream>>>(__VA_ARGS__)
 

@@ -472,11 +472,20 @@ Fused* ensure_fused(Chunk* c, int max_iters)
 #endif
         F->point_blocks = launch_blocks(c, c->inner.ntiles);
         {
+            // Segment walks: at most one segment per warp, and at most one wave of the
+            // resident blocks, so that no partial second wave trails the first.
+            int occ_pair = occupancy(k_cg_sweep_b, 256);
+            occ_pair = std::min(occ_pair, occupancy(k_ppcg_sweep_b, 256));
+            occ_pair = std::min(occ_pair, occupancy(k_dc_update, 256));
+            const long wave_pair = (long)sms * occ_pair;
             const long warps = make_seg(g).nseg;  // one 64-cell segment per warp at most
             const long blocks = (warps + 7) / 8;
-            F->pair_blocks = (int)std::max<long>(1, std::min<long>(blocks, c->red.max_blocks));
+            F->pair_blocks =
+                (int)std::max<long>(1, std::min<long>(std::min<long>(blocks, wave_pair), c->red.max_blocks));
+            const long wave_quad = (long)sms * occupancy(k_cg32_sweep_b, 256);
             const long qwarps = (long)((g.nx + 127) / 128) * g.ny * g.nz;  // one 128-cell segment per warp
-            F->quad_blocks = (int)std::max<long>(1, std::min<long>((qwarps + 7) / 8, c->red.max_blocks));
+            F->quad_blocks =
+                (int)std::max<long>(1, std::min<long>(std::min<long>((qwarps + 7) / 8, wave_quad), c->red.max_blocks));
         }
     }
     if (F->cap < max_iters + 2) {
