@@ -647,9 +647,10 @@ def main():
                      "traffic": traffic, "alg_bytes_per_launch": g["alg_bytes"],
                      "launch_ms": g["kernel_ms"][dom], "kernel_ms": g["kernel_ms"]},
         "clocks": g["clocks"],
-        # 2 fused launches per CG iteration, 1 per Chebyshev iteration, and about 27
-        # per-call launches per timestep (set-up, halo updates, the switch, finalise).
-        "gpu_launches": int(sum(2 * c + h + 27 for c, h in zip(g["cg_steps"], g["cheby_steps"]))),
+        # 2 fused launches per CG iteration, 1 per two Chebyshev iterations (a launch ending
+        # at a convergence check may hold one), and about 27 per-call launches per timestep
+        # (set-up, halo updates, the switch, finalise).
+        "gpu_launches": int(sum(2 * c + (h + 1) // 2 + 27 for c, h in zip(g["cg_steps"], g["cheby_steps"]))),
         "cpu_baseline": cpu,
     }
     if e2e:
