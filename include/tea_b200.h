@@ -165,7 +165,8 @@ typedef struct {
     double eigmin, eigmax;  /* scaled eigenvalue bounds at the switch (0 if none) */
     int corrections;        /* FP32_REFINED: outer corrections */
     int warm_start_used;    /* 1 when the solve started from an attached network's guess */
-    double warm_r0_plain;   /* with a network attached: sum r^2 of the start u = u0 */
+    double warm_r0_plain;   /* with a network attached: sum r^2 of the start u = u0
+                               (0 on a timestep the back-off skipped) */
     double warm_r0_guess;   /* ... and of the start u = u0 + the network's du */
     double reserved[5];
 } tea_solve_result;
@@ -189,8 +190,10 @@ void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* params,
  * residual r0 = u0 - A u0, which scales input and output).  A chunk with a network
  * attached starts each ext_tea_leaf_solve_ from u0 + du, smoothed by 8 damped Jacobi
  * sweeps in FP64, when that start has the smaller FP64 residual (else from u0, as the
- * reference does) and converges to the same tolerance.  All functions return a TEA_*
- * status.
+ * reference does) and converges to the same tolerance.  After three rejected guesses in a
+ * row the chunk solves 4 timesteps without predicting, then tries again (8, 16, at most 32
+ * timesteps after further rejections); an accepted guess ends the back-off.  All functions
+ * return a TEA_* status.
  * --------------------------------------------------------------------------------- */
 
 /* New network with seeded He-initialised weights on the current device: levels 2..5,
@@ -209,8 +212,8 @@ int tea_ws_pairs_(const int* net, int* count);
  * beats u0 on average), and the device milliseconds per step. */
 int tea_ws_train_(const int* net, const int* steps, const int* batch, const int* crop, const double* lr,
                   const int* seed, double* loss_first, double* loss_last, double* ms_per_step);
-/* Attaches the network to a chunk (net 0 detaches); sides must be multiples of
- * 2^(levels-1) for the guess to be used. */
+/* Attaches the network to a chunk (net 0 detaches) and clears its back-off; sides must
+ * be multiples of 2^(levels-1) for the guess to be used. */
 int tea_ws_attach_(const int* chunk, const int* net);
 /* The network's du for the chunk's current step, into a host array [ny][nx], and the
  * device milliseconds of the prediction. */

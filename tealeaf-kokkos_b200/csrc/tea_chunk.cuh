@@ -81,6 +81,8 @@ struct Chunk {
     int device = 0;
     void* fused = nullptr;    // whole-solve state (tea_fused.cuh)
     void* ws = nullptr;       // attached warm-start network (tea_warmstart.cu), not owned
+    int ws_reject_streak = 0; // consecutive timesteps whose guess was rejected
+    int ws_skip = 0;          // timesteps left to solve without a guess (back-off)
     long long h2d_bytes = 0;  // host<->device bytes moved for this chunk (inputs, results)
     long long d2h_bytes = 0;
 };

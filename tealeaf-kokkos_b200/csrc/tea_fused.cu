@@ -813,10 +813,14 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
         eps = P->eps_rel * P->eps_rel * bb;
     }
     // Learned warm start (a network attached with tea_ws_attach_): keep u = u0 + du when its
-    // FP64 residual is smaller than that of u = u0, and restart CG from it.
+    // FP64 residual is smaller than that of u = u0, and restart CG from it.  After three
+    // rejected guesses in a row the prediction is skipped for 4 timesteps, then 8, 16 and
+    // at most 32 before the next try; an accepted guess ends the back-off.
     int ws_used = 0;
     double ws_r0_plain = 0.0, ws_r0_guess = 0.0;
-    if (c->ws && cg_like) {
+    const bool ws_try = c->ws && cg_like && c->ws_skip == 0;
+    if (c->ws && cg_like && c->ws_skip > 0) --c->ws_skip;
+    if (ws_try) {
         int one = 1;
         ext_calculate_2norm_(chunk, &ws_r0_plain, &one);  // r = u0 - A u0 after the set-up
         if (ws_predict_into(c, c->f.u)) {
@@ -831,8 +835,10 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
                 rro = ((volatile double*)c->h_out)[0];
                 c->d2h_bytes += sizeof(double);
                 ws_used = 1;
+                c->ws_reject_streak = 0;
                 halo(c, {5}, 1);
             } else {
+                if (++c->ws_reject_streak >= 3) c->ws_skip = 4 << std::min(c->ws_reject_streak - 3, 3);
                 // The set-up's state: inner u = u0 with its reflected halo, r = u0 - A u
                 // (the same operations as the set-up's r = u - A u), p and rro untouched.
                 k_ws_restore<<<launch_blocks(c, c->inner.ntiles), dim3(TILE_X, TILE_Y), 0, c->stream>>>(

@@ -1024,6 +1024,8 @@ TEA_EXPORT int tea_ws_attach_(const int* chunk, const int* net)
     Net* N = get_net(net);
     if (!N) return TEA_ERR_BAD_ARGUMENT;
     c->ws = N;
+    c->ws_reject_streak = 0;
+    c->ws_skip = 0;
     return TEA_OK;
 }
 
