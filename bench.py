@@ -55,10 +55,12 @@ WORDS = {  # algorithmic FP64 words per interior cell of one launch
     "cg_sweep_b": 3,   # read r, w; write r
     "cheby_iterate": 7,  # read u, u0, p, Kx, Ky; write u', p
     "cheby_pair": 7,  # the same words for two iterations (one pass)
+    "cheby_quad": 7,  # four iterations per pass: read u, u0, p, Kx, Ky; write u, p
 }
-KERNEL_IDS = {"cg_sweep_a": 2, "cheby_pair": 6, "cg_sweep_b": 5}
+KERNEL_IDS = {"cg_sweep_a": 2, "cheby_quad": 11, "cheby_pair": 6, "cg_sweep_b": 5}
 ALL_KERNEL_IDS = {"ppcg_inner": 1, "cg_sweep_a": 2, "cheby_iterate": 3, "jacobi": 4, "cg_sweep_b": 5,
-                  "cheby_pair": 6, "cg32_sweep_a": 7, "cg32_sweep_b": 8, "cheby32_pair": 9, "ppcg_pair": 10}
+                  "cheby_pair": 6, "cg32_sweep_a": 7, "cg32_sweep_b": 8, "cheby32_pair": 9, "ppcg_pair": 10,
+                  "cheby_quad": 11, "cheby32_quad": 12}
 PROFILES = ROOT / "profiles"
 # Per-timestep iteration counts of this deck (CG iterations before the Chebyshev switch,
 # Chebyshev iterations after it) for simulation steps 1..20, measured with this build; the
@@ -315,14 +317,17 @@ def gpu_arm(args, world, precision=0, kernels=True, ws_net=0):
     mean_cg = sum(cg) / len(cg)
     mean_ch = sum(cheby) / len(cheby)
     if kernels:
+        # Chebyshev iterations run four per pass, with a two-iteration pass ending at each
+        # convergence check (4 + 4 + 2 per 10 iterations once the checks start).
         share = {"cg_sweep_a": mean_cg * kernel_ms["cg_sweep_a"], "cg_sweep_b": mean_cg * kernel_ms["cg_sweep_b"],
-                 "cheby_pair": mean_ch / 2.0 * kernel_ms["cheby_pair"]}
+                 "cheby_quad": mean_ch / 5.0 * kernel_ms["cheby_quad"],
+                 "cheby_pair": mean_ch / 10.0 * kernel_ms["cheby_pair"]}
         dominant = max(share, key=share.get)
         alg_bytes = WORDS[dominant] * 8 * cells
     else:
         dominant, alg_bytes = None, None
-    # Chebyshev iterations run in pairs (one pass each), apart from convergence-check steps.
-    step_words = (WORDS["cg_sweep_a"] + WORDS["cg_sweep_b"]) * mean_cg + WORDS["cheby_pair"] * mean_ch / 2.0
+    # Chebyshev passes: 7 words per pass of four or two iterations (3 passes per 10 iterations).
+    step_words = (WORDS["cg_sweep_a"] + WORDS["cg_sweep_b"]) * mean_cg + WORDS["cheby_pair"] * mean_ch * 0.3
     return {
         "sec_per_step": sec_per_step, "ms_total": ms_max, "clocks": clock_info, "iterations": iters,
         "cg_steps": cg, "cheby_steps": cheby, "kernel_ms": kernel_ms, "dominant": dominant,
@@ -565,7 +570,7 @@ def kernel_only(args):
     # FP32 kernels: their FP32 words counted as half FP64 words.
     words = {"ppcg_inner": 8, "cg_sweep_a": 8, "cheby_iterate": 7, "jacobi": 5, "cg_sweep_b": 3,
              "cheby_pair": 7, "cg32_sweep_a": 4, "cg32_sweep_b": 1.5, "cheby32_pair": 3.5,
-             "ppcg_pair": 8}[args.kernel]
+             "ppcg_pair": 8, "cheby_quad": 7, "cheby32_quad": 3.5}[args.kernel]
     gbs = words * 8 * CELLS * CELLS / (ms.value / 1e3) / 1e9 if ms.value > 0 else None
     print(json.dumps({"kernel": args.kernel, "ms_per_launch": ms.value, "algorithmic_gbs": gbs}))
     lib.ext_finalise_()
@@ -647,10 +652,10 @@ def main():
                      "traffic": traffic, "alg_bytes_per_launch": g["alg_bytes"],
                      "launch_ms": g["kernel_ms"][dom], "kernel_ms": g["kernel_ms"]},
         "clocks": g["clocks"],
-        # 2 fused launches per CG iteration, 1 per two Chebyshev iterations (a launch ending
-        # at a convergence check may hold one), and about 27 per-call launches per timestep
-        # (set-up, halo updates, the switch, finalise).
-        "gpu_launches": int(sum(2 * c + (h + 1) // 2 + 27 for c, h in zip(g["cg_steps"], g["cheby_steps"]))),
+        # 2 fused launches per CG iteration, about 3 per 10 Chebyshev iterations (passes of
+        # four, and of two ending at each convergence check), and about 27 per-call launches
+        # per timestep (set-up, halo updates, the switch, finalise).
+        "gpu_launches": int(sum(2 * c + (3 * h + 9) // 10 + 27 for c, h in zip(g["cg_steps"], g["cheby_steps"]))),
         "cpu_baseline": cpu,
     }
     if e2e:

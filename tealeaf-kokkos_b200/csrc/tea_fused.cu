@@ -62,6 +62,8 @@ struct Fused {
     RingLaunch ring[RING_OPS];  // grid and segment rows of k_ring2d per sweep (2D)
     RingLaunch pair;            // k_cheby2_ring2d<OpCheby> (2D); blocks 0: one iteration per launch
     RingLaunch pair32;          // k_cheby2_ring2d<OpCheby32> (2D)
+    RingLaunch quad;            // k_cheby4_ring2d<OpCheby> (2D); blocks 0: pairs only
+    RingLaunch quad32;          // k_cheby4_ring2d<OpCheby32> (2D)
     RingLaunch ring3[RING_OPS]; // grid and z-segment planes of k_ring3d per sweep (3D)
     RingLaunch ppcg2;           // k_ppcg2_ring3d (3D) / k_ppcg2_ring2d (2D); blocks 0: single steps only
     int stencil_mode = 0;  // 0: the faster kernel per sweep, 1: register pipeline only, 2: ring only
@@ -121,6 +123,8 @@ int occupancy(K kernel, int threads)
 #if TEA_DIM == 2
 constexpr size_t ppcg2_2d_smem_bytes = (size_t)RWARPS * C2_RQ * C2_NA * Pair2Geom<double>::STRIP * sizeof(double);
 #endif
+
+constexpr bool kUseQuad = true;  // four-iteration Chebyshev passes (2D)
 
 // PPCG inner steps that run as two-step passes: an even number of pairs, none holding the
 // last step (which forms the 2-norm).
@@ -465,6 +469,10 @@ Fused* ensure_fused(Chunk* c, int max_iters)
                 const int occ3 =
                     smem_occupancy(k_cheby2_ring2d<OpCheby32>, (int)cheby2_smem_bytes<OpCheby32>());
                 F->pair32 = ring_launch(g, sms, occ3, Pair2Geom<float>::OUT, mb);
+                const int occq = smem_occupancy(k_cheby4_ring2d<OpCheby>, (int)cheby4_smem_bytes<OpCheby>());
+                F->quad = ring_launch(g, sms, occq, PassGeom<double, 4, C4_RP>::OUT, mb);
+                const int occq32 = smem_occupancy(k_cheby4_ring2d<OpCheby32>, (int)cheby4_smem_bytes<OpCheby32>());
+                F->quad32 = ring_launch(g, sms, occq32, PassGeom<float, 4, C4_RP>::OUT, mb);
                 const int occ4 = smem_occupancy(k_ppcg2_ring2d, (int)ppcg2_2d_smem_bytes);
                 F->ppcg2 = ring_launch(g, sms, occ4, Pair2Geom<double>::OUT, mb);
             }
@@ -545,6 +553,12 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         break;
     case LOOP_CHEBY:
 #if TEA_DIM == 2
+        if (F->quad.blocks > 0 && kUseQuad) {
+            FusedArgs ap = a;
+            ap.seg_rows = F->quad.rows;
+            k_cheby4_ring2d<OpCheby><<<F->quad.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby>(), s>>>(ap);
+            break;
+        }
         if (F->pair.blocks > 0) {
             FusedArgs ap = a;
             ap.seg_rows = F->pair.rows;
@@ -556,6 +570,13 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         break;
     case LOOP_CHEBY32:
 #if TEA_DIM == 2
+        if (F->quad32.blocks > 0 && kUseQuad) {
+            FusedArgs ap = a;
+            ap.seg_rows = F->quad32.rows;
+            k_cheby4_ring2d<OpCheby32>
+                <<<F->quad32.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby32>(), s>>>(ap);
+            break;
+        }
         if (F->pair32.blocks > 0) {
             FusedArgs ap = a;
             ap.seg_rows = F->pair32.rows;
@@ -1125,7 +1146,8 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
 // Measurement hook: `reps` back-to-back launches of one fused kernel on the chunk's
 // stream between two CUDA events, on the chunk's current fields (their values change).
 // kernel: 1 PPCG inner step, 2 CG/PPCG sweep A, 3 Chebyshev iteration, 4 Jacobi sweep,
-// 10 two PPCG inner steps in one pass (3D).
+// 10 two PPCG inner steps in one pass, 11/12 four Chebyshev iterations in one pass (2D,
+// FP64/FP32).
 TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const int* reps, double* ms_per_launch)
 {
     *ms_per_launch = 0.0;
@@ -1188,6 +1210,21 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
             break;
 #endif
 #if TEA_DIM == 2
+        case 11:
+        case 12:
+            if (F->quad.blocks > 0) {
+                FusedArgs ap = a;
+                if (*kernel == 11) {
+                    ap.seg_rows = F->quad.rows;
+                    k_cheby4_ring2d<OpCheby>
+                        <<<F->quad.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby>(), c->stream>>>(ap);
+                } else {
+                    ap.seg_rows = F->quad32.rows;
+                    k_cheby4_ring2d<OpCheby32>
+                        <<<F->quad32.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby32>(), c->stream>>>(ap);
+                }
+            }
+            break;
         case 10:
             if (F->ppcg2.blocks > 0) {
                 FusedArgs ap = a;

@@ -1705,31 +1705,44 @@ struct OpCheby {
         s.cheby_calc_steps = s.cheby_calc_steps + 1;
         end_iteration(a, s, PHASE_CHEBY);
     }
-    // Two-iteration kernel (k_cheby2_ring2d): a pair runs unless the first iteration is a
-    // convergence check (which must end a launch) or the last one max_iters allows.
-    __device__ bool pair_ok(const FusedArgs& a) const
+    // Passes of nit iterations (k_cheby2_ring2d, k_cheby4_ring2d): a pass runs unless one of
+    // its first nit - 1 iterations is a convergence check (which must end a launch) or it
+    // would go past max_iters.
+    __device__ bool pass_ok(const FusedArgs& a, int nit) const
     {
         const SolveState& st = *a.st;
-        return !((st.n >= st.est_itc) && (st.n % 10 == 0)) && st.n + 1 <= st.max_iters;
+        for (int k = 0; k < nit - 1; ++k) {
+            const int it = st.n + k;
+            if (it >= st.est_itc && it % 10 == 0) return false;
+        }
+        return st.n + nit - 1 <= st.max_iters;
     }
-    __device__ void pair_coefs(const FusedArgs& a, double& al2, double& be2, bool& check2) const
+    // Coefficients of the pass's iteration l (0-based).
+    __device__ void pass_coefs(const FusedArgs& a, int l, double& al_l, double& be_l) const
+    {
+        const int k = a.st->cheby_calc_steps - 1 + l;
+        al_l = a.ch_alphas[k];
+        be_l = a.ch_betas[k];
+    }
+    __device__ bool pass_check(const FusedArgs& a, int nit) const
     {
         const SolveState& st = *a.st;
-        al2 = a.ch_alphas[st.cheby_calc_steps];
-        be2 = a.ch_betas[st.cheby_calc_steps];
-        check2 = (st.n + 1 >= st.est_itc) && ((st.n + 1) % 10 == 0);
+        const int it = st.n + nit - 1;
+        return it >= st.est_itc && it % 10 == 0;
     }
     __device__ const double* pair_rhs(const FusedArgs& a) const { return a.u0; }
     __device__ const double* pair_mi(const FusedArgs& a) const { return precond ? a.mi : nullptr; }
-    __device__ void pair_control(const FusedArgs& a, const double* v, bool check2) const
+    __device__ void pass_control(const FusedArgs& a, const double* v, int nit, bool check_last) const
     {
         if (a.timing) return;
         SolveState& s = *a.st;
         s.par_u ^= 1;
         s.par_p ^= 1;
-        s.cheby_calc_steps = s.cheby_calc_steps + 1;
-        end_iteration(a, s, PHASE_CHEBY);  // cannot end the loop (pair_ok)
-        if (check2) s.error = v[0];
+        for (int k = 0; k < nit - 1; ++k) {
+            s.cheby_calc_steps = s.cheby_calc_steps + 1;
+            end_iteration(a, s, PHASE_CHEBY);  // cannot end the loop (pass_ok)
+        }
+        if (check_last) s.error = v[0];
         s.cheby_calc_steps = s.cheby_calc_steps + 1;
         end_iteration(a, s, PHASE_CHEBY);
     }
@@ -1778,33 +1791,51 @@ constexpr size_t cheby2_smem_bytes()
         : ring_smem_bytes<Op>();
 }
 
-// Op: OpCheby (FP64, the reference's iteration) or OpCheby32 (the FP32 inner solve).
-template <class Op>
-__global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
+// NIT Chebyshev iterations in one pass over the 2D field (temporal blocking), the
+// generalisation of the two-iteration pass above.  Level l (iteration l of the pass) is
+// computed one row behind level l - 1: at loop step t, level l is at row t - l + 1, so
+// each level reads the three rows of level l - 1 it needs from registers.  Each level loses
+// one cell of its strip on each side, so a warp writes the cells of lanes FL .. 31 - FL
+// (FL = ceil(NIT / VEC)), OUT = (32 - 2 FL) * VEC columns per strip, and row segments
+// overlap by NIT - 1 rows.  At the domain's edges every level uses the cell's own value
+// as its outside neighbour, which is what the reference's halo update after each iteration
+// gives.  u and p go to the other buffers, as in the pair.  Per cell the operations and
+// their order are those of NIT single iterations, so results are bit-identical.
+template <class T, int NIT, int RPN>
+struct PassGeom {
+    static constexpr int VEC = RingGeom<T>::VEC;
+    static constexpr int STRIP = RingGeom<T>::STRIP;
+    static constexpr int FL = (NIT + VEC - 1) / VEC;  // first lane that writes
+    static constexpr int OUT = (32 - 2 * FL) * VEC;
+    static constexpr int RQ = NIT + RPN + 1;           // ring rows per warp
+};
+
+template <class Op, int NIT, int RPN>
+constexpr size_t chebyN_smem_bytes()
 {
     using T = typename Op::T;
-    constexpr int VEC = Pair2Geom<T>::VEC, STRIP = Pair2Geom<T>::STRIP, OUT = Pair2Geom<T>::OUT;
-    extern __shared__ __align__(16) unsigned char s_ring_raw[];
-    Op op;
-    op.begin(a);
-    if (!op.pair_ok(a)) {
-        ring2d_body(a, op, s_ring_raw);
-        return;
-    }
-    const T al1 = op.al, be1 = op.be;
-    T al2, be2;
-    bool check2;
-    op.pair_coefs(a, al2, be2, check2);
+    return (size_t)RWARPS * PassGeom<T, NIT, RPN>::RQ * C2_NA * PassGeom<T, NIT, RPN>::STRIP * sizeof(T);
+}
+
+template <class Op, int NIT, int RPN>
+__device__ __forceinline__ void chebyN_body(const FusedArgs& a, Op& op, unsigned char* s_ring_raw)
+{
+    using T = typename Op::T;
+    using G = PassGeom<T, NIT, RPN>;
+    constexpr int VEC = G::VEC, STRIP = G::STRIP, OUT = G::OUT, FL = G::FL, RQ = G::RQ;
+    T al[NIT], be[NIT];
+#pragma unroll
+    for (int l = 0; l < NIT; ++l) op.pass_coefs(a, l, al[l], be[l]);
+    const bool checkN = op.pass_check(a, NIT);
     const T* mi = op.pair_mi(a);
     const bool precond = mi != nullptr;
-    const T* ucur = op.ucur;
     T* unew = op.unew;
     T* pnew = op.pnext;
     const Geom& g = a.g;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * C2_RQ * C2_NA * STRIP;
-    const T* src[C2_NA] = {ucur, op.pair_rhs(a), op.pcur, mi, op.coef_x(a), op.coef_y(a)};
+    T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * RQ * C2_NA * STRIP;
+    const T* src[C2_NA] = {op.ucur, op.pair_rhs(a), op.pcur, mi, op.coef_x(a), op.coef_y(a)};
     DDVec<1> acc;
     acc.zero();
     const int xlast = g.X - HALO_PAD - 1;
@@ -1814,20 +1845,21 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
     const long nseg = (long)per_x * per_y;
     const long gw = (long)blockIdx.x * RWARPS + warp, nw = (long)gridDim.x * RWARPS;
     const int cmax = (int)g.pitch - 2 * VEC + 2;
-    const bool out_lane = lane >= 1 && lane <= 30;
+    const bool out_lane = lane >= FL && lane <= 31 - FL;
     const T zero = (T)0;
     for (long sgi = gw; sgi < nseg; sgi += nw) {
         const int xs = (int)(sgi % per_x), ys = (int)(sgi / per_x);
-        const int c = OUT * xs + VEC * lane - (VEC - 2);  // the lane's first column
-        // Lane 0 of the first strip starts left of column 0 (FP32: at column -2): it only feeds
-        // lane 1, whose first cell is the first inner column and reflects there, so any in-row
-        // data will do; it copies from c + VEC, which keeps the 16-byte alignment (c mod VEC).
+        // Lane FL of the strip starts at its first output column; lanes left of it in the
+        // first strip start left of column 0 and only feed cells whose outside neighbour is
+        // their own value, so they copy from c + VEC (in-row, 16-byte aligned).
+        const int c = OUT * xs + VEC * (lane - FL) + HALO_PAD;
         const int cc = min(c < 0 ? c + VEC : c, cmax);
         const int j0 = HALO_PAD + a.seg_rows * ys;
         const int j1 = min(j0 + a.seg_rows, ylast + 1);
-        const int a0 = j0 == HALO_PAD ? HALO_PAD : j0 - 1;  // first row of iteration 1
-        const int rlast = min(j1 + 1, ylast + 1);             // last ring row
-        auto slot = [&](int r) { return ring + (size_t)((r - a0 + 1) % C2_RQ) * C2_NA * STRIP; };
+        const int a0 = max(HALO_PAD, j0 - (NIT - 1));        // first row of level 1
+        const int t_last = j1 + NIT - 2;                    // level NIT reaches row j1 - 1
+        const int rlast = min(t_last + 1, ylast + 1);       // last ring row
+        auto slot = [&](int r) { return ring + (size_t)((r - a0 + 1) % RQ) * C2_NA * STRIP; };
         auto issue = [&](int r) {
             if (r <= rlast) {
                 T* base = slot(r);
@@ -1841,119 +1873,139 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
             }
             cp_async_commit();
         };
-        for (int r = a0 - 1; r <= a0 + C2_RP + 1; ++r) issue(r);
-        cp_async_wait<C2_RP + 1>();
+        // One level at row s: the operand rows (m: s-1, cv: s, n: s+1) of the level below,
+        // its p at row s, and the ring row s (and s+1 for Ky).  Returns u and p of the level.
+        auto level = [&](int l, int s, const T* m, const T* cv, const T* n, const T* pin, T* uo, T* po, bool last) {
+            // Rows above the segment's first ring row are never needed (s is uniform in the
+            // warp, so the shuffles below stay warp-uniform).
+            if (s < a0 || s > ylast) return;
+            const T* rs = slot(s);
+            const T* rs1 = slot(s + 1);
+            const T up = __shfl_up_sync(0xffffffffu, cv[VEC - 1], 1);
+            const T dn = __shfl_down_sync(0xffffffffu, cv[0], 1);
+            T kx[VEC + 1];
+            ld_vec(rs + C2_KX * STRIP + VEC * lane, kx);
+            kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
+            T ky0[VEC], ky1[VEC], rhs[VEC], m0[VEC];
+            ld_vec(rs + C2_KY * STRIP + VEC * lane, ky0);
+            ld_vec(rs1 + C2_KY * STRIP + VEC * lane, ky1);
+            ld_vec(rs + C2_U0 * STRIP + VEC * lane, rhs);
+            if (precond) ld_vec(rs + C2_MI * STRIP + VEC * lane, m0);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                NbT<T> nb;
+                nb.zm = nb.zp = zero;
+                nb.c = cv[q];
+                nb.xm = c + q == HALO_PAD ? cv[q] : (q == 0 ? up : cv[q > 0 ? q - 1 : 0]);
+                nb.xp = c + q == xlast ? cv[q] : (q == VEC - 1 ? dn : cv[q < VEC - 1 ? q + 1 : q]);
+                nb.ym = s == HALO_PAD ? cv[q] : m[q];
+                nb.yp = s == ylast ? cv[q] : n[q];
+                const T w = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], zero, zero);
+                const T r = rhs[q] - w;
+                po[q] = al[l] * pin[q] + be[l] * (precond ? m0[q] * r : r);
+                uo[q] = cv[q] + po[q];
+                if (last && checkN && out_lane && c + q <= xlast) dd_add(acc.v[0], (double)r * (double)r);
+            }
+        };
+        // Rows a0 - 1 .. a0 + RPN + 1 first; each step then issues the next new row, so row
+        // t + 1 has exactly RPN groups after it at the top of step t.
+        for (int r = a0 - 1; r <= a0 + RPN + 1; ++r) issue(r);
+        cp_async_wait<RPN + 1>();
         __syncwarp();
-        // u at rows t-1 (um) and t (uc); iteration-1 u at rows t-2 (vm) and t-1 (vc); its p at t-1 (qv).
-        T um[VEC], uc[VEC], vm[VEC], vc[VEC], qv[VEC];
+        T um[VEC], uc[VEC];
         ld_vec(slot(a0 - 1) + C2_U * STRIP + VEC * lane, um);
         ld_vec(slot(a0) + C2_U * STRIP + VEC * lane, uc);
+        // Level L (iteration L + 1) keeps its u at rows s - 1 (M) and s (C) and its p at row
+        // s (P), where s is the row it reached at the previous step.
+        T M[NIT][VEC], C[NIT][VEC], P[NIT][VEC];
 #pragma unroll
-        for (int q = 0; q < VEC; ++q) vm[q] = vc[q] = qv[q] = zero;
-        for (int t = a0; t <= j1; ++t) {
-            cp_async_wait<C2_RP>();
+        for (int l = 0; l < NIT; ++l)
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) M[l][q] = C[l][q] = P[l][q] = zero;
+        for (int t = a0; t <= t_last; ++t) {
+            cp_async_wait<RPN>();
             __syncwarp();
-            const T* rp = slot(t - 1);
-            const T* rc = slot(t);
-            const T* rn = slot(t + 1);
-            T un[VEC];
-            ld_vec(rn + C2_U * STRIP + VEC * lane, un);
-            // Iteration 1 at row t.
-            T v[VEC], pv[VEC];
-            if (t <= ylast) {
-                T kx[VEC + 1], ky0[VEC], ky1[VEC], u0[VEC], p0[VEC], m0[VEC];
-                ld_vec(rc + C2_KX * STRIP + VEC * lane, kx);
-                kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
-                ld_vec(rc + C2_KY * STRIP + VEC * lane, ky0);
-                ld_vec(rn + C2_KY * STRIP + VEC * lane, ky1);
-                ld_vec(rc + C2_U0 * STRIP + VEC * lane, u0);
-                ld_vec(rc + C2_P * STRIP + VEC * lane, p0);
-                if (precond) ld_vec(rc + C2_MI * STRIP + VEC * lane, m0);
-                const T up = __shfl_up_sync(0xffffffffu, uc[VEC - 1], 1);
-                const T dn = __shfl_down_sync(0xffffffffu, uc[0], 1);
+            T un[VEC], p0[VEC];
+            ld_vec(slot(t + 1) + C2_U * STRIP + VEC * lane, un);
+            ld_vec(slot(t) + C2_P * STRIP + VEC * lane, p0);
+            T N[NIT][VEC], PN[NIT][VEC];
 #pragma unroll
-                for (int q = 0; q < VEC; ++q) {
-                    NbT<T> nb;
-                    nb.zm = nb.zp = zero;
-                    nb.c = uc[q];
-                    nb.xm = c + q == HALO_PAD ? uc[q] : (q == 0 ? up : uc[q > 0 ? q - 1 : 0]);
-                    nb.xp = c + q == xlast ? uc[q] : (q == VEC - 1 ? dn : uc[q < VEC - 1 ? q + 1 : q]);
-                    nb.ym = um[q];
-                    nb.yp = un[q];
-                    const T w = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], zero, zero);
-                    const T r = u0[q] - w;
-                    pv[q] = al1 * p0[q] + be1 * (precond ? m0[q] * r : r);
-                    v[q] = uc[q] + pv[q];
-                }
-            } else {
-                // Row ylast + 1 is the halo: the reflection of row ylast.
+            for (int l = 0; l < NIT; ++l)
 #pragma unroll
-                for (int q = 0; q < VEC; ++q) {
-                    v[q] = vc[q];
-                    pv[q] = zero;
-                }
+                for (int q = 0; q < VEC; ++q) N[l][q] = PN[l][q] = zero;
+            level(0, t, um, uc, un, p0, N[0], PN[0], NIT == 1 && t >= j0);
+#pragma unroll
+            for (int l = 1; l < NIT; ++l) {
+                const int s = t - l;
+                level(l, s, M[l - 1], C[l - 1], N[l - 1], P[l - 1], N[l], PN[l], l == NIT - 1 && s >= j0);
             }
-            if (t == HALO_PAD) {
-                // Row 1 is the halo: the reflection of row 2.
-#pragma unroll
-                for (int q = 0; q < VEC; ++q) vc[q] = v[q];
-            }
-            // Iteration 2 at row s = t - 1.
-            const int srow = t - 1;
-            if (srow >= j0) {
-                T kx[VEC + 1], ky0[VEC], ky1[VEC], u0[VEC], m0[VEC], u2[VEC], p2[VEC];
-                ld_vec(rp + C2_KX * STRIP + VEC * lane, kx);
-                kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
-                ld_vec(rp + C2_KY * STRIP + VEC * lane, ky0);
-                ld_vec(rc + C2_KY * STRIP + VEC * lane, ky1);
-                ld_vec(rp + C2_U0 * STRIP + VEC * lane, u0);
-                if (precond) ld_vec(rp + C2_MI * STRIP + VEC * lane, m0);
-                const T up = __shfl_up_sync(0xffffffffu, vc[VEC - 1], 1);
-                const T dn = __shfl_down_sync(0xffffffffu, vc[0], 1);
-                const long i = fidx(g, c, srow, 0);
-#pragma unroll
-                for (int q = 0; q < VEC; ++q) {
-                    NbT<T> nb;
-                    nb.zm = nb.zp = zero;
-                    nb.c = vc[q];
-                    nb.xm = c + q == HALO_PAD ? vc[q] : (q == 0 ? up : vc[q > 0 ? q - 1 : 0]);
-                    nb.xp = c + q == xlast ? vc[q] : (q == VEC - 1 ? dn : vc[q < VEC - 1 ? q + 1 : q]);
-                    nb.ym = vm[q];
-                    nb.yp = v[q];
-                    const T w = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], zero, zero);
-                    const T r = u0[q] - w;
-                    p2[q] = al2 * qv[q] + be2 * (precond ? m0[q] * r : r);
-                    u2[q] = vc[q] + p2[q];
-                    if (check2 && out_lane && c + q <= xlast) dd_add(acc.v[0], (double)r * (double)r);
-                }
-                if (out_lane && c + VEC - 1 <= xlast) {
-                    st_vec(unew + i, u2);
-                    st_vec(pnew + i, p2);
-                } else if (out_lane) {
+            const int sl = t - NIT + 1;  // the row the last level reached
+            if (sl >= j0 && sl <= ylast && out_lane) {
+                const long i = fidx(g, c, sl, 0);
+                if (c + VEC - 1 <= xlast) {
+                    st_vec(unew + i, N[NIT - 1]);
+                    st_vec(pnew + i, PN[NIT - 1]);
+                } else {
 #pragma unroll
                     for (int q = 0; q < VEC; ++q) {
                         if (c + q <= xlast) {
-                            unew[i + q] = u2[q];
-                            pnew[i + q] = p2[q];
+                            unew[i + q] = N[NIT - 1][q];
+                            pnew[i + q] = PN[NIT - 1][q];
                         }
                     }
                 }
             }
 #pragma unroll
+            for (int l = 0; l < NIT; ++l)
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    M[l][q] = C[l][q];
+                    C[l][q] = N[l][q];
+                    P[l][q] = PN[l][q];
+                }
+#pragma unroll
             for (int q = 0; q < VEC; ++q) {
-                vm[q] = vc[q];
-                vc[q] = v[q];
-                qv[q] = pv[q];
                 um[q] = uc[q];
                 uc[q] = un[q];
             }
             __syncwarp();
-            issue(t + C2_RP + 2);  // into the slot of row t - 1, which no lane reads any more
+            issue(t + RPN + 2);  // into the slot of row t - NIT + 1, which no lane reads any more
         }
         cp_async_wait<0>();
         __syncwarp();
     }
-    grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.pair_control(a, v, check2); });
+    grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.pass_control(a, v, NIT, checkN); });
+}
+
+// Op: OpCheby (FP64, the reference's iteration) or OpCheby32 (the FP32 inner solve).  Two
+// iterations when the state allows (pass_ok), else one.
+template <class Op>
+__global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
+{
+    extern __shared__ __align__(16) unsigned char s_ring_raw[];
+    Op op;
+    op.begin(a);
+    if (op.pass_ok(a, 2)) chebyN_body<Op, 2, C2_RP>(a, op, s_ring_raw);
+    else ring2d_body(a, op, s_ring_raw);
+}
+
+// Four iterations when the state allows, else two, else one.
+constexpr int C4_RP = 1;  // ring rows in flight beyond row t+1 in the four-iteration pass
+template <class Op>
+constexpr size_t cheby4_smem_bytes()
+{
+    return chebyN_smem_bytes<Op, 4, C4_RP>() > cheby2_smem_bytes<Op>() ? chebyN_smem_bytes<Op, 4, C4_RP>()
+                                                                          : cheby2_smem_bytes<Op>();
+}
+template <class Op>
+__global__ void __launch_bounds__(RWARPS * 32) k_cheby4_ring2d(FusedArgs a)
+{
+    extern __shared__ __align__(16) unsigned char s_ring_raw[];
+    Op op;
+    op.begin(a);
+    if (op.pass_ok(a, 4)) chebyN_body<Op, 4, C4_RP>(a, op, s_ring_raw);
+    else if (op.pass_ok(a, 2)) chebyN_body<Op, 2, C2_RP>(a, op, s_ring_raw);
+    else ring2d_body(a, op, s_ring_raw);
 }
 
 // Two PPCG inner steps in one pass over the 2D field (temporal blocking), the 2D form of
@@ -2631,24 +2683,30 @@ struct OpCheby32 {
         s.n_inner = j + 1;
         finish(a, s, check != 0, v[0]);
     }
-    // Two-iteration kernel: a pair unless iteration j is a check or the last allowed.
-    __device__ bool pair_ok(const FusedArgs&) const { return (j % 10 != 0) && j + 1 < jmax; }
-    __device__ void pair_coefs(const FusedArgs& a, float& al2, float& be2, bool& check2) const
+    // Passes of nit iterations: none of iterations j .. j + nit - 2 is a check and the pass
+    // stays below the correction's limit.
+    __device__ bool pass_ok(const FusedArgs&, int nit) const
     {
-        al2 = (float)a.ch_alphas[j];
-        be2 = (float)a.ch_betas[j];
-        check2 = ((j + 1) % 10 == 0);
+        for (int k = 0; k < nit - 1; ++k)
+            if ((j + k) % 10 == 0) return false;
+        return j + nit - 1 < jmax;
     }
+    __device__ void pass_coefs(const FusedArgs& a, int l, float& al_l, float& be_l) const
+    {
+        al_l = (float)a.ch_alphas[j - 1 + l];
+        be_l = (float)a.ch_betas[j - 1 + l];
+    }
+    __device__ bool pass_check(const FusedArgs&, int nit) const { return (j + nit - 1) % 10 == 0; }
     __device__ const float* pair_rhs(const FusedArgs& a) const { return a.r32; }
     __device__ const float* pair_mi(const FusedArgs&) const { return nullptr; }
-    __device__ void pair_control(const FusedArgs& a, const double* v, bool check2) const
+    __device__ void pass_control(const FusedArgs& a, const double* v, int nit, bool check_last) const
     {
         if (a.timing) return;
         SolveState& s = *a.st;
         s.par_u ^= 1;
         s.par_p ^= 1;
-        s.n_inner = j + 2;
-        finish(a, s, check2, v[0]);
+        s.n_inner = j + nit;
+        finish(a, s, check_last, v[0]);
     }
 };
 

@@ -81,3 +81,20 @@ def test_fused_ppcg_inner_step_splits(dim, inner):
     for a, b in zip(fused, percall):
         for k in FIELDS:
             assert same(a[k], b[k]), f"{dim}D {inner} inner steps, step {a['step']} {k}: {a[k]!r} vs {b[k]!r}"
+
+
+def test_fused_chebyshev_2048_equals_per_call():
+    """A 2048^2 Chebyshev timestep, fused against per-call bit for bit.  The small golden
+    decks run the multi-iteration passes on few, short segments; at this size every warp
+    streams a long segment under full memory load, where an asynchronous copy read before
+    it has landed would show (a four-iteration pass with a miscounted copy schedule passed
+    every small deck and failed here)."""
+    spec = tea.DeckSpec(dim=2, cells=2048, states=16, seed=2048, solver="chebyshev", end_step=1, dt=0.004,
+                        eps=1e-15, eps_rel=1e-10, max_iters=20000, presteps=30, summary_frequency=1,
+                        check_result=False)
+    deck = tea.seeded_deck(spec)
+    sf, rf = tea.run_deck(deck, 2, fused=True, summary_every_step=True)
+    sp, rp = tea.run_deck(deck, 2, summary_every_step=True)
+    assert rf[0]["cheby_steps"] > 100  # the Chebyshev phase ran
+    for k in FIELDS:
+        assert same(rf[0][k], rp[0][k]), f"{k}: fused {rf[0][k]!r} per-call {rp[0][k]!r}"
