@@ -124,8 +124,6 @@ int occupancy(K kernel, int threads)
 constexpr size_t ppcg2_2d_smem_bytes = (size_t)RWARPS * C2_RQ * C2_NA * Pair2Geom<double>::STRIP * sizeof(double);
 #endif
 
-constexpr bool kUseQuad = true;  // four-iteration Chebyshev passes (2D)
-
 // PPCG inner steps that run as two-step passes: an even number of pairs, none holding the
 // last step (which forms the 2-norm).
 // Two-step PPCG passes per outer iteration: every step in pairs when the count is even (the
@@ -553,7 +551,7 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         break;
     case LOOP_CHEBY:
 #if TEA_DIM == 2
-        if (F->quad.blocks > 0 && kUseQuad) {
+        if (F->quad.blocks > 0) {
             FusedArgs ap = a;
             ap.seg_rows = F->quad.rows;
             k_cheby4_ring2d<OpCheby><<<F->quad.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby>(), s>>>(ap);
@@ -570,7 +568,7 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         break;
     case LOOP_CHEBY32:
 #if TEA_DIM == 2
-        if (F->quad32.blocks > 0 && kUseQuad) {
+        if (F->quad32.blocks > 0) {
             FusedArgs ap = a;
             ap.seg_rows = F->quad32.rows;
             k_cheby4_ring2d<OpCheby32>
