@@ -124,6 +124,9 @@ int occupancy(K kernel, int threads)
 constexpr size_t ppcg2_2d_smem_bytes = (size_t)RWARPS * C2_RQ * C2_NA * Pair2Geom<double>::STRIP * sizeof(double);
 #endif
 
+// CG iterations per launch of the while node's body.
+constexpr int kCgUnroll = 4;
+
 // PPCG inner steps that run as two-step passes: an even number of pairs, none holding the
 // last step (which forms the 2-norm).
 // Two-step PPCG passes per outer iteration: every step in pairs when the count is even (the
@@ -546,8 +549,13 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
     cudaStream_t s = c->stream;
     switch (kind) {
     case LOOP_CG:
-        stencil<OpSweepA>(F, a, s);
-        k_cg_sweep_b<<<F->pair_blocks, 256, 0, s>>>(a);
+        // Unrolled: the while node relaunches its body once per kCgUnroll iterations.  Once
+        // an iteration ends the loop (cont = 0), the kernels of the later copies return at
+        // once, so the iterations run are exactly those of the rolled loop.
+        for (int k = 0; k < kCgUnroll; ++k) {
+            stencil<OpSweepA>(F, a, s);
+            k_cg_sweep_b<<<F->pair_blocks, 256, 0, s>>>(a);
+        }
         break;
     case LOOP_CHEBY:
 #if TEA_DIM == 2
@@ -691,6 +699,7 @@ void pull_state(Chunk* c, Fused* F)
 // Run loop `kind` from the current state until its exit; the host state is refreshed.
 void run_loop(Chunk* c, Fused* F, int kind, int inner_steps)
 {
+    F->h_st->cont = 1;  // the body runs at least once (the while node's default)
     push_state(c, F);
     if (F->use_graph && build_loop(c, F, kind, inner_steps)) {
         TEA_CK(cudaGraphLaunch(F->loops[kind].exec, c->stream));
@@ -1164,6 +1173,7 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
     F->h_st->pending_p = 1;
     F->h_st->pending_u = 1;
     F->h_st->n = 1;
+    F->h_st->cont = 1;
     F->h_st->est_itc = 1 << 30;
     F->h_st->max_iters = std::max(F->h_st->max_iters, 2);
     F->h_st->cheby_calc_steps = 1;

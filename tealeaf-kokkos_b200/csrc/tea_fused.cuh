@@ -1023,7 +1023,8 @@ struct OpSweepA {
     double* pnew;
     double beta, alpha;
     int pend_p, pend_u, precond;
-    __device__ bool skip(const FusedArgs&) { return false; }
+    // An unrolled copy of the CG loop's body after the loop has ended (see enqueue_body).
+    __device__ bool skip(const FusedArgs& a) { return a.st->cont == 0; }
     __device__ void begin(const FusedArgs& a)
     {
         const SolveState& s = *a.st;
@@ -1164,6 +1165,7 @@ __device__ __forceinline__ void st2(double* p, double a, double b) { *reinterpre
 // rrn = sum r.r or r.z; then beta = rrn/rro and the end-of-iteration test.
 __global__ void __launch_bounds__(256) k_cg_sweep_b(FusedArgs a)
 {
+    if (a.st->cont == 0) return;  // an unrolled copy after the loop has ended (uniform)
     const SolveState& s = *a.st;
     const double alpha = s.alpha;
     const int precond = s.precond;
