@@ -652,10 +652,12 @@ def main():
                      "traffic": traffic, "alg_bytes_per_launch": g["alg_bytes"],
                      "launch_ms": g["kernel_ms"][dom], "kernel_ms": g["kernel_ms"]},
         "clocks": g["clocks"],
-        # 2 fused launches per CG iteration, about 3 per 10 Chebyshev iterations (passes of
-        # four, and of two ending at each convergence check), and about 27 per-call launches
-        # per timestep (set-up, halo updates, the switch, finalise).
-        "gpu_launches": int(sum(2 * c + (3 * h + 9) // 10 + 27 for c, h in zip(g["cg_steps"], g["cheby_steps"]))),
+        # 8 fused launches per four CG iterations (the graph's loop body holds four; the
+        # launches after the last iteration return at once), about 3 per 10 Chebyshev
+        # iterations (passes of four, and of two ending at each convergence check), and
+        # about 27 per-call launches per timestep (set-up, halo updates, the switch, finalise).
+        "gpu_launches": int(sum(8 * ((c + 3) // 4) + (3 * h + 9) // 10 + 27
+                                for c, h in zip(g["cg_steps"], g["cheby_steps"]))),
         "cpu_baseline": cpu,
     }
     if e2e:
