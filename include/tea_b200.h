@@ -56,7 +56,8 @@ int tea_chunk_dims_(const int* chunk, int* dims);
 int tea_read_field_(const int* chunk, const int* field, double* out);
 int tea_write_field_(const int* chunk, const int* field, const double* in);
 
-/* Last recorded status (0 = TEA_OK) and clear it. */
+/* Last recorded status (0 = TEA_OK) and clear it.  Waits for the kernels still queued
+ * on every chunk's stream first, so that their faults are included. */
 void ext_get_status_(int* status);
 /* Message for the last non-zero status (empty string if none). */
 const char* tea_last_error(void);

@@ -5,9 +5,12 @@
  * 2D extension layer (crtrott/TeaLeaf-Kokkos, tealeaf_2d/ext_chunk.cpp and
  * tealeaf_2d/ext_core.cpp), cited per entry.  Signatures, argument meaning and
  * call order are the reference's: gfortran name mangling (trailing underscore),
- * every argument by pointer, 1-based chunk ids, every call synchronous.  The
- * fields live in device memory (one B200) instead of Kokkos Views; results are
- * the same numbers (see the parity tests).
+ * every argument by pointer, 1-based chunk ids.  A call that returns data to the
+ * host (a reduction, the field summary, a packed face) returns when its kernels
+ * have finished; a call that only updates fields returns when its kernels are
+ * queued on the chunk's stream, like the reference's Kokkos parallel_for
+ * (tealeaf_2d/ext_core.cpp:21-24).  The fields live in device memory (one B200)
+ * instead of Kokkos Views; results are the same numbers (see the parity tests).
  *
  * Two arguments are declared `bool*` in the reference but receive Fortran
  * INTEGER literals 1/0 from the driver (tealeaf_2d/tea_solve.f90:262,670); they

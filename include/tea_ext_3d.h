@@ -4,7 +4,8 @@
  * Each declaration replaces the same-named extern "C" function of the reference's
  * 3D extension layer (crtrott/TeaLeaf-Kokkos, tealeaf_3d/ext_chunk.cpp and
  * tealeaf_3d/ext_core.cpp), cited per entry.  Conventions as in tea_ext_2d.h:
- * gfortran mangling, by-pointer arguments, 1-based chunk ids, synchronous calls;
+ * gfortran mangling, by-pointer arguments, 1-based chunk ids, field-only calls
+ * returning once their kernels are queued;
  * `bool*` arguments of the reference are `const void*` read by their first byte.
  * The 3D ABI differs from the 2D one in ext_init_ (z extent), ext_initialise_chunk_
  * (zMin, dz), ext_generate_chunk_ (stateZMin/stateZMax), ext_pack_message_

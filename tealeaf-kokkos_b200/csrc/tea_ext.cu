@@ -1,7 +1,9 @@
 // The drop-in C ABI of the TeaLeaf B200 library (include/tea_ext_2d.h, tea_ext_3d.h,
 // tea_b200.h).  Compiled once per dimension: -DTEA_DIM=2 -> libtea2d_b200.so,
-// -DTEA_DIM=3 -> libtea3d_b200.so.  Every entry point is synchronous, like the
-// reference's (each Kokkos dispatch there ends with a fence or a reduction copy-back).
+// -DTEA_DIM=3 -> libtea3d_b200.so.  An entry point that hands data to the host (a
+// reduction, a field summary, a packed face, a field read) returns once its kernels have
+// finished; one that only updates fields returns once they are queued on the chunk's
+// stream, as the reference's Kokkos parallel_for dispatches do (tealeaf_2d/ext_core.cpp:21-24).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -53,6 +55,14 @@ void sync(Chunk* c)
 {
     TEA_CK(cudaGetLastError());
     TEA_CK(cudaStreamSynchronize(c->stream));
+}
+
+// End of an entry point that only updates fields: launch errors are reported now, faults
+// inside its kernels at the next synchronisation (the next reduction, field read or
+// ext_get_status_).
+static void issued(Chunk*)
+{
+    TEA_CK(cudaGetLastError());
 }
 
 Chunk* create_chunk(int nx, int ny, int nz, int rank)
@@ -336,7 +346,7 @@ void update_halo(Chunk* c, const int* neighbours, const int* fields, int depth)
         bx = std::min<long>(bx, 4096);
         k_update_halo<<<dim3((unsigned)std::max<long>(bx, 1), job.nseg), threads, 0, c->stream>>>(c->g, job);
     }
-    sync(c);
+    issued(c);
 }
 
 }  // namespace tea
@@ -523,7 +533,7 @@ TEA_EXPORT void ext_set_field_kernel_(const int* chunk)
     Chunk* c = get_chunk(chunk);
     if (!c) return;
     LAUNCH(k_set_field, c->full, c->g, c->full, c->f);
-    sync(c);
+    issued(c);
 }
 
 TEA_EXPORT void ext_solver_copy_u_(const int* chunk)
@@ -531,7 +541,7 @@ TEA_EXPORT void ext_solver_copy_u_(const int* chunk)
     Chunk* c = get_chunk(chunk);
     if (!c) return;
     LAUNCH_PAIRS(k_copy_u, c->g, c->f);
-    sync(c);
+    issued(c);
 }
 
 TEA_EXPORT void ext_calculate_residual_(const int* chunk)
@@ -539,7 +549,7 @@ TEA_EXPORT void ext_calculate_residual_(const int* chunk)
     Chunk* c = get_chunk(chunk);
     if (!c) return;
     LAUNCH_PAIRS(k_residual, c->g, c->f);
-    sync(c);
+    issued(c);
 }
 
 TEA_EXPORT void ext_calculate_2norm_(const int* chunk, double* norm, const void* normArray)
@@ -556,7 +566,7 @@ TEA_EXPORT void ext_solver_finalise_(const int* chunk)
     Chunk* c = get_chunk(chunk);
     if (!c) return;
     LAUNCH_PAIRS(k_finalise, c->g, c->f);
-    sync(c);
+    issued(c);
 }
 
 // ===================================================================== Jacobi
@@ -580,7 +590,7 @@ TEA_EXPORT void ext_jacobi_kernel_init_(const int* chunk, const int* coefficient
     const double ry = *dt / (c->dy * c->dy);
     const double rz = DIM == 3 ? *dt / (c->dz * c->dz) : 0.0;
     LAUNCH(k_jacobi_init, c->full, c->g, c->full, c->f, *coefficient == 1 ? 1 : 0, rx, ry, rz);
-    sync(c);
+    issued(c);
 }
 
 TEA_EXPORT void ext_jacobi_kernel_solve_(const int* chunk, double* error)
@@ -631,7 +641,7 @@ TEA_EXPORT void ext_cg_calc_p_(const int* chunk, const double* beta)
     Chunk* c = get_chunk(chunk);
     if (!c) return;
     LAUNCH_PAIRS(k_cg_calc_p, c->g, c->f, *beta, c->preconditioner);
-    sync(c);
+    issued(c);
 }
 
 // ===================================================================== Chebyshev
@@ -645,7 +655,7 @@ TEA_EXPORT void ext_cheby_solver_init_(const int* chunk, double* alphas, double*
     store_coefs(c, alphas, betas, *maxChebyIters);
     LAUNCH(k_cheby_init, c->inner, c->g, c->inner, c->f, *theta, c->preconditioner);
     LAUNCH_PAIRS(k_cheby_calc_u, c->g, c->f);
-    sync(c);
+    issued(c);
 }
 
 TEA_EXPORT void ext_cheby_solver_iterate_(const int* chunk, const int* chebyCalcStep)
@@ -661,7 +671,7 @@ TEA_EXPORT void ext_cheby_solver_iterate_(const int* chunk, const int* chebyCalc
     LAUNCH_PAIRS(k_cheby_iterate, c->g, c->f, c->h_alphas[step], c->h_betas[step],
            c->preconditioner);
     LAUNCH_PAIRS(k_cheby_calc_u, c->g, c->f);
-    sync(c);
+    issued(c);
 }
 
 // ===================================================================== PPCG
@@ -680,7 +690,7 @@ TEA_EXPORT void ext_ppcg_init_sd_(const int* chunk)
     Chunk* c = get_chunk(chunk);
     if (!c) return;
     LAUNCH_PAIRS(k_ppcg_init_sd, c->g, c->f, c->theta, c->preconditioner);
-    sync(c);
+    issued(c);
 }
 
 TEA_EXPORT void ext_ppcg_inner_(const int* chunk, int* currentStep)
@@ -694,7 +704,7 @@ TEA_EXPORT void ext_ppcg_inner_(const int* chunk, int* currentStep)
     }
     LAUNCH_PAIRS(k_ppcg_calc_u, c->g, c->f);
     LAUNCH_PAIRS(k_ppcg_calc_sd, c->g, c->f, c->h_alphas[step], c->h_betas[step], c->preconditioner);
-    sync(c);
+    issued(c);
 }
 
 // ===================================================================== inspection / status
@@ -743,6 +753,9 @@ TEA_EXPORT int tea_write_field_(const int* chunk, const int* field, const double
 
 TEA_EXPORT void ext_get_status_(int* status)
 {
+    // Faults of kernels still queued by field-updating entry points are reported first.
+    for (Chunk* c : chunks())
+        if (c) sync(c);
     StatusStore& s = status_store();
     *status = s.status;
     s.status = 0;

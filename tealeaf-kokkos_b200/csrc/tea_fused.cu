@@ -683,10 +683,13 @@ bool build_loop(Chunk* c, Fused* F, int kind, int inner_steps)
     return true;
 }
 
+// The host record is pinned and the host rewrites it right after most pushes, so the copy
+// has read it before this returns.
 void push_state(Chunk* c, Fused* F)
 {
     TEA_CK(cudaMemcpyAsync(F->d_st, F->h_st, sizeof(SolveState), cudaMemcpyHostToDevice, c->stream));
     c->h2d_bytes += sizeof(SolveState);
+    sync(c);
 }
 
 void pull_state(Chunk* c, Fused* F)
