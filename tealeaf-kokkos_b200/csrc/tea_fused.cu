@@ -1163,14 +1163,18 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
     *ms_per_launch = 0.0;
     Chunk* c = get_chunk(chunk);
     if (!c || *reps < 1) return;
-    Fused* F = ensure_fused(c, 1);
+    // Coefficient arrays for at least kTimingIters iterations, so that a pass of four
+    // Chebyshev iterations reads stored coefficients even before any solve has run.
+    constexpr int kTimingIters = 8;
+    Fused* F = ensure_fused(c, kTimingIters);
     if (*kernel >= 7 && !ensure_fp32(c, F)) return;
     FusedArgs a = F->base;
     a.step = 1;
     a.timing = 1;
     // Steady-state operands: sweep A applies a pending p and u update, as it does in every
-    // CG iteration after the first; the Chebyshev kernels see an iteration that is neither
-    // a convergence check nor the last one.
+    // CG iteration after the first; the Chebyshev kernels see iterations that are neither
+    // a convergence check nor past max_iters, so the four-iteration pass runs as a pass of
+    // four (with max_iters below 4 it falls back to its two-iteration body).
     pull_state(c, F);
     const SolveState saved = *F->h_st;
     F->h_st->pending_p = 1;
@@ -1178,7 +1182,7 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
     F->h_st->n = 1;
     F->h_st->cont = 1;
     F->h_st->est_itc = 1 << 30;
-    F->h_st->max_iters = std::max(F->h_st->max_iters, 2);
+    F->h_st->max_iters = std::max(F->h_st->max_iters, kTimingIters);
     F->h_st->cheby_calc_steps = 1;
     F->h_st->n_inner = 1;
     F->h_st->inner_max = 1 << 30;
