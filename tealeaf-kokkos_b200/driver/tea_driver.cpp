@@ -317,6 +317,8 @@ struct Backend {
     int (*transfer_bytes)(const int*, long long*, long long*) = nullptr;
     int (*ws_record)(const int*, const int*) = nullptr;
     int (*ws_attach)(const int*, const int*) = nullptr;
+    int (*chunk_dims)(const int*, int*) = nullptr;             // tea_chunk_dims_ (visit output)
+    int (*read_field)(const int*, const int*, double*) = nullptr;  // tea_read_field_
 
     template <class F>
     void bind(F& fp, const char* name, bool required = true)
@@ -361,6 +363,8 @@ struct Backend {
         bind(transfer_bytes, "tea_transfer_bytes_", false);
         bind(ws_record, "tea_ws_record_", false);
         bind(ws_attach, "tea_ws_attach_", false);
+        bind(chunk_dims, "tea_chunk_dims_", false);
+        bind(read_field, "tea_read_field_", false);
     }
 
     void close()
@@ -380,6 +384,35 @@ struct Backend {
 };
 
 // ----------------------------------------------------------------------------- output
+
+// v in Fortran's E12.4 edit descriptor (right-justified in 12 characters, mantissa
+// 0.dddd, exponent E+dd, or +ddd without the E beyond two digits), the format of the
+// reference's graphics files.  out holds at least 13 characters.
+void fortran_e12_4(char* out, double v)
+{
+    if (std::isnan(v)) {
+        std::snprintf(out, 13, "%12s", "NaN");
+        return;
+    }
+    if (std::isinf(v)) {
+        std::snprintf(out, 13, "%12s", v > 0 ? "Infinity" : "-Infinity");
+        return;
+    }
+    const char* sign = std::signbit(v) ? "-" : "";
+    char body[32];
+    if (v == 0.0) {
+        std::snprintf(body, sizeof(body), "%s0.0000E+00", sign);
+    } else {
+        char m[32];
+        std::snprintf(m, sizeof(m), "%.3E", std::fabs(v));  // d.dddE+xx, rounded to 4 digits
+        const char digits[5] = {m[0], m[2], m[3], m[4], 0};
+        const int e = std::atoi(m + 6) + 1;  // 0.dddd x 10^e
+        const int ae = e < 0 ? -e : e;
+        if (ae <= 99) std::snprintf(body, sizeof(body), "%s0.%sE%c%02d", sign, digits, e < 0 ? '-' : '+', ae);
+        else std::snprintf(body, sizeof(body), "%s0.%s%c%03d", sign, digits, e < 0 ? '-' : '+', ae);
+    }
+    std::snprintf(out, 13, "%12.12s", body);  // body has at most 11 characters
+}
 
 struct Log {
     FILE* file = nullptr;
@@ -437,6 +470,9 @@ struct Runner {
     int chunk = 1;
     int neighbours[6] = {-1, -1, -1, -1, -1, -1};  // every face EXTERNAL_FACE on one rank
     int lx = 0, ly = 0, lz = 0;                    // this rank's chunk, inner cells
+    double cx0 = 0.0, cy0 = 0.0, cz0 = 0.0;        // this rank's chunk: first vertex
+    double cdx = 0.0, cdy = 0.0, cdz = 0.0;        // and cell widths
+    bool visit_started = false;
     std::vector<double> snd, rcv;
 
     bool split() const { return comm && comm->size > 1; }
@@ -591,6 +627,8 @@ struct Runner {
         double xmin = cfg.xmin + dx * 0.0;
         double ymin = cfg.ymin + dy * (cfg.dim == 2 ? off : 0.0);
         double zmin = cfg.zmin + dz * (cfg.dim == 3 ? off : 0.0);
+        cx0 = xmin; cy0 = ymin; cz0 = zmin;
+        cdx = dx; cdy = dy; cdz = dz;
         if (cfg.dim == 2)
             reinterpret_cast<void (*)(const int*, const double*, const double*, const double*, const double*)>(
                 be.initialise_chunk)(&chunk, &xmin, &ymin, &dx, &dy);
@@ -851,6 +889,75 @@ struct Runner {
         rec->est_itc = est_itc;
     }
 
+    // visit(), tealeaf_2d/visit.f90:23-112 and tealeaf_3d/visit.f90: graphics output into
+    // the working directory.  Rank 0 keeps the index tea.visit ("!NBLOCKS n" once, then
+    // one line per rank's file at each call) and every rank writes its chunk as the
+    // legacy-VTK rectilinear grid tea.<rank+1>.<step>.vtk (five-digit fields), with the
+    // reference's header lines and Fortran E12.4 numbers.  The reference's files stop
+    // after declaring two field arrays without values (and print an unset z extent in
+    // 2D); these carry the cells' density, energy and temperature (u) as CELL_DATA, read
+    // from the backend, and a 2D grid is one cell deep in z, so VTK readers accept them.
+    // The index lists every rank's file, where the reference lists rank 0's chunks only.
+    void visit()
+    {
+        if (!be.chunk_dims || !be.read_field) fail("visit output needs tea_chunk_dims_ and tea_read_field_");
+        const int nranks = split() ? comm->size : 1, rank = split() ? comm->rank : 0;
+        const int tag = step % 100000;  // the five digits of WRITE(i6) step+100000
+        if (rank == 0) {
+            FILE* f = std::fopen("tea.visit", visit_started ? "a" : "w");
+            if (!f) fail("cannot write tea.visit");
+            if (!visit_started) std::fprintf(f, "!NBLOCKS %5d\n", nranks);
+            for (int r = 0; r < nranks; ++r) std::fprintf(f, "tea.%05d.%05d.vtk\n", (r + 1) % 100000, tag);
+            std::fclose(f);
+        }
+        visit_started = true;
+        int dims[3] = {0, 0, 0};
+        if (be.chunk_dims(&chunk, dims) != 0) fail("visit: tea_chunk_dims_ failed");
+        const size_t padded = (size_t)dims[0] * dims[1] * dims[2];
+        const int nz = cfg.dim == 3 ? lz : 1;
+        const long ncells = (long)lx * ly * nz;
+        char name[64];
+        std::snprintf(name, sizeof(name), "tea.%05d.%05d.vtk", (rank + 1) % 100000, tag);
+        FILE* f = std::fopen(name, "w");
+        if (!f) fail("cannot write %s", name);
+        char num[32];
+        auto put = [&](double v) {
+            fortran_e12_4(num, v);
+            std::fputs(num, f);
+            std::fputc('\n', f);
+        };
+        std::fprintf(f, "# vtk DataFile Version 3.0\nvtk output\nASCII\nDATASET RECTILINEAR_GRID\n");
+        std::fprintf(f, "DIMENSIONS%12d%12d%12d\n", lx + 1, ly + 1, cfg.dim == 3 ? lz + 1 : 1);
+        std::fprintf(f, "X_COORDINATES %5d double\n", lx + 1);
+        for (int k = 0; k <= lx; ++k) put(cx0 + cdx * (double)k);
+        std::fprintf(f, "Y_COORDINATES %5d double\n", ly + 1);
+        for (int k = 0; k <= ly; ++k) put(cy0 + cdy * (double)k);
+        if (cfg.dim == 3) {
+            std::fprintf(f, "Z_COORDINATES %5d double\n", lz + 1);
+            for (int k = 0; k <= lz; ++k) put(cz0 + cdz * (double)k);
+        } else {
+            std::fprintf(f, "Z_COORDINATES %5d double\n", 1);
+            put(0.0);
+        }
+        std::fprintf(f, "CELL_DATA %ld\nFIELD FieldData 3\n", ncells);
+        std::vector<double> buf(padded);
+        const int kPad = 2;  // the flat arrays hold two halo cells before the inner ones
+        const struct { const char* name; int id; } out[3] = {
+            {"density", FIELD_DENSITY}, {"energy", FIELD_ENERGY1}, {"temperature", FIELD_U}};
+        for (const auto& o : out) {
+            if (be.read_field(&chunk, &o.id, buf.data()) != 0) fail("visit: tea_read_field_(%d) failed", o.id);
+            std::fprintf(f, "%s 1 %ld double\n", o.name, ncells);
+            for (int ii = 0; ii < nz; ++ii)
+                for (int jj = 0; jj < ly; ++jj)
+                    for (int kk = 0; kk < lx; ++kk) {
+                        const size_t zi = cfg.dim == 3 ? (size_t)(ii + kPad) : 0;
+                        put(buf[(size_t)(kk + kPad) + (size_t)dims[0] * ((size_t)(jj + kPad) + (size_t)dims[1] * zi)]);
+                    }
+        }
+        if (std::fclose(f) != 0) fail("cannot write %s", name);
+        be.check_status("visit");
+    }
+
     int run(tea_run_summary* sum, tea_step_record* steps, int max_steps)
     {
         start(sum);
@@ -886,6 +993,7 @@ struct Runner {
                 rec.has_summary = 1;
                 summarised = true;
             }
+            if (cfg.visit_frequency != 0 && step % cfg.visit_frequency == 0) visit();
             const double wall = now_seconds() - t0;
             log.line(" Wall clock %.15g", wall);
             const double cells = (double)cfg.x_cells * cfg.y_cells * (cfg.dim == 3 ? cfg.z_cells : 1);
@@ -898,6 +1006,7 @@ struct Runner {
                 rec.vol = v[0]; rec.mass = v[1]; rec.ie = v[2]; rec.temp = v[3];
                 rec.has_summary = 1;
                 summarised = true;
+                if (cfg.visit_frequency != 0) visit();
             } else if (opt->summary_every_step && !summarised) {
                 double v[4];
                 be.field_summary(&chunk, &v[0], &v[1], &v[2], &v[3]);
