@@ -59,6 +59,20 @@ def seeded_cases():
     spec = tea.DeckSpec(dim=3, cells=48, states=12, seed=256, solver="cg", end_step=2, eps=1e-15,
                         summary_frequency=1)
     cases.append({"name": "3d_cg_12states_48", "dim": 3, "deck": tea.seeded_deck(spec)})
+    # Non-square, ragged grids on the square domain, so dx != dy (!= dz): a kernel that
+    # mixed up two extents or two cell widths would still pass every square deck above.
+    for dim, shape, solver, seed in ((2, (97, 41), "cg", 900), (2, (33, 150), "chebyshev", 901),
+                                     (2, (97, 41), "ppcg", 902), (2, (33, 150), "jacobi", 903),
+                                     (3, (19, 11, 27), "cg", 904), (3, (29, 23, 9), "chebyshev", 905),
+                                     (3, (19, 11, 27), "ppcg", 906), (3, (29, 23, 9), "jacobi", 907)):
+        spec = tea.DeckSpec(dim=dim, cells=shape[0], states=6, seed=seed, solver=solver, end_step=3, eps=1e-15,
+                            max_iters=20000 if solver == "jacobi" else 1000, presteps=20, inner_steps=6,
+                            summary_frequency=1)
+        deck = tea.seeded_deck(spec)
+        for axis, n in zip("yz", shape[1:]):
+            deck = deck.replace(f"{axis}_cells={shape[0]}\n", f"{axis}_cells={n}\n")
+        name = f"{dim}d_{solver}_" + "x".join(str(n) for n in shape)
+        cases.append({"name": name, "dim": dim, "deck": deck})
     return cases
 
 
@@ -86,11 +100,22 @@ def main():
         kat[str(dim)] = {"deck": k["deck"].read_text(), "test_problem": k["test_problem"],
                          "expected_temp": k["expected"], "threshold_percent": 0.001, "source": k["source"]}
     (HERE / "kat_decks.json").write_text(json.dumps(kat, indent=1) + "\n")
+    # A case whose deck is unchanged keeps its recorded run (the reference is deterministic
+    # at one thread); new or changed decks are run.
+    old = json.loads((HERE / "ref_runs.json").read_text()) if (HERE / "ref_runs.json").exists() else {}
+
+    def ref_of(name, dim, deck):
+        if name in old and old[name]["deck"] == deck:
+            return old[name]["ref"]
+        return run_ref(dim, deck, 1)
+
     runs = {}
     for dim in (2, 3):
-        runs[f"kat_{dim}d"] = {"dim": dim, "deck": kat[str(dim)]["deck"], "ref": run_ref(dim, kat[str(dim)]["deck"], 1)}
+        runs[f"kat_{dim}d"] = {"dim": dim, "deck": kat[str(dim)]["deck"],
+                               "ref": ref_of(f"kat_{dim}d", dim, kat[str(dim)]["deck"])}
     for case in seeded_cases():
-        runs[case["name"]] = {"dim": case["dim"], "deck": case["deck"], "ref": run_ref(case["dim"], case["deck"], 1)}
+        runs[case["name"]] = {"dim": case["dim"], "deck": case["deck"],
+                              "ref": ref_of(case["name"], case["dim"], case["deck"])}
         print(case["name"], [r["iterations"] for r in runs[case["name"]]["ref"]["records"]], flush=True)
     (HERE / "ref_runs.json").write_text(json.dumps(runs, indent=1) + "\n")
 
