@@ -16,8 +16,8 @@ reference) on data resident in HBM.
 Timing: W untimed timesteps, then K timesteps between CUDA events recorded on the
 library's own stream, barrier + synchronize on both sides, max over ranks.  Every field
 array is 135 MB (> 126 MB of L2), so no L2 flush is needed between steps.  With N > 1
-(torchrun) each rank solves its own replica of the workload (this build does not shard
-the solve) and rank 0 prints one JSON line.
+(torchrun) each rank solves its own replica of the workload (the benchmark does not split
+one solve over ranks) and rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -63,7 +63,7 @@ ALL_KERNEL_IDS = {"ppcg_inner": 1, "cg_sweep_a": 2, "cheby_iterate": 3, "jacobi"
                   "cheby_quad": 11, "cheby32_quad": 12}
 PROFILES = ROOT / "profiles"
 # Per-timestep iteration counts of this deck (CG iterations before the Chebyshev switch,
-# Chebyshev iterations after it) for simulation steps 1..20, measured with this build; the
+# Chebyshev iterations after it) for simulation steps 1..20, measured with this library; the
 # reference's counts agree within +-1 (tests/test_gpu_solvers.py).  They scale the
 # reference arm's per-iteration costs to seconds per timestep.
 STEP_COUNTS = {
