@@ -1,7 +1,7 @@
 /*
  * ORACLE -- test infrastructure only.  Never linked into, loaded by, or called from
  * the product path (libtea{2,3}d_b200.so, the driver).  Only tests/, the smoke check
- * and bench.py's CPU-baseline leg load it, as the checker.
+ * and bench.py's CPU-baseline leg load it, to compare the CUDA library's results with.
  *
  * A plain-C, single-threaded restatement of the reference's extension kernels
  * (crtrott/TeaLeaf-Kokkos tealeaf_2d|3d/ext_*.hpp functors and the ext_* entry points
