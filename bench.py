@@ -685,6 +685,10 @@ def main():
         line["fp32_refined_learned"] = {
             "value": learned["sec_per_step"], "unit": "s", "speedup_vs_fp64": g["sec_per_step"] / learned["sec_per_step"],
             "iterations": learned["iterations"], "warm_start_used": learned["warm_start_used"],
+            # Iterations saved per timestep against FP32-refined alone (negative: more).
+            "iterations_saved": ([a - b for a, b in zip(refined["iterations"], learned["iterations"])]
+                                 if refined else None),
+            "seconds_saved_per_step": saved,
             "warm_r0_ratio": learned["warm_r0_ratio"], "corrections": learned["corrections"],
             "field_summary_max_rel_diff_vs_fp64": diff,
             "training": {"pairs": learned["pairs"], "layouts": "4 seeded 1024^2 layouts x 6 timesteps",
