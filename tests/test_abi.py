@@ -42,3 +42,26 @@ def test_driver_exports():
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         tea.load_library(tmp_path / "libtea2d_b200.so")
+
+
+def _cuda_device_present() -> bool:
+    import torch
+
+    return torch.cuda.is_available()
+
+
+@pytest.mark.skipif(_cuda_device_present(), reason="a CUDA device is present")
+def test_no_device_is_reported_not_hidden():
+    """Without a GPU the CUDA library has no CPU path: ext_init_ records TEA_ERR_NO_DEVICE
+    (status 6) with a message, and the driver stops with an error instead of running."""
+    lib = tea.cuda_library(2)
+    x, y, rank = ctypes.c_int(8), ctypes.c_int(8), ctypes.c_int(0)
+    lib.ext_init_(ctypes.byref(x), ctypes.byref(y), ctypes.byref(rank))
+    status = ctypes.c_int(-1)
+    lib.ext_get_status_(ctypes.byref(status))
+    lib.tea_last_error.restype = ctypes.c_char_p
+    assert status.value == 6
+    assert b"no CPU path" in lib.tea_last_error()
+    spec = tea.DeckSpec(dim=2, cells=16, states=3, end_step=1)
+    with pytest.raises(RuntimeError, match="status 6"):
+        tea.run_deck(tea.seeded_deck(spec), 2)
