@@ -613,6 +613,8 @@ def main():
     refined = None if args.no_refined else gpu_arm(args, world, precision=1, kernels=False)
     learned = None if args.no_refined or args.no_learned else learned_arm(args, world)
     e2e = None if args.no_e2e else e2e_arm(args)
+    if e2e and world > 1:
+        e2e["value"] = dist_max(e2e["value"], world)  # the slowest replica, as for value
     per_call = None if args.no_per_call else per_call_arm()
     if rank != 0:
         dist_done(world)
