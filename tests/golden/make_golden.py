@@ -65,15 +65,26 @@ def seeded_cases():
                                      (2, (97, 41), "ppcg", 902), (2, (33, 150), "jacobi", 903),
                                      (3, (19, 11, 27), "cg", 904), (3, (29, 23, 9), "chebyshev", 905),
                                      (3, (19, 11, 27), "ppcg", 906), (3, (29, 23, 9), "jacobi", 907)):
-        spec = tea.DeckSpec(dim=dim, cells=shape[0], states=6, seed=seed, solver=solver, end_step=3, eps=1e-15,
-                            max_iters=20000 if solver == "jacobi" else 1000, presteps=20, inner_steps=6,
-                            summary_frequency=1)
-        deck = tea.seeded_deck(spec)
-        for axis, n in zip("yz", shape[1:]):
-            deck = deck.replace(f"{axis}_cells={shape[0]}\n", f"{axis}_cells={n}\n")
-        name = f"{dim}d_{solver}_" + "x".join(str(n) for n in shape)
-        cases.append({"name": name, "dim": dim, "deck": deck})
+        cases.append(_non_square(dim, shape, solver, seed, "plain"))
+    # The same grids with the diagonal preconditioner and with the density coefficient.
+    for dim, shape, solver, seed, variant in ((2, (97, 41), "chebyshev", 910, "precond"),
+                                              (2, (33, 150), "ppcg", 911, "density"),
+                                              (3, (19, 11, 27), "cg", 912, "precond"),
+                                              (3, (29, 23, 9), "ppcg", 913, "precond")):
+        cases.append(_non_square(dim, shape, solver, seed, variant))
     return cases
+
+
+def _non_square(dim, shape, solver, seed, variant):
+    spec = tea.DeckSpec(dim=dim, cells=shape[0], states=6, seed=seed, solver=solver, end_step=3, eps=1e-15,
+                        max_iters=20000 if solver == "jacobi" else 1000, presteps=20, inner_steps=6,
+                        inverse_density=(variant != "density"), preconditioner=(variant == "precond"),
+                        summary_frequency=1)
+    deck = tea.seeded_deck(spec)
+    for axis, n in zip("yz", shape[1:]):
+        deck = deck.replace(f"{axis}_cells={shape[0]}\n", f"{axis}_cells={n}\n")
+    name = f"{dim}d_{solver}_" + "x".join(str(n) for n in shape) + ("" if variant == "plain" else f"_{variant}")
+    return {"name": name, "dim": dim, "deck": deck}
 
 
 def run_ref(dim: int, deck: str, threads: int) -> dict:
