@@ -2,7 +2,8 @@
 // restated over the C++ driver.  Usage:
 //   tea_leaf [--dim 2|3] [--backend LIB] [--fused] [--out tea.out] [--quiet]
 //            [--summary-every-step] [--end-step N] [--json FILE] [deck]
-// The deck defaults to ./tea.in.  --json writes the run summary and per-step records.
+// The deck defaults to ./tea.in; a missing deck is replaced by the reference's default
+// one.  --json writes the run summary and per-step records.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -23,6 +24,36 @@ static std::string num(double v)
     char b[40];
     std::snprintf(b, sizeof(b), "%.17g", v);
     return b;
+}
+
+// initialise.f90:69-97 (tealeaf_2d, tealeaf_3d): when the input deck cannot be opened, the
+// reference writes this default one in its place and runs it -- a 10 x 10 (x 2 in 3D)
+// mesh with five states, Jacobi, test_problem 1.  The lines are the reference's, the 3D
+// deck's "rectangle" included (the 3D parser knows only "cuboid", so those states keep
+// no geometry there, and here).
+static void write_default_deck(const std::string& path, int dim)
+{
+    std::vector<std::string> lines = {
+        "*tea",
+        " state 1 density=100.0 energy=0.0001",
+        " state 2 density=0.1 energy=25.0 geometry=rectangle xmin=0.0 xmax=1.0 ymin=1.0 ymax=2.0",
+        " state 3 density=0.1 energy=0.1 geometry=rectangle xmin=1.0 xmax=6.0 ymin=1.0 ymax=2.0",
+        " state 4 density=0.1 energy=0.1 geometry=rectangle xmin=5.0 xmax=6.0 ymin=1.0 ymax=8.0",
+        " state 5 density=0.1 energy=0.1 geometry=rectangle xmin=5.0 xmax=10.0 ymin=7.0 ymax=8.0",
+        " x_cells=10",
+        " y_cells=10"};
+    if (dim == 3) lines.push_back(" z_cells=2");
+    lines.push_back(" xmin=0.0");
+    lines.push_back(" ymin=0.0");
+    if (dim == 3) lines.push_back(" zmin=0.0");
+    lines.push_back(" xmax=10.0");
+    lines.push_back(" ymax=10.0");
+    if (dim == 3) lines.push_back(" zmax=10.0");
+    for (const char* l : {" initial_timestep=0.004", " end_step=10", " tl_max_iters=1000", " test_problem 1",
+                          " tl_use_jacobi", " tl_eps=1.0e-15", "*endtea"})
+        lines.push_back(l);
+    std::ofstream out(path);
+    for (const auto& l : lines) out << l << "\n";
 }
 
 int main(int argc, char** argv)
@@ -54,6 +85,7 @@ int main(int argc, char** argv)
         std::fprintf(stderr, "--backend LIB is required (libtea2d_b200.so / libtea3d_b200.so)\n");
         return 2;
     }
+    if (!std::ifstream(deck_path)) write_default_deck(deck_path, opt.dim);
     std::ifstream in(deck_path);
     if (!in) {
         std::fprintf(stderr, "cannot read %s\n", deck_path.c_str());

@@ -2,6 +2,7 @@
 read_input, and the switch-time scalar algorithms (eigenvalues, Chebyshev coefficients).
 Runs on the CPU against the oracle backend."""
 import ctypes
+import os
 
 import numpy as np
 import pytest
@@ -131,3 +132,35 @@ def test_chebyshev_coefficients_recurrence():
         assert be[k] == 2.0 * rho_new / delta
         rho_old = rho_new
     assert th.value == theta
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_default_deck_when_none_exists(tmp_path, dim):
+    """initialise.f90:69-97: with no input deck the reference writes its default one
+    (10 x 10 [x 2] cells, five states, Jacobi, test_problem 1) and runs it; the tea_leaf
+    executable does the same.  Against the compiled reference (when built) on that deck,
+    every per-step record is identical."""
+    import json
+    import subprocess
+
+    from conftest import PORT, REFLIB
+
+    runs = {}
+    for name, lib in (("port", PORT[dim]), ("ref", REFLIB[dim])):
+        if name == "ref" and not lib.exists():
+            continue
+        d = tmp_path / name
+        d.mkdir()
+        subprocess.run([str(tea.tea_leaf_exe()), "--dim", str(dim), "--backend", str(lib), "--quiet",
+                        "--summary-every-step", "--json", "out.json"], cwd=d, check=True, capture_output=True,
+                       env=dict(os.environ, OMP_NUM_THREADS="1"))
+        deck = (d / "tea.in").read_text().splitlines()
+        assert deck[0] == "*tea" and deck[-1] == "*endtea"
+        assert " tl_use_jacobi" in deck and " test_problem 1" in deck
+        assert (" z_cells=2" in deck) == (dim == 3)
+        runs[name] = json.loads((d / "out.json").read_text())
+        assert runs[name]["steps"] == 10 and runs[name]["test_problem"] == 1
+    if "ref" in runs:
+        keys = ("iterations", "error", "vol", "mass", "ie", "temp")
+        for a, b in zip(runs["port"]["records"], runs["ref"]["records"]):
+            assert all(a[k] == b[k] for k in keys), (a, b)
