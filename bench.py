@@ -401,7 +401,7 @@ def reference_costs(threads: int, n_cg=40, n_cheby=40):
             deck = deck.replace("*endtea", "tl_ch_cg_errswitch\ntl_ch_cg_epslim=1e300\n*endtea")
         with tempfile.TemporaryDirectory() as td:
             (pathlib.Path(td) / "tea.in").write_text(deck)
-            subprocess.run([str(tea.tea_leaf_exe()), "--dim", "2", "--backend", str(ref), "--quiet", "--json",
+            subprocess.run([str(tea.tea_leaf_exe()), "--dim", "2", "--backend", str(ref), "--quiet", "--no-out", "--json",
                             str(pathlib.Path(td) / "o.json"), str(pathlib.Path(td) / "tea.in")],
                            check=True, env=env, capture_output=True, timeout=1200)
             return json.loads((pathlib.Path(td) / "o.json").read_text())["records"][0]

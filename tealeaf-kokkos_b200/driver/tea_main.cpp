@@ -1,9 +1,10 @@
 // tea_leaf executable: the command-line entry of the reference (tealeaf_2d/tea_leaf.f90:35-104)
 // restated over the C++ driver.  Usage:
-//   tea_leaf [--dim 2|3] [--backend LIB] [--fused] [--out tea.out] [--quiet]
-//            [--summary-every-step] [--end-step N] [--json FILE] [deck]
-// The deck defaults to ./tea.in; a missing deck is replaced by the reference's default
-// one.  --json writes the run summary and per-step records.
+//   tea_leaf [--dim 2|3] [--backend LIB] [--fused] [--out FILE | --no-out] [--quiet]
+//            [--summary-every-step] [--end-step N] [--json FILE] [deck [output]]
+// As in the reference (tea_leaf.f90:68-85), the deck defaults to ./tea.in and the output
+// log to ./tea.out; a missing deck is replaced by the reference's default one.  --json
+// writes the run summary and per-step records.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -61,7 +62,8 @@ int main(int argc, char** argv)
     tea_run_options opt;
     std::memset(&opt, 0, sizeof(opt));
     opt.dim = 2;
-    std::string deck_path = "tea.in", backend, out_path, json_path;
+    std::string deck_path = "tea.in", backend, out_path = "tea.out", json_path;
+    int positional = 0;
     for (int i = 1; i < argc; ++i) {
         std::string a = argv[i];
         auto need = [&](const char* what) -> std::string {
@@ -75,11 +77,13 @@ int main(int argc, char** argv)
         else if (a == "--backend") backend = need("--backend");
         else if (a == "--fused") opt.use_fused_solve = 1;
         else if (a == "--out") out_path = need("--out");
+        else if (a == "--no-out") out_path.clear();
         else if (a == "--quiet") opt.quiet = 1;
         else if (a == "--summary-every-step") opt.summary_every_step = 1;
         else if (a == "--end-step") opt.end_step_override = std::atoi(need("--end-step").c_str());
         else if (a == "--json") json_path = need("--json");
-        else deck_path = a;
+        else if (positional++ == 0) deck_path = a;
+        else out_path = a;
     }
     if (backend.empty()) {
         std::fprintf(stderr, "--backend LIB is required (libtea2d_b200.so / libtea3d_b200.so)\n");

@@ -93,7 +93,7 @@ def run_ref(dim: int, deck: str, threads: int) -> dict:
     tmp.mkdir(exist_ok=True)
     (tmp / "tea.in").write_text(deck)
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="false")
-    subprocess.run([str(tea.tea_leaf_exe()), "--dim", str(dim), "--backend", str(lib), "--quiet",
+    subprocess.run([str(tea.tea_leaf_exe()), "--dim", str(dim), "--backend", str(lib), "--quiet", "--no-out",
                     "--summary-every-step", "--json", str(tmp / "out.json"), str(tmp / "tea.in")],
                    check=True, env=env, capture_output=True)
     out = json.loads((tmp / "out.json").read_text())

@@ -160,7 +160,22 @@ def test_default_deck_when_none_exists(tmp_path, dim):
         assert (" z_cells=2" in deck) == (dim == 3)
         runs[name] = json.loads((d / "out.json").read_text())
         assert runs[name]["steps"] == 10 and runs[name]["test_problem"] == 1
+        log = (d / "tea.out").read_text()  # the reference's default output file
+        assert log.count(" Step ") == 10 and "Iteration count" in log
     if "ref" in runs:
         keys = ("iterations", "error", "vol", "mass", "ie", "temp")
         for a, b in zip(runs["port"]["records"], runs["ref"]["records"]):
             assert all(a[k] == b[k] for k in keys), (a, b)
+
+
+def test_positional_deck_and_output(tmp_path):
+    """tea_leaf.f90:68-85: the first argument replaces tea.in and the second tea.out."""
+    import subprocess
+
+    from conftest import PORT
+
+    (tmp_path / "my.in").write_text(BASE.format(extra="end_step=2"))
+    subprocess.run([str(tea.tea_leaf_exe()), "--dim", "2", "--backend", str(PORT[2]), "--quiet", "my.in", "my.out"],
+                   cwd=tmp_path, check=True, capture_output=True)
+    assert not (tmp_path / "tea.in").exists() and not (tmp_path / "tea.out").exists()
+    assert (tmp_path / "my.out").read_text().count(" Step ") == 2

@@ -73,7 +73,7 @@ def test_port_bitwise_equals_live_reference(tmp_path):
         deck = tea.seeded_deck(spec)
         (tmp_path / "tea.in").write_text(deck)
         env = dict(os.environ, OMP_NUM_THREADS="1")
-        subprocess.run([str(tea.tea_leaf_exe()), "--dim", str(dim), "--backend", str(REFLIB[dim]), "--quiet",
+        subprocess.run([str(tea.tea_leaf_exe()), "--dim", str(dim), "--backend", str(REFLIB[dim]), "--quiet", "--no-out",
                         "--summary-every-step", "--json", str(tmp_path / "r.json"), str(tmp_path / "tea.in")],
                        check=True, env=env, capture_output=True)
         ref = json.loads((tmp_path / "r.json").read_text())["records"]
