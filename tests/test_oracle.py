@@ -81,3 +81,28 @@ def test_port_bitwise_equals_live_reference(tmp_path):
         for a, b in zip(recs, ref):
             for k in FIELDS:
                 assert same(a[k], b[k]), (dim, k, a[k], b[k])
+
+
+TINY = [(2, (7, 5), "cg"), (2, (1, 9), "cg"), (2, (9, 1), "ppcg"), (2, (2, 2), "chebyshev"), (2, (3, 1), "jacobi"),
+        (3, (8, 8, 8), "cg"), (3, (3, 4, 5), "ppcg"), (3, (1, 6, 2), "chebyshev"), (3, (2, 1, 3), "jacobi")]
+
+
+@pytest.mark.skipif(not REFLIB[2].exists(), reason="oracle/_ref not built (needs the reference sources)")
+@pytest.mark.parametrize("dim,shape,solver", TINY)
+def test_port_bitwise_equals_live_reference_on_tiny_grids(tmp_path, dim, shape, solver):
+    """Grids down to one cell wide in an axis, against the compiled reference."""
+    spec = tea.DeckSpec(dim=dim, cells=shape[0], states=4, seed=50, solver=solver, end_step=2, eps=1e-15,
+                        max_iters=2000, presteps=5, inner_steps=4, summary_frequency=1)
+    deck = tea.seeded_deck(spec)
+    for axis, n in zip("yz", shape[1:]):
+        deck = deck.replace(f"{axis}_cells={shape[0]}\n", f"{axis}_cells={n}\n")
+    (tmp_path / "tea.in").write_text(deck)
+    subprocess.run([str(tea.tea_leaf_exe()), "--dim", str(dim), "--backend", str(REFLIB[dim]), "--quiet", "--no-out",
+                    "--summary-every-step", "--json", str(tmp_path / "r.json"), str(tmp_path / "tea.in")],
+                   check=True, env=dict(os.environ, OMP_NUM_THREADS="1"), capture_output=True)
+    ref = json.loads((tmp_path / "r.json").read_text())["records"]
+    _, recs = tea.run_deck(deck, dim, backend=port_lib(dim, SUM_SEQUENTIAL), summary_every_step=True)
+    assert len(recs) == len(ref) == 2
+    for a, b in zip(recs, ref):
+        for k in FIELDS:
+            assert same(a[k], b[k]), (shape, solver, b["step"], k, a[k], b[k])
