@@ -62,16 +62,11 @@ ALL_KERNEL_IDS = {"ppcg_inner": 1, "cg_sweep_a": 2, "cheby_iterate": 3, "jacobi"
                   "cheby_pair": 6, "cg32_sweep_a": 7, "cg32_sweep_b": 8, "cheby32_pair": 9, "ppcg_pair": 10,
                   "cheby_quad": 11, "cheby32_quad": 12}
 PROFILES = ROOT / "profiles"
-# Per-timestep iteration counts of this deck (CG iterations before the Chebyshev switch,
-# Chebyshev iterations after it) for simulation steps 1..20, measured with this library; the
-# reference's counts agree within +-1 (tests/test_gpu_solvers.py).  They scale the
-# reference arm's per-iteration costs to seconds per timestep.
-STEP_COUNTS = {
-    1: (5550, 3890), 2: (5046, 3924), 3: (4540, 3960), 4: (4037, 3993), 5: (3563, 4027),
-    6: (3135, 4085), 7: (2750, 4150), 8: (2412, 4208), 9: (2084, 4286), 10: (1796, 4344),
-    11: (1563, 4387), 12: (1287, 4403), 13: (1249, 4421), 14: (1060, 4450), 15: (1043, 4477),
-    16: (766, 4564), 17: (721, 4579), 18: (762, 4598), 19: (779, 4631), 20: (753, 4687),
-}
+# The reference's own per-timestep iteration counts on this deck (its Kokkos-OpenMP kernels,
+# oracle/_ref, 30 timesteps at 4096^2), recorded by tests/golden/make_golden_large.py.  They
+# scale the reference arm's measured per-iteration costs to whole timesteps.
+REF_LARGE = ROOT / "tests" / "golden" / "ref_large.json"
+REF_CASE = "c2_2d4096_cheby"
 
 
 def workload_spec(steps=1):
@@ -417,8 +412,38 @@ def reference_costs(threads: int, n_cg=40, n_cheby=40):
             "cg_iters": a["iterations"], "cheby_run_iters": b["iterations"]}
 
 
-def cpu_estimate(costs, mean_cg, mean_cheby):
-    return costs["t_cg"] * mean_cg + costs["t_cheby"] * mean_cheby
+def reference_counts():
+    """{timestep: (CG iterations, Chebyshev loop passes)} of the reference on the benchmark
+    deck, and the thread count they were recorded at.  The reference prints n - 1 for a
+    solve that exits in loop pass n (tealeaf_2d/tea_solve.f90:543); passes 1 .. switch - 1
+    are CG, the rest Chebyshev."""
+    d = json.loads(REF_LARGE.read_text())[REF_CASE]
+    spec = workload_spec(steps=len(d["ref"]["records"]))
+    spec.summary_frequency = 1
+    if d["deck"] != tea.seeded_deck(spec):
+        raise ValueError(f"{REF_LARGE.name}: {REF_CASE} was recorded on another deck")
+    counts = {}
+    for r in d["ref"]["records"]:
+        cg = r["switch_step"] - 1 if r["switch_step"] > 0 else r["iterations"] + 1
+        counts[r["step"]] = (cg, r["iterations"] + 1 - cg)
+    return counts, d["threads"]
+
+
+def counts_for(steps):
+    """The reference's counts for `steps`; a timestep beyond the recorded ones takes the last
+    recorded timestep's counts.  Returns (list, note)."""
+    counts, threads = reference_counts()
+    last = max(counts)
+    out = [counts[min(s, last)] for s in steps]
+    beyond = [s for s in steps if s > last]
+    note = (f"the reference's own counts for timesteps {steps[0]}-{steps[-1]} (recorded at {threads} threads)"
+            + (f"; timesteps {beyond[0]}-{beyond[-1]} take timestep {last}'s" if beyond else ""))
+    return out, note
+
+
+def cpu_estimate(costs, cg, cheby_passes):
+    # The first Chebyshev pass runs about two iterations' work (init, one iterate, two norms).
+    return costs["t_cg"] * cg + costs["t_cheby"] * (cheby_passes + 1)
 
 
 def host_threads():
@@ -429,40 +454,49 @@ def host_threads():
 
 
 def reference_arm(args, rank, world):
-    """--impl reference: the reference's CPU implementation on this box's host cores."""
+    """--impl reference: the reference's CPU implementation on this box's host cores.  Each
+    step times a bounded sample of the timestep it stands for (reference_costs: CG and
+    Chebyshev iterations of the reference's kernels on this deck) and scales the measured
+    per-iteration costs by the reference's own iteration counts for that timestep."""
     if rank != 0:
         dist_done(world)
         return
     threads = host_threads()
     steps = list(range(args.warmup + 1, args.warmup + args.steps + 1))
-    counts = [STEP_COUNTS.get(s) for s in steps]
     line = {"impl": "reference", "metric": METRIC, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": False}
-    if not (ROOT / "oracle" / "_ref" / "libtea_ref2d.so").exists() or None in counts:
-        line["unavailable"] = ("oracle/_ref (the reference's Kokkos-OpenMP kernels built from its sources) is not "
-                               "built" if None not in counts else "iteration counts of this deck are not recorded")
+    try:
+        counts, note = counts_for(steps)
+        if not (ROOT / "oracle" / "_ref" / "libtea_ref2d.so").exists():
+            raise FileNotFoundError("oracle/_ref (the reference's Kokkos-OpenMP kernels built from its sources) "
+                                    "is not built")
+    except (OSError, ValueError, KeyError) as exc:
+        line["unavailable"] = str(exc)
         print(json.dumps(line))
         dist_done(world)
         return
-    mean_cg = sum(c[0] for c in counts) / len(counts)
-    mean_ch = sum(c[1] for c in counts) / len(counts)
     for _ in range(args.warmup):
         reference_costs(threads, 10, 10)
-    samples = []
-    for _ in range(args.steps):
-        c = reference_costs(threads, 60, 60)
-        samples.append(cpu_estimate(c, mean_cg, mean_ch))
+    samples, per_iter = [], []
+    for cg, ch in counts:
+        c = reference_costs(threads, 40, 40)
+        samples.append(cpu_estimate(c, cg, ch))
+        per_iter.append((c["t_cg"], c["t_cheby"]))
     value = statistics.mean(samples)
+    mean_cg = sum(c[0] for c in counts) / len(counts)
+    mean_ch = sum(c[1] for c in counts) / len(counts)
     line.update({
         "value": value, "ms_per_step": value * 1000.0, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded 16-state layout)",
         "config": {"workload": "2d_4096x4096_16states_chebyshev_rel1e-10", "cells": CELLS * CELLS,
-                   "solver": SOLVER, "timesteps_timed": steps},
+                   "solver": SOLVER, "timesteps_timed": steps, "per_step_s": samples,
+                   "ms_per_iteration_cg_cheby": [statistics.mean(t[0] for t in per_iter) * 1e3,
+                                                 statistics.mean(t[1] for t in per_iter) * 1e3]},
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference",
-                         "sample": "per step: the first timestep cut after 60 CG iterations, and with the Chebyshev "
-                                   "switch forced at iteration 20 cut 60 iterations later; per-iteration costs "
-                                   f"scaled by this deck's counts (mean {mean_cg:.0f} CG + {mean_ch:.0f} Chebyshev "
-                                   "iterations per timestep)"},
+                         "sample": "per step: the first timestep of the deck cut after 40 CG iterations, and with "
+                                   "the Chebyshev switch forced at iteration 20 cut 40 iterations later; the "
+                                   f"per-iteration costs scaled by {note} (mean {mean_cg:.0f} CG + {mean_ch:.0f} "
+                                   "Chebyshev iterations per timestep)"},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
     print(json.dumps(line))
@@ -623,19 +657,18 @@ def main():
     dom = g["dominant"]
     achieved = g["alg_bytes"] / (g["kernel_ms"][dom] / 1000.0) / 1e9
     traffic = load_traffic(dom)
-    mean_cg = sum(g["cg_steps"]) / len(g["cg_steps"])
-    mean_ch = sum(g["cheby_steps"]) / len(g["cheby_steps"])
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         try:
             threads = host_threads()
+            counts, note = counts_for(list(range(args.warmup + 1, args.warmup + args.steps + 1)))
             costs = reference_costs(threads)
-            cpu = {"value": cpu_estimate(costs, mean_cg, mean_ch), "unit": "s", "cores": threads, "kind": "reference",
+            cpu = {"value": statistics.mean(cpu_estimate(costs, cg, ch) for cg, ch in counts), "unit": "s",
+                   "cores": threads, "kind": "reference",
                    "sample": (f"the first timestep cut after 40 CG iterations, and with the Chebyshev switch forced "
                               f"at iteration 20 cut 40 iterations later ({costs['wall']:.1f} s of CPU work); "
                               f"{costs['t_cg'] * 1e3:.2f} ms per CG and {costs['t_cheby'] * 1e3:.2f} ms per Chebyshev "
-                              f"iteration scaled by the timed steps' mean {mean_cg:.0f} CG + {mean_ch:.0f} Chebyshev "
-                              "iterations")}
+                              f"iteration scaled by {note}")}
         except Exception as exc:  # noqa: BLE001
             cpu = {"value": None, "unit": "s", "cores": None, "kind": "reference", "sample": f"unavailable: {exc}"}
     line = {

@@ -70,9 +70,8 @@ struct Chunk {
     std::vector<double> vx, vy, vz, cx, cy, cz;
     double *d_vx = nullptr, *d_vy = nullptr, *d_vz = nullptr, *d_cx = nullptr, *d_cy = nullptr,
            *d_cz = nullptr;
-    // Chebyshev / PPCG coefficients (host copy + device copy).
+    // Chebyshev / PPCG coefficients (host copy; the kernels take them by value).
     std::vector<double> h_alphas, h_betas;
-    double *d_alphas = nullptr, *d_betas = nullptr;
     cudaStream_t stream = nullptr;
     RedScratch red{};
     double* h_out = nullptr;  // mapped pinned host memory for reduction results
@@ -122,6 +121,15 @@ inline void set_status(int code, const char* fmt, ...)
             ::tea::set_status(3, "%s failed at %s:%d: %s", #call, __FILE__, __LINE__,              \
                               cudaGetErrorString(tea_ck_e));                                       \
     } while (0)
+
+// Host<->device copy ordered on `s` and complete on return.  The library's streams are
+// non-blocking, so a plain cudaMemcpy (legacy stream) is not ordered with their kernels,
+// and from pageable memory it may return before the data has landed.
+inline cudaError_t copy_on(cudaStream_t s, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, s);
+    return e != cudaSuccess ? e : cudaStreamSynchronize(s);
+}
 
 inline int launch_blocks(const Chunk* c, long ntiles)
 {

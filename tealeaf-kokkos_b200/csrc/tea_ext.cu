@@ -164,7 +164,7 @@ void destroy_chunk(Chunk* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int id = 1; id < F_COUNT; ++id)
         if (c->alloc[id]) cudaFree(c->alloc[id]);
-    double* small[] = {c->d_vx, c->d_vy, c->d_vz, c->d_cx, c->d_cy, c->d_cz, c->d_alphas, c->d_betas};
+    double* small[] = {c->d_vx, c->d_vy, c->d_vz, c->d_cx, c->d_cy, c->d_cz};
     for (double* p : small)
         if (p) cudaFree(p);
     if (c->red.partials) cudaFree(c->red.partials);
@@ -187,13 +187,6 @@ void store_coefs(Chunk* c, const double* alphas, const double* betas, int n)
     if (n < 1) n = 1;
     c->h_alphas.assign(alphas, alphas + n);
     c->h_betas.assign(betas, betas + n);
-    if (c->d_alphas) TEA_CK(cudaFree(c->d_alphas));
-    if (c->d_betas) TEA_CK(cudaFree(c->d_betas));
-    c->d_alphas = c->d_betas = nullptr;
-    TEA_CK(cudaMalloc(&c->d_alphas, sizeof(double) * n));
-    TEA_CK(cudaMalloc(&c->d_betas, sizeof(double) * n));
-    TEA_CK(cudaMemcpy(c->d_alphas, alphas, sizeof(double) * n, cudaMemcpyHostToDevice));
-    TEA_CK(cudaMemcpy(c->d_betas, betas, sizeof(double) * n, cudaMemcpyHostToDevice));
     c->h2d_bytes += 2 * sizeof(double) * (long long)n;
 }
 
@@ -214,12 +207,12 @@ void init_axis(std::vector<double>& vertex, std::vector<double>& cell, int dimsN
 void upload_coords(Chunk* c)
 {
     const Geom& g = c->g;
-    TEA_CK(cudaMemcpy(c->d_vx, c->vx.data(), sizeof(double) * (g.X + 1), cudaMemcpyHostToDevice));
-    TEA_CK(cudaMemcpy(c->d_vy, c->vy.data(), sizeof(double) * (g.Y + 1), cudaMemcpyHostToDevice));
-    TEA_CK(cudaMemcpy(c->d_vz, c->vz.data(), sizeof(double) * (g.Z + 1), cudaMemcpyHostToDevice));
-    TEA_CK(cudaMemcpy(c->d_cx, c->cx.data(), sizeof(double) * g.X, cudaMemcpyHostToDevice));
-    TEA_CK(cudaMemcpy(c->d_cy, c->cy.data(), sizeof(double) * g.Y, cudaMemcpyHostToDevice));
-    TEA_CK(cudaMemcpy(c->d_cz, c->cz.data(), sizeof(double) * g.Z, cudaMemcpyHostToDevice));
+    TEA_CK(copy_on(c->stream, c->d_vx, c->vx.data(), sizeof(double) * (g.X + 1), cudaMemcpyHostToDevice));
+    TEA_CK(copy_on(c->stream, c->d_vy, c->vy.data(), sizeof(double) * (g.Y + 1), cudaMemcpyHostToDevice));
+    TEA_CK(copy_on(c->stream, c->d_vz, c->vz.data(), sizeof(double) * (g.Z + 1), cudaMemcpyHostToDevice));
+    TEA_CK(copy_on(c->stream, c->d_cx, c->cx.data(), sizeof(double) * g.X, cudaMemcpyHostToDevice));
+    TEA_CK(copy_on(c->stream, c->d_cy, c->cy.data(), sizeof(double) * g.Y, cudaMemcpyHostToDevice));
+    TEA_CK(copy_on(c->stream, c->d_cz, c->cz.data(), sizeof(double) * g.Z, cudaMemcpyHostToDevice));
 }
 
 void initialise_chunk(Chunk* c, double xmin, double ymin, double zmin, double dx, double dy, double dz)
@@ -265,8 +258,8 @@ void generate_chunk(Chunk* c, int n, const double* den, const double* en, const 
     int* dg = nullptr;
     TEA_CK(cudaMalloc(&d, sizeof(double) * h.size()));
     TEA_CK(cudaMalloc(&dg, sizeof(int) * n));
-    TEA_CK(cudaMemcpy(d, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
-    TEA_CK(cudaMemcpy(dg, geo, sizeof(int) * n, cudaMemcpyHostToDevice));
+    TEA_CK(copy_on(c->stream, d, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+    TEA_CK(copy_on(c->stream, dg, geo, sizeof(int) * n, cudaMemcpyHostToDevice));
     c->h2d_bytes += (long long)(sizeof(double) * h.size() + sizeof(int) * n);
     StateTable st;
     st.n = n;
@@ -457,7 +450,7 @@ static void pack_message(const int* chunk, const int* fields, const int* offsets
         if (!fields[fid - 1]) continue;
         double* ext = buffer + offsets[fid - 1];
         if (!do_pack) {
-            TEA_CK(cudaMemcpy(dbuf, ext, sizeof(double) * len, cudaMemcpyHostToDevice));
+            TEA_CK(copy_on(c->stream, dbuf, ext, sizeof(double) * len, cudaMemcpyHostToDevice));
             c->h2d_bytes += (long long)sizeof(double) * len;
         }
         const int blocks = (int)std::min<long>((len + 255) / 256, 4096);
@@ -465,7 +458,7 @@ static void pack_message(const int* chunk, const int* fields, const int* offsets
                                                            do_pack ? 1 : 0, exact ? 1 : 0);
         sync(c);
         if (do_pack) {
-            TEA_CK(cudaMemcpy(ext, dbuf, sizeof(double) * len, cudaMemcpyDeviceToHost));
+            TEA_CK(copy_on(c->stream, ext, dbuf, sizeof(double) * len, cudaMemcpyDeviceToHost));
             c->d2h_bytes += (long long)sizeof(double) * len;
         }
     }

@@ -49,8 +49,11 @@ NoAllocScratch* g_scratch_addr[kMaxDevices] = {};
 
 // Calculate2Norm (tealeaf_2d/ext_solver_methods.hpp:70-92) over the inner domain of a flat
 // padded array (x fastest, HALO_PAD = 2 on every side), one block per 2048 consecutive
-// inner cells; sums in double-double, block partials merged in block order by the last
-// block to arrive, which rounds once -- the same value ext_calculate_2norm_ returns.
+// inner cells; sums in double-double.  The last block to arrive merges the block partials
+// in a fixed order (lane-strided, then a butterfly) and rounds once.  That order is not
+// ext_calculate_2norm_'s, so the two agree because the double-double sum carries far more
+// bits than the result keeps, not by construction: they can differ in the last bit only
+// where the exact sum lies within about n * 2^-106 of a rounding boundary.
 __global__ void __launch_bounds__(kNoAllocThreads) k_2norm_noalloc(const double* __restrict__ field, int nx, int ny,
                                                                    long long ncells, NoAllocScratch* scratch,
                                                                    double* out)
@@ -113,14 +116,22 @@ __global__ void __launch_bounds__(kNoAllocThreads) k_2norm_noalloc(const double*
     }
 }
 
-// Device address of the static scratch on the current device, looked up once per device.
+// Device address of the static scratch on the current device, looked up once per device
+// (on the first call there).  The cached address assumes the device is not reset while the
+// library is loaded: cudaDeviceReset recreates the module, and the array with it.
 NoAllocScratch* scratch_for_current_device(int* status)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (e != cudaSuccess) {
         set_status(TEA_ERR_CUDA, "tea_2norm_noalloc_: cudaGetDevice: %s", cudaGetErrorString(e));
         *status = TEA_ERR_CUDA;
+        return nullptr;
+    }
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_status(TEA_ERR_BAD_ARGUMENT, "tea_2norm_noalloc_: device %d is beyond the %d devices it serves", dev,
+                   kMaxDevices);
+        *status = TEA_ERR_BAD_ARGUMENT;
         return nullptr;
     }
     std::lock_guard<std::mutex> lock(g_setup_mutex);

@@ -598,24 +598,24 @@ int transfer_params(Net* N, float* host, bool to_device, bool grads)
                 for (int t = 0; t < 9; ++t)
                     for (int ci = 0; ci < ci_o; ++ci)
                         buf[((size_t)co * 9 + t) * c.cin + ci] = host[off + ((long)co * 9 + t) * ci_o + ci];
-            WS_CK(cudaMemcpy(dw, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice));
-            WS_CK(cudaMemcpy(db, host + off + (long)c.cout * 9 * ci_o, sizeof(float) * c.cout, cudaMemcpyHostToDevice));
+            WS_CK(copy_on(N->stream, dw, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice));
+            WS_CK(copy_on(N->stream, db, host + off + (long)c.cout * 9 * ci_o, sizeof(float) * c.cout, cudaMemcpyHostToDevice));
         } else {
-            WS_CK(cudaMemcpy(buf.data(), dw, sizeof(float) * buf.size(), cudaMemcpyDeviceToHost));
+            WS_CK(copy_on(N->stream, buf.data(), dw, sizeof(float) * buf.size(), cudaMemcpyDeviceToHost));
             for (int co = 0; co < c.cout; ++co)
                 for (int t = 0; t < 9; ++t)
                     for (int ci = 0; ci < ci_o; ++ci)
                         host[off + ((long)co * 9 + t) * ci_o + ci] = buf[((size_t)co * 9 + t) * c.cin + ci];
-            WS_CK(cudaMemcpy(host + off + (long)c.cout * 9 * ci_o, db, sizeof(float) * c.cout, cudaMemcpyDeviceToHost));
+            WS_CK(copy_on(N->stream, host + off + (long)c.cout * 9 * ci_o, db, sizeof(float) * c.cout, cudaMemcpyDeviceToHost));
         }
         off += (long)c.cout * 9 * ci_o + c.cout;
     }
     const int nh = N->ch[0] + 1;
     float* dh = grads ? N->ghw : N->hw;
     if (to_device)
-        WS_CK(cudaMemcpy(dh, host + off, sizeof(float) * nh, cudaMemcpyHostToDevice));
+        WS_CK(copy_on(N->stream, dh, host + off, sizeof(float) * nh, cudaMemcpyHostToDevice));
     else
-        WS_CK(cudaMemcpy(host + off, dh, sizeof(float) * nh, cudaMemcpyDeviceToHost));
+        WS_CK(copy_on(N->stream, host + off, dh, sizeof(float) * nh, cudaMemcpyDeviceToHost));
     if (to_device && !grads) refresh_bf16(N);
     return TEA_OK;
 }
@@ -624,11 +624,11 @@ int check_err(Net* N, const char* what)
 {
     WS_CK(cudaStreamSynchronize(N->stream));
     int e = 0;
-    WS_CK(cudaMemcpy(&e, N->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    WS_CK(copy_on(N->stream, &e, N->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
         set_status(TEA_ERR_CUDA, "warm start: %s: a tensor-core wait timed out", what);
         int z = 0;
-        cudaMemcpy(N->d_err, &z, sizeof(int), cudaMemcpyHostToDevice);
+        copy_on(N->stream, N->d_err, &z, sizeof(int), cudaMemcpyHostToDevice);
         return TEA_ERR_CUDA;
     }
     return TEA_OK;
@@ -753,8 +753,8 @@ TEA_EXPORT int tea_ws_create_(const int* levels, const int* base, const int* see
             for (int t = 0; t < 9; ++t)
                 for (int ci = 0; ci < ci_real; ++ci) w[((long)co * 9 + t) * c.cin + ci] = sd * nd(rng);
         for (auto& v : b) v = 0.01f * nd(rng);
-        WS_CK(cudaMemcpy(c.w, w.data(), sizeof(float) * nw, cudaMemcpyHostToDevice));
-        WS_CK(cudaMemcpy(c.b, b.data(), sizeof(float) * c.cout, cudaMemcpyHostToDevice));
+        WS_CK(copy_on(N->stream, c.w, w.data(), sizeof(float) * nw, cudaMemcpyHostToDevice));
+        WS_CK(copy_on(N->stream, c.b, b.data(), sizeof(float) * c.cout, cudaMemcpyHostToDevice));
     }
     const int nh = N->ch[0] + 1;
     for (float** p : {&N->hw, &N->ghw, &N->mh, &N->vh})
@@ -869,17 +869,17 @@ TEA_EXPORT int tea_ws_eval_host_(const int* net, const float* x, const float* ta
     }
     if (target) backward(N);
     if ((rc = check_err(N, "eval"))) return rc;
-    WS_CK(cudaMemcpy(y, N->y, sizeof(float) * pix, cudaMemcpyDeviceToHost));
+    WS_CK(copy_on(N->stream, y, N->y, sizeof(float) * pix, cudaMemcpyDeviceToHost));
     if (target) {
         if (kxy) {
             std::vector<float> v(2 * (size_t)*n);
-            WS_CK(cudaMemcpy(v.data(), N->d_img, sizeof(float) * v.size(), cudaMemcpyDeviceToHost));
+            WS_CK(copy_on(N->stream, v.data(), N->d_img, sizeof(float) * v.size(), cudaMemcpyDeviceToHost));
             double r = 0.0;
             for (int b = 0; b < *n; ++b) r += v[2 * b + 1] > 0.f ? (double)v[2 * b] / v[2 * b + 1] : 0.0;
             if (loss) *loss = r / *n;
         } else {
             float s = 0.f;
-            WS_CK(cudaMemcpy(&s, N->d_sums, sizeof(float), cudaMemcpyDeviceToHost));
+            WS_CK(copy_on(N->stream, &s, N->d_sums, sizeof(float), cudaMemcpyDeviceToHost));
             if (loss) *loss = (double)s / (double)pix;
         }
         if (grads && (rc = transfer_params(N, grads, false, true))) return rc;
@@ -1060,8 +1060,8 @@ TEA_EXPORT int tea_ws_predict_(const int* net, const int* chunk, double* du, dou
         rc = TEA_ERR_BAD_ARGUMENT;
     } else if (du) {
         std::vector<double> u(c->field_elems), u0(c->field_elems);
-        cudaMemcpy(u.data(), tmp, sizeof(double) * c->field_elems, cudaMemcpyDeviceToHost);
-        cudaMemcpy(u0.data(), c->alloc[F_U0], sizeof(double) * c->field_elems, cudaMemcpyDeviceToHost);
+        copy_on(c->stream, u.data(), tmp, sizeof(double) * c->field_elems, cudaMemcpyDeviceToHost);
+        copy_on(c->stream, u0.data(), c->alloc[F_U0], sizeof(double) * c->field_elems, cudaMemcpyDeviceToHost);
         for (long i = 0; i < pix; ++i) {
             const long f = kLeadPad + fidx(g, HALO_PAD + (int)(i % g.nx), HALO_PAD + (int)(i / g.nx), 0);
             du[i] = u[f] - u0[f];

@@ -1,7 +1,7 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in the build container (it needs /root/reference and oracle/_ref built by
-``make -C oracle ref``):
+It needs the reference's sources (``TEA_REFERENCE``, default ``/root/reference``) and
+oracle/_ref built from them by ``make -C oracle ref REF=$TEA_REFERENCE``:
 
     python tests/golden/make_golden.py
 
@@ -25,7 +25,7 @@ import sys
 
 HERE = pathlib.Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF = pathlib.Path("/root/reference")
+REF = pathlib.Path(os.environ.get("TEA_REFERENCE", "/root/reference"))
 sys.path.insert(0, str(ROOT))
 
 import __graft_entry__  # noqa: E402
@@ -87,7 +87,7 @@ def _non_square(dim, shape, solver, seed, variant):
     return {"name": name, "dim": dim, "deck": deck}
 
 
-def run_ref(dim: int, deck: str, threads: int) -> dict:
+def run_ref(dim: int, deck: str, threads: int, keep_extra=()) -> dict:
     lib = ROOT / "oracle" / "_ref" / f"libtea_ref{dim}d.so"
     tmp = HERE / f"_tmp_{os.getpid()}"
     tmp.mkdir(exist_ok=True)
@@ -100,7 +100,8 @@ def run_ref(dim: int, deck: str, threads: int) -> dict:
     for p in tmp.iterdir():
         p.unlink()
     tmp.rmdir()
-    keep = ("step", "iterations", "error", "exact_error", "vol", "mass", "ie", "temp", "switch_step", "est_itc")
+    keep = ("step", "iterations", "error", "exact_error", "vol", "mass", "ie", "temp", "switch_step", "est_itc",
+            *keep_extra)
     return {"temp": out["temp"], "qa_diff": out["qa_diff"], "kat_passed": out["kat_passed"],
             "records": [{k: r[k] for k in keep} for r in out["records"]]}
 
