@@ -63,6 +63,7 @@ struct Fused {
     RingLaunch pair;            // k_cheby2_ring2d<OpCheby> (2D); blocks 0: one iteration per launch
     RingLaunch pair32;          // k_cheby2_ring2d<OpCheby32> (2D)
     RingLaunch quad;            // k_cheby4_ring2d<OpCheby> (2D); blocks 0: pairs only
+    RingLaunch quadp;           // the same with the preconditioner (mi staged: more shared memory)
     RingLaunch quad32;          // k_cheby4_ring2d<OpCheby32> (2D)
     RingLaunch ring3[RING_OPS]; // grid and z-segment planes of k_ring3d per sweep (3D)
     RingLaunch ppcg2;           // k_ppcg2_ring3d (3D) / k_ppcg2_ring2d (2D); blocks 0: single steps only
@@ -470,10 +471,14 @@ Fused* ensure_fused(Chunk* c, int max_iters)
                 const int occ3 =
                     smem_occupancy(k_cheby2_ring2d<OpCheby32>, (int)cheby2_smem_bytes<OpCheby32>());
                 F->pair32 = ring_launch(g, sms, occ3, Pair2Geom<float>::OUT, mb);
-                const int occq = smem_occupancy(k_cheby4_ring2d<OpCheby>, (int)cheby4_smem_bytes<OpCheby>());
-                F->quad = ring_launch(g, sms, occq, PassGeom<double, 4, C4_RP>::OUT, mb);
-                const int occq32 = smem_occupancy(k_cheby4_ring2d<OpCheby32>, (int)cheby4_smem_bytes<OpCheby32>());
-                F->quad32 = ring_launch(g, sms, occq32, PassGeom<float, 4, C4_RP>::OUT, mb);
+                // The larger (preconditioned) size last: it stays the kernel's opt-in limit.
+                const int occq = smem_occupancy(k_cheby4_ring2d<OpCheby>, (int)cheby4_smem_bytes<OpCheby>(false));
+                F->quad = ring_launch(g, sms, occq, SkewGeom<double, 4, C4_RP>::OUT, mb);
+                const int occqp = smem_occupancy(k_cheby4_ring2d<OpCheby>, (int)cheby4_smem_bytes<OpCheby>(true));
+                F->quadp = ring_launch(g, sms, occqp, SkewGeom<double, 4, C4_RP>::OUT, mb);
+                const int occq32 =
+                    smem_occupancy(k_cheby4_ring2d<OpCheby32>, (int)cheby4_smem_bytes<OpCheby32>(false));
+                F->quad32 = ring_launch(g, sms, occq32, SkewGeom<float, 4, C4_RP>::OUT, mb);
                 const int occ4 = smem_occupancy(k_ppcg2_ring2d, (int)ppcg2_2d_smem_bytes);
                 F->ppcg2 = ring_launch(g, sms, occ4, Pair2Geom<double>::OUT, mb);
             }
@@ -543,6 +548,18 @@ bool ensure_fp32(Chunk* c, Fused* F)
     return true;
 }
 
+#if TEA_DIM == 2
+// The four-iteration FP64 Chebyshev pass, with the launch of the solve's preconditioner
+// setting (with mi staged it needs more shared memory per warp).
+void launch_cheby4(Fused* F, const FusedArgs& a, bool precond, cudaStream_t s)
+{
+    const RingLaunch& L = precond ? F->quadp : F->quad;
+    FusedArgs ap = a;
+    ap.seg_rows = L.rows;
+    k_cheby4_ring2d<OpCheby><<<L.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby>(precond), s>>>(ap);
+}
+#endif
+
 // Enqueue one iteration of loop `kind` on the chunk's stream.
 void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs& a)
 {
@@ -560,9 +577,7 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
     case LOOP_CHEBY:
 #if TEA_DIM == 2
         if (F->quad.blocks > 0) {
-            FusedArgs ap = a;
-            ap.seg_rows = F->quad.rows;
-            k_cheby4_ring2d<OpCheby><<<F->quad.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby>(), s>>>(ap);
+            launch_cheby4(F, a, F->h_st->precond != 0, s);
             break;
         }
         if (F->pair.blocks > 0) {
@@ -580,7 +595,7 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
             FusedArgs ap = a;
             ap.seg_rows = F->quad32.rows;
             k_cheby4_ring2d<OpCheby32>
-                <<<F->quad32.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby32>(), s>>>(ap);
+                <<<F->quad32.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby32>(false), s>>>(ap);
             break;
         }
         if (F->pair32.blocks > 0) {
@@ -637,7 +652,8 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
 bool build_loop(Chunk* c, Fused* F, int kind, int inner_steps)
 {
     Loop& L = F->loops[kind];
-    const int key = kind == LOOP_PPCG ? inner_steps : 0;
+    // The Chebyshev body's launch depends on the preconditioner (its shared memory).
+    const int key = kind == LOOP_PPCG ? inner_steps : (kind == LOOP_CHEBY ? F->h_st->precond : 0);
     if (L.exec && L.key == key) return true;
     if (L.exec) cudaGraphExecDestroy(L.exec);
     if (L.graph) cudaGraphDestroy(L.graph);
@@ -1230,13 +1246,11 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
             if (F->quad.blocks > 0) {
                 FusedArgs ap = a;
                 if (*kernel == 11) {
-                    ap.seg_rows = F->quad.rows;
-                    k_cheby4_ring2d<OpCheby>
-                        <<<F->quad.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby>(), c->stream>>>(ap);
+                    launch_cheby4(F, a, saved.precond != 0, c->stream);
                 } else {
                     ap.seg_rows = F->quad32.rows;
                     k_cheby4_ring2d<OpCheby32>
-                        <<<F->quad32.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby32>(), c->stream>>>(ap);
+                        <<<F->quad32.blocks, RWARPS * 32, cheby4_smem_bytes<OpCheby32>(false), c->stream>>>(ap);
                 }
             }
             break;

@@ -1979,6 +1979,221 @@ __device__ __forceinline__ void chebyN_body(const FusedArgs& a, Op& op, unsigned
     grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.pass_control(a, v, NIT, checkN); });
 }
 
+// NIT Chebyshev iterations in one pass with the levels skewed by two rows: at loop step t,
+// level l (iteration l of the pass) computes row t - 2l.  Level l at row s reads level
+// l - 1 at rows s - 1, s, s + 1, which level l - 1 produced at steps t - 3, t - 2, t - 1, so
+// no level waits on another within a step and a lane's NIT * VEC cell updates of a step are
+// independent chains (with one row of skew, as in chebyN_body, each level waits for the
+// one below, and the pass was bound by that dependency latency).  The strips, the
+// overlap of strips and segments, the edge handling and the per-cell operations are those of
+// chebyN_body, so the results are the same bits.
+//
+// Rings, per warp: the coefficient rows (u0, Kx, Ky and, when preconditioned, mi) of rows
+// t - 2(NIT - 1) .. t + 1 + RPN, which every level reads, and the operand rows (u, p) of
+// rows t - 1 .. t + 1 + RPN, which only level 0 reads.  Each level keeps its last three u
+// rows and two p rows in registers for the level above.  Away from the domain's edges
+// (warp-uniform per level and row) a cell takes its neighbours without the edge selects.
+template <class T, int NIT, int RPN>
+struct SkewGeom {
+    static constexpr int VEC = RingGeom<T>::VEC;
+    static constexpr int STRIP = RingGeom<T>::STRIP;
+    static constexpr int FL = (NIT + VEC - 1) / VEC;  // first lane that writes
+    static constexpr int OUT = (32 - 2 * FL) * VEC;
+    static constexpr int RQC = 2 * (NIT - 1) + RPN + 2;  // coefficient ring rows per warp
+    static constexpr int RQO = RPN + 3;                  // operand ring rows per warp
+};
+enum { S_U0 = 0, S_KX = 1, S_KY = 2, S_MI = 3 };  // coefficient arrays of a ring row
+
+template <class T, int NIT, int RPN>
+constexpr size_t chebyS_warp_bytes(bool precond)
+{
+    using G = SkewGeom<T, NIT, RPN>;
+    return (size_t)((precond ? 4 : 3) * G::RQC + 2 * G::RQO) * G::STRIP * sizeof(T);
+}
+
+// PRE: the preconditioned form (mi staged and applied); the caller picks it from op.pair_mi.
+template <class Op, int NIT, int RPN, bool PRE>
+__device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned char* s_ring_raw)
+{
+    using T = typename Op::T;
+    using G = SkewGeom<T, NIT, RPN>;
+    constexpr int VEC = G::VEC, STRIP = G::STRIP, OUT = G::OUT, FL = G::FL, RQC = G::RQC, RQO = G::RQO;
+    T al[NIT], be[NIT];
+#pragma unroll
+    for (int l = 0; l < NIT; ++l) op.pass_coefs(a, l, al[l], be[l]);
+    const bool checkN = op.pass_check(a, NIT);
+    const T* mi = op.pair_mi(a);
+    constexpr bool precond = PRE;
+    constexpr int nc = PRE ? 4 : 3;
+    T* unew = op.unew;
+    T* pnew = op.pnext;
+    const Geom& g = a.g;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    T* cring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * (nc * RQC + 2 * RQO) * STRIP;
+    T* oring = cring + (size_t)nc * RQC * STRIP;
+    const T* csrc[4] = {op.pair_rhs(a), op.coef_x(a), op.coef_y(a), mi};
+    const T* usrc = op.ucur;
+    const T* psrc = op.pcur;
+    DDVec<1> acc;
+    acc.zero();
+    const int xlast = g.X - HALO_PAD - 1;
+    const int ylast = g.Y - HALO_PAD - 1;
+    const int per_x = (g.nx + OUT - 1) / OUT;
+    const int per_y = (g.ny + a.seg_rows - 1) / a.seg_rows;
+    const long nseg = (long)per_x * per_y;
+    const long gw = (long)blockIdx.x * RWARPS + warp, nw = (long)gridDim.x * RWARPS;
+    const int cmax = (int)g.pitch - 2 * VEC + 2;
+    const bool out_lane = lane >= FL && lane <= 31 - FL;
+    const T zero = (T)0;
+    auto wrap_c = [](int x) { return x >= RQC ? x - RQC : x; };  // x < 2 RQC
+    auto wrap_o = [](int x) { return x >= RQO ? x - RQO : x; };  // x < 2 RQO
+    for (long sgi = gw; sgi < nseg; sgi += nw) {
+        const int xs = (int)(sgi % per_x), ys = (int)(sgi / per_x);
+        const int c = OUT * xs + VEC * (lane - FL) + HALO_PAD;
+        const int cc = min(c < 0 ? c + VEC : c, cmax);
+        // Does the strip hold the first or the last inner column (edge selects needed)?
+        const bool xedge = __any_sync(0xffffffffu, c == HALO_PAD || (c <= xlast && xlast < c + VEC));
+        const int j0 = HALO_PAD + a.seg_rows * ys;
+        const int j1 = min(j0 + a.seg_rows, ylast + 1);
+        const int a0 = max(HALO_PAD, j0 - (NIT - 1));        // first row of level 1
+        const int t_last = j1 - 1 + 2 * (NIT - 1);          // the last level reaches row j1 - 1
+        const int rlast = min(j1 + NIT - 1, ylast + 1);     // last ring row (level 0 needs rows to j1 + NIT - 2)
+        // Ring index of row r is (r - a0 + 1) mod RQC (coefficients) and mod RQO (operands).
+        auto issue = [&](int r, int ci, int oi) {
+            if (r <= rlast) {
+                T* cb = cring + (size_t)ci * nc * STRIP + VEC * lane;
+                T* ob = oring + (size_t)oi * 2 * STRIP + VEC * lane;
+                const int urow = refl(r, g.Y);
+                const int irow = min(max(r, HALO_PAD), ylast + 1);
+#pragma unroll
+                for (int k = 0; k < nc; ++k) cp_async_16(cb + k * STRIP, csrc[k] + fidx(g, cc, irow, 0));
+                cp_async_16(ob, usrc + fidx(g, cc, urow, 0));
+                cp_async_16(ob + STRIP, psrc + fidx(g, cc, irow, 0));
+            }
+            cp_async_commit();
+        };
+        // Level l at row s (ring index ci): the operand rows m (s - 1), cv (s), n (s + 1) and
+        // p of the level below; u and p of the level into uo, po.  Rows outside the level's
+        // cone (above the segment's first ring row, or past the rows the last level needs)
+        // are skipped; s and l are warp-uniform, so the shuffles stay uniform.
+        auto level = [&](int l, int s, int ci, const T* m, const T* cv, const T* n, const T* pin, T* uo, T* po,
+                         bool last) {
+            if (s < a0 || s > ylast || s > j1 + NIT - 2 - l) return;
+            const T* rs = cring + (size_t)ci * nc * STRIP + VEC * lane;
+            const T* rs1 = cring + (size_t)wrap_c(ci + 1) * nc * STRIP + VEC * lane;
+            const T up = __shfl_up_sync(0xffffffffu, cv[VEC - 1], 1);
+            const T dn = __shfl_down_sync(0xffffffffu, cv[0], 1);
+            T kx[VEC + 1];
+            ld_vec(rs + S_KX * STRIP, kx);
+            kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
+            T ky0[VEC], ky1[VEC], rhs[VEC], m0[VEC];
+            ld_vec(rs + S_KY * STRIP, ky0);
+            ld_vec(rs1 + S_KY * STRIP, ky1);
+            ld_vec(rs + S_U0 * STRIP, rhs);
+            if (precond) ld_vec(rs + S_MI * STRIP, m0);
+            const bool edge = xedge || s == HALO_PAD || s == ylast;
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                NbT<T> nb;
+                nb.zm = nb.zp = zero;
+                nb.c = cv[q];
+                if (edge) {
+                    nb.xm = c + q == HALO_PAD ? cv[q] : (q == 0 ? up : cv[q > 0 ? q - 1 : 0]);
+                    nb.xp = c + q == xlast ? cv[q] : (q == VEC - 1 ? dn : cv[q < VEC - 1 ? q + 1 : q]);
+                    nb.ym = s == HALO_PAD ? cv[q] : m[q];
+                    nb.yp = s == ylast ? cv[q] : n[q];
+                } else {
+                    nb.xm = q == 0 ? up : cv[q > 0 ? q - 1 : 0];
+                    nb.xp = q == VEC - 1 ? dn : cv[q < VEC - 1 ? q + 1 : q];
+                    nb.ym = m[q];
+                    nb.yp = n[q];
+                }
+                const T w = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], zero, zero);
+                const T r = rhs[q] - w;
+                po[q] = al[l] * pin[q] + be[l] * (precond ? m0[q] * r : r);
+                uo[q] = cv[q] + po[q];
+                if (last && checkN && out_lane && c + q <= xlast) dd_add(acc.v[0], (double)r * (double)r);
+            }
+        };
+        // Rows a0 - 1 .. a0 + RPN + 1 first; each step then issues the next new row, so row
+        // t + 1 has exactly RPN groups after it at the top of step t.
+        for (int r = a0 - 1; r <= a0 + RPN + 1; ++r) issue(r, (r - a0 + 1) % RQC, (r - a0 + 1) % RQO);
+        cp_async_wait<RPN + 1>();
+        __syncwarp();
+        T um[VEC], uc[VEC];
+        ld_vec(oring + VEC * lane, um);                                   // row a0 - 1
+        ld_vec(oring + (size_t)(1 % RQO) * 2 * STRIP + VEC * lane, uc);  // row a0
+        // Level l < NIT - 1 keeps the u rows it produced at the last three steps (H[l][0]:
+        // step t - 1, i.e. row t - 1 - 2l) and its p of the last two steps.
+        T H[NIT - 1][3][VEC], PH[NIT - 1][2][VEC];
+#pragma unroll
+        for (int l = 0; l < NIT - 1; ++l)
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) H[l][0][q] = H[l][1][q] = H[l][2][q] = PH[l][0][q] = PH[l][1][q] = zero;
+        int ct = 1 % RQC, ot = 1 % RQO;  // ring indices of row t
+        for (int t = a0; t <= t_last; ++t) {
+            cp_async_wait<RPN>();
+            __syncwarp();
+            T un[VEC], p0[VEC];
+            ld_vec(oring + (size_t)wrap_o(ot + 1) * 2 * STRIP + VEC * lane, un);
+            ld_vec(oring + (size_t)ot * 2 * STRIP + STRIP + VEC * lane, p0);
+            T NU[NIT][VEC], NP[NIT][VEC];
+#pragma unroll
+            for (int l = 0; l < NIT; ++l)
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) NU[l][q] = NP[l][q] = zero;
+            level(0, t, ct, um, uc, un, p0, NU[0], NP[0], NIT == 1 && t >= j0);
+#pragma unroll
+            for (int l = 1; l < NIT; ++l) {
+                const int s = t - 2 * l;
+                level(l, s, wrap_c(ct + RQC - 2 * l), H[l - 1][2], H[l - 1][1], H[l - 1][0], PH[l - 1][1], NU[l],
+                      NP[l], l == NIT - 1 && s >= j0);
+            }
+            const int sl = t - 2 * (NIT - 1);  // the row the last level reached
+            if (sl >= j0 && sl < j1 && out_lane) {
+                const long i = fidx(g, c, sl, 0);
+                if (c + VEC - 1 <= xlast) {
+                    st_vec(unew + i, NU[NIT - 1]);
+                    st_vec(pnew + i, NP[NIT - 1]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) {
+                        if (c + q <= xlast) {
+                            unew[i + q] = NU[NIT - 1][q];
+                            pnew[i + q] = NP[NIT - 1][q];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int l = 0; l < NIT - 1; ++l)
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    H[l][2][q] = H[l][1][q];
+                    H[l][1][q] = H[l][0][q];
+                    H[l][0][q] = NU[l][q];
+                    PH[l][1][q] = PH[l][0][q];
+                    PH[l][0][q] = NP[l][q];
+                }
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                um[q] = uc[q];
+                uc[q] = un[q];
+            }
+            __syncwarp();
+            // Row t + RPN + 2 goes into the coefficient slot of row t - 2(NIT - 1) and the
+            // operand slot of row t - 1, which no lane reads any more.
+            issue(t + RPN + 2, wrap_c(ct + RPN + 2), wrap_o(ot + RPN + 2));
+            ct = wrap_c(ct + 1);
+            ot = wrap_o(ot + 1);
+        }
+        cp_async_wait<0>();
+        __syncwarp();
+    }
+    grid_reduce_then<1>(acc, a.red, [&](const double* v) { op.pass_control(a, v, NIT, checkN); });
+}
+
 // Op: OpCheby (FP64, the reference's iteration) or OpCheby32 (the FP32 inner solve).  Two
 // iterations when the state allows (pass_ok), else one.
 template <class Op>
@@ -1991,23 +2206,30 @@ __global__ void __launch_bounds__(RWARPS * 32) k_cheby2_ring2d(FusedArgs a)
     else ring2d_body(a, op, s_ring_raw);
 }
 
-// Four iterations when the state allows, else two, else one.
+// Four iterations (skewed levels) when the state allows, else two, else one.  The shared
+// memory a launch needs depends on whether mi is staged (the preconditioned FP64 solve).
 constexpr int C4_RP = 1;  // ring rows in flight beyond row t+1 in the four-iteration pass
 template <class Op>
-constexpr size_t cheby4_smem_bytes()
+constexpr size_t cheby4_smem_bytes(bool precond)
 {
-    return chebyN_smem_bytes<Op, 4, C4_RP>() > cheby2_smem_bytes<Op>() ? chebyN_smem_bytes<Op, 4, C4_RP>()
-                                                                          : cheby2_smem_bytes<Op>();
+    using T = typename Op::T;
+    const size_t quad = (size_t)RWARPS * chebyS_warp_bytes<T, 4, C4_RP>(precond);
+    return quad > cheby2_smem_bytes<Op>() ? quad : cheby2_smem_bytes<Op>();
 }
 template <class Op>
-__global__ void __launch_bounds__(RWARPS * 32) k_cheby4_ring2d(FusedArgs a)
+__global__ void __launch_bounds__(RWARPS * 32, 3) k_cheby4_ring2d(FusedArgs a)
 {
     extern __shared__ __align__(16) unsigned char s_ring_raw[];
     Op op;
     op.begin(a);
-    if (op.pass_ok(a, 4)) chebyN_body<Op, 4, C4_RP>(a, op, s_ring_raw);
-    else if (op.pass_ok(a, 2)) chebyN_body<Op, 2, C2_RP>(a, op, s_ring_raw);
-    else ring2d_body(a, op, s_ring_raw);
+    if (op.pass_ok(a, 4)) {
+        if (op.pair_mi(a)) chebyS_body<Op, 4, C4_RP, true>(a, op, s_ring_raw);
+        else chebyS_body<Op, 4, C4_RP, false>(a, op, s_ring_raw);
+    } else if (op.pass_ok(a, 2)) {
+        chebyN_body<Op, 2, C2_RP>(a, op, s_ring_raw);
+    } else {
+        ring2d_body(a, op, s_ring_raw);
+    }
 }
 
 // Two PPCG inner steps in one pass over the 2D field (temporal blocking), the 2D form of

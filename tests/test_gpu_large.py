@@ -1,0 +1,84 @@
+"""Parity at the benchmark configurations' own sizes, against the reference's own runs.
+
+tests/golden/ref_large.json holds the reference's Kokkos-OpenMP kernels (oracle/_ref,
+driven by the C++ driver, make_golden_large.py) on:
+
+* C1: 2D 512^2, 6 seeded states, CG, eps 1e-15, 10 timesteps;
+* C2: 2D 4096^2, 16 seeded states, Chebyshev (30 CG presteps) to relative residual 1e-10
+  for 30 timesteps, and PPCG (10 inner steps) to relative residual 1e-8 for timestep 1;
+* C3: 3D 256^3, 12 seeded states, CG and PPCG to relative residual 1e-10, timestep 1.
+
+The CUDA library runs each deck through the whole-solve entry point (the benchmark's
+path) and through the per-call ext_* entry points (the path an unchanged Fortran driver
+takes).  Bars: field summary within 1e-10 relative per step; iteration counts within 1 for
+CG and PPCG and within 10 for Chebyshev, whose residual is only tested every tenth
+iteration once n >= est_itc (tealeaf_2d/tea_solve.f90:260), so a rounding difference in
+the error moves the exit by one check; the Chebyshev switch step within 1.  The
+FP32-refined form is held to the FP64 reference's field summary within 1e-9.
+"""
+import json
+
+import pytest
+
+from conftest import GOLDEN, rel, tea
+
+pytestmark = pytest.mark.gpu
+
+FIELD_SUMMARY_TOL = 1e-10
+FP32_FIELD_SUMMARY_TOL = 1e-9
+ITER_TOL = {"tl_use_cg": 1, "tl_use_ppcg": 1, "tl_use_chebyshev": 10}
+PER_CALL_STEPS = 2  # per-call runs of the 30-timestep deck stop after this many timesteps
+
+
+def _cases():
+    return json.loads((GOLDEN / "ref_large.json").read_text())
+
+
+def _solver(deck):
+    return next(k for k in ITER_TOL if k in deck)
+
+
+def _check(name, got, ref, deck, steps):
+    tol = ITER_TOL[_solver(deck)]
+    assert len(got) >= steps and len(ref) >= steps
+    for a, b in zip(got[:steps], ref[:steps]):
+        assert abs(a["iterations"] - b["iterations"]) <= tol, (name, a["step"], a["iterations"], b["iterations"])
+        if b["switch_step"]:
+            assert abs(a["switch_step"] - b["switch_step"]) <= 1, (name, a["step"], a["switch_step"],
+                                                                   b["switch_step"])
+        for k in ("vol", "mass", "ie", "temp"):
+            assert rel(a[k], b[k]) <= FIELD_SUMMARY_TOL, (name, a["step"], k, a[k], b[k], rel(a[k], b[k]))
+
+
+@pytest.mark.parametrize("name", sorted(_cases()))
+def test_whole_solve_matches_reference_at_size(name):
+    case = _cases()[name]
+    ref = case["ref"]["records"]
+    _, got = tea.run_deck(case["deck"], case["dim"], fused=True, summary_every_step=True)
+    _check(name, got, ref, case["deck"], len(ref))
+
+
+@pytest.mark.parametrize("name", sorted(_cases()))
+def test_per_call_path_matches_reference_at_size(name):
+    case = _cases()[name]
+    ref = case["ref"]["records"]
+    steps = min(len(ref), PER_CALL_STEPS if len(ref) > 10 else len(ref))
+    _, got = tea.run_deck(case["deck"], case["dim"], fused=False, summary_every_step=True, end_step=steps)
+    _check(name, got, ref, case["deck"], steps)
+
+
+FP32_CASES = [("c2_2d4096_cheby", 3), ("c3_3d256_cg", 1), ("c3_3d256_ppcg", 1)]
+
+
+@pytest.mark.parametrize("name,steps", [c for c in FP32_CASES if c[0] in _cases()])
+def test_fp32_refined_within_1e9_of_fp64_reference_at_size(name, steps):
+    case = _cases()[name]
+    ref = case["ref"]["records"]
+    _, got = tea.run_deck(case["deck"], case["dim"], fused=True, precision=tea.PRECISION_FP32_REFINED,
+                          summary_every_step=True, end_step=steps)
+    for a, b in zip(got[:steps], ref[:steps]):
+        assert a["corrections"] >= 1
+        if a["exact_error"] or b["exact_error"]:
+            assert a["exact_error"] < a["eps_used"], (name, a["step"], a["exact_error"], a["eps_used"])
+        for k in ("vol", "mass", "ie", "temp"):
+            assert rel(a[k], b[k]) <= FP32_FIELD_SUMMARY_TOL, (name, a["step"], k, a[k], b[k], rel(a[k], b[k]))

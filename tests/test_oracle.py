@@ -106,3 +106,18 @@ def test_port_bitwise_equals_live_reference_on_tiny_grids(tmp_path, dim, shape, 
     for a, b in zip(recs, ref):
         for k in FIELDS:
             assert same(a[k], b[k]), (shape, solver, b["step"], k, a[k], b[k])
+
+
+def test_port_bitwise_equals_reference_at_c1_size():
+    """The 2D 512^2 configuration (6 seeded states, CG, eps 1e-15, 10 timesteps; about 11,000
+    iterations) at its stated size: the port, with its sums in the reference's single-thread
+    order, reproduces every per-step iteration count, error, exact error and field summary
+    of the reference's own kernels (tests/golden/ref_large.json, recorded at one thread)."""
+    case = json.loads((pathlib.Path(__file__).parent / "golden" / "ref_large.json").read_text())["c1_2d512_cg"]
+    assert case["threads"] == 1
+    _, recs = tea.run_deck(case["deck"], 2, backend=port_lib(2, SUM_SEQUENTIAL), summary_every_step=True)
+    ref = case["ref"]["records"]
+    assert len(recs) == len(ref) == 10
+    for a, b in zip(recs, ref):
+        for k in FIELDS:
+            assert same(a[k], b[k]), f"step {b['step']} {k}: port {a[k]!r} reference {b[k]!r}"
