@@ -60,7 +60,7 @@ WORDS = {  # algorithmic FP64 words per interior cell of one launch
 KERNEL_IDS = {"cg_sweep_a": 2, "cheby_quad": 11, "cheby_pair": 6, "cg_sweep_b": 5}
 ALL_KERNEL_IDS = {"ppcg_inner": 1, "cg_sweep_a": 2, "cheby_iterate": 3, "jacobi": 4, "cg_sweep_b": 5,
                   "cheby_pair": 6, "cg32_sweep_a": 7, "cg32_sweep_b": 8, "cheby32_pair": 9, "ppcg_pair": 10,
-                  "cheby_quad": 11, "cheby32_quad": 12}
+                  "cheby_quad": 11, "cheby32_quad": 12, "ppcg32_pair": 13}
 PROFILES = ROOT / "profiles"
 # The reference's own per-timestep iteration counts on this deck (its Kokkos-OpenMP kernels,
 # oracle/_ref, 30 timesteps at 4096^2), recorded by tests/golden/make_golden_large.py.  They
@@ -513,31 +513,44 @@ WORKLOADS_3D = {
 }
 
 
-def workload_3d(args):
-    """--workload NAME: s/timestep of a 3D configuration, plain FP64 and FP32-refined, each
-    timestep's solve timed by the driver around the synchronous ext_tea_leaf_solve_ call."""
-    w = WORKLOADS_3D[args.workload]
+INNER_SOLVERS = {0: "cg", 1: "chebyshev", 2: "ppcg"}
+
+
+def run_3d(workload, warmup, steps):
+    """s/timestep of a 3D configuration, plain FP64 and FP32-refined on the same deck, each
+    timestep's solve timed by the driver around the synchronous ext_tea_leaf_solve_ call
+    (the reference's wall clock around tea_leaf(), tealeaf_2d/diffuse.f90:74-85); the first
+    `warmup` timesteps are run and not timed."""
+    w = WORKLOADS_3D[workload]
     spec = tea.DeckSpec(dim=3, cells=w["cells"], states=w["states"], seed=w["seed"], solver=w["solver"],
-                        end_step=args.warmup + args.steps, dt=0.004, eps=1e-15, eps_rel=EPS_REL, max_iters=20000,
+                        end_step=warmup + steps, dt=0.004, eps=1e-15, eps_rel=EPS_REL, max_iters=20000,
                         presteps=30, inner_steps=10, check_result=True, summary_frequency=0)
     deck = tea.seeded_deck(spec)
-    out = {"workload": args.workload, "cells": w["cells"] ** 3, "solver": w["solver"], "unit": "s/timestep",
-           "timesteps_timed": list(range(args.warmup + 1, args.warmup + args.steps + 1))}
+    out = {"workload": workload, "cells": w["cells"] ** 3, "states": w["states"], "solver": w["solver"],
+           "unit": "s/timestep", "rel_residual": EPS_REL, "timesteps_timed": list(range(warmup + 1, warmup + steps + 1))}
     summaries = {}
     for name, precision in (("fp64", tea.PRECISION_FP64), ("fp32_refined", tea.PRECISION_FP32_REFINED)):
         summary, recs = tea.run_deck(deck, 3, fused=True, precision=precision, summary_every_step=True)
-        timed = recs[args.warmup:args.warmup + args.steps]
+        timed = recs[warmup:warmup + steps]
         summaries[name] = summary
         out[name] = {"s_per_step": sum(r["solve_seconds"] for r in timed) / len(timed),
+                     "per_step_s": [r["solve_seconds"] for r in timed],
                      "iterations": [r["iterations"] for r in timed],
                      "switch_step": [r["switch_step"] for r in timed],
                      "cheby_steps": [r["cheby_steps"] for r in timed],
                      "corrections": [r["corrections"] for r in timed],
                      "exact_error_over_eps": [r["exact_error"] / r["eps_used"] for r in timed]}
+        if precision == tea.PRECISION_FP32_REFINED:
+            out[name]["inner_solver"] = [INNER_SOLVERS.get(r["inner_solver"], "?") for r in timed]
     out["speedup_fp32_refined"] = out["fp64"]["s_per_step"] / out["fp32_refined"]["s_per_step"]
     out["field_summary_max_rel_diff"] = max(
         tea.rel_diff(summaries["fp64"][k], summaries["fp32_refined"][k]) for k in ("vol", "mass", "ie", "temp"))
-    print(json.dumps(out))
+    return out
+
+
+def workload_3d(args):
+    """--workload NAME: run_3d of that configuration with the command line's steps."""
+    print(json.dumps(run_3d(args.workload, args.warmup, args.steps)))
 
 
 def learned_arm(args, world):
@@ -566,7 +579,7 @@ def learned_arm(args, world):
 # Algorithmic FP64-equivalent words per cell of each fused kernel in 3D (FP32 words count
 # half): the 7-point sweeps read one more coefficient array than their 2D forms.
 WORDS_3D = {"ppcg_inner": 9, "cg_sweep_a": 9, "cheby_iterate": 8, "jacobi": 6, "cg_sweep_b": 3, "cheby_pair": 8,
-            "cg32_sweep_a": 4.5, "cg32_sweep_b": 1.5, "cheby32_pair": 4, "ppcg_pair": 9}
+            "cg32_sweep_a": 4.5, "cg32_sweep_b": 1.5, "cheby32_pair": 4, "ppcg_pair": 9, "ppcg32_pair": 4.5}
 
 
 def kernel_only_3d(args):
@@ -574,7 +587,7 @@ def kernel_only_3d(args):
     (the FP32-refined form for the FP32 kernels, so that their arrays exist), then K launched
     1 + reps times back to back on the chunk's live fields."""
     w = WORKLOADS_3D[args.workload]
-    fp32 = args.kernel.startswith(("cg32", "cheby32"))
+    fp32 = args.kernel.startswith(("cg32", "cheby32", "ppcg32"))
     spec = tea.DeckSpec(dim=3, cells=w["cells"], states=w["states"], seed=w["seed"], solver=w["solver"], end_step=1,
                         dt=0.004, eps=1e-15, eps_rel=EPS_REL, max_iters=20000, presteps=30, inner_steps=10,
                         check_result=False, summary_frequency=0)
@@ -623,6 +636,8 @@ def main():
     ap.add_argument("--no-refined", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-per-call", action="store_true", help="skip timing the per-call ext_* path")
+    ap.add_argument("--no-3d", action="store_true",
+                    help="skip the 3D 512^3 PPCG line (plain FP64 against FP32-refined, 1 + 5 timesteps each)")
     ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS),
                     help="only launch one fused kernel --reps times on the 4096^2 workload, or after one "
                          "timestep of --workload (for ncu captures)")
@@ -650,6 +665,9 @@ def main():
     if e2e and world > 1:
         e2e["value"] = dist_max(e2e["value"], world)  # the slowest replica, as for value
     per_call = None if args.no_per_call else per_call_arm()
+    # The 3D 512^3 PPCG configuration: plain FP64 against FP32-refined (FP32 PPCG
+    # corrections), one warm-up timestep and five timed ones each.
+    c5 = None if args.no_3d else run_3d("3d512_ppcg", 1, 5)
     if rank != 0:
         dist_done(world)
         return
@@ -732,6 +750,8 @@ def main():
                          "loss_first": learned["loss_first"], "loss_last": learned["loss_last"]},
             "amortised_after_steps": (cost / saved) if saved and saved > 0 else None,
             "clocks": learned["clocks"]}
+    if c5:
+        line["c5_3d512_ppcg"] = c5
     if per_call:
         # The same deck through the per-call ext_* entry points (what an unchanged Fortran
         # driver calls), timestep 2; the fused arm's timesteps are later ones.

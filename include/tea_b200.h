@@ -169,7 +169,10 @@ typedef struct {
     double warm_r0_plain;   /* with a network attached: sum r^2 of the start u = u0
                                (0 on a timestep the back-off skipped) */
     double warm_r0_guess;   /* ... and of the start u = u0 + the network's du */
-    double reserved[5];
+    int inner_solver;       /* FP32_REFINED: inner solver of the last correction: 0 CG,
+                               1 Chebyshev, 2 PPCG */
+    int pad;
+    double reserved[4];
 } tea_solve_result;
 
 /* Whole implicit solve of one timestep on the device: the control flow of

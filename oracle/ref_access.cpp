@@ -78,3 +78,64 @@ extern "C" int tea_write_field_(const int* chunk, const int* field, const double
     std::memcpy(v.ptr_on_device(), in, sizeof(double) * c->fullDomain);
     return 0;
 }
+
+// ext_initialise_chunk_ with the cell centres a one-thread dispatch computes.
+//
+// InitialiseChunkVertices (tealeaf_2d/ext_initialise_chunk.hpp:13-61, tealeaf_3d: the
+// same with z) writes vertex(index) and reads vertex(index + 1) in one parallel_for, so a
+// cell centre depends on whether the thread owning index + 1 has run yet.  On one thread
+// it never has: cell(i) = 0.5 * (vertex(i) + the value vertex(i + 1) held before the
+// call).  On several OpenMP threads the cells at the ends of the threads' index ranges get
+// the written value instead, and circles/spheres are painted differently along those
+// columns, rows and planes.  This build renames the reference's entry point (objcopy in
+// oracle/Makefile) and runs it through this wrapper, which recomputes the cell centres as
+// the one-thread run does, so that fixtures recorded on several threads describe the same
+// problem as one-thread runs (and as the oracle and the CUDA library, which follow the
+// one-thread result).
+#include <vector>
+
+namespace {
+
+std::vector<double> snapshot(const FieldView& v)
+{
+    std::vector<double> out(v.dimension_0());
+    if (!out.empty()) std::memcpy(out.data(), v.ptr_on_device(), sizeof(double) * out.size());
+    return out;
+}
+
+void one_thread_centres(const FieldView& vertex, const FieldView& cell, const std::vector<double>& old, int n)
+{
+    for (int i = 0; i < n; ++i) cell(i) = 0.5 * (vertex(i) + old[i + 1]);
+}
+
+}  // namespace
+
+#if TEA_DIM == 2
+extern "C" void ref_initialise_chunk_orig_(const int* chunk, const double* xMin, const double* yMin,
+                                           const double* dx, const double* dy);
+
+extern "C" void ext_initialise_chunk_(const int* chunk, const double* xMin, const double* yMin, const double* dx,
+                                      const double* dy)
+{
+    TeaLeafChunk<DEVICE>* c = chunk_at(chunk);
+    const std::vector<double> vx = snapshot(c->vertexX), vy = snapshot(c->vertexY);
+    ref_initialise_chunk_orig_(chunk, xMin, yMin, dx, dy);
+    one_thread_centres(c->vertexX, c->cellX, vx, c->dims.x);
+    one_thread_centres(c->vertexY, c->cellY, vy, c->dims.y);
+}
+#else
+extern "C" void ref_initialise_chunk_orig_(const int* chunk, const double* xMin, const double* yMin,
+                                           const double* zMin, const double* dx, const double* dy,
+                                           const double* dz);
+
+extern "C" void ext_initialise_chunk_(const int* chunk, const double* xMin, const double* yMin, const double* zMin,
+                                      const double* dx, const double* dy, const double* dz)
+{
+    TeaLeafChunk<DEVICE>* c = chunk_at(chunk);
+    const std::vector<double> vx = snapshot(c->vertexX), vy = snapshot(c->vertexY), vz = snapshot(c->vertexZ);
+    ref_initialise_chunk_orig_(chunk, xMin, yMin, zMin, dx, dy, dz);
+    one_thread_centres(c->vertexX, c->cellX, vx, c->dims.x);
+    one_thread_centres(c->vertexY, c->cellY, vy, c->dims.y);
+    one_thread_centres(c->vertexZ, c->cellZ, vz, c->dims.z);
+}
+#endif

@@ -94,7 +94,7 @@ class StepRecord(ctypes.Structure):
         ("ie", ctypes.c_double), ("temp", ctypes.c_double), ("has_summary", ctypes.c_int),
         ("switch_step", ctypes.c_int), ("est_itc", ctypes.c_int), ("warm_start_used", ctypes.c_int),
         ("wall_end", ctypes.c_double), ("h2d_bytes", ctypes.c_longlong), ("d2h_bytes", ctypes.c_longlong),
-        ("corrections", ctypes.c_int), ("pad2", ctypes.c_int),
+        ("corrections", ctypes.c_int), ("inner_solver", ctypes.c_int),
     ]
 
 
@@ -221,7 +221,7 @@ class SolveResult(ctypes.Structure):
         ("error", ctypes.c_double), ("exact_error", ctypes.c_double), ("eps_used", ctypes.c_double),
         ("eigmin", ctypes.c_double), ("eigmax", ctypes.c_double), ("corrections", ctypes.c_int),
         ("warm_start_used", ctypes.c_int), ("warm_r0_plain", ctypes.c_double), ("warm_r0_guess", ctypes.c_double),
-        ("reserved", ctypes.c_double * 5),
+        ("inner_solver", ctypes.c_int), ("pad", ctypes.c_int), ("reserved", ctypes.c_double * 4),
     ]
 
 

@@ -36,7 +36,10 @@ void update_halo(Chunk* c, const int* neighbours, const int* fields, int depth);
 
 namespace {
 
-enum { LOOP_CG = 0, LOOP_CHEBY = 1, LOOP_PPCG = 2, LOOP_JACOBI = 3, LOOP_CG32 = 4, LOOP_CHEBY32 = 5, LOOP_COUNT = 6 };
+enum {
+    LOOP_CG = 0, LOOP_CHEBY = 1, LOOP_PPCG = 2, LOOP_JACOBI = 3, LOOP_CG32 = 4, LOOP_CHEBY32 = 5, LOOP_PPCG32 = 6,
+    LOOP_COUNT = 7
+};
 
 struct Loop {
     cudaGraph_t graph = nullptr;
@@ -53,7 +56,7 @@ struct Fused {
     SolveState* d_st = nullptr;
     SolveState* h_st = nullptr;  // pinned
     double* alt[3] = {nullptr, nullptr, nullptr};  // allocations of u, p, sd second buffers
-    float* alloc32[8] = {};  // FP32 arrays of the defect-correction form (allocated on first use)
+    float* alloc32[10] = {};  // FP32 arrays of the defect-correction form (allocated on first use)
     double *d_cg_alphas = nullptr, *d_cg_betas = nullptr;
     double *d_ch_alphas = nullptr, *d_ch_betas = nullptr;
     int cap = 0;  // entries of the coefficient arrays
@@ -67,6 +70,7 @@ struct Fused {
     RingLaunch quad32;          // k_cheby4_ring2d<OpCheby32> (2D)
     RingLaunch ring3[RING_OPS]; // grid and z-segment planes of k_ring3d per sweep (3D)
     RingLaunch ppcg2;           // k_ppcg2_ring3d (3D) / k_ppcg2_ring2d (2D); blocks 0: single steps only
+    RingLaunch ppcg2_32;        // k_ppcg2_ring3d<PpcgF32> (3D): the FP32 inner PPCG; blocks 0: none
     int stencil_mode = 0;  // 0: the faster kernel per sweep, 1: register pipeline only, 2: ring only
     Loop loops[LOOP_COUNT];
     bool use_graph = true;
@@ -449,9 +453,12 @@ Fused* ensure_fused(Chunk* c, int max_iters)
             setup_ring3<OpSweepA32>(F, g, sms, mb);
             setup_ring3<OpOuterResid>(F, g, sms, mb);
             setup_ring3<OpCheby32>(F, g, sms, mb);
-            const int occ = smem_occupancy(k_ppcg2_ring3d<PPCG2_TY, PPCG2_RP>,
-                                           (int)ppcg2_smem_bytes<PPCG2_TY, PPCG2_RP>(), PPCG2_TY * 32);
+            const int occ = smem_occupancy(k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP>,
+                                           (int)ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP>(), PPCG2_TY * 32);
             F->ppcg2 = ring3_launch(g, sms, occ, 30 * RingGeom<double>::VEC, PPCG2_TY - 2, mb);
+            const int occ32 = smem_occupancy(k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP>,
+                                             (int)ppcg2_smem_bytes<float, PPCG2_TY, PPCG2_RP>(), PPCG2_TY * 32);
+            F->ppcg2_32 = ring3_launch(g, sms, occ32, 30 * RingGeom<float>::VEC, PPCG2_TY - 2, mb);
         }
 #else
         {
@@ -527,8 +534,8 @@ bool ensure_fp32(Chunk* c, Fused* F)
 {
     if (F->alloc32[0]) return true;
     const size_t bytes = c->field_elems * sizeof(float);
-    for (int k = 0; k < 8; ++k) {
-        if (k == 2 && DIM != 3) continue;
+    for (int k = 0; k < 10; ++k) {
+        if ((k == 2 || k >= 8) && DIM != 3) continue;  // Kz and the inner PPCG's sd (3D only)
         TEA_CK(cudaMalloc(&F->alloc32[k], bytes));
         if (!F->alloc32[k]) return false;
         TEA_CK(cudaMemset(F->alloc32[k], 0, bytes));
@@ -545,6 +552,8 @@ bool ensure_fp32(Chunk* c, Fused* F)
     a.p32[1] = F->alloc32[7] + kLeadPad;
     a.dc32[0] = a.d32;
     a.dc32[1] = a.w32;
+    a.sd32[0] = DIM == 3 ? F->alloc32[8] + kLeadPad : nullptr;
+    a.sd32[1] = DIM == 3 ? F->alloc32[9] + kLeadPad : nullptr;
     return true;
 }
 
@@ -624,8 +633,8 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
 #if TEA_DIM == 2
             k_ppcg2_ring2d<<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, s>>>(ak);
 #else
-            k_ppcg2_ring3d<PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
-                                                ppcg2_smem_bytes<PPCG2_TY, PPCG2_RP>(), s>>>(ak);
+            k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
+                                                         ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP>(), s>>>(ak);
 #endif
         }
         for (int k = k0; k <= inner_steps; ++k) {
@@ -644,6 +653,26 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         stencil<OpSweepA32>(F, a, s);
         k_cg32_sweep_b<<<F->quad_blocks, 256, 0, s>>>(a);
         break;
+    case LOOP_PPCG32: {
+        // One FP32 inner PPCG iteration (3D, an even number of inner steps, all in pairs):
+        // p = r + beta p and w = A p with p.w, then d += alpha p, r -= alpha w, sd = r / theta,
+        // then the inner steps; the last pair forms r.r and ends the iteration.
+#if TEA_DIM == 3
+        stencil<OpSweepA32>(F, a, s);
+        const int pairs = inner_steps / 2;
+        FusedArgs ab = a;
+        ab.r_in_w = pairs & 1;
+        k_ppcg32_sweep_b<<<F->quad_blocks, 256, 0, s>>>(ab);
+        for (int m = 1, k0 = 1; m <= pairs; ++m, k0 += 2) {
+            FusedArgs ak = ab;
+            ak.step = k0;
+            ak.seg_rows = F->ppcg2_32.rows;
+            k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP><<<F->ppcg2_32.blocks, PPCG2_TY * 32,
+                                                         ppcg2_smem_bytes<float, PPCG2_TY, PPCG2_RP>(), s>>>(ak);
+        }
+#endif
+        break;
+    }
     }
 }
 
@@ -653,7 +682,8 @@ bool build_loop(Chunk* c, Fused* F, int kind, int inner_steps)
 {
     Loop& L = F->loops[kind];
     // The Chebyshev body's launch depends on the preconditioner (its shared memory).
-    const int key = kind == LOOP_PPCG ? inner_steps : (kind == LOOP_CHEBY ? F->h_st->precond : 0);
+    const int key = (kind == LOOP_PPCG || kind == LOOP_PPCG32) ? inner_steps
+                                                               : (kind == LOOP_CHEBY ? F->h_st->precond : 0);
     if (L.exec && L.key == key) return true;
     if (L.exec) cudaGraphExecDestroy(L.exec);
     if (L.graph) cudaGraphDestroy(L.graph);
@@ -922,13 +952,15 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
     bool p_halo_fresh = true;
 
     int corrections = 0;
+    int last_inner_mode = 0;  // FP32-refined: inner solver of the last correction kept
     if (P->precision == TEA_PRECISION_FP32_REFINED) {
         // Defect correction: FP64 outer residual, update and convergence test; FP32 inner
         // solves.  CG and Jacobi decks: every inner solve is CG.  Chebyshev and PPCG decks:
         // the first inner solve is CG, whose scalars give the Lanczos eigenvalue bounds
-        // (computed in FP64 on the host), and the following ones are Chebyshev -- the
-        // plain solve's CG-then-Chebyshev order, with the spectrum taken from a CG run
-        // long enough to resolve it.
+        // (computed in FP64 on the host), and the following ones are Chebyshev (PPCG decks
+        // in 3D with an even number of inner steps: PPCG with the deck's inner steps) --
+        // the plain solve's CG-then-Chebyshev/PPCG order, with the spectrum taken from a CG
+        // run long enough to resolve it.
         if (!ensure_fp32(c, F)) {
             R->status = TEA_ERR_CUDA;
             return;
@@ -938,7 +970,9 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
         const double tol = P->inner_tol > 0.0 ? P->inner_tol : 1e-4;
         // Chebyshev decks: the first correction's inner CG also estimates the spectrum.
         const bool want_cheby = cheby || ppcg;
-        bool inner_cheby = false;
+        int inner_mode = 0;  // the inner solve: 0 CG, 1 Chebyshev, 2 PPCG
+        const bool ppcg_inner = ppcg && DIM == 3 && P->ppcg_inner_steps >= 2 && P->ppcg_inner_steps % 2 == 0 &&
+                                F->ppcg2_32.blocks > 0;
         int total_inner = 0, presteps_done = 0, cg_inner = 0;
         bool converged = false;
         for (int guard = 0; !converged && guard < P->max_iters + 2; ++guard) {
@@ -958,20 +992,22 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
             const int remaining = P->max_iters - used;
             s.inner_max = P->inner_max_iters > 0 ? std::min(P->inner_max_iters, remaining) : remaining;
             s.tol2 = tol * tol * s.rro;
-            s.n_inner = inner_cheby ? 1 : 0;
+            s.n_inner = inner_mode == 1 ? 1 : 0;
             s.cont = 1;
             s.inner_diverged = 0;
-            run_loop(c, F, inner_cheby ? LOOP_CHEBY32 : LOOP_CG32, 0);
+            run_loop(c, F, inner_mode == 1 ? LOOP_CHEBY32 : (inner_mode == 2 ? LOOP_PPCG32 : LOOP_CG32),
+                     P->ppcg_inner_steps);
             total_inner += s.n_inner;
-            if (!inner_cheby) cg_inner += s.n_inner;
+            if (inner_mode == 0) cg_inner += s.n_inner;
             if (s.inner_diverged) {
                 // The estimated spectrum missed part of it: drop this correction and solve
                 // the remaining ones with CG.
-                inner_cheby = false;
+                inner_mode = 0;
                 s.inner_cheby = 0;
                 continue;
             }
             k_dc_update<<<F->pair_blocks, 256, 0, c->stream>>>(a);
+            last_inner_mode = inner_mode;
             s.pending_p = 0;
             s.pending_u = 0;
             ++corrections;
@@ -1003,8 +1039,8 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
                     const double rho = (rk - 1.0) / (rk + 1.0);
                     s.theta = theta;
                     s.cheby_rho2 = rho * rho;
-                    s.inner_cheby = 1;
-                    inner_cheby = true;
+                    inner_mode = ppcg_inner ? 2 : 1;
+                    s.inner_cheby = inner_mode;
                     switch_step = n + 1;
                 }
             }
@@ -1164,6 +1200,7 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
     R->eigmin = eigmin;
     R->eigmax = eigmax;
     R->corrections = corrections;
+    R->inner_solver = last_inner_mode;
     R->warm_start_used = ws_used;
     R->warm_r0_plain = ws_r0_plain;
     R->warm_r0_guess = ws_r0_guess;
@@ -1266,8 +1303,18 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
             if (F->ppcg2.blocks > 0) {
                 FusedArgs ap = a;
                 ap.seg_rows = F->ppcg2.rows;
-                k_ppcg2_ring3d<PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
-                                                    ppcg2_smem_bytes<PPCG2_TY, PPCG2_RP>(), c->stream>>>(ap);
+                k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
+                                                             ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP>(),
+                                                             c->stream>>>(ap);
+            }
+            break;
+        case 13:
+            if (F->ppcg2_32.blocks > 0) {
+                FusedArgs ap = a;
+                ap.seg_rows = F->ppcg2_32.rows;
+                k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP><<<F->ppcg2_32.blocks, PPCG2_TY * 32,
+                                                             ppcg2_smem_bytes<float, PPCG2_TY, PPCG2_RP>(),
+                                                             c->stream>>>(ap);
             }
             break;
 #endif

@@ -18,6 +18,7 @@
 // CUDA graph whose while-node reads the continue flag set there.
 #pragma once
 
+#include <type_traits>
 #include "tea_chunk.cuh"
 
 
@@ -44,7 +45,7 @@ struct SolveState {
     int nonfinite;
     // FP32 inner solve of the defect-correction form.
     int n_inner, inner_max;
-    int inner_cheby;     // the inner solve is Chebyshev (else CG)
+    int inner_cheby;     // the inner solve: 0 CG, 1 Chebyshev, 2 PPCG
     int inner_diverged;  // the inner Chebyshev residual stalled or grew (bounds too narrow)
     double cheby_rho2;   // squared Chebyshev contraction per iteration for the bounds in use
     double tol2;
@@ -72,6 +73,7 @@ struct FusedArgs {
     float *kx32, *ky32, *kz32, *r32, *w32, *d32;
     float* p32[2];
     float* dc32[2];  // iterate of the inner Chebyshev solve (ping-pong over d32, w32)
+    float* sd32[2];  // sd of the inner PPCG solve
 };
 
 
@@ -1382,44 +1384,91 @@ struct OpPPCGInner {
 // w, and writes it to the other.  With an odd number of pairs sweep B leaves r in w
 // (r_in_w), so the last pair writes r back into r.  A pair whose second step is the last
 // inner step also forms that step's sum r.r and ends the outer iteration.
-template <int TY, int RP>
+// Arrays, scalars and end of the outer iteration of the two-step PPCG pass: the FP64
+// solve's (PpcgF64), or the FP32 inner PPCG of the defect-correction form (PpcgF32: the
+// correction d in place of u, FP32 r, w, sd and coefficients, no preconditioner).
+struct PpcgF64 {
+    using T = double;
+    __device__ static T* sd(const FusedArgs& a, int b) { return a.sd[b]; }
+    __device__ static T* r(const FusedArgs& a) { return a.r; }
+    __device__ static T* w(const FusedArgs& a) { return a.w; }
+    __device__ static T* u(const FusedArgs& a) { return a.u[0]; }
+    __device__ static const T* mi(const FusedArgs& a) { return a.st->precond ? a.mi : nullptr; }
+    __device__ static const T* kx(const FusedArgs& a) { return a.kx; }
+    __device__ static const T* ky(const FusedArgs& a) { return a.ky; }
+    __device__ static const T* kz(const FusedArgs& a) { return a.kz; }
+    __device__ static void control(const FusedArgs& a, const double* v) { OpPPCGInner<true>().control(a, v); }
+};
+struct PpcgF32 {
+    using T = float;
+    __device__ static T* sd(const FusedArgs& a, int b) { return a.sd32[b]; }
+    __device__ static T* r(const FusedArgs& a) { return a.r32; }
+    __device__ static T* w(const FusedArgs& a) { return a.w32; }
+    __device__ static T* u(const FusedArgs& a) { return a.d32; }
+    __device__ static const T* mi(const FusedArgs&) { return nullptr; }
+    __device__ static const T* kx(const FusedArgs& a) { return a.kx32; }
+    __device__ static const T* ky(const FusedArgs& a) { return a.ky32; }
+    __device__ static const T* kz(const FusedArgs& a) { return a.kz32; }
+    // End of an inner PPCG iteration: beta for the next p = r + beta p (applied by the FP32
+    // sweep A), and the inner loop test of the FP32 CG (stop below tol2 or at inner_max).
+    __device__ static void control(const FusedArgs& a, const double* v)
+    {
+        if (a.timing) return;
+        SolveState& s = *a.st;
+        const double rrn = v[0];
+        s.rrn = rrn;
+        s.beta = rrn / s.rro;
+        s.rro = rrn;
+        s.last_beta = s.beta;
+        s.pending_p = 1;
+        s.pending_u = 0;
+        s.n_inner = s.n_inner + 1;
+        if (!isfinite(rrn)) s.inner_diverged = 1;  // the correction is dropped; CG takes over
+        const int cont = isfinite(rrn) && rrn >= s.tol2 && s.n_inner < s.inner_max;
+        s.cont = cont;
+        if (a.use_handle) cudaGraphSetConditional(a.handle, cont ? 1u : 0u);
+    }
+};
+
+template <class T, int TY, int RP>
 constexpr size_t ppcg2_smem_bytes()
 {
-    return (size_t)(RP + 3) * Ring3Rows<OpPPCGInner<false>, TY>::ROWS * RingGeom<double>::WIDTH * sizeof(double)
-        + (size_t)2 * TY * RingGeom<double>::STRIP * sizeof(double);
+    return (size_t)(RP + 3) * Ring3Rows<OpPPCGInner<false>, TY>::ROWS * RingGeom<T>::WIDTH * sizeof(T)
+        + (size_t)2 * TY * RingGeom<T>::STRIP * sizeof(T);
 }
 
-template <int TY, int RP>
+template <class P, int TY, int RP>
 __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
 {
+    using T = typename P::T;
     extern __shared__ __align__(16) unsigned char s_raw[];
     using R = Ring3Rows<OpPPCGInner<false>, TY>;
-    constexpr int VEC = RingGeom<double>::VEC, STRIP = RingGeom<double>::STRIP, OFF = RingGeom<double>::OFF;
-    constexpr int RWT = RingGeom<double>::WIDTH;
+    constexpr int VEC = RingGeom<T>::VEC, STRIP = RingGeom<T>::STRIP, OFF = RingGeom<T>::OFF;
+    constexpr int RWT = RingGeom<T>::WIDTH;
     constexpr int OUT = 30 * VEC;
     constexpr int RQ = RP + 3;
     constexpr int SLOT = R::ROWS * RWT;
     constexpr int IN_R = R::IN, IN_U = R::IN + TY, IN_MI = R::IN + 2 * TY;
-    double* ring = reinterpret_cast<double*>(s_raw);
-    double* s1 = ring + (size_t)RQ * SLOT;  // step k's sd: [plane parity][TY rows][STRIP]
+    T* ring = reinterpret_cast<T*>(s_raw);
+    T* s1 = ring + (size_t)RQ * SLOT;  // step k's sd: [plane parity][TY rows][STRIP]
     const Geom& g = a.g;
     const int k = a.step;
     const int m = (k + 1) >> 1;
-    const double* __restrict__ sdk = a.sd[(m - 1) & 1];
-    double* __restrict__ sdo = a.sd[m & 1];
-    const double* __restrict__ rin = ((m - 1 + a.r_in_w) & 1) ? a.w : a.r;
-    double* __restrict__ rout = ((m + a.r_in_w) & 1) ? a.w : a.r;
-    double* __restrict__ U = a.u[0];
-    const bool precond = a.st->precond != 0;
+    const T* __restrict__ sdk = P::sd(a, (m - 1) & 1);
+    T* __restrict__ sdo = P::sd(a, m & 1);
+    const T* __restrict__ rin = ((m - 1 + a.r_in_w) & 1) ? P::w(a) : P::r(a);
+    T* __restrict__ rout = ((m + a.r_in_w) & 1) ? P::w(a) : P::r(a);
+    T* __restrict__ U = P::u(a);
+    const T* __restrict__ MI = P::mi(a);
+    const bool precond = MI != nullptr;
     const bool last = k + 1 == a.st->inner_steps;  // step k+1 ends the outer iteration
     DDVec<1> acc;
     acc.zero();
-    const double* __restrict__ MI = precond ? a.mi : nullptr;
-    const double al1 = a.ch_alphas[k - 1], be1 = a.ch_betas[k - 1];
-    const double al2 = a.ch_alphas[k], be2 = a.ch_betas[k];
-    const double* __restrict__ KX = a.kx;
-    const double* __restrict__ KY = a.ky;
-    const double* __restrict__ KZ = a.kz;
+    const T al1 = (T)a.ch_alphas[k - 1], be1 = (T)a.ch_betas[k - 1];
+    const T al2 = (T)a.ch_alphas[k], be2 = (T)a.ch_betas[k];
+    const T* __restrict__ KX = P::kx(a);
+    const T* __restrict__ KY = P::ky(a);
+    const T* __restrict__ KZ = P::kz(a);
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const int xlast = g.X - HALO_PAD - 1;
@@ -1456,7 +1505,7 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
         // step k's planes, Kz also for plane zl+1.
         auto issue = [&](int p) {
             if (p <= zl + 1) {
-                double* base = slot(p);
+                T* base = slot(p);
                 const int pr = refl(min(p, zlast + 1), g.Z);
                 const int pi = min(p, zlast + 1);
                 const int col = OFF + VEC * lane;
@@ -1475,20 +1524,19 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
             }
             cp_async_commit();
         };
-        auto own = [&](const double* base, int row, double* v) { ld_vec(base + row * RWT + OFF + VEC * lane, v); };
+        auto own = [&](const T* base, int row, T* v) { ld_vec(base + row * RWT + OFF + VEC * lane, v); };
         // Step k at plane p from sd at planes p-1 (A), p (B), p+1 (C): r1, u1 and sd1 at the
         // lane's cells; sd1 also into the shared plane buffer.
-        auto step1 = [&](int p, const double* A, const double* B, const double* C, double* r1, double* u1,
-                         double* t1) {
-            const double* cur = slot(p);
-            const double* nxt = slot(p + 1);
-            const double up = __shfl_up_sync(0xffffffffu, B[VEC - 1], 1);
-            const double dn = __shfl_down_sync(0xffffffffu, B[0], 1);
-            double kx[VEC + 1];
+        auto step1 = [&](int p, const T* A, const T* B, const T* C, T* r1, T* u1, T* t1) {
+            const T* cur = slot(p);
+            const T* nxt = slot(p + 1);
+            const T up = __shfl_up_sync(0xffffffffu, B[VEC - 1], 1);
+            const T dn = __shfl_down_sync(0xffffffffu, B[0], 1);
+            T kx[VEC + 1];
             own(cur, R::KX + w, kx);
             kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
             if (p <= zl && row_in) {
-                double ky0[VEC], ky1[VEC], kz0[VEC], kz1[VEC], ym[VEC], yp[VEC], rr[VEC], uu[VEC], mi[VEC];
+                T ky0[VEC], ky1[VEC], kz0[VEC], kz1[VEC], ym[VEC], yp[VEC], rr[VEC], uu[VEC], mi[VEC];
                 own(cur, R::KY + w, ky0);
                 own(cur, R::KY + w + 1, ky1);
                 own(cur, R::KZ + w, kz0);
@@ -1500,7 +1548,7 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
                 if (precond) own(cur, IN_MI + w, mi);
 #pragma unroll
                 for (int q = 0; q < VEC; ++q) {
-                    Nb nb;
+                    NbT<T> nb;
                     nb.c = B[q];
                     nb.xm = c + q == HALO_PAD ? B[q] : (q == 0 ? up : B[q > 0 ? q - 1 : 0]);
                     nb.xp = c + q == xlast ? B[q] : (q == VEC - 1 ? dn : B[q < VEC - 1 ? q + 1 : q]);
@@ -1508,26 +1556,26 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
                     nb.yp = yp[q];
                     nb.zm = A[q];
                     nb.zp = C[q];
-                    const double s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], kz0[q], kz1[q]);
-                    const double r = rr[q] - s;
+                    const T s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], kz0[q], kz1[q]);
+                    const T r = rr[q] - s;
                     r1[q] = r;
                     u1[q] = uu[q] + B[q];
                     t1[q] = al1 * B[q] + be1 * (precond ? mi[q] * r : r);
                 }
             } else {
 #pragma unroll
-                for (int q = 0; q < VEC; ++q) r1[q] = u1[q] = t1[q] = 0.0;
+                for (int q = 0; q < VEC; ++q) r1[q] = u1[q] = t1[q] = (T)0;
             }
             st_vec(s1 + ((size_t)(p & 1) * TY + w) * STRIP + VEC * lane, t1);
         };
         for (int p = zf - 1; p < zf - 1 + RQ; ++p) issue(p);
         cp_async_wait<RQ - 3>();
         __syncthreads();
-        double sA[VEC], sB[VEC], sC[VEC];  // sd at planes z, z+1, z+2 (the warp's row)
-        double tm[VEC], tc[VEC], tn[VEC];  // step k's sd at planes z-1, z, z+1
-        double r1c[VEC], u1c[VEC], r1n[VEC], u1n[VEC];
+        T sA[VEC], sB[VEC], sC[VEC];  // sd at planes z, z+1, z+2 (the warp's row)
+        T tm[VEC], tc[VEC], tn[VEC];  // step k's sd at planes z-1, z, z+1
+        T r1c[VEC], u1c[VEC], r1n[VEC], u1n[VEC];
         {
-            double sM[VEC];
+            T sM[VEC];
             own(slot(zf - 1), R::RAW + w + 1, sM);
             own(slot(zf), R::RAW + w + 1, sA);
             own(slot(zf + 1), R::RAW + w + 1, sB);
@@ -1543,27 +1591,27 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
             step1(z + 1, sA, sB, sC, r1n, u1n, tn);
             if (z >= z0) {
                 // Step k+1 at plane z.
-                const double* cur = slot(z);
-                const double* nxt = slot(z + 1);
-                const double up = __shfl_up_sync(0xffffffffu, tc[VEC - 1], 1);
-                const double dn = __shfl_down_sync(0xffffffffu, tc[0], 1);
-                double kx[VEC + 1];
+                const T* cur = slot(z);
+                const T* nxt = slot(z + 1);
+                const T up = __shfl_up_sync(0xffffffffu, tc[VEC - 1], 1);
+                const T dn = __shfl_down_sync(0xffffffffu, tc[0], 1);
+                T kx[VEC + 1];
                 own(cur, R::KX + w, kx);
                 kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
                 if (row_out && lane_out) {
-                    double ky0[VEC], ky1[VEC], kz0[VEC], kz1[VEC], ym[VEC], yp[VEC], mi[VEC];
+                    T ky0[VEC], ky1[VEC], kz0[VEC], kz1[VEC], ym[VEC], yp[VEC], mi[VEC];
                     own(cur, R::KY + w, ky0);
                     own(cur, R::KY + w + 1, ky1);
                     own(cur, R::KZ + w, kz0);
                     own(nxt, R::KZ + w, kz1);
                     if (precond) own(cur, IN_MI + w, mi);
-                    const double* sp = s1 + (size_t)(z & 1) * TY * STRIP + VEC * lane;
+                    const T* sp = s1 + (size_t)(z & 1) * TY * STRIP + VEC * lane;
                     if (j > HALO_PAD) ld_vec(sp + (w - 1) * STRIP, ym);
                     if (j < ylast) ld_vec(sp + (w + 1) * STRIP, yp);
-                    double r2[VEC], u2[VEC], d2[VEC];
+                    T r2[VEC], u2[VEC], d2[VEC];
 #pragma unroll
                     for (int q = 0; q < VEC; ++q) {
-                        Nb nb;
+                        NbT<T> nb;
                         nb.c = tc[q];
                         nb.xm = c + q == HALO_PAD ? tc[q] : (q == 0 ? up : tc[q > 0 ? q - 1 : 0]);
                         nb.xp = c + q == xlast ? tc[q] : (q == VEC - 1 ? dn : tc[q < VEC - 1 ? q + 1 : q]);
@@ -1571,12 +1619,12 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
                         nb.yp = j == ylast ? tc[q] : yp[q];
                         nb.zm = z == HALO_PAD ? tc[q] : tm[q];
                         nb.zp = z == zlast ? tc[q] : tn[q];
-                        const double s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], kz0[q], kz1[q]);
-                        const double r = r1c[q] - s;
+                        const T s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], kz0[q], kz1[q]);
+                        const T r = r1c[q] - s;
                         r2[q] = r;
                         u2[q] = u1c[q] + tc[q];
                         d2[q] = al2 * tc[q] + be2 * (precond ? mi[q] * r : r);
-                        if (last && c + q <= xlast) dd_add(acc.v[0], r * r);
+                        if (last && c + q <= xlast) dd_add(acc.v[0], (double)r * (double)r);
                     }
                     const long i = fidx(g, c, j, z);
                     if (c + VEC - 1 <= xlast) {
@@ -1608,8 +1656,8 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
         cp_async_wait<0>();
         __syncthreads();  // the next unit's copies reuse slots other warps may still read
     }
-    // The last inner step's sum r.r and the end of the outer iteration, as OpPPCGInner<true>.
-    if (last) grid_reduce_then<1>(acc, a.red, [&](const double* v) { OpPPCGInner<true>().control(a, v); });
+    // The last inner step's sum r.r and the end of the outer iteration.
+    if (last) grid_reduce_then<1>(acc, a.red, [&](const double* v) { P::control(a, v); });
 }
 #endif
 
@@ -2074,31 +2122,33 @@ __device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned
             cp_async_commit();
         };
         // Level l at row s (ring index ci): the operand rows m (s - 1), cv (s), n (s + 1) and
-        // p of the level below; u and p of the level into uo, po.  Rows outside the level's
-        // cone (above the segment's first ring row, or past the rows the last level needs)
-        // are skipped; s and l are warp-uniform, so the shuffles stay uniform.
-        auto level = [&](int l, int s, int ci, const T* m, const T* cv, const T* n, const T* pin, T* uo, T* po,
-                         bool last) {
-            if (s < a0 || s > ylast || s > j1 + NIT - 2 - l) return;
+        // p of the level below; u, p and r of the level into uo, po, ro.  Every level runs at
+        // every step, also at rows outside its useful range (above the segment's first ring
+        // row, past the rows the last level needs, past the domain), whose values reach no
+        // stored or summed cell: the step then has no branch, and the levels' independent
+        // chains interleave.  EDGE (warp-uniform): some cell of the step sits at a domain
+        // edge, where the neighbour is the cell's own value.
+        auto level = [&](auto edge_tag, int l, int s, int ci, const T* m, const T* cv, const T* n, const T* pin,
+                         T* uo, T* po, T* ro) {
+            constexpr bool EDGE = decltype(edge_tag)::value;
             const T* rs = cring + (size_t)ci * nc * STRIP + VEC * lane;
             const T* rs1 = cring + (size_t)wrap_c(ci + 1) * nc * STRIP + VEC * lane;
             const T up = __shfl_up_sync(0xffffffffu, cv[VEC - 1], 1);
             const T dn = __shfl_down_sync(0xffffffffu, cv[0], 1);
             T kx[VEC + 1];
             ld_vec(rs + S_KX * STRIP, kx);
-            kx[VEC] = __shfl_down_sync(0xffffffffu, kx[0], 1);
+            kx[VEC] = rs[S_KX * STRIP + VEC];  // the next lane's first Kx (lane 31: never used)
             T ky0[VEC], ky1[VEC], rhs[VEC], m0[VEC];
             ld_vec(rs + S_KY * STRIP, ky0);
             ld_vec(rs1 + S_KY * STRIP, ky1);
             ld_vec(rs + S_U0 * STRIP, rhs);
-            if (precond) ld_vec(rs + S_MI * STRIP, m0);
-            const bool edge = xedge || s == HALO_PAD || s == ylast;
+            if constexpr (PRE) ld_vec(rs + S_MI * STRIP, m0);
 #pragma unroll
             for (int q = 0; q < VEC; ++q) {
                 NbT<T> nb;
                 nb.zm = nb.zp = zero;
                 nb.c = cv[q];
-                if (edge) {
+                if constexpr (EDGE) {
                     nb.xm = c + q == HALO_PAD ? cv[q] : (q == 0 ? up : cv[q > 0 ? q - 1 : 0]);
                     nb.xp = c + q == xlast ? cv[q] : (q == VEC - 1 ? dn : cv[q < VEC - 1 ? q + 1 : q]);
                     nb.ym = s == HALO_PAD ? cv[q] : m[q];
@@ -2111,9 +2161,12 @@ __device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned
                 }
                 const T w = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], zero, zero);
                 const T r = rhs[q] - w;
-                po[q] = al[l] * pin[q] + be[l] * (precond ? m0[q] * r : r);
-                uo[q] = cv[q] + po[q];
-                if (last && checkN && out_lane && c + q <= xlast) dd_add(acc.v[0], (double)r * (double)r);
+                T pr;
+                if constexpr (PRE) pr = al[l] * pin[q] + be[l] * (m0[q] * r);
+                else pr = al[l] * pin[q] + be[l] * r;
+                po[q] = pr;
+                uo[q] = cv[q] + pr;
+                ro[q] = r;
             }
         };
         // Rows a0 - 1 .. a0 + RPN + 1 first; each step then issues the next new row, so row
@@ -2138,19 +2191,27 @@ __device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned
             T un[VEC], p0[VEC];
             ld_vec(oring + (size_t)wrap_o(ot + 1) * 2 * STRIP + VEC * lane, un);
             ld_vec(oring + (size_t)ot * 2 * STRIP + STRIP + VEC * lane, p0);
-            T NU[NIT][VEC], NP[NIT][VEC];
+            T NU[NIT][VEC], NP[NIT][VEC], RR[VEC];
+            auto levels = [&](auto edge_tag) {
+                level(edge_tag, 0, t, ct, um, uc, un, p0, NU[0], NP[0], RR);
 #pragma unroll
-            for (int l = 0; l < NIT; ++l)
+                for (int l = 1; l < NIT; ++l)
+                    level(edge_tag, l, t - 2 * l, wrap_c(ct + RQC - 2 * l), H[l - 1][2], H[l - 1][1], H[l - 1][0],
+                          PH[l - 1][1], NU[l], NP[l], RR);
+            };
+            bool yedge = false;
 #pragma unroll
-                for (int q = 0; q < VEC; ++q) NU[l][q] = NP[l][q] = zero;
-            level(0, t, ct, um, uc, un, p0, NU[0], NP[0], NIT == 1 && t >= j0);
-#pragma unroll
-            for (int l = 1; l < NIT; ++l) {
-                const int s = t - 2 * l;
-                level(l, s, wrap_c(ct + RQC - 2 * l), H[l - 1][2], H[l - 1][1], H[l - 1][0], PH[l - 1][1], NU[l],
-                      NP[l], l == NIT - 1 && s >= j0);
-            }
+            for (int l = 0; l < NIT; ++l) yedge = yedge || t - 2 * l == HALO_PAD || t - 2 * l == ylast;
+            if (xedge || yedge) levels(std::true_type{});
+            else levels(std::false_type{});
+            // The last level's sum r.r on a convergence-check pass, over the cells it writes
+            // (adding 0.0 leaves a double-double sum unchanged).
             const int sl = t - 2 * (NIT - 1);  // the row the last level reached
+            if (checkN && sl >= j0 && sl < j1) {
+#pragma unroll
+                for (int q = 0; q < VEC; ++q)
+                    dd_add(acc.v[0], out_lane && c + q <= xlast ? (double)RR[q] * (double)RR[q] : 0.0);
+            }
             if (sl >= j0 && sl < j1 && out_lane) {
                 const long i = fidx(g, c, sl, 0);
                 if (c + VEC - 1 <= xlast) {
@@ -2603,7 +2664,7 @@ struct OpOuterResid {
     __device__ bool skip(const FusedArgs&) { return false; }
     __device__ void begin(const FusedArgs& a)
     {
-        cheby = a.st->inner_cheby;
+        cheby = a.st->inner_cheby == 1;
         theta32 = (float)a.st->theta;
     }
     __device__ Raw load_raw(const FusedArgs& a, long i) const
@@ -2986,13 +3047,47 @@ __global__ void __launch_bounds__(256) k_cg32_sweep_b(FusedArgs a)
 }
 
 // u += d in FP64, after the pending d += alpha p of the last inner iteration.
+// The FP32 inner PPCG's CGCalcUr + PPCGInitSd (the FP32 form of k_ppcg_sweep_b, no
+// preconditioner): d += alpha p, r -= alpha w (into w when the two-step passes start there),
+// sd = r / theta into sd32[0].
+__global__ void __launch_bounds__(256) k_ppcg32_sweep_b(FusedArgs a)
+{
+    const SolveState& s = *a.st;
+    const float alpha = (float)s.alpha, theta = (float)s.theta;
+    const float* __restrict__ P = a.p32[s.par_p];
+    float* __restrict__ D = a.d32;
+    const float* R = a.r32;
+    const float* W = a.w32;
+    float* RD = a.r_in_w ? a.w32 : a.r32;
+    float* __restrict__ SD = a.sd32[0];
+    walk_quads(a.g, [&](long i, int n) {
+        if (n == 4) {
+            const float4 d4 = *reinterpret_cast<const float4*>(D + i), p4 = *reinterpret_cast<const float4*>(P + i);
+            const float4 r4 = *reinterpret_cast<const float4*>(R + i), w4 = *reinterpret_cast<const float4*>(W + i);
+            *reinterpret_cast<float4*>(D + i) =
+                make_float4(d4.x + alpha * p4.x, d4.y + alpha * p4.y, d4.z + alpha * p4.z, d4.w + alpha * p4.w);
+            const float r0 = r4.x - alpha * w4.x, r1 = r4.y - alpha * w4.y;
+            const float r2 = r4.z - alpha * w4.z, r3 = r4.w - alpha * w4.w;
+            *reinterpret_cast<float4*>(RD + i) = make_float4(r0, r1, r2, r3);
+            *reinterpret_cast<float4*>(SD + i) = make_float4(r0 / theta, r1 / theta, r2 / theta, r3 / theta);
+        } else {
+            for (int k = 0; k < n; ++k) {
+                D[i + k] = D[i + k] + alpha * P[i + k];
+                const float r = R[i + k] - alpha * W[i + k];
+                RD[i + k] = r;
+                SD[i + k] = r / theta;
+            }
+        }
+    });
+}
+
 __global__ void __launch_bounds__(256) k_dc_update(FusedArgs a)
 {
     const SolveState& s = *a.st;
     const float alpha = (float)s.last_alpha;
     const int pend = s.inner_cheby ? 0 : s.pending_u;
     const float* __restrict__ P = a.p32[s.par_p];
-    const float* __restrict__ D = s.inner_cheby ? a.dc32[s.par_u] : a.d32;
+    const float* __restrict__ D = s.inner_cheby == 1 ? a.dc32[s.par_u] : a.d32;
     walk_pairs(a.g, [&](long i, bool two) {
         const int n = two ? 2 : 1;
         for (int k = 0; k < n; ++k) {

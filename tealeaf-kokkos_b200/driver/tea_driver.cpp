@@ -721,6 +721,7 @@ struct Runner {
             rec->switch_step = r.switch_step;
             rec->est_itc = r.est_itc;
             rec->corrections = r.corrections;
+            rec->inner_solver = r.inner_solver;
             rec->warm_start_used = r.warm_start_used;
             if (opt->ws_net && opt->ws_mode == 1) {
                 if (!be.ws_record || be.ws_record(&opt->ws_net, &chunk) != 0) fail("warm start: cannot record pair");

@@ -53,7 +53,8 @@ typedef struct {
     long long h2d_bytes;     /* backend host->device bytes so far (0 if not reported) */
     long long d2h_bytes;     /* backend device->host bytes so far */
     int corrections;         /* FP32-refined solves: outer corrections */
-    int pad2;
+    int inner_solver;        /* FP32-refined solves: inner solver of the last correction
+                                (0 CG, 1 Chebyshev, 2 PPCG) */
 } tea_step_record;
 
 typedef struct {

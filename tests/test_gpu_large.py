@@ -13,7 +13,11 @@ path) and through the per-call ext_* entry points (the path an unchanged Fortran
 takes).  Bars: field summary within 1e-10 relative per step; iteration counts within 1 for
 CG and PPCG and within 10 for Chebyshev, whose residual is only tested every tenth
 iteration once n >= est_itc (tealeaf_2d/tea_solve.f90:260), so a rounding difference in
-the error moves the exit by one check; the Chebyshev switch step within 1.  The
+the error moves the exit by one check; the Chebyshev switch step within 1.  Where the
+fixture also holds the reference's counts at other thread counts (the 512^2 deck, whose
+absolute eps 1e-15 sits at the rounding floor of sum r^2: the reference itself gives 834
+iterations at step 10 on one or two threads and 837 on four or eight), the count must lie
+within 1 of the range the reference's own runs span.  The
 FP32-refined form is held to the FP64 reference's field summary within 1e-9.
 """
 import json
@@ -38,16 +42,21 @@ def _solver(deck):
     return next(k for k in ITER_TOL if k in deck)
 
 
-def _check(name, got, ref, deck, steps):
+def _check(name, got, ref, deck, steps, by_threads=None):
     tol = ITER_TOL[_solver(deck)]
     assert len(got) >= steps and len(ref) >= steps
-    for a, b in zip(got[:steps], ref[:steps]):
-        assert abs(a["iterations"] - b["iterations"]) <= tol, (name, a["step"], a["iterations"], b["iterations"])
-        if b["switch_step"]:
-            assert abs(a["switch_step"] - b["switch_step"]) <= 1, (name, a["step"], a["switch_step"],
-                                                                   b["switch_step"])
+    bad = []
+    for i, (a, b) in enumerate(zip(got[:steps], ref[:steps])):
+        counts = [b["iterations"]] + [v[i] for v in (by_threads or {}).values()]
+        lo, hi = min(counts) - tol, max(counts) + tol
+        if not lo <= a["iterations"] <= hi:
+            bad.append(("iterations", a["step"], a["iterations"], counts))
+        if b["switch_step"] and abs(a["switch_step"] - b["switch_step"]) > 1:
+            bad.append(("switch_step", a["step"], a["switch_step"], b["switch_step"]))
         for k in ("vol", "mass", "ie", "temp"):
-            assert rel(a[k], b[k]) <= FIELD_SUMMARY_TOL, (name, a["step"], k, a[k], b[k], rel(a[k], b[k]))
+            if rel(a[k], b[k]) > FIELD_SUMMARY_TOL:
+                bad.append((k, a["step"], a[k], b[k], rel(a[k], b[k])))
+    assert not bad, (name, bad)
 
 
 @pytest.mark.parametrize("name", sorted(_cases()))
@@ -55,7 +64,7 @@ def test_whole_solve_matches_reference_at_size(name):
     case = _cases()[name]
     ref = case["ref"]["records"]
     _, got = tea.run_deck(case["deck"], case["dim"], fused=True, summary_every_step=True)
-    _check(name, got, ref, case["deck"], len(ref))
+    _check(name, got, ref, case["deck"], len(ref), case.get("iterations_by_threads"))
 
 
 @pytest.mark.parametrize("name", sorted(_cases()))
@@ -64,7 +73,7 @@ def test_per_call_path_matches_reference_at_size(name):
     ref = case["ref"]["records"]
     steps = min(len(ref), PER_CALL_STEPS if len(ref) > 10 else len(ref))
     _, got = tea.run_deck(case["deck"], case["dim"], fused=False, summary_every_step=True, end_step=steps)
-    _check(name, got, ref, case["deck"], steps)
+    _check(name, got, ref, case["deck"], steps, case.get("iterations_by_threads"))
 
 
 FP32_CASES = [("c2_2d4096_cheby", 3), ("c3_3d256_cg", 1), ("c3_3d256_ppcg", 1)]
