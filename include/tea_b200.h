@@ -135,8 +135,15 @@ typedef struct {
     int inner_max_iters;    /* FP32_REFINED: inner iterations per correction, 0 = no limit */
     double inner_tol;       /* FP32_REFINED: relative drop of the inner residual per
                                correction, 0 = 1e-4 */
-    int reserved[4];        /* must be zero */
+    int inner_solver;       /* FP32_REFINED, corrections after the first (CG) one:
+                               TEA_INNER_DECK (0) the deck's method -- Chebyshev for
+                               Chebyshev decks, PPCG for PPCG decks (3D, even inner
+                               steps; else Chebyshev); TEA_INNER_CHEBYSHEV (1) Chebyshev
+                               for both */
+    int reserved[3];        /* must be zero */
 } tea_solve_params;
+
+enum { TEA_INNER_DECK = 0, TEA_INNER_CHEBYSHEV = 1 };
 
 /* Precision forms of ext_tea_leaf_solve_. */
 enum {

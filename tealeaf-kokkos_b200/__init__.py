@@ -210,7 +210,7 @@ class SolveParams(ctypes.Structure):
         ("ppcg_inner_steps", ctypes.c_int), ("check_result", ctypes.c_int), ("dt", ctypes.c_double),
         ("eps", ctypes.c_double), ("ch_cg_epslim", ctypes.c_double), ("eps_rel", ctypes.c_double),
         ("precision", ctypes.c_int), ("inner_max_iters", ctypes.c_int), ("inner_tol", ctypes.c_double),
-        ("reserved", ctypes.c_int * 4),
+        ("inner_solver", ctypes.c_int), ("reserved", ctypes.c_int * 3),
     ]
 
 

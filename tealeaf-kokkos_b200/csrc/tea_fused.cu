@@ -971,8 +971,8 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
         // Chebyshev decks: the first correction's inner CG also estimates the spectrum.
         const bool want_cheby = cheby || ppcg;
         int inner_mode = 0;  // the inner solve: 0 CG, 1 Chebyshev, 2 PPCG
-        const bool ppcg_inner = ppcg && DIM == 3 && P->ppcg_inner_steps >= 2 && P->ppcg_inner_steps % 2 == 0 &&
-                                F->ppcg2_32.blocks > 0;
+        const bool ppcg_inner = ppcg && P->inner_solver == TEA_INNER_DECK && DIM == 3 &&
+                                P->ppcg_inner_steps >= 2 && P->ppcg_inner_steps % 2 == 0 && F->ppcg2_32.blocks > 0;
         int total_inner = 0, presteps_done = 0, cg_inner = 0;
         bool converged = false;
         for (int guard = 0; !converged && guard < P->max_iters + 2; ++guard) {

@@ -2071,7 +2071,6 @@ __device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned
     for (int l = 0; l < NIT; ++l) op.pass_coefs(a, l, al[l], be[l]);
     const bool checkN = op.pass_check(a, NIT);
     const T* mi = op.pair_mi(a);
-    constexpr bool precond = PRE;
     constexpr int nc = PRE ? 4 : 3;
     T* unew = op.unew;
     T* pnew = op.pnext;
@@ -2138,11 +2137,12 @@ __device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned
             T kx[VEC + 1];
             ld_vec(rs + S_KX * STRIP, kx);
             kx[VEC] = rs[S_KX * STRIP + VEC];  // the next lane's first Kx (lane 31: never used)
-            T ky0[VEC], ky1[VEC], rhs[VEC], m0[VEC];
+            T ky0[VEC], ky1[VEC], rhs[VEC], m0[PRE ? VEC : 1];
             ld_vec(rs + S_KY * STRIP, ky0);
             ld_vec(rs1 + S_KY * STRIP, ky1);
             ld_vec(rs + S_U0 * STRIP, rhs);
             if constexpr (PRE) ld_vec(rs + S_MI * STRIP, m0);
+            else (void)m0;
 #pragma unroll
             for (int q = 0; q < VEC; ++q) {
                 NbT<T> nb;
@@ -2174,30 +2174,37 @@ __device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned
         for (int r = a0 - 1; r <= a0 + RPN + 1; ++r) issue(r, (r - a0 + 1) % RQC, (r - a0 + 1) % RQO);
         cp_async_wait<RPN + 1>();
         __syncwarp();
-        T um[VEC], uc[VEC];
-        ld_vec(oring + VEC * lane, um);                                   // row a0 - 1
-        ld_vec(oring + (size_t)(1 % RQO) * 2 * STRIP + VEC * lane, uc);  // row a0
-        // Level l < NIT - 1 keeps the u rows it produced at the last three steps (H[l][0]:
-        // step t - 1, i.e. row t - 1 - 2l) and its p of the last two steps.
-        T H[NIT - 1][3][VEC], PH[NIT - 1][2][VEC];
+        // Register windows of three rows, indexed by the step's phase k = (t - a0) mod 3 so
+        // that the loop, unrolled by three, moves no registers: U0 holds level 0's operand
+        // rows (row r at (r - a0 + 1) mod 3: rows t - 1, t, t + 1 at k, k + 1, k + 2), and
+        // H[l] / PH[l] the u / p rows level l < NIT - 1 produced at the last three steps
+        // (step s at (s - a0) mod 3: steps t - 3, t - 2, t - 1 at k, k + 1, k + 2).
+        T U0[3][VEC], H[NIT - 1][3][VEC], PH[NIT - 1][3][VEC];
+        ld_vec(oring + VEC * lane, U0[0]);                                   // row a0 - 1
+        ld_vec(oring + (size_t)(1 % RQO) * 2 * STRIP + VEC * lane, U0[1]);  // row a0
 #pragma unroll
         for (int l = 0; l < NIT - 1; ++l)
 #pragma unroll
-            for (int q = 0; q < VEC; ++q) H[l][0][q] = H[l][1][q] = H[l][2][q] = PH[l][0][q] = PH[l][1][q] = zero;
+            for (int h = 0; h < 3; ++h)
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) H[l][h][q] = PH[l][h][q] = zero;
         int ct = 1 % RQC, ot = 1 % RQO;  // ring indices of row t
-        for (int t = a0; t <= t_last; ++t) {
+        // One step at row t of phase K.
+        auto step = [&](auto phase_tag, int t) {
+            constexpr int K = decltype(phase_tag)::value;
+            constexpr int K1 = (K + 1) % 3, K2 = (K + 2) % 3;
             cp_async_wait<RPN>();
             __syncwarp();
-            T un[VEC], p0[VEC];
-            ld_vec(oring + (size_t)wrap_o(ot + 1) * 2 * STRIP + VEC * lane, un);
+            T p0[VEC];
+            ld_vec(oring + (size_t)wrap_o(ot + 1) * 2 * STRIP + VEC * lane, U0[K2]);  // row t + 1
             ld_vec(oring + (size_t)ot * 2 * STRIP + STRIP + VEC * lane, p0);
             T NU[NIT][VEC], NP[NIT][VEC], RR[VEC];
             auto levels = [&](auto edge_tag) {
-                level(edge_tag, 0, t, ct, um, uc, un, p0, NU[0], NP[0], RR);
+                level(edge_tag, 0, t, ct, U0[K], U0[K1], U0[K2], p0, NU[0], NP[0], RR);
 #pragma unroll
                 for (int l = 1; l < NIT; ++l)
-                    level(edge_tag, l, t - 2 * l, wrap_c(ct + RQC - 2 * l), H[l - 1][2], H[l - 1][1], H[l - 1][0],
-                          PH[l - 1][1], NU[l], NP[l], RR);
+                    level(edge_tag, l, t - 2 * l, wrap_c(ct + RQC - 2 * l), H[l - 1][K], H[l - 1][K1], H[l - 1][K2],
+                          PH[l - 1][K1], NU[l], NP[l], RR);
             };
             bool yedge = false;
 #pragma unroll
@@ -2227,28 +2234,32 @@ __device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned
                     }
                 }
             }
+            // Step t's rows replace those of step t - 3 (slot K).
 #pragma unroll
             for (int l = 0; l < NIT - 1; ++l)
 #pragma unroll
                 for (int q = 0; q < VEC; ++q) {
-                    H[l][2][q] = H[l][1][q];
-                    H[l][1][q] = H[l][0][q];
-                    H[l][0][q] = NU[l][q];
-                    PH[l][1][q] = PH[l][0][q];
-                    PH[l][0][q] = NP[l][q];
+                    H[l][K][q] = NU[l][q];
+                    PH[l][K][q] = NP[l][q];
                 }
-#pragma unroll
-            for (int q = 0; q < VEC; ++q) {
-                um[q] = uc[q];
-                uc[q] = un[q];
-            }
             __syncwarp();
             // Row t + RPN + 2 goes into the coefficient slot of row t - 2(NIT - 1) and the
             // operand slot of row t - 1, which no lane reads any more.
             issue(t + RPN + 2, wrap_c(ct + RPN + 2), wrap_o(ot + RPN + 2));
             ct = wrap_c(ct + 1);
             ot = wrap_o(ot + 1);
+        };
+        using P0 = std::integral_constant<int, 0>;
+        using P1 = std::integral_constant<int, 1>;
+        using P2 = std::integral_constant<int, 2>;
+        int t = a0;
+        for (; t + 2 <= t_last; t += 3) {
+            step(P0{}, t);
+            step(P1{}, t + 1);
+            step(P2{}, t + 2);
         }
+        if (t <= t_last) step(P0{}, t);
+        if (t + 1 <= t_last) step(P1{}, t + 1);
         cp_async_wait<0>();
         __syncwarp();
     }

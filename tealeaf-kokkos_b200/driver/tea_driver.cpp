@@ -90,6 +90,7 @@ struct Config {
     int precision = 0;          // tl_precision fp64 | fp32 (whole-solve path only)
     int inner_max_iters = 0;    // tl_inner_max_iters
     double inner_tol = 0.0;     // tl_inner_tol
+    int inner_solver = 0;       // tl_inner_solver deck | chebyshev
     std::vector<State> states;  // states[0] is state 1
 };
 
@@ -233,6 +234,12 @@ Config parse_deck(const std::string& text, int dim)
                 else if (v == "fp32") cfg.precision = TEA_PRECISION_FP32_REFINED;
                 else fail("read_input: tl_precision must be fp64 or fp32, not %s", v.c_str());
             } else if (word == "tl_inner_tol") cfg.inner_tol = getrval(next_word(true));
+            else if (word == "tl_inner_solver") {
+                const std::string v = next_word(true);
+                if (v == "deck") cfg.inner_solver = TEA_INNER_DECK;
+                else if (v == "chebyshev") cfg.inner_solver = TEA_INNER_CHEBYSHEV;
+                else fail("read_input: tl_inner_solver must be deck or chebyshev, not %s", v.c_str());
+            }
             else if (word == "tl_inner_max_iters") cfg.inner_max_iters = getival(next_word(true));
             else if (word == "state") {
                 int s = getival(next_word(true));
@@ -700,6 +707,7 @@ struct Runner {
             p.precision = cfg.precision;
             p.inner_max_iters = cfg.inner_max_iters;
             p.inner_tol = cfg.inner_tol;
+            p.inner_solver = cfg.inner_solver;
             tea_solve_result r;
             std::memset(&r, 0, sizeof(r));
             be.whole_solve(&chunk, &p, &r);
