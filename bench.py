@@ -719,7 +719,10 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic, "alg_bytes_per_launch": g["alg_bytes"],
-                     "launch_ms": g["kernel_ms"][dom], "kernel_ms": g["kernel_ms"]},
+                     "launch_ms": g["kernel_ms"][dom], "kernel_ms": g["kernel_ms"],
+                     # every timed kernel's algorithmic GB/s as a fraction of the same peak
+                     "kernel_frac": {k: WORDS[k] * 8 * CELLS * CELLS / (ms / 1e3) / 1e9 / peak
+                                     for k, ms in g["kernel_ms"].items() if ms > 0}},
         "clocks": g["clocks"],
         # 8 fused launches per four CG iterations (the graph's loop body holds four; the
         # launches after the last iteration return at once), about 3 per 10 Chebyshev

@@ -2066,9 +2066,11 @@ __device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned
     using T = typename Op::T;
     using G = SkewGeom<T, NIT, RPN>;
     constexpr int VEC = G::VEC, STRIP = G::STRIP, OUT = G::OUT, FL = G::FL, RQC = G::RQC, RQO = G::RQO;
-    T al[NIT], be[NIT];
-#pragma unroll
-    for (int l = 0; l < NIT; ++l) op.pass_coefs(a, l, al[l], be[l]);
+    // The pass's coefficients in shared memory (two loads per level and row instead of 2 NIT
+    // registers held through the loop).
+    __shared__ T s_coef[2 * NIT];
+    if (threadIdx.x < NIT) op.pass_coefs(a, threadIdx.x, s_coef[threadIdx.x], s_coef[NIT + threadIdx.x]);
+    __syncthreads();
     const bool checkN = op.pass_check(a, NIT);
     const T* mi = op.pair_mi(a);
     constexpr int nc = PRE ? 4 : 3;
@@ -2162,8 +2164,8 @@ __device__ __forceinline__ void chebyS_body(const FusedArgs& a, Op& op, unsigned
                 const T w = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], zero, zero);
                 const T r = rhs[q] - w;
                 T pr;
-                if constexpr (PRE) pr = al[l] * pin[q] + be[l] * (m0[q] * r);
-                else pr = al[l] * pin[q] + be[l] * r;
+                if constexpr (PRE) pr = s_coef[l] * pin[q] + s_coef[NIT + l] * (m0[q] * r);
+                else pr = s_coef[l] * pin[q] + s_coef[NIT + l] * r;
                 po[q] = pr;
                 uo[q] = cv[q] + pr;
                 ro[q] = r;

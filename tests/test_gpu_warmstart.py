@@ -167,6 +167,15 @@ def test_training_reduces_loss_and_warm_started_solves_converge(capsys):
         with capsys.disabled():
             print(f"\nwarm start: loss {first:.3f} -> {last:.3f}; CG iterations {it_warm} vs {it_plain} from u0 "
                   f"({100.0 * (it_warm - it_plain) / it_plain:+.1f}%)")
-        assert it_warm <= 1.5 * it_plain  # the fallback bounds the residual, not the count
+        # A rejected guess restores the plain start bit for bit: until the first accepted
+        # guess the two runs are the same run.
+        for a, b in zip(warm, plain):
+            if a["warm_start_used"]:
+                break
+            assert a["iterations"] == b["iterations"] and a["temp"] == b["temp"], (a["step"], a, b)
+        # What the network gains on these decks, as recorded on a B200: a loss of 7.0-7.2 %
+        # more CG iterations (1884-1888 against 1761).  The bar holds that recorded loss, so
+        # that a worse network fails here rather than passing inside a loose bound.
+        assert it_warm <= 1.10 * it_plain, (it_warm, it_plain)
     finally:
         net.close()
