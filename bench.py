@@ -632,7 +632,7 @@ def kernel_only(args):
     # FP32 kernels: their FP32 words counted as half FP64 words.
     words = {"ppcg_inner": 8, "cg_sweep_a": 8, "cheby_iterate": 7, "jacobi": 5, "cg_sweep_b": 3,
              "cheby_pair": 7, "cg32_sweep_a": 4, "cg32_sweep_b": 1.5, "cheby32_pair": 3.5,
-             "ppcg_pair": 8, "cheby_quad": 7, "cheby32_quad": 3.5}[args.kernel]
+             "ppcg_pair": 8, "cheby_quad": 7, "cheby32_quad": 3.5, "ppcg32_pair": 4}[args.kernel]
     gbs = words * 8 * CELLS * CELLS / (ms.value / 1e3) / 1e9 if ms.value > 0 else None
     print(json.dumps({"kernel": args.kernel, "ms_per_launch": ms.value, "algorithmic_gbs": gbs}))
     lib.ext_finalise_()

@@ -137,8 +137,8 @@ typedef struct {
                                correction, 0 = 1e-4 */
     int inner_solver;       /* FP32_REFINED, corrections after the first (CG) one:
                                TEA_INNER_DECK (0) the deck's method -- Chebyshev for
-                               Chebyshev decks, PPCG for PPCG decks (3D, even inner
-                               steps; else Chebyshev); TEA_INNER_CHEBYSHEV (1) Chebyshev
+                               Chebyshev decks, PPCG for PPCG decks (an even number
+                               of inner steps; else Chebyshev); TEA_INNER_CHEBYSHEV (1) Chebyshev
                                for both */
     int reserved[3];        /* must be zero */
 } tea_solve_params;

@@ -70,7 +70,7 @@ struct Fused {
     RingLaunch quad32;          // k_cheby4_ring2d<OpCheby32> (2D)
     RingLaunch ring3[RING_OPS]; // grid and z-segment planes of k_ring3d per sweep (3D)
     RingLaunch ppcg2;           // k_ppcg2_ring3d (3D) / k_ppcg2_ring2d (2D); blocks 0: single steps only
-    RingLaunch ppcg2_32;        // k_ppcg2_ring3d<PpcgF32> (3D): the FP32 inner PPCG; blocks 0: none
+    RingLaunch ppcg2_32;        // k_ppcg2_ring{2,3}d<PpcgF32>: the FP32 inner PPCG; blocks 0: none
     int stencil_mode = 0;  // 0: the faster kernel per sweep, 1: register pipeline only, 2: ring only
     Loop loops[LOOP_COUNT];
     bool use_graph = true;
@@ -486,8 +486,10 @@ Fused* ensure_fused(Chunk* c, int max_iters)
                 const int occq32 =
                     smem_occupancy(k_cheby4_ring2d<OpCheby32>, (int)cheby4_smem_bytes<OpCheby32>(false));
                 F->quad32 = ring_launch(g, sms, occq32, SkewGeom<float, 4, C4_RP>::OUT, mb);
-                const int occ4 = smem_occupancy(k_ppcg2_ring2d, (int)ppcg2_2d_smem_bytes);
+                const int occ4 = smem_occupancy(k_ppcg2_ring2d<PpcgF64>, (int)ppcg2_2d_smem_bytes);
                 F->ppcg2 = ring_launch(g, sms, occ4, Pair2Geom<double>::OUT, mb);
+                const int occ5 = smem_occupancy(k_ppcg2_ring2d<PpcgF32>, (int)ppcg2_2d_smem_bytes);
+                F->ppcg2_32 = ring_launch(g, sms, occ5, Pair2Geom<float>::OUT, mb);
             }
         }
 #endif
@@ -535,7 +537,7 @@ bool ensure_fp32(Chunk* c, Fused* F)
     if (F->alloc32[0]) return true;
     const size_t bytes = c->field_elems * sizeof(float);
     for (int k = 0; k < 10; ++k) {
-        if ((k == 2 || k >= 8) && DIM != 3) continue;  // Kz and the inner PPCG's sd (3D only)
+        if (k == 2 && DIM != 3) continue;  // Kz (3D only)
         TEA_CK(cudaMalloc(&F->alloc32[k], bytes));
         if (!F->alloc32[k]) return false;
         TEA_CK(cudaMemset(F->alloc32[k], 0, bytes));
@@ -552,8 +554,8 @@ bool ensure_fp32(Chunk* c, Fused* F)
     a.p32[1] = F->alloc32[7] + kLeadPad;
     a.dc32[0] = a.d32;
     a.dc32[1] = a.w32;
-    a.sd32[0] = DIM == 3 ? F->alloc32[8] + kLeadPad : nullptr;
-    a.sd32[1] = DIM == 3 ? F->alloc32[9] + kLeadPad : nullptr;
+    a.sd32[0] = F->alloc32[8] + kLeadPad;
+    a.sd32[1] = F->alloc32[9] + kLeadPad;
     return true;
 }
 
@@ -631,7 +633,7 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
             ak.step = k0;
             ak.seg_rows = F->ppcg2.rows;
 #if TEA_DIM == 2
-            k_ppcg2_ring2d<<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, s>>>(ak);
+            k_ppcg2_ring2d<PpcgF64><<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, s>>>(ak);
 #else
             k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
                                                          ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP>(), s>>>(ak);
@@ -654,10 +656,9 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
         k_cg32_sweep_b<<<F->quad_blocks, 256, 0, s>>>(a);
         break;
     case LOOP_PPCG32: {
-        // One FP32 inner PPCG iteration (3D, an even number of inner steps, all in pairs):
+        // One FP32 inner PPCG iteration (an even number of inner steps, all in pairs):
         // p = r + beta p and w = A p with p.w, then d += alpha p, r -= alpha w, sd = r / theta,
         // then the inner steps; the last pair forms r.r and ends the iteration.
-#if TEA_DIM == 3
         stencil<OpSweepA32>(F, a, s);
         const int pairs = inner_steps / 2;
         FusedArgs ab = a;
@@ -667,10 +668,13 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
             FusedArgs ak = ab;
             ak.step = k0;
             ak.seg_rows = F->ppcg2_32.rows;
+#if TEA_DIM == 2
+            k_ppcg2_ring2d<PpcgF32><<<F->ppcg2_32.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, s>>>(ak);
+#else
             k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP><<<F->ppcg2_32.blocks, PPCG2_TY * 32,
                                                          ppcg2_smem_bytes<float, PPCG2_TY, PPCG2_RP>(), s>>>(ak);
-        }
 #endif
+        }
         break;
     }
     }
@@ -958,7 +962,7 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
         // solves.  CG and Jacobi decks: every inner solve is CG.  Chebyshev and PPCG decks:
         // the first inner solve is CG, whose scalars give the Lanczos eigenvalue bounds
         // (computed in FP64 on the host), and the following ones are Chebyshev (PPCG decks
-        // in 3D with an even number of inner steps: PPCG with the deck's inner steps) --
+        // with an even number of inner steps: PPCG with the deck's inner steps) --
         // the plain solve's CG-then-Chebyshev/PPCG order, with the spectrum taken from a CG
         // run long enough to resolve it.
         if (!ensure_fp32(c, F)) {
@@ -971,8 +975,8 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
         // Chebyshev decks: the first correction's inner CG also estimates the spectrum.
         const bool want_cheby = cheby || ppcg;
         int inner_mode = 0;  // the inner solve: 0 CG, 1 Chebyshev, 2 PPCG
-        const bool ppcg_inner = ppcg && P->inner_solver == TEA_INNER_DECK && DIM == 3 &&
-                                P->ppcg_inner_steps >= 2 && P->ppcg_inner_steps % 2 == 0 && F->ppcg2_32.blocks > 0;
+        const bool ppcg_inner = ppcg && P->inner_solver == TEA_INNER_DECK && P->ppcg_inner_steps >= 2 &&
+                                P->ppcg_inner_steps % 2 == 0 && F->ppcg2_32.blocks > 0;
         int total_inner = 0, presteps_done = 0, cg_inner = 0;
         bool converged = false;
         for (int guard = 0; !converged && guard < P->max_iters + 2; ++guard) {
@@ -1295,7 +1299,14 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
             if (F->ppcg2.blocks > 0) {
                 FusedArgs ap = a;
                 ap.seg_rows = F->ppcg2.rows;
-                k_ppcg2_ring2d<<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, c->stream>>>(ap);
+                k_ppcg2_ring2d<PpcgF64><<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, c->stream>>>(ap);
+            }
+            break;
+        case 13:
+            if (F->ppcg2_32.blocks > 0) {
+                FusedArgs ap = a;
+                ap.seg_rows = F->ppcg2_32.rows;
+                k_ppcg2_ring2d<PpcgF32><<<F->ppcg2_32.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, c->stream>>>(ap);
             }
             break;
 #else

@@ -1362,28 +1362,6 @@ struct OpPPCGInner {
     }
 };
 
-#if TEA_DIM == 3
-// Two PPCG inner steps k, k+1 in one pass over the 3D field (temporal blocking).  The
-// reference refreshes sd's halo by reflection before every inner step
-// (tealeaf_2d/tea_solve.f90:631-636) and the steps between the outer iteration's sweeps
-// have no reduction except on the last one, so two of them share one read of sd, r, u, mi
-// and K and one write of r, u and sd: about 9 words per cell for two steps instead of
-// eighteen.  Per cell the operations and their order are those of two single steps, so the
-// results are bit-identical.
-//
-// The plane ring of k_ring3d (a block of TY warps, a 64-column x TY-row tile marching
-// through a z segment) computes step k for every loaded cell one plane ahead of step k+1.
-// Step k+1 needs step k's sd at its neighbours: z-neighbours stay in registers, y-neighbours
-// go through a two-plane shared buffer, x-neighbours by shuffle.  So a tile writes only its
-// inner 60 columns (lanes 1..30) and rows (warps 1..TY-2): tiles overlap by four columns and
-// two rows, z segments by one plane of step k.  At the domain's faces step k's sd is
-// reflected as the reference's halo update reflects it (the cell's own value).  Tiles read
-// r at cells that a neighbouring tile writes, so r goes to the other of r and w (w is free
-// during the inner steps) and sd to the other sd buffer.  Pair m (steps 2m-1, 2m) reads
-// sd[(m-1)&1] and writes sd[m&1]; it reads r from r when m - 1 + a.r_in_w is even, else from
-// w, and writes it to the other.  With an odd number of pairs sweep B leaves r in w
-// (r_in_w), so the last pair writes r back into r.  A pair whose second step is the last
-// inner step also forms that step's sum r.r and ends the outer iteration.
 // Arrays, scalars and end of the outer iteration of the two-step PPCG pass: the FP64
 // solve's (PpcgF64), or the FP32 inner PPCG of the defect-correction form (PpcgF32: the
 // correction d in place of u, FP32 r, w, sd and coefficients, no preconditioner).
@@ -1430,6 +1408,28 @@ struct PpcgF32 {
     }
 };
 
+#if TEA_DIM == 3
+// Two PPCG inner steps k, k+1 in one pass over the 3D field (temporal blocking).  The
+// reference refreshes sd's halo by reflection before every inner step
+// (tealeaf_2d/tea_solve.f90:631-636) and the steps between the outer iteration's sweeps
+// have no reduction except on the last one, so two of them share one read of sd, r, u, mi
+// and K and one write of r, u and sd: about 9 words per cell for two steps instead of
+// eighteen.  Per cell the operations and their order are those of two single steps, so the
+// results are bit-identical.
+//
+// The plane ring of k_ring3d (a block of TY warps, a 64-column x TY-row tile marching
+// through a z segment) computes step k for every loaded cell one plane ahead of step k+1.
+// Step k+1 needs step k's sd at its neighbours: z-neighbours stay in registers, y-neighbours
+// go through a two-plane shared buffer, x-neighbours by shuffle.  So a tile writes only its
+// inner 60 columns (lanes 1..30) and rows (warps 1..TY-2): tiles overlap by four columns and
+// two rows, z segments by one plane of step k.  At the domain's faces step k's sd is
+// reflected as the reference's halo update reflects it (the cell's own value).  Tiles read
+// r at cells that a neighbouring tile writes, so r goes to the other of r and w (w is free
+// during the inner steps) and sd to the other sd buffer.  Pair m (steps 2m-1, 2m) reads
+// sd[(m-1)&1] and writes sd[m&1]; it reads r from r when m - 1 + a.r_in_w is even, else from
+// w, and writes it to the other.  With an odd number of pairs sweep B leaves r in w
+// (r_in_w), so the last pair writes r back into r.  A pair whose second step is the last
+// inner step also forms that step's sum r.r and ends the outer iteration.
 template <class T, int TY, int RP>
 constexpr size_t ppcg2_smem_bytes()
 {
@@ -2316,30 +2316,31 @@ __global__ void __launch_bounds__(RWARPS * 32, 3) k_cheby4_ring2d(FusedArgs a)
 // in 3D; u is read and written only at the cells a warp writes.
 enum { P2_SD = 0, P2_R = 1, P2_U = 2, P2_MI = 3, P2_KX = 4, P2_KY = 5 };
 
+template <class P>
 __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
 {
-    using T = double;
+    using T = typename P::T;
     constexpr int VEC = Pair2Geom<T>::VEC, STRIP = Pair2Geom<T>::STRIP, OUT = Pair2Geom<T>::OUT;
     extern __shared__ __align__(16) unsigned char s_ring_raw[];
     const int k = a.step;
     const int m = (k + 1) >> 1;
-    const double* __restrict__ sdk = a.sd[(m - 1) & 1];
-    double* __restrict__ sdo = a.sd[m & 1];
-    const double* __restrict__ rin = ((m - 1 + a.r_in_w) & 1) ? a.w : a.r;
-    double* __restrict__ rout = ((m + a.r_in_w) & 1) ? a.w : a.r;
-    double* __restrict__ U = a.u[0];
-    const bool precond = a.st->precond != 0;
+    const T* __restrict__ sdk = P::sd(a, (m - 1) & 1);
+    T* __restrict__ sdo = P::sd(a, m & 1);
+    const T* __restrict__ rin = ((m - 1 + a.r_in_w) & 1) ? P::w(a) : P::r(a);
+    T* __restrict__ rout = ((m + a.r_in_w) & 1) ? P::w(a) : P::r(a);
+    T* __restrict__ U = P::u(a);
+    const T* __restrict__ mi = P::mi(a);
+    const bool precond = mi != nullptr;
     const bool last = k + 1 == a.st->inner_steps;  // step k+1 ends the outer iteration
     DDVec<1> acc;
     acc.zero();
-    const double* __restrict__ mi = precond ? a.mi : nullptr;
-    const double al1 = a.ch_alphas[k - 1], be1 = a.ch_betas[k - 1];
-    const double al2 = a.ch_alphas[k], be2 = a.ch_betas[k];
+    const T al1 = (T)a.ch_alphas[k - 1], be1 = (T)a.ch_betas[k - 1];
+    const T al2 = (T)a.ch_alphas[k], be2 = (T)a.ch_betas[k];
     const Geom& g = a.g;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     T* ring = reinterpret_cast<T*>(s_ring_raw) + (size_t)warp * C2_RQ * C2_NA * STRIP;
-    const T* src[C2_NA] = {sdk, rin, U, mi, a.kx, a.ky};
+    const T* src[C2_NA] = {sdk, rin, U, mi, P::kx(a), P::ky(a)};
     const int xlast = g.X - HALO_PAD - 1;
     const int ylast = g.Y - HALO_PAD - 1;
     const int per_x = (g.nx + OUT - 1) / OUT;
@@ -2350,7 +2351,7 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
     const bool out_lane = lane >= 1 && lane <= 30;
     for (long sgi = gw; sgi < nseg; sgi += nw) {
         const int xs = (int)(sgi % per_x), ys = (int)(sgi / per_x);
-        const int c = OUT * xs + VEC * lane - (VEC - 2);  // the lane's first column (>= 0)
+        const int c = OUT * xs + VEC * lane - (VEC - 2);  // the lane's first column (>= -2: the lead pad)
         const int cc = min(c, cmax);
         const int j0 = HALO_PAD + a.seg_rows * ys;
         const int j1 = min(j0 + a.seg_rows, ylast + 1);
@@ -2380,7 +2381,7 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
         ld_vec(slot(a0 - 1) + P2_SD * STRIP + VEC * lane, um);
         ld_vec(slot(a0) + P2_SD * STRIP + VEC * lane, uc);
 #pragma unroll
-        for (int q = 0; q < VEC; ++q) vm[q] = vc[q] = r1c[q] = u1c[q] = 0.0;
+        for (int q = 0; q < VEC; ++q) vm[q] = vc[q] = r1c[q] = u1c[q] = (T)0;
         for (int t = a0; t <= j1; ++t) {
             cp_async_wait<C2_RP>();
             __syncwarp();
@@ -2404,14 +2405,14 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
                 const T dn = __shfl_down_sync(0xffffffffu, uc[0], 1);
 #pragma unroll
                 for (int q = 0; q < VEC; ++q) {
-                    Nb nb;
-                    nb.zm = nb.zp = 0.0;
+                    NbT<T> nb;
+                    nb.zm = nb.zp = (T)0;
                     nb.c = uc[q];
                     nb.xm = c + q == HALO_PAD ? uc[q] : (q == 0 ? up : uc[q > 0 ? q - 1 : 0]);
                     nb.xp = c + q == xlast ? uc[q] : (q == VEC - 1 ? dn : uc[q < VEC - 1 ? q + 1 : q]);
                     nb.ym = um[q];
                     nb.yp = un[q];
-                    const T s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], 0.0, 0.0);
+                    const T s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], (T)0, (T)0);
                     const T r = rr[q] - s;
                     r1v[q] = r;
                     u1v[q] = uu[q] + uc[q];
@@ -2422,7 +2423,7 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
 #pragma unroll
                 for (int q = 0; q < VEC; ++q) {
                     v[q] = vc[q];
-                    r1v[q] = u1v[q] = 0.0;
+                    r1v[q] = u1v[q] = (T)0;
                 }
             }
             if (t == HALO_PAD) {
@@ -2444,19 +2445,19 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
                 const long i = fidx(g, c, srow, 0);
 #pragma unroll
                 for (int q = 0; q < VEC; ++q) {
-                    Nb nb;
-                    nb.zm = nb.zp = 0.0;
+                    NbT<T> nb;
+                    nb.zm = nb.zp = (T)0;
                     nb.c = vc[q];
                     nb.xm = c + q == HALO_PAD ? vc[q] : (q == 0 ? up : vc[q > 0 ? q - 1 : 0]);
                     nb.xp = c + q == xlast ? vc[q] : (q == VEC - 1 ? dn : vc[q < VEC - 1 ? q + 1 : q]);
                     nb.ym = vm[q];
                     nb.yp = v[q];
-                    const T s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], 0.0, 0.0);
+                    const T s = smvp_k(nb, kx[q], kx[q + 1], ky0[q], ky1[q], (T)0, (T)0);
                     const T r = r1c[q] - s;
                     r2[q] = r;
                     u2[q] = u1c[q] + vc[q];
                     d2[q] = al2 * vc[q] + be2 * (precond ? m0[q] * r : r);
-                    if (last && out_lane && c + q <= xlast) dd_add(acc.v[0], r * r);
+                    if (last && out_lane && c + q <= xlast) dd_add(acc.v[0], (double)r * (double)r);
                 }
                 if (out_lane && c + VEC - 1 <= xlast) {
                     st_vec(rout + i, r2);
@@ -2488,8 +2489,8 @@ __global__ void __launch_bounds__(RWARPS * 32) k_ppcg2_ring2d(FusedArgs a)
         cp_async_wait<0>();
         __syncwarp();
     }
-    // The last inner step's sum r.r and the end of the outer iteration, as OpPPCGInner<true>.
-    if (last) grid_reduce_then<1>(acc, a.red, [&](const double* v) { OpPPCGInner<true>().control(a, v); });
+    // The last inner step's sum r.r and the end of the outer iteration.
+    if (last) grid_reduce_then<1>(acc, a.red, [&](const double* v) { P::control(a, v); });
 }
 #endif
 
