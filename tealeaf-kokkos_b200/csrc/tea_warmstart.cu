@@ -397,8 +397,34 @@ void conv(Net* N, View x, View y, const bf16* w, const float* bias, int relu, Vi
 
 void wgrad(Net* N, View x, View gy, Conv& L, int n, int H, int W)
 {
-    const int tiles = 9 * ((L.cin + 31) / 32) * ((L.cout + 31) / 32);
     const long npix = (long)n * H * W;
+    // The tensor cores when the shapes fit their kernel (N = cin + 16 <= 256, M = 128 >= cout,
+    // 16-byte channel groups), the CUDA cores otherwise and as the tests' reference.
+    const bool tc_fits = L.cin + 16 <= 256 && L.cout <= 128 && L.cin % 16 == 0 && x.cs % 8 == 0 && x.co % 8 == 0 &&
+                         gy.cs % 8 == 0 && gy.co % 8 == 0;
+    if (!N->use_ref && tc_fits) {
+        WgradArgs a;
+        a.x = x.p;
+        a.xcs = x.cs;
+        a.xco = x.co;
+        a.gy = gy.p;
+        a.gcs = gy.cs;
+        a.gco = gy.co;
+        a.n = n;
+        a.H = H;
+        a.W = W;
+        a.cin = L.cin;
+        a.cout = L.cout;
+        a.gw = L.gw;
+        a.gb = L.gb;
+        a.err = N->d_err;
+        const int bytes = (int)wgrad_tc_smem_bytes(L.cin);
+        cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        const long slices = std::max<long>(1, std::min<long>((2L * N->sms + 8) / 9, (npix + WT_KP - 1) / WT_KP));
+        k_wgrad_tc<<<dim3(9, (unsigned)slices), WT_THREADS, bytes, N->stream>>>(a);
+        return;
+    }
+    const int tiles = 9 * ((L.cin + 31) / 32) * ((L.cout + 31) / 32);
     const int splits = (int)std::max<long>(1, std::min<long>((N->sms * 8 + tiles - 1) / tiles, (npix + 255) / 256));
     k_wgrad<<<dim3(tiles, splits), 256, 0, N->stream>>>(x.p, x.cs, x.co, gy.p, gy.cs, gy.co, n, H, W, L.cin, L.cout,
                                                         L.gw, L.gb);

@@ -305,5 +305,194 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
     }
 }
 
+// ----------------------------------------------------------------------------- tensor-core weight gradient
+
+// k_wgrad_tc: the weight and bias gradients of a 3x3 convolution on the tensor cores.  Per
+// tap t, gW[co][t][ci] = sum_p gy[p][co] x[p + tap t][ci] is a GEMM with the pixels as its K
+// dimension: D[co][ci] (float32, tensor memory) += A[co][p] B[ci][p], A = gy and B = the
+// input shifted by the tap.  Both are staged straight from their NHWC rows, whose 16-byte
+// chunks hold 8 consecutive channels of one pixel: the MN-major, non-swizzled canonical
+// layout (a core matrix is 8 channels x 8 pixels, 128 bytes; core matrices adjacent along
+// the channels, SBO = 128 bytes, and groups of 8 pixels LBO bytes apart; descriptor fields
+// as CUTLASS 4.5's cute/arch/mma_sm100_desc.hpp and the canonical layouts of
+// cute/atom/mma_traits_sm90_gmma.hpp describe them).  M is 128 (rows co >= cout are zero),
+// N is cin + 16: the column ci = cin of B is all ones, so that D[co][cin] = sum_p gy[p][co]
+// gives the bias gradient (taken from tap 0).  A block owns one tap and a slice of the
+// pixels, 64 pixels per stage (four K = 16 MMAs), two stages; one thread issues the MMAs and
+// commits them to the stage's mbarrier.  The epilogue reads D with tcgen05.ld and adds it to
+// the float32 gradients.  Every wait is bounded, as in k_conv_tc.
+constexpr int WT_THREADS = 128;
+constexpr int WT_KP = 64;  // pixels per stage
+
+struct WgradArgs {
+    const bf16* x;  // [n][H][W][xcs], channels xco .. xco+cin
+    int xcs, xco;
+    const bf16* gy;  // [n][H][W][gcs], channels gco .. gco+cout
+    int gcs, gco;
+    int n, H, W, cin, cout;
+    float* gw;  // [cout][9][cin], accumulated
+    float* gb;  // [cout] or null, accumulated
+    int* err;
+};
+
+__host__ __device__ constexpr size_t wgrad_tc_smem_bytes(int cin)
+{
+    return 2 * ((size_t)128 * WT_KP * 2 + (size_t)(cin + 16) * WT_KP * 2) + 1024 + 64;
+}
+
+__global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char s_raw[];
+    unsigned char* base = s_raw + ((1024 - (smem_u32(s_raw) & 1023u)) & 1023u);
+    const int nb = a.cin + 16;  // N: the cin channels, the ones column and padding
+    const size_t a_bytes = (size_t)128 * WT_KP * 2, b_bytes = (size_t)nb * WT_KP * 2;
+    bf16* sA[2] = {reinterpret_cast<bf16*>(base), reinterpret_cast<bf16*>(base + a_bytes + b_bytes)};
+    bf16* sB[2] = {reinterpret_cast<bf16*>(base + a_bytes), reinterpret_cast<bf16*>(base + 2 * a_bytes + b_bytes)};
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * (a_bytes + b_bytes));
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+    int* s_abort = reinterpret_cast<int*>(tmem_slot + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int t = blockIdx.x;  // tap
+    const int dy = t / 3 - 1, dx = t % 3 - 1;
+    const int ncols = tmem_cols(nb);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        *s_abort = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    const uint32_t idesc = umma_idesc_bf16(128, nb) | (1u << 15) | (1u << 16);  // A and B MN-major
+    const uint32_t lbo_a = 128 / 8 * 128, lbo_b = (uint32_t)nb / 8 * 128;    // bytes between pixel groups
+    const int gA = 16, gB = nb / 8;                                            // channel groups of 8
+    const long npix = (long)a.n * a.H * a.W;
+    const long per = (npix + gridDim.y - 1) / gridDim.y;
+    const long pbeg = (long)blockIdx.y * per, pend = min(npix, pbeg + per);
+    const long nchunks = pend > pbeg ? (pend - pbeg + WT_KP - 1) / WT_KP : 0;
+    long fill = 0;
+    bool ok = true;
+    for (long ch = 0; ch < nchunks && ok; ++ch, ++fill) {
+        const int st = (int)(fill & 1);
+        if (fill >= 2) {
+            const bool done = mbar_wait(&bar[st], (unsigned)(((fill - 2) >> 1) & 1));
+            if (!__syncthreads_and(done)) {
+                ok = false;
+                break;
+            }
+        }
+        const long p0 = pbeg + ch * WT_KP;
+        // A = gy: 16 channel groups (co 0..127; groups at or past cout are zero) x 64 pixels.
+        for (int idx = tid; idx < gA * WT_KP; idx += WT_THREADS) {
+            const int g = idx % gA, k = idx / gA;
+            const long p = p0 + k;
+            const bool valid = p < pend && g * 8 < a.cout;
+            const bf16* src = valid ? a.gy + p * a.gcs + a.gco + g * 8 : a.gy;
+            bf16* dst = sA[st] + ((size_t)(k >> 3) * lbo_a + (size_t)g * 128 + (k & 7) * 16) / 2;
+            cp_async_16z(dst, src, valid);
+        }
+        // B = x shifted by the tap: cin / 8 channel groups, then the ones column and zeros.
+        for (int idx = tid; idx < gB * WT_KP; idx += WT_THREADS) {
+            const int g = idx % gB, k = idx / gB;
+            bf16* dst = sB[st] + ((size_t)(k >> 3) * lbo_b + (size_t)g * 128 + (k & 7) * 16) / 2;
+            if (g * 8 < a.cin) {
+                const long p = p0 + k;
+                bool valid = p < pend;
+                const bf16* src = a.x;
+                if (valid) {
+                    const int xx = (int)(p % a.W);
+                    const int yy = (int)((p / a.W) % a.H);
+                    const long img = p / ((long)a.W * a.H);
+                    const int sy = yy + dy, sx = xx + dx;
+                    valid = sy >= 0 && sy < a.H && sx >= 0 && sx < a.W;
+                    if (valid) src = a.x + ((img * a.H + sy) * a.W + sx) * a.xcs + a.xco + g * 8;
+                }
+                cp_async_16z(dst, src, valid);
+            } else {
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (g * 8 == a.cin) v.x = 0x3F80u;  // bfloat16 1.0 at channel cin
+                *reinterpret_cast<uint4*>(dst) = v;
+            }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a_addr = smem_u32(sA[st]), b_addr = smem_u32(sB[st]);
+            for (int s = 0; s < WT_KP / 16; ++s) {
+                const uint64_t da = umma_desc(a_addr + s * 2 * lbo_a, lbo_a, 128);
+                const uint64_t db = umma_desc(b_addr + s * 2 * lbo_b, lbo_b, 128);
+                const uint32_t acc = (fill > 0 || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&bar[st]))
+                         : "memory");
+        }
+    }
+    if (ok && fill > 0) {
+        const long last = fill - 1;
+        const bool done = mbar_wait(&bar[last & 1], (unsigned)((last >> 1) & 1));
+        if (!__syncthreads_and(done)) ok = false;
+    }
+    if (ok && fill > 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // Warp w reads TMEM lanes 32w..32w+31 (rows co), 16 columns (ci) at a time.
+        const int co = warp * 32 + lane;
+        for (int c0 = 0; c0 < nb; c0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (co < a.cout) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int ci = c0 + j;
+                    const float v = __uint_as_float(r[j]);
+                    if (ci < a.cin) atomicAdd(&a.gw[((long)co * 9 + t) * a.cin + ci], v);
+                    else if (ci == a.cin && t == 0 && a.gb) atomicAdd(&a.gb[co], v);
+                }
+            }
+        }
+    }
+    if (!ok) {
+        *s_abort = 1;
+        if (a.err) atomicExch(a.err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (*s_abort) {
+        for (int s = 0; s < 2; ++s) {
+            const long f = ((fill - 1) & 1) == s ? fill - 1 : fill - 2;
+            if (f >= 0) mbar_wait(&bar[s], (unsigned)((f >> 1) & 1));
+        }
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+    }
+}
+
 }  // namespace ws
 }  // namespace tea

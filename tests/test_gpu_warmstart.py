@@ -1,6 +1,6 @@
 """The learned warm start on the GPU: the network's kernels against the CPU oracle, the
-tensor-core convolution against the CUDA-core one, training, and what the trained
-network gains in the solve.
+tensor-core convolution and weight gradient against the CUDA-core ones, training, and
+what the trained network gains in the solve.
 
 There is no reference counterpart (TeaLeaf has no learned component); the numerics are
 held to oracle/warmstart_oracle.py (float64, itself pinned by finite differences in
@@ -129,6 +129,28 @@ def test_tensor_core_convolution_equals_cuda_cores():
         net.set_reference_conv(False)
         y_tc, _, _ = net.eval(x)
         assert _rel_l2(y_tc, y_ref) <= 1e-2, _rel_l2(y_tc, y_ref)
+    finally:
+        net.close()
+
+
+def test_tensor_core_weight_gradients_equal_cuda_cores():
+    """The weight and bias gradients on the tensor cores (k_wgrad_tc: per tap a GEMM over
+    the pixels, MN-major operands straight from the NHWC rows, a ones column for the bias)
+    against the CUDA-core kernel, on 32768 pixels per layer (many pixel slices per tap)."""
+    levels, base = 3, 32
+    p, x, t = _case(levels, base, 2, 128, seed=9)
+    net = tea.WarmStart(levels, base, seed=0)
+    try:
+        net.set_params(_flat(p, levels, base))
+        net.set_reference_conv(True)
+        _, _, g_ref = net.eval(x, t)
+        net.set_reference_conv(False)
+        _, _, g_tc = net.eval(x, t)
+        gr, gt = _split(g_ref, levels, base), _split(g_tc, levels, base)
+        for k in gr:
+            a, b = gt[k].reshape(-1).astype(np.float64), gr[k].reshape(-1).astype(np.float64)
+            cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
+            assert cos >= 0.999 and _rel_l2(a, b) <= 3e-2, (k, cos, _rel_l2(a, b))
     finally:
         net.close()
 
