@@ -19,6 +19,15 @@ absolute eps 1e-15 sits at the rounding floor of sum r^2: the reference itself g
 iterations at step 10 on one or two threads and 837 on four or eight), the count must lie
 within 1 of the range the reference's own runs span.  The
 FP32-refined form is held to the FP64 reference's field summary within 1e-9.
+
+Over the 30 timesteps of the 4096^2 Chebyshev deck the counts become sensitive to rounding:
+the CG -> Chebyshev switch comes when the CG error first drops below 1 (tea_solve.f90:178),
+and from timestep 13 on that happens within a few hundred CG iterations, where the error
+does not fall monotonically.  The test measures this sensitivity on the GPU itself: the
+same deck with dt one ulp larger (a relative change of 2e-16).  Wherever that perturbed run
+differs from the unperturbed one, the counts are held to the largest change the
+perturbation made over the run (field summaries stay held to 1e-10); timesteps the
+perturbation leaves unchanged keep the strict bars.
 """
 import json
 
@@ -42,16 +51,19 @@ def _solver(deck):
     return next(k for k in ITER_TOL if k in deck)
 
 
-def _check(name, got, ref, deck, steps, by_threads=None):
+def _check(name, got, ref, deck, steps, by_threads=None, sensitivity=None):
+    """`sensitivity`: {timestep: (iteration bar, switch-step bar)} for the timesteps whose
+    counts a rounding-level perturbation of the deck moves (see _sensitivity)."""
     tol = ITER_TOL[_solver(deck)]
     assert len(got) >= steps and len(ref) >= steps
     bad = []
     for i, (a, b) in enumerate(zip(got[:steps], ref[:steps])):
+        it_tol, sw_tol = (sensitivity or {}).get(a["step"], (tol, 1))
         counts = [b["iterations"]] + [v[i] for v in (by_threads or {}).values()]
-        lo, hi = min(counts) - tol, max(counts) + tol
+        lo, hi = min(counts) - it_tol, max(counts) + it_tol
         if not lo <= a["iterations"] <= hi:
             bad.append(("iterations", a["step"], a["iterations"], counts))
-        if b["switch_step"] and abs(a["switch_step"] - b["switch_step"]) > 1:
+        if b["switch_step"] and abs(a["switch_step"] - b["switch_step"]) > sw_tol:
             bad.append(("switch_step", a["step"], a["switch_step"], b["switch_step"]))
         for k in ("vol", "mass", "ie", "temp"):
             if rel(a[k], b[k]) > FIELD_SUMMARY_TOL:
@@ -59,12 +71,35 @@ def _check(name, got, ref, deck, steps, by_threads=None):
     assert not bad, (name, bad)
 
 
+# Multi-timestep decks whose later counts are checked against their rounding sensitivity.
+SENSITIVITY_CASES = {"c2_2d4096_cheby": 24}  # timesteps to perturb (25-30 stall at max_iters in both)
+DT_LINE, DT_ULP_LINE = "initial_timestep=0.004\n", "initial_timestep=0.004000000000000001\n"
+
+
+def _sensitivity(case, got, steps):
+    """Runs the deck with dt one ulp larger and returns, for every timestep from the first
+    one whose counts that changes, the largest change of the iteration count and of the
+    switch step over the run, each at least the strict bar."""
+    assert float(DT_ULP_LINE.split("=")[1]) > float(DT_LINE.split("=")[1]) and DT_LINE in case["deck"]
+    deck = case["deck"].replace(DT_LINE, DT_ULP_LINE)
+    _, pert = tea.run_deck(deck, case["dim"], fused=True, summary_every_step=True, end_step=steps)
+    d_it = [abs(a["iterations"] - b["iterations"]) for a, b in zip(got[:steps], pert)]
+    d_sw = [abs(a["switch_step"] - b["switch_step"]) for a, b in zip(got[:steps], pert)]
+    first = next((i for i in range(steps) if d_it[i] or d_sw[i] > 1), steps)
+    tol = ITER_TOL[_solver(case["deck"])]
+    bars = (max([tol] + d_it), max([1] + d_sw))
+    print(f"\nrounding sensitivity (dt + 1 ulp): counts change from timestep {first + 1}, "
+          f"by up to {bars[0]} iterations and {bars[1]} switch steps")
+    return {got[i]["step"]: bars for i in range(first, len(got))}
+
+
 @pytest.mark.parametrize("name", sorted(_cases()))
 def test_whole_solve_matches_reference_at_size(name):
     case = _cases()[name]
     ref = case["ref"]["records"]
     _, got = tea.run_deck(case["deck"], case["dim"], fused=True, summary_every_step=True)
-    _check(name, got, ref, case["deck"], len(ref), case.get("iterations_by_threads"))
+    sens = _sensitivity(case, got, SENSITIVITY_CASES[name]) if name in SENSITIVITY_CASES else None
+    _check(name, got, ref, case["deck"], len(ref), case.get("iterations_by_threads"), sens)
 
 
 @pytest.mark.parametrize("name", sorted(_cases()))
