@@ -516,14 +516,16 @@ WORKLOADS_3D = {
 INNER_SOLVERS = {0: "cg", 1: "chebyshev", 2: "ppcg"}
 
 
-def run_3d(workload, warmup, steps, arm_steps=None):
+def run_3d(workload, warmup, steps, arm_steps=None, ws=None):
     """s/timestep of a 3D configuration, plain FP64 and FP32-refined on the same deck, each
     timestep's solve timed by the driver around the synchronous ext_tea_leaf_solve_ call
     (the reference's wall clock around tea_leaf(), tealeaf_2d/diffuse.f90:74-85); the first
     `warmup` timesteps are run and not timed.  FP32-refined corrects with the deck's own
     method (PPCG decks: FP32 PPCG); on PPCG and Chebyshev decks `fp32_refined_cheby_inner`
-    also times it with FP32 Chebyshev corrections (tl_inner_solver chebyshev).  `arm_steps`
-    maps an arm's name to a smaller number of timed timesteps."""
+    also times it with FP32 Chebyshev corrections (tl_inner_solver chebyshev), and with a
+    trained 3D network `ws` (train_3d_network) `fp32_refined_cheby_inner_learned` times that
+    form with the learned warm start attached.  `arm_steps` maps an arm's name to a smaller
+    number of timed timesteps."""
     w = WORKLOADS_3D[workload]
     spec = tea.DeckSpec(dim=3, cells=w["cells"], states=w["states"], seed=w["seed"], solver=w["solver"],
                         end_step=warmup + steps, dt=0.004, eps=1e-15, eps_rel=EPS_REL, max_iters=20000,
@@ -536,11 +538,17 @@ def run_3d(workload, warmup, steps, arm_steps=None):
     arms = [("fp64", tea.PRECISION_FP64, deck, n("fp64")),
             ("fp32_refined", tea.PRECISION_FP32_REFINED, deck, n("fp32_refined"))]
     if w["solver"] in ("ppcg", "chebyshev"):
-        arms.append(("fp32_refined_cheby_inner", tea.PRECISION_FP32_REFINED,
-                     deck.replace("*endtea", "tl_inner_solver chebyshev\n*endtea"), n("fp32_refined_cheby_inner")))
+        cheby_deck = deck.replace("*endtea", "tl_inner_solver chebyshev\n*endtea")
+        arms.append(("fp32_refined_cheby_inner", tea.PRECISION_FP32_REFINED, cheby_deck,
+                     n("fp32_refined_cheby_inner")))
+        if ws:
+            arms.append(("fp32_refined_cheby_inner_learned", tea.PRECISION_FP32_REFINED, cheby_deck,
+                         n("fp32_refined_cheby_inner_learned")))
     for name, precision, dk, nsteps in arms:
+        learned = name.endswith("_learned")
         summary, recs = tea.run_deck(dk, 3, fused=True, precision=precision, summary_every_step=True,
-                                     end_step=warmup + nsteps)
+                                     end_step=warmup + nsteps, ws_net=ws["net"].id if learned else 0,
+                                     ws_mode=tea.WS_ATTACH if learned else 0)
         timed = recs[warmup:warmup + nsteps]
         summaries[name] = summary
         out[name] = {"s_per_step": sum(r["solve_seconds"] for r in timed) / len(timed),
@@ -552,9 +560,22 @@ def run_3d(workload, warmup, steps, arm_steps=None):
                      "exact_error_over_eps": [r["exact_error"] / r["eps_used"] for r in timed]}
         if precision == tea.PRECISION_FP32_REFINED:
             out[name]["inner_solver"] = [INNER_SOLVERS.get(r["inner_solver"], "?") for r in timed]
+        if learned:
+            out[name]["warm_start_used"] = [r["warm_start_used"] for r in timed]
+            out[name]["warm_r0_ratio"] = [r["warm_r0_guess"] / r["warm_r0_plain"] if r["warm_r0_plain"] else None
+                                          for r in timed]
     for name in [a[0] for a in arms[1:]]:
         out[name]["speedup_vs_fp64"] = out["fp64"]["s_per_step"] / out[name]["s_per_step"]
     out["speedup_fp32_refined"] = out["fp32_refined"]["speedup_vs_fp64"]
+    if ws and "fp32_refined_cheby_inner_learned" in out:
+        a, b = out["fp32_refined_cheby_inner"], out["fp32_refined_cheby_inner_learned"]
+        saved = a["s_per_step"] - b["s_per_step"]
+        cost = ws["record_s"] + ws["train_s"]
+        b["iterations_saved"] = ([x - y for x, y in zip(a["iterations"], b["iterations"])]
+                                 if len(a["iterations"]) == len(b["iterations"]) else None)
+        b["seconds_saved_per_step"] = saved
+        b["training"] = {k: v for k, v in ws.items() if k != "net"}
+        b["amortised_after_steps"] = cost / saved if saved > 0 else None
     # Field summaries after the same timesteps (each arm's last timestep).
     last = {a[0]: a[3] for a in arms}
     out["field_summary_max_rel_diff"] = {
@@ -563,9 +584,81 @@ def run_3d(workload, warmup, steps, arm_steps=None):
     return out
 
 
+def train_3d_network():
+    """The 512^3 configuration's learned warm start: a 3D U-Net (3 levels, 24 base channels,
+    3x3x3 convolutions, bfloat16) trained by the library's own kernels on pairs the 3D
+    solver generates at 128^3 (four seeded 24-state layouts, timesteps 1-6 of each)."""
+    t0 = time.perf_counter()
+    net = tea.WarmStart(3, 24, seed=512, dim=3)
+    for k in range(4):
+        spec = tea.DeckSpec(dim=3, cells=128, states=24, seed=513 + k, solver="ppcg", end_step=6, dt=0.004,
+                            eps=1e-15, eps_rel=EPS_REL, max_iters=20000, presteps=30, inner_steps=10,
+                            check_result=False, summary_frequency=0)
+        tea.run_deck(tea.seeded_deck(spec), 3, fused=True, ws_net=net.id, ws_mode=tea.WS_RECORD)
+    t_record = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    loss_first, loss_last, ms_step = net.train(steps=1000, batch=4, crop=32, lr=1e-4, seed=512)
+    return {"net": net, "pairs": net.pairs(), "layouts": "4 seeded 128^3 24-state layouts x 6 timesteps",
+            "record_s": t_record, "train_s": time.perf_counter() - t1, "train_ms_per_step": ms_step, "steps": 1000,
+            "batch": "4 crops of 32^3", "loss_first": loss_first, "loss_last": loss_last,
+            "network": "3D U-Net, 3 levels, 24/48/96 channels, 3x3x3 convolutions, bfloat16 weights"}
+
+
 def workload_3d(args):
-    """--workload NAME: run_3d of that configuration with the command line's steps."""
-    print(json.dumps(run_3d(args.workload, args.warmup, args.steps)))
+    """--workload NAME: run_3d of that configuration with the command line's steps (the
+    512^3 PPCG configuration with its trained 3D network when --learned is given)."""
+    ws = train_3d_network() if args.learned else None
+    out = run_3d(args.workload, args.warmup, args.steps, ws=ws)
+    if ws:
+        ws["net"].close()
+    print(json.dumps(out))
+
+
+def learned_2d_at_scale(args):
+    """--workload 2d4096_learned: the 2D learned configuration at its stated scale.  A 4-level
+    U-Net (32/64/64/64 channels, about half a million parameters) is trained by the
+    library's kernels on 4032 pairs the solver generates from 64 seeded 1024^2 layouts (63
+    timesteps each); then the 4096^2 deck runs with PPCG for --steps timesteps in the
+    FP32-refined form (FP32 PPCG corrections; FP64 PPCG stalls above 1e-10 on this deck), with
+    and without the learned warm start, through the driver (deck in, field summary out)."""
+    t0 = time.perf_counter()
+    net = tea.WarmStart(4, 32, seed=SEED, max_channels=64)
+    for k in range(64):
+        spec = tea.DeckSpec(dim=2, cells=1024, states=STATES, seed=SEED + 100 + k, solver="cg", end_step=63,
+                            dt=0.004, eps=1e-15, eps_rel=EPS_REL, max_iters=20000, summary_frequency=0,
+                            check_result=False)
+        tea.run_deck(tea.seeded_deck(spec), 2, fused=True, ws_net=net.id, ws_mode=tea.WS_RECORD)
+    t_record = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    loss_first, loss_last, ms_step = net.train(steps=4000, batch=8, crop=128, lr=1e-4, seed=SEED)
+    t_train = time.perf_counter() - t1
+    spec = tea.DeckSpec(dim=2, cells=CELLS, states=STATES, seed=SEED, solver="ppcg", end_step=args.steps, dt=0.004,
+                        eps=1e-15, eps_rel=EPS_REL, max_iters=20000, presteps=30, inner_steps=10,
+                        check_result=False, summary_frequency=0)
+    deck = tea.seeded_deck(spec)
+    out = {"workload": "2d_4096x4096_16states_ppcg_rel1e-10_learned", "timesteps": args.steps,
+           "network": {"levels": 4, "channels": [32, 64, 64, 64], "params": net.param_count(),
+                       "pairs": net.pairs(), "layouts": "64 seeded 1024^2 layouts x 63 timesteps (CG, FP64)",
+                       "record_s": t_record, "train_s": t_train, "train_ms_per_step": ms_step, "train_steps": 4000,
+                       "batch": "8 crops of 128^2", "loss_first": loss_first, "loss_last": loss_last}}
+    runs = {}
+    for name, ws_net in (("fp32_refined", 0), ("fp32_refined_learned", net.id)):
+        summary, recs = tea.run_deck(deck, 2, fused=True, precision=tea.PRECISION_FP32_REFINED,
+                                     summary_every_step=True, ws_net=ws_net, ws_mode=tea.WS_ATTACH if ws_net else 0)
+        runs[name] = (summary, recs)
+        out[name] = {"s_per_step": sum(r["solve_seconds"] for r in recs) / len(recs),
+                     "iterations": sum(r["iterations"] for r in recs),
+                     "exact_error_over_eps_max": max(r["exact_error"] / r["eps_used"] for r in recs),
+                     "warm_start_used": sum(r["warm_start_used"] for r in recs)}
+    a, b = out["fp32_refined"], out["fp32_refined_learned"]
+    saved = a["s_per_step"] - b["s_per_step"]
+    b["iterations_saved"] = a["iterations"] - b["iterations"]
+    b["seconds_saved_per_step"] = saved
+    b["amortised_after_steps"] = (t_record + t_train) / saved if saved > 0 else None
+    b["field_summary_max_rel_diff"] = max(tea.rel_diff(runs["fp32_refined"][0][k], runs["fp32_refined_learned"][0][k])
+                                          for k in ("vol", "mass", "ie", "temp"))
+    net.close()
+    print(json.dumps(out))
 
 
 def learned_arm(args, world):
@@ -657,11 +750,16 @@ def main():
                     help="only launch one fused kernel --reps times on the 4096^2 workload, or after one "
                          "timestep of --workload (for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--workload", choices=sorted(WORKLOADS_3D),
-                    help="time a 3D configuration instead (plain FP64 and FP32-refined, through the driver)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS_3D) + ["2d4096_learned"],
+                    help="time a 3D configuration instead (plain FP64 and FP32-refined, through the driver), or "
+                         "the 2D learned configuration at its stated scale (2d4096_learned)")
+    ap.add_argument("--learned", action="store_true", help="with --workload 3d512_ppcg: also the learned warm start")
     args = ap.parse_args()
     if args.kernel:
         kernel_only(args)
+        return
+    if args.workload == "2d4096_learned":
+        learned_2d_at_scale(args)
         return
     if args.workload:
         workload_3d(args)
@@ -683,7 +781,10 @@ def main():
     # The 3D 512^3 PPCG configuration: plain FP64 against FP32-refined with FP32 PPCG
     # corrections (the deck's method; two timed timesteps, it is the slowest arm) and with
     # FP32 Chebyshev corrections, one warm-up timestep and five timed ones otherwise.
-    c5 = None if args.no_3d else run_3d("3d512_ppcg", 1, 5, {"fp32_refined": 2})
+    ws3 = None if args.no_3d or args.no_learned else train_3d_network()
+    c5 = None if args.no_3d else run_3d("3d512_ppcg", 1, 5, {"fp32_refined": 2}, ws=ws3)
+    if ws3:
+        ws3["net"].close()
     if rank != 0:
         dist_done(world)
         return

@@ -194,11 +194,14 @@ void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* params,
                          tea_solve_result* result);
 
 /* ---------------------------------------------------------------------------------
- * Learned warm start (no counterpart in the reference; 2D).  A U-Net of `levels`
- * levels and `base` channels at full resolution (doubling per level), bfloat16 weights
- * and activations with float32 accumulation, predicts the timestep increment
- * du = u(n+1) - u0 from u0 = density*energy, density, Kx and Ky (through the plain start's
- * residual r0 = u0 - A u0, which scales input and output).  A chunk with a network
+ * Learned warm start (no counterpart in the reference).  A U-Net of `levels` levels and
+ * `base` channels at full resolution (doubling per level), bfloat16 weights and
+ * activations with float32 accumulation, predicts the timestep increment
+ * du = u(n+1) - u0 from u0 = density*energy, density, Kx, Ky (and Kz) -- through the plain
+ * start's residual r0 = u0 - A u0, which scales input and output.  The 2D library's
+ * network is made of 3x3 convolutions and 2x2 average pooling over [ny][nx] images, the 3D
+ * library's of 3x3x3 convolutions and 2x2x2 pooling over [nz][ny][nx] volumes, with 5
+ * input features instead of 4 (log10(1 + Kz) added).  A chunk with a network
  * attached starts each ext_tea_leaf_solve_ from u0 + du, smoothed by 8 damped Jacobi
  * sweeps in FP64, when that start has the smaller FP64 residual (else from u0, as the
  * reference does) and converges to the same tolerance.  After three rejected guesses in a
@@ -208,15 +211,18 @@ void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* params,
  * --------------------------------------------------------------------------------- */
 
 /* New network with seeded He-initialised weights on the current device: levels 2..5,
- * base 16, 32 or 64.  Writes its id (1-based). */
+ * base 16, 24, 32 or 64.  Writes its id (1-based).  tea_ws_create_capped_ stops the
+ * doubling of the channel count at max_channels (0: no limit; 4 levels of base 32 capped
+ * at 64 give 32/64/64/64 channels, about half a million parameters). */
 int tea_ws_create_(const int* levels, const int* base, const int* seed, int* net);
+int tea_ws_create_capped_(const int* levels, const int* base, const int* max_channels, const int* seed, int* net);
 int tea_ws_destroy_(const int* net);
 /* Records a training pair from the chunk's last ext_tea_leaf_solve_ (its features and
  * (u - u0) / max|u0|), kept in device memory by the network. */
 int tea_ws_record_(const int* net, const int* chunk);
 int tea_ws_pairs_(const int* net, int* count);
-/* Adam training: `steps` steps on `batch` random crop x crop windows of the recorded
- * pairs (crop a multiple of 2^(levels-1)).  The loss is, per crop, the energy norm of the
+/* Adam training: `steps` steps on `batch` random crop x crop windows (crop^3 in 3D) of
+ * the recorded pairs (crop a multiple of 2^(levels-1)).  The loss is, per crop, the energy norm of the
  * smoothed guess's error relative to that of the plain start, e.A e / du.A du with
  * e = M^8 (du_pred - du), A the solver's operator on the crop and M the smoothing sweep.
  * Writes that loss averaged over the first and over the last 10 steps (below 1: the guess
@@ -226,17 +232,21 @@ int tea_ws_train_(const int* net, const int* steps, const int* batch, const int*
 /* Attaches the network to a chunk (net 0 detaches) and clears its back-off; sides must
  * be multiples of 2^(levels-1) for the guess to be used. */
 int tea_ws_attach_(const int* chunk, const int* net);
-/* The network's du for the chunk's current step, into a host array [ny][nx], and the
- * device milliseconds of the prediction. */
+/* The network's du for the chunk's current step, into a host array [ny][nx] ([nz][ny][nx]
+ * in 3D), and the device milliseconds of the prediction. */
 int tea_ws_predict_(const int* net, const int* chunk, double* du, double* ms);
-/* Test hooks: parameters in the order of the CPU oracle (per 3x3 layer w[co][9][cin],
- * then b; head w, head b), the choice of convolution (0 tensor cores, 1 CUDA cores),
- * and forward/backward on host images [n][H][W][4] (target null: forward only; kxy null:
- * mean squared error, else the residual loss with face coefficients [n][H][W][2]). */
+/* Test hooks: parameters in the order of the CPU oracle (per layer w[co][taps][cin], 9
+ * taps in 2D and 27 in 3D, then b; head w, head b), the choice of convolution (0 tensor
+ * cores, 1 CUDA cores), and forward/backward on host images [n][D][H][W][F] (F = 4 input
+ * features in 2D, where D must be 1, and 5 in 3D; target null: forward only; kxy null:
+ * mean squared error, else the residual loss with face coefficients [n][D][H][W][K],
+ * K = 2 in 2D and 3 in 3D).  tea_ws_eval_host_ is tea_ws_eval_volume_ with D = 1. */
 int tea_ws_param_count_(const int* net, long long* count);
 int tea_ws_get_params_(const int* net, float* params);
 int tea_ws_set_params_(const int* net, const float* params);
 int tea_ws_set_conv_(const int* net, const int* reference);
+int tea_ws_eval_volume_(const int* net, const float* x, const float* target, const float* kxy, const int* n,
+                        const int* D, const int* H, const int* W, float* y, double* loss, float* grads);
 int tea_ws_eval_host_(const int* net, const float* x, const float* target, const float* kxy, const int* n,
                       const int* H, const int* W, float* y, double* loss, float* grads);
 

@@ -345,14 +345,17 @@ WS_RECORD, WS_ATTACH = 1, 2  # run_deck ws_mode values
 
 
 class WarmStart:
-    """A learned warm-start network of the 2D CUDA library (tea_ws_* entry points)."""
+    """A learned warm-start network of the 2D or the 3D CUDA library (tea_ws_* entry
+    points): 3x3 convolutions over images in 2D, 3x3x3 convolutions over volumes in 3D."""
 
-    def __init__(self, levels: int = 3, base: int = 32, seed: int = 0):
-        self.lib = cuda_library(2)
+    def __init__(self, levels: int = 3, base: int = 32, seed: int = 0, dim: int = 2, max_channels: int = 0):
+        self.lib = cuda_library(dim)
+        self.dim = dim
         nid = ctypes.c_int(0)
-        self._check(self.lib.tea_ws_create_(_i(levels), _i(base), _i(seed), ctypes.byref(nid)), "create")
+        self._check(self.lib.tea_ws_create_capped_(_i(levels), _i(base), _i(max_channels), _i(seed),
+                                                   ctypes.byref(nid)), "create")
         self.id = nid.value
-        self.levels, self.base = levels, base
+        self.levels, self.base, self.max_channels = levels, base, max_channels
 
     def _check(self, rc, what):
         if rc != 0:
@@ -382,18 +385,22 @@ class WarmStart:
         self._check(self.lib.tea_ws_set_conv_(_i(self.id), _i(1 if on else 0)), "set_conv")
 
     def eval(self, x, target=None, kxy=None):
-        """x [n][H][W][4] float32 -> (y [n][H][W], loss, flat gradients or None); with kxy
-        ([n][H][W][2] face coefficients) the loss is the residual loss of training."""
+        """x [n][H][W][4] (2D) or [n][D][H][W][5] (3D) float32 -> (y [n][(D)][H][W], loss,
+        flat gradients or None); with kxy ([n][(D)][H][W][dim] face coefficients) the loss is
+        the residual loss of training."""
         x = np.ascontiguousarray(x, dtype=np.float32)
-        n, H, W, _ = x.shape
-        y = np.zeros((n, H, W), dtype=np.float32)
+        if self.dim == 3:
+            n, D, H, W, _ = x.shape
+        else:
+            (n, H, W, _), D = x.shape, 1
+        y = np.zeros(x.shape[:-1], dtype=np.float32)
         loss = ctypes.c_double(0.0)
         grads = np.zeros(self.param_count(), dtype=np.float32) if target is not None else None
         t = np.ascontiguousarray(target, dtype=np.float32) if target is not None else None
         k = np.ascontiguousarray(kxy, dtype=np.float32) if kxy is not None else None
         P = lambda a: a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
-        self._check(self.lib.tea_ws_eval_host_(_i(self.id), P(x), P(t), P(k), _i(n), _i(H), _i(W), P(y),
-                                               ctypes.byref(loss), P(grads)), "eval_host")
+        self._check(self.lib.tea_ws_eval_volume_(_i(self.id), P(x), P(t), P(k), _i(n), _i(D), _i(H), _i(W), P(y),
+                                                 ctypes.byref(loss), P(grads)), "eval_volume")
         return y, loss.value, grads
 
     def pairs(self) -> int:

@@ -1,12 +1,15 @@
 // Convolutions of the learned warm-start network (no counterpart in the reference).
 //
-// Activations are bfloat16 NHWC tensors whose channel dimension may be a slice of a wider
-// buffer (channel stride `cs`, first channel `co`), so that a decoder's concatenation is
-// written in place.  3x3 weights are stored [Cout][9][Cin] (tap t = 3*dy + dx), bfloat16,
-// with float32 biases.
+// Activations are bfloat16 channels-last tensors, [n][H][W][C] in the 2D library and
+// [n][D][H][W][C] in the 3D one (a 2D image is a volume of depth 1), whose channel
+// dimension may be a slice of a wider buffer (channel stride `cs`, first channel `co`), so
+// that a decoder's concatenation is written in place.  Weights are stored [Cout][TAPS][Cin]
+// (tap t = 3*dy + dx of a 3x3 convolution, t = 9*dz + 3*dy + dx of a 3x3x3 one), bfloat16,
+// with float32 biases.  Channel counts are multiples of 8 (16-byte chunks of a pixel's
+// channels); the tensor-core kernels pad K and N up to multiples of 16 with zeros.
 //
 // k_conv_tc is the implicit GEMM on the 5th-generation tensor cores: D[128 pixels x Cout]
-// (float32, in tensor memory) += A[128 pixels x Cin] * B[Cout x Cin]^T for each of the 9
+// (float32, in tensor memory) += A[128 pixels x Cin] * B[Cout x Cin]^T for each of the
 // taps, A gathered from the input shifted by the tap (zero padding) and B the tap's weights,
 // both staged by cp.async into shared memory in the K-major, non-swizzled canonical layout
 // (8-row x 16-byte core matrices; the descriptor fields follow CUTLASS 4.5's
@@ -26,22 +29,63 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#ifndef TEA_DIM
+#error "compile with -DTEA_DIM=2 or -DTEA_DIM=3"
+#endif
+
 namespace tea {
 namespace ws {
 
 using bf16 = __nv_bfloat16;
 
+constexpr bool WS_3D = TEA_DIM == 3;
+constexpr int TAPS = WS_3D ? 27 : 9;  // 3x3 or 3x3x3 convolutions
+
+__host__ __device__ constexpr int pad16(int c) { return (c + 15) & ~15; }
+
+// Position of pixel p in n images of D x H x W (D = 1 in 2D).
+struct Pix {
+    int x, y, z;
+    long img;
+};
+
+__device__ __forceinline__ Pix pix_of(long p, int D, int H, int W)
+{
+    Pix q;
+    q.x = (int)(p % W);
+    const long r = p / W;
+    q.y = (int)(r % H);
+    if (WS_3D) {
+        const long s = r / H;
+        q.z = (int)(s % D);
+        q.img = s / D;
+    } else {
+        q.z = 0;
+        q.img = r / H;
+    }
+    return q;
+}
+
+// The pixel tap t of a convolution reads for output pixel q, or -1 outside the image (the
+// zero padding).
+__device__ __forceinline__ long tap_src(const Pix& q, int t, int D, int H, int W)
+{
+    const int sx = q.x + t % 3 - 1, sy = q.y + (t / 3) % 3 - 1, sz = WS_3D ? q.z + t / 9 - 1 : 0;
+    if (sx < 0 || sx >= W || sy < 0 || sy >= H || sz < 0 || sz >= D) return -1;
+    return ((q.img * D + sz) * (long)H + sy) * W + sx;
+}
+
 struct ConvArgs {
-    const bf16* x;  // [n][H][W][xcs], channels xco .. xco+cin
+    const bf16* x;  // [n][D][H][W][xcs], channels xco .. xco+cin
     int xcs, xco;
-    bf16* y;  // [n][H][W][ycs], channels yco .. yco+cout
+    bf16* y;  // [n][D][H][W][ycs], channels yco .. yco+cout
     int ycs, yco;
-    const bf16* w;      // [cout][9][cin]
+    const bf16* w;      // [cout][TAPS][cin]
     const float* bias;  // [cout] or null
-    const bf16* mask;   // optional: y *= (mask > 0), mask [n][H][W][mcs] channels mco..
+    const bf16* mask;   // optional: y *= (mask > 0), mask [n][D][H][W][mcs] channels mco..
     int mcs, mco;
     int relu;
-    int n, H, W, cin, cout;
+    int n, D, H, W, cin, cout;  // D = 1 in 2D
     int* err;  // set to 1 when a bounded wait gave up
 };
 
@@ -49,20 +93,18 @@ struct ConvArgs {
 
 __global__ void __launch_bounds__(256) k_conv_ref(ConvArgs a)
 {
-    const long npix = (long)a.n * a.H * a.W;
+    const long npix = (long)a.n * a.D * a.H * a.W;
     const long total = npix * a.cout;
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
         const int co = (int)(idx % a.cout);
         const long p = idx / a.cout;
-        const int xx = (int)(p % a.W);
-        const int yy = (int)((p / a.W) % a.H);
-        const long img = p / ((long)a.W * a.H);
+        const Pix q = pix_of(p, a.D, a.H, a.W);
         float acc = a.bias ? a.bias[co] : 0.0f;
-        for (int t = 0; t < 9; ++t) {
-            const int sy = yy + t / 3 - 1, sx = xx + t % 3 - 1;
-            if (sy < 0 || sy >= a.H || sx < 0 || sx >= a.W) continue;
-            const bf16* xp = a.x + ((img * a.H + sy) * a.W + sx) * a.xcs + a.xco;
-            const bf16* wp = a.w + ((long)co * 9 + t) * a.cin;
+        for (int t = 0; t < TAPS; ++t) {
+            const long sp = tap_src(q, t, a.D, a.H, a.W);
+            if (sp < 0) continue;
+            const bf16* xp = a.x + sp * a.xcs + a.xco;
+            const bf16* wp = a.w + ((long)co * TAPS + t) * a.cin;
             for (int ci = 0; ci < a.cin; ++ci) acc += __bfloat162float(xp[ci]) * __bfloat162float(wp[ci]);
         }
         if (a.relu) acc = fmaxf(acc, 0.0f);
@@ -132,10 +174,11 @@ __device__ __forceinline__ void cp_async_16z(void* dst, const void* src, bool va
 constexpr int TC_THREADS = 128;
 constexpr int TC_M = 128;  // pixels per tile
 
-// Shared memory: two stages of A (128 x cin) and B (cout x cin) bfloat16, plus barriers.
+// Shared memory: two stages of A (128 x K) and B (N x K) bfloat16, K and N the channel
+// counts padded to multiples of 16, plus barriers.
 __host__ __device__ constexpr size_t conv_tc_smem_bytes(int cin, int cout)
 {
-    return 2 * ((size_t)TC_M * cin * 2 + (size_t)cout * cin * 2) + 1024 + 64;
+    return 2 * ((size_t)TC_M * pad16(cin) * 2 + (size_t)pad16(cout) * pad16(cin) * 2) + 1024 + 64;
 }
 
 __host__ __device__ constexpr int tmem_cols(int cout) { return cout <= 32 ? 32 : (cout <= 64 ? 64 : (cout <= 128 ? 128 : 256)); }
@@ -146,7 +189,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
     // 1024-align the operand area.
     unsigned char* base = s_raw + ((1024 - (smem_u32(s_raw) & 1023u)) & 1023u);
     const int cin = a.cin, cout = a.cout;
-    const size_t a_bytes = (size_t)TC_M * cin * 2, b_bytes = (size_t)cout * cin * 2;
+    const int kp = pad16(cin), np = pad16(cout);  // K and N of the MMAs (zero padded)
+    const size_t a_bytes = (size_t)TC_M * kp * 2, b_bytes = (size_t)np * kp * 2;
     bf16* sA[2] = {reinterpret_cast<bf16*>(base), reinterpret_cast<bf16*>(base + a_bytes + b_bytes)};
     bf16* sB[2] = {reinterpret_cast<bf16*>(base + a_bytes), reinterpret_cast<bf16*>(base + 2 * a_bytes + b_bytes)};
     uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * (a_bytes + b_bytes));
@@ -154,7 +198,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
     int* s_abort = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ncols = tmem_cols(cout);
+    const int ncols = tmem_cols(np);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(ncols)
@@ -171,17 +215,17 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    const uint32_t idesc = umma_idesc_bf16(TC_M, cout);
-    const uint32_t sbo = (uint32_t)cin * 16;  // bytes between 8-row groups
-    const int kchunks = cin / 8;              // 16-byte chunks per row
-    const long npix = (long)a.n * a.H * a.W;
+    const uint32_t idesc = umma_idesc_bf16(TC_M, np);
+    const uint32_t sbo = (uint32_t)kp * 16;  // bytes between 8-row groups
+    const int kchunks = kp / 8;              // 16-byte chunks per row (those at or past cin are zeros)
+    const long npix = (long)a.n * a.D * a.H * a.W;
     const long ntiles = (npix + TC_M - 1) / TC_M;
     long fill = 0;  // fills issued by this CTA (stage = fill & 1)
     bool ok = true;
 
     for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const long p0 = tile * TC_M;
-        for (int t = 0; t < 9 && ok; ++t, ++fill) {
+        for (int t = 0; t < TAPS && ok; ++t, ++fill) {
             const int st = (int)(fill & 1);
             if (fill >= 2) {
                 // The MMAs that last read this stage (fill - 2) must be complete; the decision
@@ -192,30 +236,27 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
                     break;
                 }
             }
-            const int dy = t / 3 - 1, dx = t % 3 - 1;
             // A: 128 rows (pixels) x kchunks 16-byte chunks.
             for (int idx = tid; idx < TC_M * kchunks; idx += TC_THREADS) {
                 const int m = idx / kchunks, c = idx % kchunks;
                 const long p = p0 + m;
-                bool valid = p < npix;
+                bool valid = p < npix && c * 8 < cin;
                 const bf16* src = a.x;
                 if (valid) {
-                    const int xx = (int)(p % a.W);
-                    const int yy = (int)((p / a.W) % a.H);
-                    const long img = p / ((long)a.W * a.H);
-                    const int sy = yy + dy, sx = xx + dx;
-                    valid = sy >= 0 && sy < a.H && sx >= 0 && sx < a.W;
-                    if (valid) src = a.x + ((img * a.H + sy) * a.W + sx) * a.xcs + a.xco + c * 8;
+                    const long sp = tap_src(pix_of(p, a.D, a.H, a.W), t, a.D, a.H, a.W);
+                    valid = sp >= 0;
+                    if (valid) src = a.x + sp * a.xcs + a.xco + c * 8;
                 }
                 bf16* dst = sA[st] + (size_t)(m >> 3) * (sbo / 2) + (size_t)c * 64 + (m & 7) * 8;
                 cp_async_16z(dst, src, valid);
             }
-            // B: cout rows x kchunks chunks of tap t.
-            for (int idx = tid; idx < cout * kchunks; idx += TC_THREADS) {
+            // B: np rows x kchunks chunks of tap t (rows at or past cout are zeros).
+            for (int idx = tid; idx < np * kchunks; idx += TC_THREADS) {
                 const int r = idx / kchunks, c = idx % kchunks;
-                const bf16* src = a.w + ((size_t)r * 9 + t) * cin + c * 8;
+                const bool valid = r < cout && c * 8 < cin;
+                const bf16* src = valid ? a.w + ((size_t)r * TAPS + t) * cin + c * 8 : a.w;
                 bf16* dst = sB[st] + (size_t)(r >> 3) * (sbo / 2) + (size_t)c * 64 + (r & 7) * 8;
-                cp_async_16z(dst, src, true);
+                cp_async_16z(dst, src, valid);
             }
             asm volatile("cp.async.wait_all;" ::: "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -223,7 +264,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
             if (tid == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t a_addr = smem_u32(sA[st]), b_addr = smem_u32(sB[st]);
-                for (int s = 0; s < cin / 16; ++s) {
+                for (int s = 0; s < kp / 16; ++s) {
                     const uint64_t da = umma_desc(a_addr + s * 256, 128, sbo);
                     const uint64_t db = umma_desc(b_addr + s * 256, 128, sbo);
                     const uint32_t acc = (t > 0 || s > 0) ? 1u : 0u;
@@ -240,7 +281,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
             }
         }
         if (!ok) break;
-        // All nine taps issued; wait for the last commit (MMAs complete in order).
+        // All taps issued; wait for the last commit (MMAs complete in order).
         const long last = fill - 1;
         const bool done = mbar_wait(&bar[last & 1], (unsigned)((last >> 1) & 1));
         if (!__syncthreads_and(done)) {
@@ -250,7 +291,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         // Epilogue: warp w reads TMEM lanes 32w..32w+31 (pixels), 16 columns at a time.
         const long p = p0 + warp * 32 + lane;
-        for (int c0 = 0; c0 < cout; c0 += 16) {
+        for (int c0 = 0; c0 < np; c0 += 16) {
             uint32_t r[16];
             const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
             asm volatile(
@@ -262,22 +303,24 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (p < npix) {
+                const int nc = min(16, cout - c0);  // real output channels in this group
                 __align__(16) bf16 out[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     float v = __uint_as_float(r[j]);
-                    if (a.bias) v += a.bias[c0 + j];
-                    if (a.relu) v = fmaxf(v, 0.0f);
-                    if (a.mask && !(__bfloat162float(a.mask[p * a.mcs + a.mco + c0 + j]) > 0.0f)) v = 0.0f;
+                    if (j < nc) {
+                        if (a.bias) v += a.bias[c0 + j];
+                        if (a.relu) v = fmaxf(v, 0.0f);
+                        if (a.mask && !(__bfloat162float(a.mask[p * a.mcs + a.mco + c0 + j]) > 0.0f)) v = 0.0f;
+                    }
                     out[j] = __float2bfloat16(v);
                 }
                 bf16* dst = a.y + p * a.ycs + a.yco + c0;
-                if ((((uintptr_t)dst) & 15u) == 0) {
+                if (nc == 16 && (((uintptr_t)dst) & 15u) == 0) {
                     reinterpret_cast<uint4*>(dst)[0] = reinterpret_cast<const uint4*>(out)[0];
                     reinterpret_cast<uint4*>(dst)[1] = reinterpret_cast<const uint4*>(out)[1];
                 } else {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) dst[j] = out[j];
+                    for (int j = 0; j < nc; ++j) dst[j] = out[j];
                 }
             }
         }
@@ -307,7 +350,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
 
 // ----------------------------------------------------------------------------- tensor-core weight gradient
 
-// k_wgrad_tc: the weight and bias gradients of a 3x3 convolution on the tensor cores.  Per
+// k_wgrad_tc: the weight and bias gradients of a convolution on the tensor cores.  Per
 // tap t, gW[co][t][ci] = sum_p gy[p][co] x[p + tap t][ci] is a GEMM with the pixels as its K
 // dimension: D[co][ci] (float32, tensor memory) += A[co][p] B[ci][p], A = gy and B = the
 // input shifted by the tap.  Both are staged straight from their NHWC rows, whose 16-byte
@@ -316,8 +359,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
 // the channels, SBO = 128 bytes, and groups of 8 pixels LBO bytes apart; descriptor fields
 // as CUTLASS 4.5's cute/arch/mma_sm100_desc.hpp and the canonical layouts of
 // cute/atom/mma_traits_sm90_gmma.hpp describe them).  M is 128 (rows co >= cout are zero),
-// N is cin + 16: the column ci = cin of B is all ones, so that D[co][cin] = sum_p gy[p][co]
-// gives the bias gradient (taken from tap 0).  A block owns one tap and a slice of the
+// N is cin padded to a multiple of 16, plus 16: the column ci = cin of B is all ones, so
+// that D[co][cin] = sum_p gy[p][co] gives the bias gradient (taken from tap 0).  A block owns one tap and a slice of the
 // pixels, 64 pixels per stage (four K = 16 MMAs), two stages; one thread issues the MMAs and
 // commits them to the stage's mbarrier.  The epilogue reads D with tcgen05.ld and adds it to
 // the float32 gradients.  Every wait is bounded, as in k_conv_tc.
@@ -325,26 +368,26 @@ constexpr int WT_THREADS = 128;
 constexpr int WT_KP = 64;  // pixels per stage
 
 struct WgradArgs {
-    const bf16* x;  // [n][H][W][xcs], channels xco .. xco+cin
+    const bf16* x;  // [n][D][H][W][xcs], channels xco .. xco+cin
     int xcs, xco;
-    const bf16* gy;  // [n][H][W][gcs], channels gco .. gco+cout
+    const bf16* gy;  // [n][D][H][W][gcs], channels gco .. gco+cout
     int gcs, gco;
-    int n, H, W, cin, cout;
-    float* gw;  // [cout][9][cin], accumulated
+    int n, D, H, W, cin, cout;  // D = 1 in 2D
+    float* gw;  // [cout][TAPS][cin], accumulated
     float* gb;  // [cout] or null, accumulated
     int* err;
 };
 
 __host__ __device__ constexpr size_t wgrad_tc_smem_bytes(int cin)
 {
-    return 2 * ((size_t)128 * WT_KP * 2 + (size_t)(cin + 16) * WT_KP * 2) + 1024 + 64;
+    return 2 * ((size_t)128 * WT_KP * 2 + (size_t)(pad16(cin) + 16) * WT_KP * 2) + 1024 + 64;
 }
 
 __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
 {
     extern __shared__ __align__(1024) unsigned char s_raw[];
     unsigned char* base = s_raw + ((1024 - (smem_u32(s_raw) & 1023u)) & 1023u);
-    const int nb = a.cin + 16;  // N: the cin channels, the ones column and padding
+    const int nb = pad16(a.cin) + 16;  // N: the cin channels, the ones column and zeros
     const size_t a_bytes = (size_t)128 * WT_KP * 2, b_bytes = (size_t)nb * WT_KP * 2;
     bf16* sA[2] = {reinterpret_cast<bf16*>(base), reinterpret_cast<bf16*>(base + a_bytes + b_bytes)};
     bf16* sB[2] = {reinterpret_cast<bf16*>(base + a_bytes), reinterpret_cast<bf16*>(base + 2 * a_bytes + b_bytes)};
@@ -354,7 +397,6 @@ __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int t = blockIdx.x;  // tap
-    const int dy = t / 3 - 1, dx = t % 3 - 1;
     const int ncols = tmem_cols(nb);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -375,7 +417,7 @@ __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
     const uint32_t idesc = umma_idesc_bf16(128, nb) | (1u << 15) | (1u << 16);  // A and B MN-major
     const uint32_t lbo_a = 128 / 8 * 128, lbo_b = (uint32_t)nb / 8 * 128;    // bytes between pixel groups
     const int gA = 16, gB = nb / 8;                                            // channel groups of 8
-    const long npix = (long)a.n * a.H * a.W;
+    const long npix = (long)a.n * a.D * a.H * a.W;
     const long per = (npix + gridDim.y - 1) / gridDim.y;
     const long pbeg = (long)blockIdx.y * per, pend = min(npix, pbeg + per);
     const long nchunks = pend > pbeg ? (pend - pbeg + WT_KP - 1) / WT_KP : 0;
@@ -409,12 +451,9 @@ __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
                 bool valid = p < pend;
                 const bf16* src = a.x;
                 if (valid) {
-                    const int xx = (int)(p % a.W);
-                    const int yy = (int)((p / a.W) % a.H);
-                    const long img = p / ((long)a.W * a.H);
-                    const int sy = yy + dy, sx = xx + dx;
-                    valid = sy >= 0 && sy < a.H && sx >= 0 && sx < a.W;
-                    if (valid) src = a.x + ((img * a.H + sy) * a.W + sx) * a.xcs + a.xco + g * 8;
+                    const long sp = tap_src(pix_of(p, a.D, a.H, a.W), t, a.D, a.H, a.W);
+                    valid = sp >= 0;
+                    if (valid) src = a.x + sp * a.xcs + a.xco + g * 8;
                 }
                 cp_async_16z(dst, src, valid);
             } else {
@@ -470,7 +509,7 @@ __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
                 for (int j = 0; j < 16; ++j) {
                     const int ci = c0 + j;
                     const float v = __uint_as_float(r[j]);
-                    if (ci < a.cin) atomicAdd(&a.gw[((long)co * 9 + t) * a.cin + ci], v);
+                    if (ci < a.cin) atomicAdd(&a.gw[((long)co * TAPS + t) * a.cin + ci], v);
                     else if (ci == a.cin && t == 0 && a.gb) atomicAdd(&a.gb[co], v);
                 }
             }

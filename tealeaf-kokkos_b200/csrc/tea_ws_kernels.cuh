@@ -7,7 +7,7 @@
 namespace tea {
 namespace ws {
 
-struct View {  // a channel slice of an NHWC buffer
+struct View {  // a channel slice of a channels-last buffer
     bf16* p;
     int cs, co, c;  // channel stride, first channel, channels
 };
@@ -20,19 +20,18 @@ struct View {  // a channel slice of an NHWC buffer
 constexpr int WG_PIX = 64;
 
 __global__ void __launch_bounds__(256) k_wgrad(const bf16* x, int xcs, int xco, const bf16* gy, int gcs, int gco,
-                                                int n, int H, int W, int cin, int cout, float* gw, float* gb)
+                                                int n, int D, int H, int W, int cin, int cout, float* gw, float* gb)
 {
     __shared__ float s_g[WG_PIX][33];
     __shared__ float s_x[WG_PIX][33];
     const int ci_tiles = (cin + 31) / 32, co_tiles = (cout + 31) / 32;
     int b = blockIdx.x;
-    const int t = b % 9;
-    b /= 9;
+    const int t = b % TAPS;
+    b /= TAPS;
     const int cit = b % ci_tiles;
     const int cot = b / ci_tiles;
     if (cot >= co_tiles) return;
-    const int dy = t / 3 - 1, dx = t % 3 - 1;
-    const long npix = (long)n * H * W;
+    const long npix = (long)n * D * H * W;
     const long per = (npix + gridDim.y - 1) / gridDim.y;
     const long pbeg = blockIdx.y * per, pend = min(npix, pbeg + per);
     const int tid = threadIdx.x;
@@ -48,11 +47,10 @@ __global__ void __launch_bounds__(256) k_wgrad(const bf16* x, int xcs, int xco, 
                 const int co = cot * 32 + c;
                 if (co < cout) gv = __bfloat162float(gy[p * gcs + gco + co]);
                 const int ci = cit * 32 + c;
-                const int xx = (int)(p % W), yy = (int)((p / W) % H);
-                const long img = p / ((long)W * H);
-                const int sy = yy + dy, sx = xx + dx;
-                if (ci < cin && sy >= 0 && sy < H && sx >= 0 && sx < W)
-                    xv = __bfloat162float(x[((img * H + sy) * W + sx) * xcs + xco + ci]);
+                if (ci < cin) {
+                    const long sp = tap_src(pix_of(p, D, H, W), t, D, H, W);
+                    if (sp >= 0) xv = __bfloat162float(x[sp * xcs + xco + ci]);
+                }
             }
             s_g[pp][c] = gv;
             s_x[pp][c] = xv;
@@ -73,7 +71,7 @@ __global__ void __launch_bounds__(256) k_wgrad(const bf16* x, int xcs, int xco, 
     if (co < cout) {
         for (int k = 0; k < 4; ++k) {
             const int ci = cit * 32 + tci + k;
-            if (ci < cin) atomicAdd(&gw[((long)co * 9 + t) * cin + ci], acc[k]);
+            if (ci < cin) atomicAdd(&gw[((long)co * TAPS + t) * cin + ci], acc[k]);
         }
         if (gb && t == 0 && cit == 0 && tci == 0) atomicAdd(&gb[co], accb);
     }
@@ -81,69 +79,84 @@ __global__ void __launch_bounds__(256) k_wgrad(const bf16* x, int xcs, int xco, 
 
 // ----------------------------------------------------------------------------- pooling
 
-__global__ void k_avgpool(View x, bf16* y, int n, int H, int W)
+// Each coarse pixel averages its 2^dim children (2x2 in 2D, 2x2x2 in 3D); upsampling copies
+// it back to them.  D, H, W are the fine sizes (D = 1 in 2D).
+constexpr int POOL = WS_3D ? 8 : 4;
+
+__host__ __device__ __forceinline__ int coarse_d(int D) { return WS_3D ? D / 2 : 1; }
+
+// Fine pixel of child c (bit 0: x, bit 1: y, bit 2: z) of coarse pixel q.
+__device__ __forceinline__ long child_of(const Pix& q, int c, int D, int H, int W)
 {
-    const int h2 = H / 2, w2 = W / 2;
-    const long total = (long)n * h2 * w2 * x.c;
+    const int fx = 2 * q.x + (c & 1), fy = 2 * q.y + ((c >> 1) & 1), fz = WS_3D ? 2 * q.z + ((c >> 2) & 1) : 0;
+    return ((q.img * D + fz) * (long)H + fy) * W + fx;
+}
+
+// Coarse pixel of fine pixel p.
+__device__ __forceinline__ long parent_of(long p, int D, int H, int W)
+{
+    const Pix f = pix_of(p, D, H, W);
+    const int d2 = coarse_d(D);
+    return ((f.img * d2 + (WS_3D ? f.z / 2 : 0)) * (long)(H / 2) + f.y / 2) * (W / 2) + f.x / 2;
+}
+
+__global__ void k_avgpool(View x, bf16* y, int n, int D, int H, int W)
+{
+    const int d2 = coarse_d(D), h2 = H / 2, w2 = W / 2;
+    const long total = (long)n * d2 * h2 * w2 * x.c;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const int c = (int)(i % x.c);
         const long q = i / x.c;
-        const int xx = (int)(q % w2), yy = (int)((q / w2) % h2);
-        const long img = q / ((long)w2 * h2);
+        const Pix qc = pix_of(q, d2, h2, w2);
         float s = 0.f;
-        for (int d = 0; d < 4; ++d) {
-            const long p = (img * H + 2 * yy + d / 2) * W + 2 * xx + d % 2;
+        for (int d = 0; d < POOL; ++d) {
+            const long p = child_of(qc, d, D, H, W);
             s += __bfloat162float(x.p[p * x.cs + x.co + c]);
         }
-        y[q * x.c + c] = __float2bfloat16(0.25f * s);
+        y[q * x.c + c] = __float2bfloat16(s * (1.0f / POOL));
     }
 }
 
-// g_fine = (g_coarse / 4) * (act > 0) + g_skip, the gradient with respect to the
+// g_fine = (g_coarse / 2^dim) * (act > 0) + g_skip, the gradient with respect to the
 // pre-activation of an encoder level's last convolution.
-__global__ void k_avgpool_bw(const bf16* gc, View act, View gskip, bf16* gf, int n, int H, int W)
+__global__ void k_avgpool_bw(const bf16* gc, View act, View gskip, bf16* gf, int n, int D, int H, int W)
 {
     const int C = act.c;
-    const long total = (long)n * H * W * C;
+    const long total = (long)n * D * H * W * C;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const int c = (int)(i % C);
         const long p = i / C;
-        const int xx = (int)(p % W), yy = (int)((p / W) % H);
-        const long img = p / ((long)W * H);
-        const long q = (img * (H / 2) + yy / 2) * (W / 2) + xx / 2;
-        float g = 0.25f * __bfloat162float(gc[q * C + c]);
+        const long q = parent_of(p, D, H, W);
+        float g = (1.0f / POOL) * __bfloat162float(gc[q * C + c]);
         if (!(__bfloat162float(act.p[p * act.cs + act.co + c]) > 0.f)) g = 0.f;
         g += __bfloat162float(gskip.p[p * gskip.cs + gskip.co + c]);
         gf[p * C + c] = __float2bfloat16(g);
     }
 }
 
-__global__ void k_upsample(View h, View cat, int n, int H, int W)  // H, W: fine size
+__global__ void k_upsample(View h, View cat, int n, int D, int H, int W)  // D, H, W: fine size
 {
     const int C = h.c;
-    const long total = (long)n * H * W * C;
+    const long total = (long)n * D * H * W * C;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const int c = (int)(i % C);
         const long p = i / C;
-        const int xx = (int)(p % W), yy = (int)((p / W) % H);
-        const long img = p / ((long)W * H);
-        const long q = (img * (H / 2) + yy / 2) * (W / 2) + xx / 2;
+        const long q = parent_of(p, D, H, W);
         cat.p[p * cat.cs + cat.co + c] = h.p[q * h.cs + h.co + c];
     }
 }
 
-__global__ void k_upsample_bw(View gcat, bf16* gh, int n, int H, int W)  // H, W: fine size
+__global__ void k_upsample_bw(View gcat, bf16* gh, int n, int D, int H, int W)  // D, H, W: fine size
 {
-    const int C = gcat.c, h2 = H / 2, w2 = W / 2;
-    const long total = (long)n * h2 * w2 * C;
+    const int C = gcat.c, d2 = coarse_d(D), h2 = H / 2, w2 = W / 2;
+    const long total = (long)n * d2 * h2 * w2 * C;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const int c = (int)(i % C);
         const long q = i / C;
-        const int xx = (int)(q % w2), yy = (int)((q / w2) % h2);
-        const long img = q / ((long)w2 * h2);
+        const Pix qc = pix_of(q, d2, h2, w2);
         float s = 0.f;
-        for (int d = 0; d < 4; ++d) {
-            const long p = (img * H + 2 * yy + d / 2) * W + 2 * xx + d % 2;
+        for (int d = 0; d < POOL; ++d) {
+            const long p = child_of(qc, d, D, H, W);
             s += __bfloat162float(gcat.p[p * gcat.cs + gcat.co + c]);
         }
         gh[q * C + c] = __float2bfloat16(s);
@@ -204,31 +217,58 @@ __global__ void __launch_bounds__(256) k_head(const bf16* h, const float* w, con
 
 // ----------------------------------------------------------------------------- residual loss
 
-// The solver's operator on an n x H x W crop stack, A v = (1 + sum of the cell's face
-// coefficients) v - sum K_face v_neighbour, with kk[p] = (Kx, Ky) of pixel p (the faces
-// to its left and below) and the crop's outer faces taken as zero (no flux), which keeps A
-// symmetric.
-__device__ __forceinline__ float apply_a(const float* v, const float* kk, long p, int xx, int yy, int H, int W)
+// The solver's operator on an n x [D x] H x W crop stack, A v = (1 + sum of the cell's
+// face coefficients) v - sum K_face v_neighbour, with kk[NK p ..] = (Kx, Ky[, Kz]) of pixel
+// p (the faces to its left, below [and behind]) and the crop's outer faces taken as zero
+// (no flux), which keeps A symmetric.
+constexpr int NK = WS_3D ? 3 : 2;
+
+// The six (four) face coefficients of pixel q = p.
+struct Faces {
+    float xl, xr, yd, yu, zb, zf;
+};
+
+__device__ __forceinline__ Faces faces_of(const float* kk, long p, const Pix& q, int D, int H, int W)
 {
-    const float kxl = xx > 0 ? kk[2 * p] : 0.f;
-    const float kxr = xx + 1 < W ? kk[2 * (p + 1)] : 0.f;
-    const float kyd = yy > 0 ? kk[2 * p + 1] : 0.f;
-    const float kyu = yy + 1 < H ? kk[2 * (p + W) + 1] : 0.f;
-    float a = (1.f + kxl + kxr + kyd + kyu) * v[p];
-    if (xx > 0) a -= kxl * v[p - 1];
-    if (xx + 1 < W) a -= kxr * v[p + 1];
-    if (yy > 0) a -= kyd * v[p - W];
-    if (yy + 1 < H) a -= kyu * v[p + W];
+    Faces f;
+    const long page = (long)H * W;
+    f.xl = q.x > 0 ? kk[NK * p] : 0.f;
+    f.xr = q.x + 1 < W ? kk[NK * (p + 1)] : 0.f;
+    f.yd = q.y > 0 ? kk[NK * p + 1] : 0.f;
+    f.yu = q.y + 1 < H ? kk[NK * (p + W) + 1] : 0.f;
+    f.zb = WS_3D && q.z > 0 ? kk[NK * p + 2] : 0.f;
+    f.zf = WS_3D && q.z + 1 < D ? kk[NK * (p + page) + 2] : 0.f;
+    return f;
+}
+
+__device__ __forceinline__ float diag_of(const Faces& f)
+{
+    return WS_3D ? 1.f + f.xl + f.xr + f.yd + f.yu + f.zb + f.zf : 1.f + f.xl + f.xr + f.yd + f.yu;
+}
+
+__device__ __forceinline__ float apply_a(const float* v, const float* kk, long p, const Pix& q, int D, int H, int W)
+{
+    const Faces f = faces_of(kk, p, q, D, H, W);
+    float a = diag_of(f) * v[p];
+    if (q.x > 0) a -= f.xl * v[p - 1];
+    if (q.x + 1 < W) a -= f.xr * v[p + 1];
+    if (q.y > 0) a -= f.yd * v[p - W];
+    if (q.y + 1 < H) a -= f.yu * v[p + W];
+    if (WS_3D) {
+        const long page = (long)H * W;
+        if (q.z > 0) a -= f.zb * v[p - page];
+        if (q.z + 1 < D) a -= f.zf * v[p + page];
+    }
     return a;
 }
 
 // Pass 0: d = y - t.  Pass 1 (d now the smoothed error): e = A d; per image b (blockIdx.y),
 // sums[2b] += d.(A d) and sums[2b + 1] += t.(A t): the energy norm of the guess's error and
 // that of the plain start's (du = 0).
-__global__ void k_res_loss(const float* y, const float* t, const float* kk, float* d, float* e, int H, int W,
-                           float* sums, int pass)
+__global__ void k_res_loss(const float* y, const float* t, const float* kk, float* d, float* e, int D, int H,
+                           int W, float* sums, int pass)
 {
-    const long per = (long)H * W;
+    const long per = (long)D * H * W;
     const long off = (long)blockIdx.y * per;
     float s0 = 0.f, s1 = 0.f;
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < per; q += (long)gridDim.x * blockDim.x) {
@@ -236,11 +276,11 @@ __global__ void k_res_loss(const float* y, const float* t, const float* kk, floa
         if (pass == 0) {
             d[p] = y[p] - t[p];
         } else {
-            const int xx = (int)(q % W), yy = (int)(q / W);
-            const float ev = apply_a(d, kk, p, xx, yy, H, W);
+            const Pix pq = pix_of(q, D, H, W);
+            const float ev = apply_a(d, kk, p, pq, D, H, W);
             e[p] = ev;
             s0 += d[p] * ev;
-            s1 += t[p] * apply_a(t, kk, p, xx, yy, H, W);
+            s1 += t[p] * apply_a(t, kk, p, pq, D, H, W);
         }
     }
     if (pass == 0) return;
@@ -263,9 +303,10 @@ __global__ void k_res_loss(const float* y, const float* t, const float* kk, floa
 
 // dL/d(smoothed error) of L = (1/n) sum_b d_b.(A d_b) / t_b.(A t_b): 2 A d_b / (n t_b.(A t_b)),
 // with e = A d from pass 1.
-__global__ void k_res_grad(const float* e, const float* kk, const float* sums, float* gy, int n, int H, int W)
+__global__ void k_res_grad(const float* e, const float* kk, const float* sums, float* gy, int n, int D, int H,
+                           int W)
 {
-    const long per = (long)H * W;
+    const long per = (long)D * H * W;
     const long off = (long)blockIdx.y * per;
     // Crops with almost no activity (t.A t tiny) would dominate: their denominator is floored
     // at 1e-3 of the batch's largest.
@@ -287,36 +328,27 @@ __global__ void k_res_grad(const float* e, const float* kk, const float* sums, f
 constexpr int WS_SMOOTH = 8;
 constexpr float WS_OMEGA = 0.8f;
 
-__device__ __forceinline__ float diag_a(const float* kk, long p, int xx, int yy, int H, int W)
-{
-    const float kxl = xx > 0 ? kk[2 * p] : 0.f;
-    const float kxr = xx + 1 < W ? kk[2 * (p + 1)] : 0.f;
-    const float kyd = yy > 0 ? kk[2 * p + 1] : 0.f;
-    const float kyu = yy + 1 < H ? kk[2 * (p + W) + 1] : 0.f;
-    return 1.f + kxl + kxr + kyd + kyu;
-}
-
 // out = in - omega D^-1 A in (transpose = 0), or out = in - omega A tmp with tmp = D^-1 in
-// precomputed (transpose = 1); over n images of H x W.
-__global__ void k_smooth_err(const float* in, const float* tmp, float* out, const float* kk, int n, int H, int W,
-                             int transpose)
+// precomputed (transpose = 1); over n images of [D x] H x W.
+__global__ void k_smooth_err(const float* in, const float* tmp, float* out, const float* kk, int n, int D, int H,
+                             int W, int transpose)
 {
-    const long total = (long)n * H * W;
+    const long total = (long)n * D * H * W;
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < total; p += (long)gridDim.x * blockDim.x) {
-        const int xx = (int)(p % W), yy = (int)((p / W) % H);
+        const Pix q = pix_of(p, D, H, W);
         if (!transpose)
-            out[p] = in[p] - WS_OMEGA * apply_a(in, kk, p, xx, yy, H, W) / diag_a(kk, p, xx, yy, H, W);
+            out[p] = in[p] - WS_OMEGA * apply_a(in, kk, p, q, D, H, W) / diag_of(faces_of(kk, p, q, D, H, W));
         else
-            out[p] = in[p] - WS_OMEGA * apply_a(tmp, kk, p, xx, yy, H, W);
+            out[p] = in[p] - WS_OMEGA * apply_a(tmp, kk, p, q, D, H, W);
     }
 }
 
-__global__ void k_dinv(const float* in, float* out, const float* kk, int n, int H, int W)
+__global__ void k_dinv(const float* in, float* out, const float* kk, int n, int D, int H, int W)
 {
-    const long total = (long)n * H * W;
+    const long total = (long)n * D * H * W;
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < total; p += (long)gridDim.x * blockDim.x) {
-        const int xx = (int)(p % W), yy = (int)((p / W) % H);
-        out[p] = in[p] / diag_a(kk, p, xx, yy, H, W);
+        const Pix q = pix_of(p, D, H, W);
+        out[p] = in[p] / diag_of(faces_of(kk, p, q, D, H, W));
     }
 }
 
@@ -369,18 +401,18 @@ __global__ void k_adam(float* w, float* g, float* m, float* v, long count, float
     }
 }
 
-// bfloat16 copies of a 3x3 layer: w16[co][t][ci] and, for the input gradient, the
-// transposed, tap-flipped wt16[ci][t][co] = w[co][8 - t][ci].
+// bfloat16 copies of a layer: w16[co][t][ci] and, for the input gradient, the transposed,
+// tap-flipped wt16[ci][t][co] = w[co][TAPS - 1 - t][ci] (every offset of the tap negated).
 __global__ void k_weights_bf16(const float* w, bf16* w16, bf16* wt16, int cout, int cin)
 {
-    const long total = (long)cout * 9 * cin;
+    const long total = (long)cout * TAPS * cin;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const int ci = (int)(i % cin);
-        const int t = (int)((i / cin) % 9);
-        const int co = (int)(i / (9L * cin));
+        const int t = (int)((i / cin) % TAPS);
+        const int co = (int)(i / ((long)TAPS * cin));
         const bf16 v = __float2bfloat16(w[i]);
         w16[i] = v;
-        if (wt16) wt16[((long)ci * 9 + (8 - t)) * cout + co] = v;
+        if (wt16) wt16[((long)ci * TAPS + (TAPS - 1 - t)) * cout + co] = v;
     }
 }
 
