@@ -92,6 +92,11 @@ def load_traffic(kernel: str):
     return None
 
 
+def progress(msg: str) -> None:
+    """A progress line on stderr (the JSON result goes to stdout)."""
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 # ----------------------------------------------------------------------------- clocks
 
 class ClockSampler:
@@ -545,6 +550,7 @@ def run_3d(workload, warmup, steps, arm_steps=None, ws=None):
             arms.append(("fp32_refined_cheby_inner_learned", tea.PRECISION_FP32_REFINED, cheby_deck,
                          n("fp32_refined_cheby_inner_learned")))
     for name, precision, dk, nsteps in arms:
+        progress(f"{workload}: {name}, {warmup} + {nsteps} timesteps")
         learned = name.endswith("_learned")
         summary, recs = tea.run_deck(dk, 3, fused=True, precision=precision, summary_every_step=True,
                                      end_step=warmup + nsteps, ws_net=ws["net"].id if learned else 0,
@@ -584,21 +590,32 @@ def run_3d(workload, warmup, steps, arm_steps=None, ws=None):
     return out
 
 
+def train_dt(dt: float, cells: int, target_cells: int) -> float:
+    """The timestep that gives a coarser training deck the target deck's face coefficients:
+    K = dt w / h^2 with h = domain / cells, so dt scales with (target_cells / cells)^2."""
+    return dt * (target_cells / cells) ** 2
+
+
 def train_3d_network():
     """The 512^3 configuration's learned warm start: a 3D U-Net (3 levels, 24 base channels,
     3x3x3 convolutions, bfloat16) trained by the library's own kernels on pairs the 3D
-    solver generates at 128^3 (four seeded 24-state layouts, timesteps 1-6 of each)."""
+    solver generates at 128^3 (four seeded 24-state layouts, timesteps 1-6 of each), with dt
+    scaled so that the operator's coefficients match those of the 512^3 deck."""
     t0 = time.perf_counter()
     net = tea.WarmStart(3, 24, seed=512, dim=3)
     for k in range(4):
-        spec = tea.DeckSpec(dim=3, cells=128, states=24, seed=513 + k, solver="ppcg", end_step=6, dt=0.004,
+        spec = tea.DeckSpec(dim=3, cells=128, states=24, seed=513 + k, solver="ppcg", end_step=6,
+                            dt=train_dt(0.004, 128, 512),
                             eps=1e-15, eps_rel=EPS_REL, max_iters=20000, presteps=30, inner_steps=10,
                             check_result=False, summary_frequency=0)
         tea.run_deck(tea.seeded_deck(spec), 3, fused=True, ws_net=net.id, ws_mode=tea.WS_RECORD)
     t_record = time.perf_counter() - t0
+    progress(f"3D network: {net.pairs()} pairs recorded in {t_record:.1f} s; training")
     t1 = time.perf_counter()
     loss_first, loss_last, ms_step = net.train(steps=1000, batch=4, crop=32, lr=1e-4, seed=512)
-    return {"net": net, "pairs": net.pairs(), "layouts": "4 seeded 128^3 24-state layouts x 6 timesteps",
+    progress(f"3D network: loss {loss_first:.3f} -> {loss_last:.3f}, {ms_step:.2f} ms/step")
+    return {"net": net, "pairs": net.pairs(),
+            "layouts": "4 seeded 128^3 24-state layouts x 6 timesteps, dt 0.064 (the 512^3 deck's K)",
             "record_s": t_record, "train_s": time.perf_counter() - t1, "train_ms_per_step": ms_step, "steps": 1000,
             "batch": "4 crops of 32^3", "loss_first": loss_first, "loss_last": loss_last,
             "network": "3D U-Net, 3 levels, 24/48/96 channels, 3x3x3 convolutions, bfloat16 weights"}
@@ -625,7 +642,8 @@ def learned_2d_at_scale(args):
     net = tea.WarmStart(4, 32, seed=SEED, max_channels=64)
     for k in range(64):
         spec = tea.DeckSpec(dim=2, cells=1024, states=STATES, seed=SEED + 100 + k, solver="cg", end_step=63,
-                            dt=0.004, eps=1e-15, eps_rel=EPS_REL, max_iters=20000, summary_frequency=0,
+                            dt=train_dt(0.004, 1024, CELLS), eps=1e-15, eps_rel=EPS_REL, max_iters=20000,
+                            summary_frequency=0,
                             check_result=False)
         tea.run_deck(tea.seeded_deck(spec), 2, fused=True, ws_net=net.id, ws_mode=tea.WS_RECORD)
     t_record = time.perf_counter() - t0
@@ -638,7 +656,8 @@ def learned_2d_at_scale(args):
     deck = tea.seeded_deck(spec)
     out = {"workload": "2d_4096x4096_16states_ppcg_rel1e-10_learned", "timesteps": args.steps,
            "network": {"levels": 4, "channels": [32, 64, 64, 64], "params": net.param_count(),
-                       "pairs": net.pairs(), "layouts": "64 seeded 1024^2 layouts x 63 timesteps (CG, FP64)",
+                       "pairs": net.pairs(),
+                       "layouts": "64 seeded 1024^2 layouts x 63 timesteps (CG, FP64), dt 0.064 (the 4096^2 deck's K)",
                        "record_s": t_record, "train_s": t_train, "train_ms_per_step": ms_step, "train_steps": 4000,
                        "batch": "8 crops of 128^2", "loss_first": loss_first, "loss_last": loss_last}}
     runs = {}
@@ -669,7 +688,8 @@ def learned_arm(args, world):
     t0 = time.perf_counter()
     net = tea.WarmStart(3, 32, seed=SEED)
     for k in range(4):
-        spec = tea.DeckSpec(dim=2, cells=1024, states=STATES, seed=SEED + 1 + k, solver=SOLVER, end_step=6, dt=0.004,
+        spec = tea.DeckSpec(dim=2, cells=1024, states=STATES, seed=SEED + 1 + k, solver=SOLVER, end_step=6,
+                            dt=train_dt(0.004, 1024, CELLS),
                             eps=1e-15, eps_rel=EPS_REL, max_iters=20000, presteps=30, summary_frequency=0,
                             check_result=False)
         tea.run_deck(tea.seeded_deck(spec), 2, fused=True, ws_net=net.id, ws_mode=tea.WS_RECORD)
@@ -864,7 +884,8 @@ def main():
             "seconds_saved_per_step": saved,
             "warm_r0_ratio": learned["warm_r0_ratio"], "corrections": learned["corrections"],
             "field_summary_max_rel_diff_vs_fp64": diff,
-            "training": {"pairs": learned["pairs"], "layouts": "4 seeded 1024^2 layouts x 6 timesteps",
+            "training": {"pairs": learned["pairs"],
+                         "layouts": "4 seeded 1024^2 layouts x 6 timesteps, dt 0.064 (the 4096^2 deck's K)",
                          "record_s": learned["record_s"], "train_s": learned["train_s"],
                          "train_ms_per_step": learned["train_ms_per_step"], "steps": 1000,
                          "loss_first": learned["loss_first"], "loss_last": learned["loss_last"]},

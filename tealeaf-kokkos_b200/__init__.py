@@ -94,7 +94,8 @@ class StepRecord(ctypes.Structure):
         ("ie", ctypes.c_double), ("temp", ctypes.c_double), ("has_summary", ctypes.c_int),
         ("switch_step", ctypes.c_int), ("est_itc", ctypes.c_int), ("warm_start_used", ctypes.c_int),
         ("wall_end", ctypes.c_double), ("h2d_bytes", ctypes.c_longlong), ("d2h_bytes", ctypes.c_longlong),
-        ("corrections", ctypes.c_int), ("inner_solver", ctypes.c_int),
+        ("corrections", ctypes.c_int), ("inner_solver", ctypes.c_int), ("warm_r0_plain", ctypes.c_double),
+        ("warm_r0_guess", ctypes.c_double),
     ]
 
 

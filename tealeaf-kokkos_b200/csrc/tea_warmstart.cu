@@ -516,14 +516,14 @@ void forward(Net* N)
         const View out = l < L - 1 ? view(N->cat[l], N->ch[l + 1] + C, N->ch[l + 1], C) : view(N->bottom, C, 0, C);
         conv(N, view(N->A[l], C, 0, C), out, b.w16, b.b, 1, kNoView, n, D, H, W, C, C);
         if (l < L - 1) {
-            k_avgpool<<<grid_for((long)n * D * H * W / POOL * C), 256, 0, N->stream>>>(out, N->P[l], n, D, H, W);
+            k_avgpool<<<grid_for((long)n * D * H * W / POOL), 256, 0, N->stream>>>(out, N->P[l], n, D, H, W);
             h = view(N->P[l], C, 0, C);
         }
     }
     for (int l = L - 2; l >= 0; --l) {
         const int D = depth_at(N, l), H = N->wH >> l, W = N->wW >> l, C = N->ch[l], Cu = N->ch[l + 1];
         const View hin = l == L - 2 ? view(N->bottom, Cu, 0, Cu) : view(N->DB[l + 1], Cu, 0, Cu);
-        k_upsample<<<grid_for((long)n * D * H * W * Cu), 256, 0, N->stream>>>(hin, view(N->cat[l], Cu + C, 0, Cu), n,
+        k_upsample<<<grid_for((long)n * D * H * W), 256, 0, N->stream>>>(hin, view(N->cat[l], Cu + C, 0, Cu), n,
                                                                               D, H, W);
         Conv& a = dec(N, l, 0);
         Conv& b = dec(N, l, 1);
@@ -614,7 +614,7 @@ void backward(Net* N)
         wgrad(N, view(N->cat[l], Cu + C, 0, Cu + C), view(gnext, C, 0, C), a, n, D, H, W);
         conv(N, view(gnext, C, 0, C), view(N->gcat[l], Cu + C, 0, Cu + C), a.wt16, nullptr, 0,
              view(N->cat[l], Cu + C, 0, Cu + C), n, D, H, W, C, Cu + C);
-        k_upsample_bw<<<grid_for((long)n * D * H * W / POOL * Cu), 256, 0, N->stream>>>(
+        k_upsample_bw<<<grid_for((long)n * D * H * W / POOL), 256, 0, N->stream>>>(
             view(N->gcat[l], Cu + C, 0, Cu), gcur, n, D, H, W);
     }
     // gcur: gradient w.r.t. the pre-activation of enc(L-1)b.
@@ -625,7 +625,7 @@ void backward(Net* N)
         if (l < L - 1) {
             // gcur holds the gradient w.r.t. the pooled tensor P[l] (coarse); add the skip's.
             const int Cu = N->ch[l + 1];
-            k_avgpool_bw<<<grid_for((long)n * D * H * W * C), 256, 0, N->stream>>>(
+            k_avgpool_bw<<<grid_for((long)n * D * H * W), 256, 0, N->stream>>>(
                 gcur, view(N->cat[l], Cu + C, Cu, C), view(N->gcat[l], Cu + C, Cu, C), gtmp, n, D, H, W);
             std::swap(gcur, gtmp);
         }
@@ -819,8 +819,9 @@ TEA_EXPORT int tea_ws_create_capped_(const int* levels, const int* base, const i
 {
     std::lock_guard<std::mutex> lock(g_mutex);
     if (!levels || !base || !max_channels || !net || *levels < 2 || *levels > 5 ||
-        (*base != 16 && *base != 24 && *base != 32 && *base != 64) || *max_channels < 0) {
-        set_status(TEA_ERR_BAD_ARGUMENT, "tea_ws_create_: levels must be 2..5 and base 16, 24, 32 or 64");
+        (*base != 16 && *base != 24 && *base != 32 && *base != 64) || *max_channels < 0 || *max_channels % 8) {
+        set_status(TEA_ERR_BAD_ARGUMENT,
+                   "tea_ws_create_: levels must be 2..5, base 16, 24, 32 or 64, max_channels a multiple of 8");
         return TEA_ERR_BAD_ARGUMENT;
     }
     // Channels double per level, up to max_channels (0: no limit).  Every layer must fit the

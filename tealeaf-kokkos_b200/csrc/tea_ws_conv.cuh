@@ -75,6 +75,37 @@ __device__ __forceinline__ long tap_src(const Pix& q, int t, int D, int H, int W
     return ((q.img * D + sz) * (long)H + sy) * W + sx;
 }
 
+// A tile's pixel positions, decoded once per tile into shared memory so that the gathers of
+// the taps need no divisions: x, y, z of each pixel (x = -1 past the last pixel).
+struct TilePix {
+    int x, y, z, pad;
+};
+
+__device__ __forceinline__ TilePix tile_pix_of(long p, long npix, int D, int H, int W)
+{
+    TilePix t;
+    if (p < npix) {
+        const Pix q = pix_of(p, D, H, W);
+        t.x = q.x;
+        t.y = q.y;
+        t.z = q.z;
+    } else {
+        t.x = -1;
+        t.y = t.z = 0;
+    }
+    t.pad = 0;
+    return t;
+}
+
+// Whether tap (dz, dy, dx) of pixel q reads a pixel inside the image (false also when q is
+// past the last pixel), and the offset of that pixel from q.
+__device__ __forceinline__ bool tap_offset(const TilePix& q, int dz, int dy, int dx, int D, int H, int W, long& off)
+{
+    const int sx = q.x + dx, sy = q.y + dy, sz = q.z + dz;
+    off = ((long)dz * H + dy) * W + dx;
+    return q.x >= 0 && sx >= 0 && sx < W && sy >= 0 && sy < H && sz >= 0 && sz < D;
+}
+
 struct ConvArgs {
     const bf16* x;  // [n][D][H][W][xcs], channels xco .. xco+cin
     int xcs, xco;
@@ -175,10 +206,11 @@ constexpr int TC_THREADS = 128;
 constexpr int TC_M = 128;  // pixels per tile
 
 // Shared memory: two stages of A (128 x K) and B (N x K) bfloat16, K and N the channel
-// counts padded to multiples of 16, plus barriers.
+// counts padded to multiples of 16, barriers and the tile's pixel positions.
 __host__ __device__ constexpr size_t conv_tc_smem_bytes(int cin, int cout)
 {
-    return 2 * ((size_t)TC_M * pad16(cin) * 2 + (size_t)pad16(cout) * pad16(cin) * 2) + 1024 + 64;
+    return 2 * ((size_t)TC_M * pad16(cin) * 2 + (size_t)pad16(cout) * pad16(cin) * 2) + 1024 + 64 +
+           TC_M * sizeof(TilePix);
 }
 
 __host__ __device__ constexpr int tmem_cols(int cout) { return cout <= 32 ? 32 : (cout <= 64 ? 64 : (cout <= 128 ? 128 : 256)); }
@@ -196,6 +228,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
     uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * (a_bytes + b_bytes));
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
     int* s_abort = reinterpret_cast<int*>(tmem_slot + 1);
+    TilePix* s_pix = reinterpret_cast<TilePix*>(bar + 8);  // 64 bytes past the barriers
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ncols = tmem_cols(np);
@@ -225,6 +258,9 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
 
     for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const long p0 = tile * TC_M;
+        // Every thread is past the previous tile's gathers (the barrier that ends the tile).
+        s_pix[tid] = tile_pix_of(p0 + tid, npix, a.D, a.H, a.W);
+        __syncthreads();
         for (int t = 0; t < TAPS && ok; ++t, ++fill) {
             const int st = (int)(fill & 1);
             if (fill >= 2) {
@@ -237,16 +273,12 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
                 }
             }
             // A: 128 rows (pixels) x kchunks 16-byte chunks.
+            const int dz = WS_3D ? t / 9 - 1 : 0, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
             for (int idx = tid; idx < TC_M * kchunks; idx += TC_THREADS) {
-                const int m = idx / kchunks, c = idx % kchunks;
-                const long p = p0 + m;
-                bool valid = p < npix && c * 8 < cin;
-                const bf16* src = a.x;
-                if (valid) {
-                    const long sp = tap_src(pix_of(p, a.D, a.H, a.W), t, a.D, a.H, a.W);
-                    valid = sp >= 0;
-                    if (valid) src = a.x + sp * a.xcs + a.xco + c * 8;
-                }
+                const int m = idx / kchunks, c = idx - m * kchunks;
+                long off;
+                const bool valid = tap_offset(s_pix[m], dz, dy, dx, a.D, a.H, a.W, off) && c * 8 < cin;
+                const bf16* src = valid ? a.x + (p0 + m + off) * a.xcs + a.xco + c * 8 : a.x;
                 bf16* dst = sA[st] + (size_t)(m >> 3) * (sbo / 2) + (size_t)c * 64 + (m & 7) * 8;
                 cp_async_16z(dst, src, valid);
             }
@@ -380,7 +412,8 @@ struct WgradArgs {
 
 __host__ __device__ constexpr size_t wgrad_tc_smem_bytes(int cin)
 {
-    return 2 * ((size_t)128 * WT_KP * 2 + (size_t)(pad16(cin) + 16) * WT_KP * 2) + 1024 + 64;
+    return 2 * ((size_t)128 * WT_KP * 2 + (size_t)(pad16(cin) + 16) * WT_KP * 2) + 1024 + 64 +
+           2 * WT_KP * sizeof(TilePix);
 }
 
 __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
@@ -394,9 +427,11 @@ __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
     uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * (a_bytes + b_bytes));
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
     int* s_abort = reinterpret_cast<int*>(tmem_slot + 1);
+    TilePix* s_pix = reinterpret_cast<TilePix*>(bar + 8);  // [stage][WT_KP], 64 bytes past the barriers
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int t = blockIdx.x;  // tap
+    const int dz = WS_3D ? t / 9 - 1 : 0, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
     const int ncols = tmem_cols(nb);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -433,6 +468,11 @@ __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
             }
         }
         const long p0 = pbeg + ch * WT_KP;
+        // The stage's pixel positions (its previous reader, fill - 2, is complete: every
+        // thread passed the barrier after that fill's gathers).
+        TilePix* spx = s_pix + st * WT_KP;
+        if (tid < WT_KP) spx[tid] = tile_pix_of(p0 + tid, pend, a.D, a.H, a.W);
+        __syncthreads();
         // A = gy: 16 channel groups (co 0..127; groups at or past cout are zero) x 64 pixels.
         for (int idx = tid; idx < gA * WT_KP; idx += WT_THREADS) {
             const int g = idx % gA, k = idx / gA;
@@ -447,14 +487,9 @@ __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
             const int g = idx % gB, k = idx / gB;
             bf16* dst = sB[st] + ((size_t)(k >> 3) * lbo_b + (size_t)g * 128 + (k & 7) * 16) / 2;
             if (g * 8 < a.cin) {
-                const long p = p0 + k;
-                bool valid = p < pend;
-                const bf16* src = a.x;
-                if (valid) {
-                    const long sp = tap_src(pix_of(p, a.D, a.H, a.W), t, a.D, a.H, a.W);
-                    valid = sp >= 0;
-                    if (valid) src = a.x + sp * a.xcs + a.xco + g * 8;
-                }
+                long off;
+                const bool valid = tap_offset(spx[k], dz, dy, dx, a.D, a.H, a.W, off);
+                const bf16* src = valid ? a.x + (p0 + k + off) * a.xcs + a.xco + g * 8 : a.x;
                 cp_async_16z(dst, src, valid);
             } else {
                 uint4 v = make_uint4(0u, 0u, 0u, 0u);

@@ -100,20 +100,54 @@ __device__ __forceinline__ long parent_of(long p, int D, int H, int W)
     return ((f.img * d2 + (WS_3D ? f.z / 2 : 0)) * (long)(H / 2) + f.y / 2) * (W / 2) + f.x / 2;
 }
 
+// The pooling kernels take one pixel per thread and its channels 8 at a time (16-byte
+// loads and stores: channel counts, strides and offsets are multiples of 8), so that a
+// pixel's position is decoded once.
+struct Vec8 {
+    float v[8];
+};
+
+__device__ __forceinline__ Vec8 ld8(const bf16* p)
+{
+    Vec8 r;
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    const bf16* b = reinterpret_cast<const bf16*>(&u);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r.v[k] = __bfloat162float(b[k]);
+    return r;
+}
+
+__device__ __forceinline__ void st8(bf16* p, const Vec8& r)
+{
+    __align__(16) bf16 b[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) b[k] = __float2bfloat16(r.v[k]);
+    *reinterpret_cast<uint4*>(p) = *reinterpret_cast<const uint4*>(b);
+}
+
 __global__ void k_avgpool(View x, bf16* y, int n, int D, int H, int W)
 {
     const int d2 = coarse_d(D), h2 = H / 2, w2 = W / 2;
-    const long total = (long)n * d2 * h2 * w2 * x.c;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % x.c);
-        const long q = i / x.c;
+    const long total = (long)n * d2 * h2 * w2;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
         const Pix qc = pix_of(q, d2, h2, w2);
-        float s = 0.f;
-        for (int d = 0; d < POOL; ++d) {
-            const long p = child_of(qc, d, D, H, W);
-            s += __bfloat162float(x.p[p * x.cs + x.co + c]);
+        long ch[POOL];
+#pragma unroll
+        for (int d = 0; d < POOL; ++d) ch[d] = child_of(qc, d, D, H, W) * x.cs + x.co;
+        for (int c = 0; c < x.c; c += 8) {
+            Vec8 s;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s.v[k] = 0.f;
+#pragma unroll
+            for (int d = 0; d < POOL; ++d) {
+                const Vec8 v = ld8(x.p + ch[d] + c);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) s.v[k] += v.v[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s.v[k] = s.v[k] * (1.0f / POOL);
+            st8(y + q * x.c + c, s);
         }
-        y[q * x.c + c] = __float2bfloat16(s * (1.0f / POOL));
     }
 }
 
@@ -122,44 +156,58 @@ __global__ void k_avgpool(View x, bf16* y, int n, int D, int H, int W)
 __global__ void k_avgpool_bw(const bf16* gc, View act, View gskip, bf16* gf, int n, int D, int H, int W)
 {
     const int C = act.c;
-    const long total = (long)n * D * H * W * C;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const long p = i / C;
+    const long total = (long)n * D * H * W;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < total; p += (long)gridDim.x * blockDim.x) {
         const long q = parent_of(p, D, H, W);
-        float g = (1.0f / POOL) * __bfloat162float(gc[q * C + c]);
-        if (!(__bfloat162float(act.p[p * act.cs + act.co + c]) > 0.f)) g = 0.f;
-        g += __bfloat162float(gskip.p[p * gskip.cs + gskip.co + c]);
-        gf[p * C + c] = __float2bfloat16(g);
+        for (int c = 0; c < C; c += 8) {
+            const Vec8 g = ld8(gc + q * C + c);
+            const Vec8 a = ld8(act.p + p * act.cs + act.co + c);
+            const Vec8 k = ld8(gskip.p + p * gskip.cs + gskip.co + c);
+            Vec8 o;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                float v = (1.0f / POOL) * g.v[j];
+                if (!(a.v[j] > 0.f)) v = 0.f;
+                o.v[j] = v + k.v[j];
+            }
+            st8(gf + p * C + c, o);
+        }
     }
 }
 
 __global__ void k_upsample(View h, View cat, int n, int D, int H, int W)  // D, H, W: fine size
 {
     const int C = h.c;
-    const long total = (long)n * D * H * W * C;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const long p = i / C;
+    const long total = (long)n * D * H * W;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < total; p += (long)gridDim.x * blockDim.x) {
         const long q = parent_of(p, D, H, W);
-        cat.p[p * cat.cs + cat.co + c] = h.p[q * h.cs + h.co + c];
+        for (int c = 0; c < C; c += 8)
+            *reinterpret_cast<uint4*>(cat.p + p * cat.cs + cat.co + c) =
+                *reinterpret_cast<const uint4*>(h.p + q * h.cs + h.co + c);
     }
 }
 
 __global__ void k_upsample_bw(View gcat, bf16* gh, int n, int D, int H, int W)  // D, H, W: fine size
 {
     const int C = gcat.c, d2 = coarse_d(D), h2 = H / 2, w2 = W / 2;
-    const long total = (long)n * d2 * h2 * w2 * C;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const long q = i / C;
+    const long total = (long)n * d2 * h2 * w2;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
         const Pix qc = pix_of(q, d2, h2, w2);
-        float s = 0.f;
-        for (int d = 0; d < POOL; ++d) {
-            const long p = child_of(qc, d, D, H, W);
-            s += __bfloat162float(gcat.p[p * gcat.cs + gcat.co + c]);
+        long ch[POOL];
+#pragma unroll
+        for (int d = 0; d < POOL; ++d) ch[d] = child_of(qc, d, D, H, W) * gcat.cs + gcat.co;
+        for (int c = 0; c < C; c += 8) {
+            Vec8 s;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s.v[k] = 0.f;
+#pragma unroll
+            for (int d = 0; d < POOL; ++d) {
+                const Vec8 v = ld8(gcat.p + ch[d] + c);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) s.v[k] += v.v[k];
+            }
+            st8(gh + q * C + c, s);
         }
-        gh[q * C + c] = __float2bfloat16(s);
     }
 }
 

@@ -731,6 +731,8 @@ struct Runner {
             rec->corrections = r.corrections;
             rec->inner_solver = r.inner_solver;
             rec->warm_start_used = r.warm_start_used;
+            rec->warm_r0_plain = r.warm_r0_plain;
+            rec->warm_r0_guess = r.warm_r0_guess;
             if (opt->ws_net && opt->ws_mode == 1) {
                 if (!be.ws_record || be.ws_record(&opt->ws_net, &chunk) != 0) fail("warm start: cannot record pair");
             }

@@ -55,6 +55,8 @@ typedef struct {
     int corrections;         /* FP32-refined solves: outer corrections */
     int inner_solver;        /* FP32-refined solves: inner solver of the last correction
                                 (0 CG, 1 Chebyshev, 2 PPCG) */
+    double warm_r0_plain;    /* with a network attached: sum r^2 of the plain start u0 ... */
+    double warm_r0_guess;    /* ... and of the network's guess (0 when none was made) */
 } tea_step_record;
 
 typedef struct {
