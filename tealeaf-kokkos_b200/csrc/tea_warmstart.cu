@@ -288,6 +288,7 @@ struct Net {
     std::vector<Pair> pairs;
     Crop* d_crops = nullptr;
     int sms = 148;
+    int smem_per_sm = 0, smem_reserved = 0, threads_per_sm = 0;
     float out_scale = 1.f;  // the network predicts du / max|u0| * out_scale (unit RMS on the pairs)
 };
 
@@ -412,6 +413,23 @@ int ensure_workspace(Net* N, int n, int D, int H, int W, bool train)
     return TEA_OK;
 }
 
+// Blocks of a tensor-core kernel that fit on one SM at once: shared memory (with the
+// per-block reservation), threads and tensor memory (512 columns per SM).  The occupancy API
+// reports one block per SM for kernels that allocate tensor memory, whatever their size, so
+// the count is formed here from the SM's resources.
+int tc_blocks_per_sm(Net* N, int smem_bytes, int threads, int n_cols)
+{
+    if (N->smem_per_sm == 0) {
+        cudaDeviceGetAttribute(&N->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, N->device);
+        cudaDeviceGetAttribute(&N->smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, N->device);
+        cudaDeviceGetAttribute(&N->threads_per_sm, cudaDevAttrMaxThreadsPerMultiProcessor, N->device);
+    }
+    const int by_smem = N->smem_per_sm / std::max(1, smem_bytes + N->smem_reserved);
+    const int by_threads = N->threads_per_sm / threads;
+    const int by_tmem = 512 / tmem_cols(n_cols);
+    return std::max(1, std::min(std::min(by_smem, by_threads), std::min(by_tmem, 32)));
+}
+
 // y = conv(x) (3x3, or 3x3x3 in 3D) over n images of [D x] H x W.
 void conv(Net* N, View x, View y, const bf16* w, const float* bias, int relu, View mask, int n, int D, int H, int W,
           int cin, int cout)
@@ -444,10 +462,7 @@ void conv(Net* N, View x, View y, const bf16* w, const float* bias, int relu, Vi
     const long tiles = (npix + TC_M - 1) / TC_M;
     const int bytes = (int)conv_tc_smem_bytes(cin, cout);
     cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    int occ = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_tc, TC_THREADS, bytes);
-    occ = std::max(1, std::min(occ, 512 / tmem_cols(pad16(cout))));
-    const long grid = std::min<long>(tiles, (long)N->sms * occ);
+    const long grid = std::min<long>(tiles, (long)N->sms * tc_blocks_per_sm(N, bytes, TC_THREADS, pad16(cout)));
     k_conv_tc<<<(int)grid, TC_THREADS, bytes, N->stream>>>(a);
 }
 
@@ -478,8 +493,8 @@ void wgrad(Net* N, View x, View gy, Conv& L, int n, int D, int H, int W)
         a.err = N->d_err;
         const int bytes = (int)wgrad_tc_smem_bytes(L.cin);
         cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        const long slices =
-            std::max<long>(1, std::min<long>((2L * N->sms + TAPS - 1) / TAPS, (npix + WT_KP - 1) / WT_KP));
+        const long resident = (long)N->sms * tc_blocks_per_sm(N, bytes, WT_THREADS, pad16(L.cin) + 16);
+        const long slices = std::max<long>(1, std::min<long>((resident + TAPS - 1) / TAPS, (npix + WT_KP - 1) / WT_KP));
         k_wgrad_tc<<<dim3(TAPS, (unsigned)slices), WT_THREADS, bytes, N->stream>>>(a);
         return;
     }
