@@ -612,12 +612,12 @@ def train_3d_network():
     t_record = time.perf_counter() - t0
     progress(f"3D network: {net.pairs()} pairs recorded in {t_record:.1f} s; training")
     t1 = time.perf_counter()
-    loss_first, loss_last, ms_step = net.train(steps=1000, batch=4, crop=32, lr=1e-4, seed=512)
+    loss_first, loss_last, ms_step = net.train(steps=2000, batch=2, crop=64, lr=1e-3, seed=512)
     progress(f"3D network: loss {loss_first:.3f} -> {loss_last:.3f}, {ms_step:.2f} ms/step")
     return {"net": net, "pairs": net.pairs(),
             "layouts": "4 seeded 128^3 24-state layouts x 6 timesteps, dt 0.064 (the 512^3 deck's K)",
-            "record_s": t_record, "train_s": time.perf_counter() - t1, "train_ms_per_step": ms_step, "steps": 1000,
-            "batch": "4 crops of 32^3", "loss_first": loss_first, "loss_last": loss_last,
+            "record_s": t_record, "train_s": time.perf_counter() - t1, "train_ms_per_step": ms_step, "steps": 2000,
+            "batch": "2 crops of 64^3", "lr": 1e-3, "loss_first": loss_first, "loss_last": loss_last,
             "network": "3D U-Net, 3 levels, 24/48/96 channels, 3x3x3 convolutions, bfloat16 weights"}
 
 
@@ -636,32 +636,37 @@ def learned_2d_at_scale(args):
     U-Net (32/64/64/64 channels, about half a million parameters) is trained by the
     library's kernels on 4032 pairs the solver generates from 64 seeded 1024^2 layouts (63
     timesteps each); then the 4096^2 deck runs with PPCG for --steps timesteps in the
-    FP32-refined form (FP32 PPCG corrections; FP64 PPCG stalls above 1e-10 on this deck), with
-    and without the learned warm start, through the driver (deck in, field summary out)."""
+    FP32-refined form (FP32 Chebyshev corrections; FP64 PPCG stalls above 1e-10 on this deck),
+    with and without the learned warm start, through the driver (deck in, field summary out)."""
     t0 = time.perf_counter()
     net = tea.WarmStart(4, 32, seed=SEED, max_channels=64)
     for k in range(64):
         spec = tea.DeckSpec(dim=2, cells=1024, states=STATES, seed=SEED + 100 + k, solver="cg", end_step=63,
-                            dt=train_dt(0.004, 1024, CELLS), eps=1e-15, eps_rel=EPS_REL, max_iters=20000,
+                            dt=train_dt(0.004, 1024, CELLS), eps=1e-15, eps_rel=1e-8, max_iters=20000,
                             summary_frequency=0,
                             check_result=False)
         tea.run_deck(tea.seeded_deck(spec), 2, fused=True, ws_net=net.id, ws_mode=tea.WS_RECORD)
+        progress(f"2D network at scale: layout {k + 1}/64 recorded ({net.pairs()} pairs)")
     t_record = time.perf_counter() - t0
     t1 = time.perf_counter()
-    loss_first, loss_last, ms_step = net.train(steps=4000, batch=8, crop=128, lr=1e-4, seed=SEED)
+    loss_first, loss_last, ms_step = net.train(steps=4000, batch=8, crop=128, lr=3e-4, seed=SEED)
     t_train = time.perf_counter() - t1
+    progress(f"2D network at scale: loss {loss_first:.3f} -> {loss_last:.3f} in {t_train:.0f} s")
     spec = tea.DeckSpec(dim=2, cells=CELLS, states=STATES, seed=SEED, solver="ppcg", end_step=args.steps, dt=0.004,
                         eps=1e-15, eps_rel=EPS_REL, max_iters=20000, presteps=30, inner_steps=10,
                         check_result=False, summary_frequency=0)
-    deck = tea.seeded_deck(spec)
+    deck = tea.seeded_deck(spec).replace("*endtea", "tl_inner_solver chebyshev\n*endtea")
     out = {"workload": "2d_4096x4096_16states_ppcg_rel1e-10_learned", "timesteps": args.steps,
+           "form": "FP32-refined, FP32 Chebyshev corrections (tl_inner_solver chebyshev)",
            "network": {"levels": 4, "channels": [32, 64, 64, 64], "params": net.param_count(),
                        "pairs": net.pairs(),
-                       "layouts": "64 seeded 1024^2 layouts x 63 timesteps (CG, FP64), dt 0.064 (the 4096^2 deck's K)",
+                       "layouts": "64 seeded 1024^2 layouts x 63 timesteps (CG, FP64, targets to rel. residual 1e-8), "
+                                  "dt 0.064 (the 4096^2 deck's K)",
                        "record_s": t_record, "train_s": t_train, "train_ms_per_step": ms_step, "train_steps": 4000,
                        "batch": "8 crops of 128^2", "loss_first": loss_first, "loss_last": loss_last}}
     runs = {}
     for name, ws_net in (("fp32_refined", 0), ("fp32_refined_learned", net.id)):
+        progress(f"2D network at scale: {name}, {args.steps} timesteps")
         summary, recs = tea.run_deck(deck, 2, fused=True, precision=tea.PRECISION_FP32_REFINED,
                                      summary_every_step=True, ws_net=ws_net, ws_mode=tea.WS_ATTACH if ws_net else 0)
         runs[name] = (summary, recs)

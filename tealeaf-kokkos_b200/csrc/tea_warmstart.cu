@@ -460,6 +460,14 @@ void conv(Net* N, View x, View y, const bf16* w, const float* bias, int relu, Vi
         return;
     }
     const long tiles = (npix + TC_M - 1) / TC_M;
+    if (W % TC_M == 0 && conv_rows_smem_bytes(cin, cout) <= 227 * 1024) {
+        // Rows of whole 128-pixel tiles: one staged row segment serves the three x-taps.
+        const int rbytes = (int)conv_rows_smem_bytes(cin, cout);
+        cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, rbytes);
+        const long grid = std::min<long>(tiles, (long)N->sms * tc_blocks_per_sm(N, rbytes, TC_THREADS, pad16(cout)));
+        k_conv_rows<<<(int)grid, TC_THREADS, rbytes, N->stream>>>(a);
+        return;
+    }
     const int bytes = (int)conv_tc_smem_bytes(cin, cout);
     cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     const long grid = std::min<long>(tiles, (long)N->sms * tc_blocks_per_sm(N, bytes, TC_THREADS, pad16(cout)));

@@ -215,6 +215,56 @@ __host__ __device__ constexpr size_t conv_tc_smem_bytes(int cin, int cout)
 
 __host__ __device__ constexpr int tmem_cols(int cout) { return cout <= 32 ? 32 : (cout <= 64 ? 64 : (cout <= 128 ? 128 : 256)); }
 
+// Epilogue of a 128-pixel tile: warp w reads TMEM lanes 32w..32w+31 (pixels p0 + 32w + lane),
+// 16 columns at a time, adds the bias, applies ReLU and/or the mask and stores bfloat16.
+__device__ __forceinline__ void conv_epilogue(const ConvArgs& a, uint32_t tmem, long p0, long npix, int np, int warp,
+                                              int lane)
+{
+    const long p = p0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < np; c0 += 16) {
+        uint32_t r[16];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (p < npix) {
+            const int nc = min(16, a.cout - c0);  // real output channels in this group
+            __align__(16) bf16 out[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                float v = __uint_as_float(r[j]);
+                if (j < nc) {
+                    if (a.bias) v += a.bias[c0 + j];
+                    if (a.relu) v = fmaxf(v, 0.0f);
+                    if (a.mask && !(__bfloat162float(a.mask[p * a.mcs + a.mco + c0 + j]) > 0.0f)) v = 0.0f;
+                }
+                out[j] = __float2bfloat16(v);
+            }
+            bf16* dst = a.y + p * a.ycs + a.yco + c0;
+            if (nc == 16 && (((uintptr_t)dst) & 15u) == 0) {
+                reinterpret_cast<uint4*>(dst)[0] = reinterpret_cast<const uint4*>(out)[0];
+                reinterpret_cast<uint4*>(dst)[1] = reinterpret_cast<const uint4*>(out)[1];
+            } else {
+                for (int j = 0; j < nc; ++j) dst[j] = out[j];
+            }
+        }
+    }
+}
+
+// After a block gave up (a bounded wait ran out): wait, bounded, for the MMAs still in
+// flight on each stage (the last fill committed there) before their memory is released.
+__device__ __forceinline__ void drain_stages(uint64_t* bar, long fill)
+{
+    for (int s = 0; s < 2; ++s) {
+        const long f = ((fill - 1) & 1) == s ? fill - 1 : fill - 2;
+        if (f >= 0) mbar_wait(&bar[s], (unsigned)((f >> 1) & 1));
+    }
+}
+
 __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
 {
     extern __shared__ __align__(1024) unsigned char s_raw[];
@@ -321,41 +371,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
             break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // Epilogue: warp w reads TMEM lanes 32w..32w+31 (pixels), 16 columns at a time.
-        const long p = p0 + warp * 32 + lane;
-        for (int c0 = 0; c0 < np; c0 += 16) {
-            uint32_t r[16];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (p < npix) {
-                const int nc = min(16, cout - c0);  // real output channels in this group
-                __align__(16) bf16 out[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    float v = __uint_as_float(r[j]);
-                    if (j < nc) {
-                        if (a.bias) v += a.bias[c0 + j];
-                        if (a.relu) v = fmaxf(v, 0.0f);
-                        if (a.mask && !(__bfloat162float(a.mask[p * a.mcs + a.mco + c0 + j]) > 0.0f)) v = 0.0f;
-                    }
-                    out[j] = __float2bfloat16(v);
-                }
-                bf16* dst = a.y + p * a.ycs + a.yco + c0;
-                if (nc == 16 && (((uintptr_t)dst) & 15u) == 0) {
-                    reinterpret_cast<uint4*>(dst)[0] = reinterpret_cast<const uint4*>(out)[0];
-                    reinterpret_cast<uint4*>(dst)[1] = reinterpret_cast<const uint4*>(out)[1];
-                } else {
-                    for (int j = 0; j < nc; ++j) dst[j] = out[j];
-                }
-            }
-        }
+        conv_epilogue(a, tmem, p0, npix, np, warp, lane);
         // The next tile's MMAs overwrite the accumulator: every lane's reads come first.
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
@@ -366,14 +382,157 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv_tc(ConvArgs a)
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (*s_abort) {
-        // Let MMAs still in flight finish (bounded) before the memory they use is released:
-        // the last fill committed on each stage.
-        for (int s = 0; s < 2; ++s) {
-            const long f = ((fill - 1) & 1) == s ? fill - 1 : fill - 2;
-            if (f >= 0) mbar_wait(&bar[s], (unsigned)((f >> 1) & 1));
-        }
+    if (*s_abort) drain_stages(bar, fill);
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
     }
+}
+
+// ----------------------------------------------------------------------------- row-segment conv
+
+// k_conv_rows: the tensor-core convolution for images whose width is a multiple of 128.  A
+// tile is 128 consecutive pixels of one image row (x0 .. x0+127).  For each of the 3 (2D) or
+// 9 (3D) rows (dz, dy) its taps read, the row segment x0-1 .. x0+128 (130 pixels, zeros
+// outside the image) is staged once, chunk-major: the 16-byte chunk c (8 channels) of
+// pixel v at byte c * 130 * 16 + v * 16.  In the K-major, non-swizzled canonical layout that
+// is a matrix with 8-row groups 128 bytes apart (SBO) and K chunks 2080 bytes apart (LBO),
+// so the taps dx = -1, 0, 1 of that row are the same segment read from 0, 16 or 32 bytes in:
+// one staged segment serves three taps, where k_conv_tc gathers one 128-pixel slice per
+// tap.  The three taps' weights are staged beside it (the canonical layout of k_conv_tc).
+// Two stages, one thread issues the MMAs, bounded waits and the epilogue as in k_conv_tc.
+constexpr int ROW_SEG = TC_M + 2;
+constexpr int ROW_GROUPS = WS_3D ? 9 : 3;
+
+// Operand blocks start on 1024-byte boundaries.
+__host__ __device__ constexpr size_t pad1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
+__host__ __device__ constexpr size_t rows_a_bytes(int cin) { return pad1k((size_t)ROW_SEG * pad16(cin) * 2); }
+__host__ __device__ constexpr size_t rows_b_tap(int cin, int cout) { return pad1k((size_t)pad16(cout) * pad16(cin) * 2); }
+
+__host__ __device__ constexpr size_t conv_rows_smem_bytes(int cin, int cout)
+{
+    return 2 * (rows_a_bytes(cin) + 3 * rows_b_tap(cin, cout)) + 1024 + 64;
+}
+
+__global__ void __launch_bounds__(TC_THREADS) k_conv_rows(ConvArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char s_raw[];
+    unsigned char* base = s_raw + ((1024 - (smem_u32(s_raw) & 1023u)) & 1023u);
+    const int cin = a.cin, cout = a.cout;
+    const int kp = pad16(cin), np = pad16(cout);
+    const size_t a_bytes = rows_a_bytes(cin), b_tap = rows_b_tap(cin, cout), b_bytes = 3 * b_tap;
+    bf16* sA[2] = {reinterpret_cast<bf16*>(base), reinterpret_cast<bf16*>(base + a_bytes + b_bytes)};
+    bf16* sB[2] = {reinterpret_cast<bf16*>(base + a_bytes), reinterpret_cast<bf16*>(base + 2 * a_bytes + b_bytes)};
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * (a_bytes + b_bytes));
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+    int* s_abort = reinterpret_cast<int*>(tmem_slot + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ncols = tmem_cols(np);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        *s_abort = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    const uint32_t idesc = umma_idesc_bf16(TC_M, np);
+    const uint32_t lbo_a = ROW_SEG * 16;     // bytes between the segment's K chunks
+    const uint32_t sbo_b = (uint32_t)kp * 16;  // bytes between 8-row groups of the weights
+    const int kchunks = kp / 8;
+    const long npix = (long)a.n * a.D * a.H * a.W;
+    const long ntiles = npix / TC_M;  // W is a multiple of 128: tiles never straddle rows
+    long fill = 0;
+    bool ok = true;
+
+    for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const long p0 = tile * TC_M;
+        const Pix q = pix_of(p0, a.D, a.H, a.W);  // q.x = x0, a multiple of 128
+        for (int rg = 0; rg < ROW_GROUPS && ok; ++rg, ++fill) {
+            const int st = (int)(fill & 1);
+            if (fill >= 2) {
+                const bool done = mbar_wait(&bar[st], (unsigned)(((fill - 2) >> 1) & 1));
+                if (!__syncthreads_and(done)) {
+                    ok = false;
+                    break;
+                }
+            }
+            const int dz = WS_3D ? rg / 3 - 1 : 0, dy = rg % 3 - 1;
+            const int sy = q.y + dy, sz = q.z + dz;
+            const bool row_ok = sy >= 0 && sy < a.H && sz >= 0 && sz < a.D;
+            const long row = ((q.img * a.D + sz) * (long)a.H + sy) * a.W;  // first pixel of the source row
+            // A: the segment, ROW_SEG pixels x kchunks chunks, chunk-major.
+            for (int idx = tid; idx < ROW_SEG * kchunks; idx += TC_THREADS) {
+                const int v = idx / kchunks, c = idx - v * kchunks;
+                const int sx = q.x - 1 + v;
+                const bool valid = row_ok && sx >= 0 && sx < a.W && c * 8 < cin;
+                const bf16* src = valid ? a.x + (row + sx) * a.xcs + a.xco + c * 8 : a.x;
+                cp_async_16z(sA[st] + (size_t)c * ROW_SEG * 8 + (size_t)v * 8, src, valid);
+            }
+            // B: the weights of taps (dz, dy, dx = -1, 0, 1): tap index rg * 3 + (dx + 1).
+            const int per_tap = np * kchunks;
+            for (int idx = tid; idx < 3 * per_tap; idx += TC_THREADS) {
+                const int tx = idx / per_tap, rem = idx - tx * per_tap;
+                const int r = rem / kchunks, c = rem - r * kchunks;
+                const bool valid = r < cout && c * 8 < cin;
+                const bf16* src = valid ? a.w + ((size_t)r * TAPS + rg * 3 + tx) * cin + c * 8 : a.w;
+                bf16* dst = sB[st] + (size_t)tx * (b_tap / 2) + (size_t)(r >> 3) * (sbo_b / 2) + (size_t)c * 64 +
+                            (r & 7) * 8;
+                cp_async_16z(dst, src, valid);
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a_addr = smem_u32(sA[st]), b_addr = smem_u32(sB[st]);
+                for (int tx = 0; tx < 3; ++tx) {
+                    for (int s = 0; s < kp / 16; ++s) {
+                        // Output row m reads segment pixel m + tx (tap dx = tx - 1).
+                        const uint64_t da = umma_desc(a_addr + (uint32_t)tx * 16 + (uint32_t)s * 2 * lbo_a, lbo_a, 128);
+                        const uint64_t db = umma_desc(b_addr + (uint32_t)(tx * b_tap) + (uint32_t)s * 256, 128, sbo_b);
+                        const uint32_t acc = (rg > 0 || tx > 0 || s > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                            "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                            : "memory");
+                    }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&bar[st]))
+                             : "memory");
+            }
+        }
+        if (!ok) break;
+        const long last = fill - 1;
+        const bool done = mbar_wait(&bar[last & 1], (unsigned)((last >> 1) & 1));
+        if (!__syncthreads_and(done)) {
+            ok = false;
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        conv_epilogue(a, tmem, p0, npix, np, warp, lane);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    if (!ok) {
+        *s_abort = 1;
+        if (a.err) atomicExch(a.err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (*s_abort) drain_stages(bar, fill);
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
@@ -556,12 +715,7 @@ __global__ void __launch_bounds__(WT_THREADS) k_wgrad_tc(WgradArgs a)
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (*s_abort) {
-        for (int s = 0; s < 2; ++s) {
-            const long f = ((fill - 1) & 1) == s ? fill - 1 : fill - 2;
-            if (f >= 0) mbar_wait(&bar[s], (unsigned)((f >> 1) & 1));
-        }
-    }
+    if (*s_abort) drain_stages(bar, fill);
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");

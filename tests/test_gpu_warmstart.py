@@ -294,6 +294,36 @@ def test_3d_tensor_cores_equal_cuda_cores():
         net.close()
 
 
+@pytest.mark.parametrize("dim", [2, 3])
+def test_row_segment_convolution_matches_oracle_and_cuda_cores(dim):
+    """Images 128 pixels wide take the row-segment kernel (k_conv_rows: one staged row
+    segment serves the three x-taps) at full resolution and k_conv_tc below: forward and
+    every gradient against the CUDA-core kernels, and the forward against the oracle."""
+    levels, base = 2, 24
+    rng = np.random.default_rng(77 + dim)
+    p = wo.init_params(levels, base, seed=dim, dim=dim)
+    shape = (2, 4, 4, 128) if dim == 3 else (2, 8, 128)
+    x = rng.normal(size=shape + (wo.in_channels(dim),)) * 0.5
+    t = rng.normal(size=shape) * 0.1
+    net = tea.WarmStart(levels, base, seed=0, dim=dim)
+    try:
+        net.set_params(_flat(p, levels, base, dim=dim))
+        net.set_reference_conv(True)
+        y_ref, _, g_ref = net.eval(x, t)
+        net.set_reference_conv(False)
+        y_tc, _, g_tc = net.eval(x, t)
+        assert _rel_l2(y_tc, y_ref) <= 1e-2, _rel_l2(y_tc, y_ref)
+        gr, gt = _split(g_ref, levels, base, dim=dim), _split(g_tc, levels, base, dim=dim)
+        for k in gr:
+            if k == "head.b":
+                continue
+            assert _cos(gt[k], gr[k]) >= 0.999 and _rel_l2(gt[k], gr[k]) <= 3e-2, (k, _cos(gt[k], gr[k]))
+        y_o = np.stack([wo.forward(p, x[i], levels, base)[0] for i in range(x.shape[0])])
+        assert _rel_l2(y_tc, y_o) <= FWD_TOL, _rel_l2(y_tc, y_o)
+    finally:
+        net.close()
+
+
 def _deck3d(seed, steps=4, cells=32, solver="cg"):
     spec = tea.DeckSpec(dim=3, cells=cells, states=8, seed=seed, solver=solver, end_step=steps, dt=0.004, eps=1e-15,
                         eps_rel=1e-10, max_iters=20000, presteps=30, inner_steps=10, summary_frequency=1,
