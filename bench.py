@@ -770,7 +770,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-per-call", action="store_true", help="skip timing the per-call ext_* path")
     ap.add_argument("--no-3d", action="store_true",
-                    help="skip the 3D 512^3 PPCG line (plain FP64 against FP32-refined, 1 + 5 timesteps each)")
+                    help="skip the 3D lines (512^3 PPCG and 256^3 CG/PPCG, plain FP64 against FP32-refined)")
     ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS),
                     help="only launch one fused kernel --reps times on the 4096^2 workload, or after one "
                          "timestep of --workload (for ncu captures)")
@@ -810,6 +810,9 @@ def main():
     c5 = None if args.no_3d else run_3d("3d512_ppcg", 1, 5, {"fp32_refined": 2}, ws=ws3)
     if ws3:
         ws3["net"].close()
+    # The 3D 256^3 configuration: CG and PPCG, plain FP64 against FP32-refined, each with its
+    # per-step exact error and field-summary difference (one warm-up and three timed timesteps).
+    c3 = None if args.no_3d else {w: run_3d(w, 1, 3) for w in ("3d256_cg", "3d256_ppcg")}
     if rank != 0:
         dist_done(world)
         return
@@ -898,6 +901,8 @@ def main():
             "clocks": learned["clocks"]}
     if c5:
         line["c5_3d512_ppcg"] = c5
+    if c3:
+        line["c3_3d256"] = c3
     if per_call:
         # The same deck through the per-call ext_* entry points (what an unchanged Fortran
         # driver calls), timestep 2; the fused arm's timesteps are later ones.

@@ -384,6 +384,9 @@ Fused* ensure_fused(Chunk* c, int max_iters)
             TEA_CK(cudaMalloc(&F->alt[k], c->field_elems * sizeof(double)));
             if (F->alt[k]) TEA_CK(cudaMemset(F->alt[k], 0, c->field_elems * sizeof(double)));
         }
+        // The clears ran on the legacy stream, which does not order with the chunk's
+        // non-blocking stream: finish them before any kernel there can touch the arrays.
+        TEA_CK(cudaDeviceSynchronize());
         const Geom& g = c->g;
         FusedArgs& a = F->base;
         a.g = g;
@@ -522,6 +525,7 @@ Fused* ensure_fused(Chunk* c, int max_iters)
         TEA_CK(cudaMalloc(&F->d_ch_betas, sizeof(double) * F->cap));
         TEA_CK(cudaMemset(F->d_ch_alphas, 0, sizeof(double) * F->cap));
         TEA_CK(cudaMemset(F->d_ch_betas, 0, sizeof(double) * F->cap));
+        TEA_CK(cudaDeviceSynchronize());  // legacy-stream clears before the chunk's stream uses them
         F->base.cg_alphas = F->d_cg_alphas;
         F->base.cg_betas = F->d_cg_betas;
         F->base.ch_alphas = F->d_ch_alphas;
@@ -542,6 +546,7 @@ bool ensure_fp32(Chunk* c, Fused* F)
         if (!F->alloc32[k]) return false;
         TEA_CK(cudaMemset(F->alloc32[k], 0, bytes));
     }
+    TEA_CK(cudaDeviceSynchronize());  // legacy-stream clears before the chunk's stream uses them
     free_loops(F);  // graphs captured before hold null FP32 pointers
     FusedArgs& a = F->base;
     a.kx32 = F->alloc32[0] + kLeadPad;

@@ -328,6 +328,9 @@ int dalloc(T** p, size_t count)
 {
     WS_CK(cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(count, 1)));
     WS_CK(cudaMemset(*p, 0, sizeof(T) * std::max<size_t>(count, 1)));
+    // The clear runs on the legacy stream, which does not order with the library's
+    // non-blocking streams: finish it before they use the memory.
+    WS_CK(cudaDeviceSynchronize());
     return TEA_OK;
 }
 
