@@ -237,7 +237,8 @@ int tea_ws_attach_(const int* chunk, const int* net);
 int tea_ws_predict_(const int* net, const int* chunk, double* du, double* ms);
 /* Test hooks: parameters in the order of the CPU oracle (per layer w[co][taps][cin], 9
  * taps in 2D and 27 in 3D, then b; head w, head b), the choice of convolution (0 tensor
- * cores, 1 CUDA cores), and forward/backward on host images [n][D][H][W][F] (F = 4 input
+ * cores, fed by TMA where the image width is a multiple of 128; 1 CUDA cores; 2 tensor cores
+ * without TMA), and forward/backward on host images [n][D][H][W][F] (F = 4 input
  * features in 2D, where D must be 1, and 5 in 3D; target null: forward only; kxy null:
  * mean squared error, else the residual loss with face coefficients [n][D][H][W][K],
  * K = 2 in 2D and 3 in 3D).  tea_ws_eval_host_ is tea_ws_eval_volume_ with D = 1. */

@@ -385,6 +385,11 @@ class WarmStart:
     def set_reference_conv(self, on: bool) -> None:
         self._check(self.lib.tea_ws_set_conv_(_i(self.id), _i(1 if on else 0)), "set_conv")
 
+    def set_conv_mode(self, mode: int) -> None:
+        """0: tensor cores (TMA-fed where the width is a multiple of 128), 1: CUDA cores,
+        2: tensor cores without TMA."""
+        self._check(self.lib.tea_ws_set_conv_(_i(self.id), _i(mode)), "set_conv")
+
     def eval(self, x, target=None, kxy=None):
         """x [n][H][W][4] (2D) or [n][D][H][W][5] (3D) float32 -> (y [n][(D)][H][W], loss,
         flat gradients or None); with kxy ([n][(D)][H][W][dim] face coefficients) the loss is

@@ -27,7 +27,10 @@
 #include "../../include/tea_b200.h"
 #include "tea_chunk.cuh"
 #include "tea_common.cuh"
+#include "tea_ws_conv_tma.cuh"
 #include "tea_ws_kernels.cuh"
+
+#include <cudaTypedefs.h>
 
 #define TEA_EXPORT extern "C" __attribute__((visibility("default")))
 
@@ -248,6 +251,7 @@ struct Conv {
     float *w = nullptr, *b = nullptr, *gw = nullptr, *gb = nullptr, *mw = nullptr, *vw = nullptr, *mb = nullptr,
           *vb = nullptr;
     bf16 *w16 = nullptr, *wt16 = nullptr;
+    bf16 *wpk16 = nullptr, *wtpk16 = nullptr;  // w16, wt16 in the MMA's shared-memory layout (k_pack_weights)
 };
 
 struct Pair {
@@ -264,6 +268,7 @@ struct Net {
     float *hw = nullptr, *hb = nullptr, *ghw = nullptr, *ghb = nullptr, *mh = nullptr, *vh = nullptr;  // head: C0 + 1
     long step = 0;
     int use_ref = 0;  // 1: CUDA-core convolutions
+    int no_tma = 0;   // 1: the tensor-core convolutions without the TMA kernel
     cudaStream_t stream = nullptr;
     int* d_err = nullptr;
     float* d_sums = nullptr;
@@ -420,7 +425,7 @@ int ensure_workspace(Net* N, int n, int D, int H, int W, bool train)
 // per-block reservation), threads and tensor memory (512 columns per SM).  The occupancy API
 // reports one block per SM for kernels that allocate tensor memory, whatever their size, so
 // the count is formed here from the SM's resources.
-int tc_blocks_per_sm(Net* N, int smem_bytes, int threads, int n_cols)
+int tc_blocks_per_sm(Net* N, int smem_bytes, int threads, int n_cols, int tmem_bufs = 1)
 {
     if (N->smem_per_sm == 0) {
         cudaDeviceGetAttribute(&N->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, N->device);
@@ -429,13 +434,44 @@ int tc_blocks_per_sm(Net* N, int smem_bytes, int threads, int n_cols)
     }
     const int by_smem = N->smem_per_sm / std::max(1, smem_bytes + N->smem_reserved);
     const int by_threads = N->threads_per_sm / threads;
-    const int by_tmem = 512 / tmem_cols(n_cols);
+    const int by_tmem = 512 / (tmem_bufs * tmem_cols(n_cols));
     return std::max(1, std::min(std::min(by_smem, by_threads), std::min(by_tmem, 32)));
 }
 
-// y = conv(x) (3x3, or 3x3x3 in 3D) over n images of [D x] H x W.
-void conv(Net* N, View x, View y, const bf16* w, const float* bias, int relu, View mask, int n, int D, int H, int W,
-          int cin, int cout)
+// cuTensorMapEncodeTiled from the driver (looked up once; null when unavailable).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// The tensor map of an input view for k_conv_tma: dims (channels of the view, W, H, D, n),
+// boxes of 8 channels x 130 pixels x 1 x 1 x 1, zeros outside.  False when it cannot be made.
+bool input_tensor_map(View x, int cin, int n, int D, int H, int W, CUtensorMap* map)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || (x.cs % 8) || (x.co % 8) || (cin % 8)) return false;
+    const cuuint64_t dims[5] = {(cuuint64_t)cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D, (cuuint64_t)n};
+    const cuuint64_t px = (cuuint64_t)x.cs * sizeof(bf16);
+    const cuuint64_t strides[4] = {px, px * W, px * W * H, px * W * H * D};
+    const cuuint32_t box[5] = {8, 130, 1, 1, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)(x.p + x.co), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// y = conv(x) (3x3, or 3x3x3 in 3D) over n images of [D x] H x W; wpk is w packed by
+// k_pack_weights (used by the TMA kernel).
+void conv(Net* N, View x, View y, const bf16* w, const bf16* wpk, const float* bias, int relu, View mask, int n, int D,
+          int H, int W, int cin, int cout)
 {
     ConvArgs a;
     a.x = x.p;
@@ -463,6 +499,21 @@ void conv(Net* N, View x, View y, const bf16* w, const float* bias, int relu, Vi
         return;
     }
     const long tiles = (npix + TC_M - 1) / TC_M;
+    if (W % TC_M == 0 && wpk && !N->no_tma && conv_tma_smem_bytes(cin, cout, 2) <= 227 * 1024) {
+        // Whole 128-pixel row tiles, every operand moved by TMA.
+        CUtensorMap map;
+        if (input_tensor_map(x, cin, n, D, H, W, &map)) {
+            // As many stages (2..4) as leave room for two blocks per SM.
+            const size_t stage = tma_stage_bytes(cin, cout);
+            const int stages = (int)std::max<size_t>(2, std::min<size_t>(TMA_MAX_STAGES, (113 * 1024 - 1216) / stage));
+            const int tbytes = (int)conv_tma_smem_bytes(cin, cout, stages);
+            cudaFuncSetAttribute(k_conv_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, tbytes);
+            const long grid =
+                std::min<long>(tiles, (long)N->sms * tc_blocks_per_sm(N, tbytes, TMA_THREADS, pad16(cout), 2));
+            k_conv_tma<<<(int)grid, TMA_THREADS, tbytes, N->stream>>>(a, wpk, stages, map);
+            return;
+        }
+    }
     if (W % TC_M == 0 && conv_rows_smem_bytes(cin, cout) <= 227 * 1024) {
         // Rows of whole 128-pixel tiles: one staged row segment serves the three x-taps.
         const int rbytes = (int)conv_rows_smem_bytes(cin, cout);
@@ -538,9 +589,9 @@ void forward(Net* N)
         const int D = depth_at(N, l), H = N->wH >> l, W = N->wW >> l, C = N->ch[l];
         Conv& a = enc(N, l, 0);
         Conv& b = enc(N, l, 1);
-        conv(N, h, view(N->A[l], C, 0, C), a.w16, a.b, 1, kNoView, n, D, H, W, a.cin, C);
+        conv(N, h, view(N->A[l], C, 0, C), a.w16, a.wpk16, a.b, 1, kNoView, n, D, H, W, a.cin, C);
         const View out = l < L - 1 ? view(N->cat[l], N->ch[l + 1] + C, N->ch[l + 1], C) : view(N->bottom, C, 0, C);
-        conv(N, view(N->A[l], C, 0, C), out, b.w16, b.b, 1, kNoView, n, D, H, W, C, C);
+        conv(N, view(N->A[l], C, 0, C), out, b.w16, b.wpk16, b.b, 1, kNoView, n, D, H, W, C, C);
         if (l < L - 1) {
             k_avgpool<<<grid_for((long)n * D * H * W / POOL), 256, 0, N->stream>>>(out, N->P[l], n, D, H, W);
             h = view(N->P[l], C, 0, C);
@@ -553,9 +604,9 @@ void forward(Net* N)
                                                                               D, H, W);
         Conv& a = dec(N, l, 0);
         Conv& b = dec(N, l, 1);
-        conv(N, view(N->cat[l], Cu + C, 0, Cu + C), view(N->DA[l], C, 0, C), a.w16, a.b, 1, kNoView, n, D, H, W,
+        conv(N, view(N->cat[l], Cu + C, 0, Cu + C), view(N->DA[l], C, 0, C), a.w16, a.wpk16, a.b, 1, kNoView, n, D, H, W,
              Cu + C, C);
-        conv(N, view(N->DA[l], C, 0, C), view(N->DB[l], C, 0, C), b.w16, b.b, 1, kNoView, n, D, H, W, C, C);
+        conv(N, view(N->DA[l], C, 0, C), view(N->DB[l], C, 0, C), b.w16, b.wpk16, b.b, 1, kNoView, n, D, H, W, C, C);
     }
 }
 
@@ -635,10 +686,10 @@ void backward(Net* N)
         Conv& a = dec(N, l, 0);
         Conv& b = dec(N, l, 1);
         wgrad(N, view(N->DA[l], C, 0, C), view(gcur, C, 0, C), b, n, D, H, W);
-        conv(N, view(gcur, C, 0, C), view(gnext, C, 0, C), b.wt16, nullptr, 0, view(N->DA[l], C, 0, C), n, D, H, W,
+        conv(N, view(gcur, C, 0, C), view(gnext, C, 0, C), b.wt16, b.wtpk16, nullptr, 0, view(N->DA[l], C, 0, C), n, D, H, W,
              C, C);
         wgrad(N, view(N->cat[l], Cu + C, 0, Cu + C), view(gnext, C, 0, C), a, n, D, H, W);
-        conv(N, view(gnext, C, 0, C), view(N->gcat[l], Cu + C, 0, Cu + C), a.wt16, nullptr, 0,
+        conv(N, view(gnext, C, 0, C), view(N->gcat[l], Cu + C, 0, Cu + C), a.wt16, a.wtpk16, nullptr, 0,
              view(N->cat[l], Cu + C, 0, Cu + C), n, D, H, W, C, Cu + C);
         k_upsample_bw<<<grid_for((long)n * D * H * W / POOL), 256, 0, N->stream>>>(
             view(N->gcat[l], Cu + C, 0, Cu), gcur, n, D, H, W);
@@ -656,22 +707,27 @@ void backward(Net* N)
             std::swap(gcur, gtmp);
         }
         wgrad(N, view(N->A[l], C, 0, C), view(gcur, C, 0, C), b, n, D, H, W);
-        conv(N, view(gcur, C, 0, C), view(gnext, C, 0, C), b.wt16, nullptr, 0, view(N->A[l], C, 0, C), n, D, H, W, C,
+        conv(N, view(gcur, C, 0, C), view(gnext, C, 0, C), b.wt16, b.wtpk16, nullptr, 0, view(N->A[l], C, 0, C), n, D, H, W, C,
              C);
         const View xin = l == 0 ? view(N->x0, IN_PAD, 0, IN_PAD) : view(N->P[l - 1], N->ch[l - 1], 0, N->ch[l - 1]);
         wgrad(N, xin, view(gnext, C, 0, C), a, n, D, H, W);
         if (l > 0) {
             const int Cp = N->ch[l - 1];
-            conv(N, view(gnext, C, 0, C), view(gcur, Cp, 0, Cp), a.wt16, nullptr, 0, kNoView, n, D, H, W, C, Cp);
+            conv(N, view(gnext, C, 0, C), view(gcur, Cp, 0, Cp), a.wt16, a.wtpk16, nullptr, 0, kNoView, n, D, H, W, C, Cp);
         }
     }
 }
 
 void refresh_bf16(Net* N)
 {
-    for (Conv& c : N->conv)
+    for (Conv& c : N->conv) {
         k_weights_bf16<<<grid_for((long)c.cout * TAPS * c.cin), 256, 0, N->stream>>>(c.w, c.w16, c.wt16, c.cout,
                                                                                       c.cin);
+        k_pack_weights<<<grid_for((long)TAPS * pad16(c.cout) * pad16(c.cin)), 256, 0, N->stream>>>(c.w16, c.wpk16,
+                                                                                                 c.cout, c.cin);
+        k_pack_weights<<<grid_for((long)TAPS * pad16(c.cout) * pad16(c.cin)), 256, 0, N->stream>>>(c.wt16, c.wtpk16,
+                                                                                                 c.cin, c.cout);
+    }
 }
 
 void adam_step(Net* N, float lr)
@@ -890,6 +946,8 @@ TEA_EXPORT int tea_ws_create_capped_(const int* levels, const int* base, const i
         for (float** p : {&c.b, &c.gb, &c.mb, &c.vb})
             if (dalloc(p, c.cout)) return TEA_ERR_CUDA;
         if (dalloc(&c.w16, nw) || dalloc(&c.wt16, nw)) return TEA_ERR_CUDA;
+        const long npk = (long)TAPS * pad16(c.cout) * pad16(c.cin);
+        if (dalloc(&c.wpk16, npk) || dalloc(&c.wtpk16, npk)) return TEA_ERR_CUDA;
         const int ci_real = k == 0 ? N_FEAT : c.cin;
         const float sd = sqrtf(2.f / ((float)TAPS * ci_real));
         std::vector<float> w(nw, 0.f), b(c.cout);
@@ -931,7 +989,7 @@ TEA_EXPORT int tea_ws_destroy_(const int* net)
     free_workspace(N);
     for (Conv& c : N->conv)
         for (void* p : {(void*)c.w, (void*)c.b, (void*)c.gw, (void*)c.gb, (void*)c.mw, (void*)c.vw, (void*)c.mb,
-                        (void*)c.vb, (void*)c.w16, (void*)c.wt16})
+                        (void*)c.vb, (void*)c.w16, (void*)c.wt16, (void*)c.wpk16, (void*)c.wtpk16})
             cudaFree(p);
     for (void* p : {(void*)N->hw, (void*)N->ghw, (void*)N->mh, (void*)N->vh, (void*)N->d_err, (void*)N->d_sums,
                     (void*)N->d_scale, (void*)N->d_partial, (void*)N->d_crops, (void*)N->d_img, (void*)N->r0buf,
@@ -951,7 +1009,8 @@ TEA_EXPORT int tea_ws_set_conv_(const int* net, const int* reference)
 {
     Net* N = get_net(net);
     if (!N) return TEA_ERR_BAD_ARGUMENT;
-    N->use_ref = *reference ? 1 : 0;
+    N->use_ref = *reference == 1 ? 1 : 0;
+    N->no_tma = *reference == 2 ? 1 : 0;
     return TEA_OK;
 }
 

@@ -294,10 +294,12 @@ def test_3d_tensor_cores_equal_cuda_cores():
         net.close()
 
 
+@pytest.mark.parametrize("mode", [0, 2], ids=["tma", "cp_async"])
 @pytest.mark.parametrize("dim", [2, 3])
-def test_row_segment_convolution_matches_oracle_and_cuda_cores(dim):
-    """Images 128 pixels wide take the row-segment kernel (k_conv_rows: one staged row
-    segment serves the three x-taps) at full resolution and k_conv_tc below: forward and
+def test_row_segment_convolution_matches_oracle_and_cuda_cores(dim, mode):
+    """Images 128 pixels wide take the row-segment kernels at full resolution (one staged row
+    segment serves the three x-taps), k_conv_tc below: k_conv_tma (mode 0: segments and
+    packed weights moved by TMA) and k_conv_rows (mode 2: per-thread copies).  Forward and
     every gradient against the CUDA-core kernels, and the forward against the oracle."""
     levels, base = 2, 24
     rng = np.random.default_rng(77 + dim)
@@ -308,9 +310,9 @@ def test_row_segment_convolution_matches_oracle_and_cuda_cores(dim):
     net = tea.WarmStart(levels, base, seed=0, dim=dim)
     try:
         net.set_params(_flat(p, levels, base, dim=dim))
-        net.set_reference_conv(True)
+        net.set_conv_mode(1)
         y_ref, _, g_ref = net.eval(x, t)
-        net.set_reference_conv(False)
+        net.set_conv_mode(mode)
         y_tc, _, g_tc = net.eval(x, t)
         assert _rel_l2(y_tc, y_ref) <= 1e-2, _rel_l2(y_tc, y_ref)
         gr, gt = _split(g_ref, levels, base, dim=dim), _split(g_tc, levels, base, dim=dim)
