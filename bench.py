@@ -511,6 +511,7 @@ def reference_arm(args, rank, world):
 # The other configurations' 3D workloads (seeded box/sphere layouts): timed through the
 # public driver (tea_run_deck: deck in, field summary out), plain FP64 and FP32-refined.
 WORKLOADS_3D = {
+    "3d128_ppcg": dict(cells=128, solver="ppcg", states=24, seed=512),
     "3d256_cg": dict(cells=256, solver="cg", states=12, seed=256),
     "3d256_ppcg": dict(cells=256, solver="ppcg", states=12, seed=256),
     "3d256_cheby": dict(cells=256, solver="chebyshev", states=12, seed=256),
@@ -715,10 +716,39 @@ WORDS_3D = {"ppcg_inner": 9, "cg_sweep_a": 9, "cheby_iterate": 8, "jacobi": 6, "
             "cg32_sweep_a": 4.5, "cg32_sweep_b": 1.5, "cheby32_pair": 4, "ppcg_pair": 9, "ppcg32_pair": 4.5}
 
 
+def ws_predict_3d(args):
+    """--workload NAME --kernel ws_predict: the 3D warm-start network's prediction (3 levels,
+    24/48/96 channels, seeded weights) on the configuration's chunk after one timestep solved
+    to a relative residual of 1e-3 (the prediction's cost does not depend on the state),
+    `reps` times; device milliseconds of each."""
+    w = WORKLOADS_3D[args.workload]
+    spec = tea.DeckSpec(dim=3, cells=w["cells"], states=w["states"], seed=w["seed"], solver=w["solver"], end_step=1,
+                        dt=0.004, eps=1e-15, eps_rel=1e-3, max_iters=20000, presteps=30, inner_steps=10,
+                        check_result=False, summary_frequency=0)
+    tea.run_deck(tea.seeded_deck(spec), 3, fused=True, keep_chunk=True)
+    lib = tea.cuda_library(3)
+    net = tea.WarmStart(3, 24, seed=512, dim=3)
+    ms = ctypes.c_double(0.0)
+    times = []
+    for _ in range(args.reps):
+        rc = lib.tea_ws_predict_(ctypes.byref(ctypes.c_int(net.id)), ctypes.byref(ctypes.c_int(1)), None,
+                                 ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"tea_ws_predict_: status {rc}")
+        times.append(ms.value)
+    print(json.dumps({"workload": args.workload, "kernel": "ws_predict", "cells": w["cells"] ** 3,
+                      "predict_ms": times}))
+    net.close()
+    lib.ext_finalise_()
+
+
 def kernel_only_3d(args):
     """--workload NAME --kernel K: one timestep of the 3D configuration through the driver
     (the FP32-refined form for the FP32 kernels, so that their arrays exist), then K launched
     1 + reps times back to back on the chunk's live fields."""
+    if args.kernel == "ws_predict":
+        ws_predict_3d(args)
+        return
     w = WORKLOADS_3D[args.workload]
     fp32 = args.kernel.startswith(("cg32", "cheby32", "ppcg32"))
     spec = tea.DeckSpec(dim=3, cells=w["cells"], states=w["states"], seed=w["seed"], solver=w["solver"], end_step=1,
@@ -771,7 +801,7 @@ def main():
     ap.add_argument("--no-per-call", action="store_true", help="skip timing the per-call ext_* path")
     ap.add_argument("--no-3d", action="store_true",
                     help="skip the 3D lines (512^3 PPCG and 256^3 CG/PPCG, plain FP64 against FP32-refined)")
-    ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS),
+    ap.add_argument("--kernel", choices=sorted(ALL_KERNEL_IDS) + ["ws_predict"],
                     help="only launch one fused kernel --reps times on the 4096^2 workload, or after one "
                          "timestep of --workload (for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
