@@ -134,7 +134,8 @@ typedef struct {
                                TEA_PRECISION_FP32_REFINED */
     int inner_max_iters;    /* FP32_REFINED: inner iterations per correction, 0 = no limit */
     double inner_tol;       /* FP32_REFINED: relative drop of the inner residual per
-                               correction, 0 = 1e-4 */
+                               correction, 0 = 1e-4; a correction also stops once its
+                               sum r^2 is below a tenth of the outer target */
     int inner_solver;       /* FP32_REFINED, corrections after the first (CG) one:
                                TEA_INNER_DECK (0) the deck's method -- Chebyshev for
                                Chebyshev decks, PPCG for PPCG decks (an even number

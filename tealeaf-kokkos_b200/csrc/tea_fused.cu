@@ -78,6 +78,10 @@ struct Fused {
 
 Fused* fused_of(Chunk* c) { return static_cast<Fused*>(c->fused); }
 
+// FP32-refined form: an inner solve may stop once its sum r^2 is below this fraction of the
+// outer target eps (the rounding of the FP32 correction is far below it at that point).
+constexpr double kInnerTargetMargin = 0.1;
+
 // After a warm start replaced u (and r = u0 - A u was recomputed): the CG start
 // p = z = Mi r (preconditioned) or p = r, and rro = sum r.p -- CGCalcRRO's last part.
 __global__ void __launch_bounds__(BLOCK) k_ws_restart(Geom g, Box inner, Fields f, int precond, RedScratch rs,
@@ -1000,7 +1004,10 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
             }
             const int remaining = P->max_iters - used;
             s.inner_max = P->inner_max_iters > 0 ? std::min(P->inner_max_iters, remaining) : remaining;
-            s.tol2 = tol * tol * s.rro;
+            // The inner solve reduces the correction's residual by tol, or stops sooner once
+            // the outer target is met with a margin (sum r^2 at a tenth of eps): the last
+            // correction needs only the reduction that is left.
+            s.tol2 = std::max(tol * tol * s.rro, kInnerTargetMargin * eps);
             s.n_inner = inner_mode == 1 ? 1 : 0;
             s.cont = 1;
             s.inner_diverged = 0;
