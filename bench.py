@@ -328,10 +328,14 @@ def gpu_arm(args, world, precision=0, kernels=True, ws_net=0):
         dominant, alg_bytes = None, None
     # Chebyshev passes: 7 words per pass of four or two iterations (3 passes per 10 iterations).
     step_words = (WORDS["cg_sweep_a"] + WORDS["cg_sweep_b"]) * mean_cg + WORDS["cheby_pair"] * mean_ch * 0.3
+    # The same timestep counted in canonical words per iteration (each iteration's arrays
+    # once, fusion and temporal blocking not credited): CG 12, Chebyshev 7 (2D).
+    canon_words = CANONICAL_WORDS[2]["cg"] * mean_cg + CANONICAL_WORDS[2]["cheby"] * mean_ch
     return {
         "sec_per_step": sec_per_step, "ms_total": ms_max, "clocks": clock_info, "iterations": iters,
         "cg_steps": cg, "cheby_steps": cheby, "kernel_ms": kernel_ms, "dominant": dominant,
         "alg_bytes": alg_bytes, "step_alg_gbs": step_words * 8 * cells / sec_per_step / 1e9,
+        "step_canonical_gbs": canon_words * 8 * cells / sec_per_step / 1e9, "canonical_words": canon_words,
         "cells_iters_per_s": cells * (sum(iters) / len(iters)) / sec_per_step,
         "warmup_iterations": [r["iterations"] for r in warm], "bad_status": [r["status"] for r in bad],
         "corrections": [r["corrections"] for r in results], "summary": summaries,
@@ -521,6 +525,26 @@ WORKLOADS_3D = {
 
 INNER_SOLVERS = {0: "cg", 1: "chebyshev", 2: "ppcg"}
 
+# Canonical FP64 words per interior cell of one iteration, each array counted once as the
+# reference's unfused kernels touch it: CG (w = A p with p.w; u, r update with r.r; p update)
+# 12 in 2D and 13 in 3D, a Chebyshev iteration 7 / 8, a PPCG inner step 8 / 9 (its outer
+# iteration is a CG iteration plus the inner steps).
+CANONICAL_WORDS = {2: {"cg": 12, "cheby": 7, "ppcg_inner": 8}, 3: {"cg": 13, "cheby": 8, "ppcg_inner": 9}}
+
+
+def canonical_step_words(dim, solver, iterations, cheby_steps, inner_steps=10):
+    """Canonical words per cell of one timestep: the reference prints n - 1 for a solve
+    that ends in loop pass n, passes 1 .. switch - 1 being CG and the rest Chebyshev or
+    PPCG outer iterations (cheby_steps of them)."""
+    w = CANONICAL_WORDS[dim]
+    n = iterations + 1
+    if solver == "cg":
+        return w["cg"] * n
+    cg = max(n - cheby_steps, 0)
+    if solver == "chebyshev":
+        return w["cg"] * cg + w["cheby"] * cheby_steps
+    return w["cg"] * cg + (w["cg"] + inner_steps * w["ppcg_inner"]) * cheby_steps
+
 
 def run_3d(workload, warmup, steps, arm_steps=None, ws=None):
     """s/timestep of a 3D configuration, plain FP64 and FP32-refined on the same deck, each
@@ -567,6 +591,11 @@ def run_3d(workload, warmup, steps, arm_steps=None, ws=None):
                      "exact_error_over_eps": [r["exact_error"] / r["eps_used"] for r in timed]}
         if precision == tea.PRECISION_FP32_REFINED:
             out[name]["inner_solver"] = [INNER_SOLVERS.get(r["inner_solver"], "?") for r in timed]
+        if precision == tea.PRECISION_FP64:
+            words = [canonical_step_words(3, w["solver"], r["iterations"], r["cheby_steps"]) for r in timed]
+            gbs = [wd * 8 * w["cells"] ** 3 / r["solve_seconds"] / 1e9 for wd, r in zip(words, timed)]
+            out[name]["step_canonical"] = {"gbs": gbs, "frac": [x / load_peaks()[0] for x in gbs],
+                                           "words_per_cell": words}
         if learned:
             out[name]["warm_start_used"] = [r["warm_start_used"] for r in timed]
             out[name]["warm_r0_ratio"] = [r["warm_r0_guess"] / r["warm_r0_plain"] if r["warm_r0_plain"] else None
@@ -875,6 +904,12 @@ def main():
                    "iterations": g["iterations"], "cg_steps": g["cg_steps"], "cheby_steps": g["cheby_steps"]},
         "cells_iterations_per_s": g["cells_iters_per_s"],
         "step_algorithmic_gbs": g["step_alg_gbs"],
+        # The whole timestep's rate in canonical bytes (every iteration's arrays counted once
+        # as an unfused iteration reads and writes them: CG 12 words per cell, Chebyshev 7),
+        # against the measured copy peak; fusion and temporal blocking take it above the
+        # kernels' own fractions, and past 1.0 where they save more than the kernels lose.
+        "step_canonical": {"gbs": g["step_canonical_gbs"], "frac": g["step_canonical_gbs"] / load_peaks()[0],
+                           "words_per_cell": g["canonical_words"]},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic, "alg_bytes_per_launch": g["alg_bytes"],
