@@ -1008,6 +1008,14 @@ TEA_EXPORT void ext_tea_leaf_solve_(const int* chunk, const tea_solve_params* P,
             // the outer target is met with a margin (sum r^2 at a tenth of eps): the last
             // correction needs only the reduction that is left.
             s.tol2 = std::max(tol * tol * s.rro, kInnerTargetMargin * eps);
+            // The first correction of a Chebyshev or PPCG deck is the CG whose scalars give the
+            // eigenvalue bounds: it ends where the plain solve switches (error <= 1 after the
+            // presteps, or <= tl_ch_cg_epslim after 20 iterations with tl_ch_cg_errswitch,
+            // tealeaf_2d/tea_solve.f90:172-179), whose bounds carry the plain solve's own
+            // Chebyshev or PPCG phase, or at the inner tolerance if that comes first.
+            const bool first_cg = want_cheby && inner_mode == 0 && corrections == 0;
+            s.switch_err = first_cg ? (P->ch_cg_errswitch ? P->ch_cg_epslim : 1.0) : 0.0;
+            s.switch_min = P->ch_cg_errswitch ? 20 : P->ch_cg_presteps;
             s.n_inner = inner_mode == 1 ? 1 : 0;
             s.cont = 1;
             s.inner_diverged = 0;

@@ -49,6 +49,10 @@ struct SolveState {
     int inner_diverged;  // the inner Chebyshev residual stalled or grew (bounds too narrow)
     double cheby_rho2;   // squared Chebyshev contraction per iteration for the bounds in use
     double tol2;
+    // The first inner CG of a Chebyshev or PPCG deck also stops at the plain solve's switch
+    // test (sum r^2 <= switch_err after switch_min iterations); 0 when it does not apply.
+    double switch_err;
+    int switch_min;
 };
 
 struct FusedArgs {
@@ -3054,7 +3058,8 @@ __global__ void __launch_bounds__(256) k_cg32_sweep_b(FusedArgs a)
         a.cg_alphas[st.n_inner] = st.alpha;
         a.cg_betas[st.n_inner] = st.beta;
         if (!isfinite(v[0])) st.nonfinite = 1;
-        const int cont = isfinite(v[0]) && v[0] >= st.tol2 && st.n_inner < st.inner_max;
+        const bool at_switch = st.switch_err > 0.0 && st.n_inner >= st.switch_min && v[0] <= st.switch_err;
+        const int cont = isfinite(v[0]) && v[0] >= st.tol2 && st.n_inner < st.inner_max && !at_switch;
         st.cont = cont;
         if (a.use_handle) cudaGraphSetConditional(a.handle, cont ? 1u : 0u);
     });
