@@ -106,3 +106,16 @@ def test_residual_loss_gradient_matches_finite_differences():
         assert abs(fd - g[idx]) <= 1e-6 * max(1.0, abs(fd)), (idx, fd, g[idx])
     # A is the operator with zero-flux edges: constants are its eigenvectors (eigenvalue 1).
     assert np.allclose(wo.apply_a(np.ones((H, W)), kx, ky), 1.0)
+
+
+def test_capped_four_level_network_has_half_a_million_parameters():
+    """The 2D learned configuration's network: 4 levels of 32 base channels whose doubling
+    stops at 64 (32/64/64/64), about half a million parameters."""
+    assert wo.channels(4, 32, 64) == [32, 64, 64, 64]
+    shapes = wo.layer_shapes(4, 32, cap=64)
+    params = sum(co * 9 * ci + co for _, co, ci in shapes) + 32 + 1
+    assert params == 471_969
+    # The 3D configuration's network: 3 levels of 24 channels, 3x3x3 taps, five inputs.
+    shapes3 = wo.layer_shapes(3, 24, wo.in_channels(3))
+    assert dict((n, (co, ci)) for n, co, ci in shapes3)["dec1a"] == (48, 96 + 48)
+    assert wo.taps(3) == 27
