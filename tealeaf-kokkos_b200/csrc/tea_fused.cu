@@ -70,6 +70,7 @@ struct Fused {
     RingLaunch quad32;          // k_cheby4_ring2d<OpCheby32> (2D)
     RingLaunch ring3[RING_OPS]; // grid and z-segment planes of k_ring3d per sweep (3D)
     RingLaunch ppcg2;           // k_ppcg2_ring3d (3D) / k_ppcg2_ring2d (2D); blocks 0: single steps only
+    RingLaunch ppcg2p;          // 3D: the same with the preconditioner (its rows staged: more shared memory)
     RingLaunch ppcg2_32;        // k_ppcg2_ring{2,3}d<PpcgF32>: the FP32 inner PPCG; blocks 0: none
     int stencil_mode = 0;  // 0: the faster kernel per sweep, 1: register pipeline only, 2: ring only
     Loop loops[LOOP_COUNT];
@@ -294,7 +295,12 @@ constexpr size_t ring3_bytes()
 #ifndef TEA_PPCG2_RP
 #define TEA_PPCG2_RP 2
 #endif
-constexpr int PPCG2_TY = TEA_PPCG2_TY, PPCG2_RP = TEA_PPCG2_RP;
+#ifndef TEA_PPCG2_RP_PLAIN
+#define TEA_PPCG2_RP_PLAIN 1
+#endif
+// The 3D two-step PPCG pass: TY rows per tile, RP planes in flight with the preconditioner,
+// RP_PLAIN without it (whose smaller ring slots then fit two blocks on an SM).
+constexpr int PPCG2_TY = TEA_PPCG2_TY, PPCG2_RP = TEA_PPCG2_RP, PPCG2_RP_PLAIN = TEA_PPCG2_RP_PLAIN;
 
 template <class Op>
 void setup_ring3(Fused* F, const Geom& g, int sms, int max_blocks)
@@ -460,11 +466,16 @@ Fused* ensure_fused(Chunk* c, int max_iters)
             setup_ring3<OpSweepA32>(F, g, sms, mb);
             setup_ring3<OpOuterResid>(F, g, sms, mb);
             setup_ring3<OpCheby32>(F, g, sms, mb);
-            const int occ = smem_occupancy(k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP>,
-                                           (int)ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP>(), PPCG2_TY * 32);
+            const int occ = smem_occupancy(k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP_PLAIN, false>,
+                                           (int)ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP_PLAIN, false>(),
+                                           PPCG2_TY * 32);
             F->ppcg2 = ring3_launch(g, sms, occ, 30 * RingGeom<double>::VEC, PPCG2_TY - 2, mb);
-            const int occ32 = smem_occupancy(k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP>,
-                                             (int)ppcg2_smem_bytes<float, PPCG2_TY, PPCG2_RP>(), PPCG2_TY * 32);
+            const int occp = smem_occupancy(k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP, true>,
+                                            (int)ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP, true>(), PPCG2_TY * 32);
+            F->ppcg2p = ring3_launch(g, sms, occp, 30 * RingGeom<double>::VEC, PPCG2_TY - 2, mb);
+            const int occ32 = smem_occupancy(k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP_PLAIN, false>,
+                                             (int)ppcg2_smem_bytes<float, PPCG2_TY, PPCG2_RP_PLAIN, false>(),
+                                             PPCG2_TY * 32);
             F->ppcg2_32 = ring3_launch(g, sms, occ32, 30 * RingGeom<float>::VEC, PPCG2_TY - 2, mb);
         }
 #else
@@ -568,7 +579,25 @@ bool ensure_fp32(Chunk* c, Fused* F)
     return true;
 }
 
+#if TEA_DIM == 3
+// The 3D two-step PPCG pass, in the form of the solve's preconditioner.
+void launch_ppcg2_3d(Fused* F, const FusedArgs& a, bool precond, cudaStream_t s)
+{
+    FusedArgs ak = a;
+    if (precond) {
+        ak.seg_rows = F->ppcg2p.rows;
+        k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP, true>
+            <<<F->ppcg2p.blocks, PPCG2_TY * 32, ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP, true>(), s>>>(ak);
+    } else {
+        ak.seg_rows = F->ppcg2.rows;
+        k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP_PLAIN, false>
+            <<<F->ppcg2.blocks, PPCG2_TY * 32, ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP_PLAIN, false>(), s>>>(ak);
+    }
+}
+#endif
+
 #if TEA_DIM == 2
+
 // The four-iteration FP64 Chebyshev pass, with the launch of the solve's preconditioner
 // setting (with mi staged it needs more shared memory per warp).
 void launch_cheby4(Fused* F, const FusedArgs& a, bool precond, cudaStream_t s)
@@ -644,8 +673,7 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
 #if TEA_DIM == 2
             k_ppcg2_ring2d<PpcgF64><<<F->ppcg2.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, s>>>(ak);
 #else
-            k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
-                                                         ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP>(), s>>>(ak);
+            launch_ppcg2_3d(F, ak, F->h_st->precond != 0, s);
 #endif
         }
         for (int k = k0; k <= inner_steps; ++k) {
@@ -680,8 +708,10 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
 #if TEA_DIM == 2
             k_ppcg2_ring2d<PpcgF32><<<F->ppcg2_32.blocks, RWARPS * 32, ppcg2_2d_smem_bytes, s>>>(ak);
 #else
-            k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP><<<F->ppcg2_32.blocks, PPCG2_TY * 32,
-                                                         ppcg2_smem_bytes<float, PPCG2_TY, PPCG2_RP>(), s>>>(ak);
+            k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP_PLAIN, false><<<F->ppcg2_32.blocks, PPCG2_TY * 32,
+                                                                      ppcg2_smem_bytes<float, PPCG2_TY, PPCG2_RP_PLAIN,
+                                                                                       false>(),
+                                                                      s>>>(ak);
 #endif
         }
         break;
@@ -694,9 +724,10 @@ void enqueue_body(Chunk* c, Fused* F, int kind, int inner_steps, const FusedArgs
 bool build_loop(Chunk* c, Fused* F, int kind, int inner_steps)
 {
     Loop& L = F->loops[kind];
-    // The Chebyshev body's launch depends on the preconditioner (its shared memory).
-    const int key = (kind == LOOP_PPCG || kind == LOOP_PPCG32) ? inner_steps
-                                                               : (kind == LOOP_CHEBY ? F->h_st->precond : 0);
+    // The Chebyshev and PPCG bodies' launches depend on the preconditioner (their shared memory).
+    const int key = kind == LOOP_PPCG ? 2 * inner_steps + (F->h_st->precond ? 1 : 0)
+                                      : (kind == LOOP_PPCG32 ? inner_steps
+                                                             : (kind == LOOP_CHEBY ? F->h_st->precond : 0));
     if (L.exec && L.key == key) return true;
     if (L.exec) cudaGraphExecDestroy(L.exec);
     if (L.graph) cudaGraphDestroy(L.graph);
@@ -1331,21 +1362,16 @@ TEA_EXPORT void tea_kernel_timing_(const int* chunk, const int* kernel, const in
             break;
 #else
         case 10:
-            if (F->ppcg2.blocks > 0) {
-                FusedArgs ap = a;
-                ap.seg_rows = F->ppcg2.rows;
-                k_ppcg2_ring3d<PpcgF64, PPCG2_TY, PPCG2_RP><<<F->ppcg2.blocks, PPCG2_TY * 32,
-                                                             ppcg2_smem_bytes<double, PPCG2_TY, PPCG2_RP>(),
-                                                             c->stream>>>(ap);
-            }
+            if (F->ppcg2.blocks > 0) launch_ppcg2_3d(F, a, saved.precond != 0, c->stream);
             break;
         case 13:
             if (F->ppcg2_32.blocks > 0) {
                 FusedArgs ap = a;
                 ap.seg_rows = F->ppcg2_32.rows;
-                k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP><<<F->ppcg2_32.blocks, PPCG2_TY * 32,
-                                                             ppcg2_smem_bytes<float, PPCG2_TY, PPCG2_RP>(),
-                                                             c->stream>>>(ap);
+                k_ppcg2_ring3d<PpcgF32, PPCG2_TY, PPCG2_RP_PLAIN, false><<<F->ppcg2_32.blocks, PPCG2_TY * 32,
+                                                                          ppcg2_smem_bytes<float, PPCG2_TY,
+                                                                                           PPCG2_RP_PLAIN, false>(),
+                                                                          c->stream>>>(ap);
             }
             break;
 #endif

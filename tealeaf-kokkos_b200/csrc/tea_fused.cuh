@@ -1434,25 +1434,42 @@ struct PpcgF32 {
 // w, and writes it to the other.  With an odd number of pairs sweep B leaves r in w
 // (r_in_w), so the last pair writes r back into r.  A pair whose second step is the last
 // inner step also forms that step's sum r.r and ends the outer iteration.
-template <class T, int TY, int RP>
+//
+// A ring slot holds, per plane, the tile's rows of each input and nothing outside the strip
+// (x-neighbours come by shuffle), and the preconditioner's rows only in the PRE form: without
+// them a slot of TY = 8 is 51 rows of 512 bytes, so that with one plane in flight (RP = 1)
+// two blocks fit on an SM.
+template <int TY, bool PRE>
+struct Ppcg2Rows {
+    static constexpr int RAW = 0;                      // sd: TY + 2 rows
+    static constexpr int IN_R = TY + 2;                // r
+    static constexpr int IN_U = IN_R + TY;             // u
+    static constexpr int IN_MI = IN_U + TY;            // mi (PRE only)
+    static constexpr int KX = IN_MI + (PRE ? TY : 0);  // TY
+    static constexpr int KY = KX + TY;                 // TY + 1
+    static constexpr int KZ = KY + TY + 1;             // TY
+    static constexpr int ROWS = KZ + TY;
+};
+
+template <class T, int TY, int RP, bool PRE>
 constexpr size_t ppcg2_smem_bytes()
 {
-    return (size_t)(RP + 3) * Ring3Rows<OpPPCGInner<false>, TY>::ROWS * RingGeom<T>::WIDTH * sizeof(T)
+    return (size_t)(RP + 3) * Ppcg2Rows<TY, PRE>::ROWS * RingGeom<T>::STRIP * sizeof(T)
         + (size_t)2 * TY * RingGeom<T>::STRIP * sizeof(T);
 }
 
-template <class P, int TY, int RP>
+template <class P, int TY, int RP, bool PRE>
 __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
 {
     using T = typename P::T;
     extern __shared__ __align__(16) unsigned char s_raw[];
-    using R = Ring3Rows<OpPPCGInner<false>, TY>;
-    constexpr int VEC = RingGeom<T>::VEC, STRIP = RingGeom<T>::STRIP, OFF = RingGeom<T>::OFF;
-    constexpr int RWT = RingGeom<T>::WIDTH;
+    using R = Ppcg2Rows<TY, PRE>;
+    constexpr int VEC = RingGeom<T>::VEC, STRIP = RingGeom<T>::STRIP, OFF = 0;
+    constexpr int RWT = STRIP;
     constexpr int OUT = 30 * VEC;
     constexpr int RQ = RP + 3;
     constexpr int SLOT = R::ROWS * RWT;
-    constexpr int IN_R = R::IN, IN_U = R::IN + TY, IN_MI = R::IN + 2 * TY;
+    constexpr int IN_R = R::IN_R, IN_U = R::IN_U, IN_MI = R::IN_MI;
     T* ring = reinterpret_cast<T*>(s_raw);
     T* s1 = ring + (size_t)RQ * SLOT;  // step k's sd: [plane parity][TY rows][STRIP]
     const Geom& g = a.g;
@@ -1463,8 +1480,8 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
     const T* __restrict__ rin = ((m - 1 + a.r_in_w) & 1) ? P::w(a) : P::r(a);
     T* __restrict__ rout = ((m + a.r_in_w) & 1) ? P::w(a) : P::r(a);
     T* __restrict__ U = P::u(a);
-    const T* __restrict__ MI = P::mi(a);
-    const bool precond = MI != nullptr;
+    const T* __restrict__ MI = PRE ? P::mi(a) : nullptr;
+    const bool precond = PRE && MI != nullptr;
     const bool last = k + 1 == a.st->inner_steps;  // step k+1 ends the outer iteration
     DDVec<1> acc;
     acc.zero();
@@ -1519,7 +1536,7 @@ __global__ void __launch_bounds__(TY * 32) k_ppcg2_ring3d(FusedArgs a)
                     if (w == TY - 1) cp_async_16(base + (R::RAW + TY + 1) * RWT + col, sdk + fidx(g, cc, r_above, pr));
                     cp_async_16(base + (IN_R + w) * RWT + col, rin + fidx(g, cc, ij, pi));
                     if (row_out && lane_out) cp_async_16(base + (IN_U + w) * RWT + col, U + fidx(g, cc, ij, pi));
-                    if (MI) cp_async_16(base + (IN_MI + w) * RWT + col, MI + fidx(g, cc, ij, pi));
+                    if (PRE && MI) cp_async_16(base + (IN_MI + w) * RWT + col, MI + fidx(g, cc, ij, pi));
                     cp_async_16(base + (R::KX + w) * RWT + col, KX + fidx(g, cc, ij, pi));
                     cp_async_16(base + (R::KY + w) * RWT + col, KY + fidx(g, cc, ij, pi));
                     if (w == TY - 1) cp_async_16(base + (R::KY + TY) * RWT + col, KY + fidx(g, cc, i_above, pi));
