@@ -18,6 +18,15 @@ library's own stream, barrier + synchronize on both sides, max over ranks.  Ever
 array is 135 MB (> 126 MB of L2), so no L2 flush is needed between steps.  With N > 1
 (torchrun) each rank solves its own replica of the workload (the benchmark does not split
 one solve over ranks) and rank 0 prints one JSON line.
+
+Beside the headline the line carries: `e2e` (the same timesteps through the public driver
+API), `roofline` (the dominant fused kernel against the measured copy peak, with its ncu
+traffic), `step_canonical` (the timestep's rate in canonical bytes), `cpu_baseline` (the
+reference's own kernels on the host cores), `per_call` (the per-call ext_* path),
+`fp32_refined` and `fp32_refined_learned` (the precision form, and with the learned warm
+start), `c5_3d512_ppcg` (3D 512^3 PPCG: plain FP64 against FP32-refined with PPCG and with
+Chebyshev corrections, and with the 3D learned warm start) and `c3_3d256` (3D 256^3 CG and
+PPCG).
 """
 from __future__ import annotations
 
